@@ -1,0 +1,324 @@
+/*
+ * mvdr.h - C ABI of the B200-native non-rigid Gauss-Newton solver.
+ *
+ * This library replaces the NonRigidSolver stage of MultiViewDynRecon
+ * (core/NonRigidSolver/NonRigidSolver.h:78-541). The reference drives that
+ * stage through three calls:
+ *
+ *   SetSolverInput(...)        core/NonRigidSolver/NonRigidSolver.h:133-140
+ *   SolveNonRigidAlignment()   core/NonRigidSolver/NonRigidSolver.h:254
+ *   SolvedNodeSE3()            core/NonRigidSolver/NonRigidSolver.h:214
+ *
+ * and they map to mvdr_set_inputs / mvdr_solve / mvdr_get_node_se3 below.
+ * The remaining entry points expose the intermediate products of the solve
+ * (term index, Jacobians, JtJ blocks, preconditioner, PCG increment) so that a
+ * caller can check them against the reference's host sanity-check routines.
+ *
+ * Conventions
+ *  - All structs are plain C, no CUDA or torch types. Streams are passed as
+ *    void* and interpreted as cudaStream_t (NULL = legacy default stream).
+ *  - Array pointers in mvdr_inputs are DEVICE pointers owned by the caller
+ *    (non-owning views, like the reference's DeviceArrayView). They must stay
+ *    valid until the next mvdr_set_inputs on the same solver.
+ *  - Every workspace buffer is allocated by mvdr_create / mvdr_batch_create.
+ *    Nothing is allocated by set_inputs, build_index, gn_iteration or solve.
+ *  - Every call returns an mvdr_status. No call aborts the process; a CUDA
+ *    error is returned as MVDR_ECUDA and its text is kept for
+ *    mvdr_last_error_string.
+ *  - A solver is used by one host thread at a time; all work is enqueued on
+ *    the stream given to each call.
+ */
+#ifndef MVDR_H_
+#define MVDR_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MVDR_ABI_VERSION 1u
+#define MVDR_MAX_VIEWS 8u
+#define MVDR_INVALID_INDEX 0xFFFFFFFFu
+
+/* Status codes. The reference aborts on these conditions instead
+ * (CHECKCUDA exit, base/DeviceAPI/safe_call.hpp:58-72; ResizeArrayOrException,
+ * base/DeviceReadWrite/DeviceBufferArray.h:134-141). */
+typedef enum mvdr_status {
+    MVDR_OK = 0,
+    MVDR_EINVAL = 1,      /* bad argument or inconsistent sizes            */
+    MVDR_ECAPACITY = 2,   /* a size exceeds the capacity given at create    */
+    MVDR_ECUDA = 3,       /* a CUDA runtime call failed                     */
+    MVDR_ETIMEOUT = 4,    /* a bounded device-side wait gave up             */
+    MVDR_ENONFINITE = 5,  /* NaN/Inf found in inputs or in the solution     */
+    MVDR_ESTATE = 6       /* call out of order (e.g. solve before inputs)   */
+} mvdr_status;
+
+/* Arithmetic of the linear solve.
+ * FP32:  everything in float; Gauss-Jordan 6x6 inverse; float dot products
+ *        (the reference's arithmetic, BlockPCG.cuh:187-458,
+ *        BlockDiagonalPreconditionerInverse.cu:7-41).
+ * MIXED: residuals, Jacobians, BSR blocks and SpMV in float; PCG dot products
+ *        and norms in double; 6x6 block Cholesky of the preconditioner in
+ *        double. */
+typedef enum mvdr_precision {
+    MVDR_PRECISION_FP32 = 0,
+    MVDR_PRECISION_MIXED = 1
+} mvdr_precision;
+
+/* How PCG applies JtJ.
+ * MATERIALIZED: off-diagonal 6x6 blocks are assembled into BSR storage once
+ *   per Gauss-Newton iteration (JtJMaterializer.cu:270-528).
+ * MATRIX_FREE: JtJ.p is evaluated per PCG iteration from the term Jacobians
+ *   through the adjoint pair J.p / Jt.y (ApplyJacobianDot.cu:127-198,
+ *   ApplyJacobianTransposeDot.cu:29-155). Unlike the reference's matrix-free
+ *   operator it includes the cross-view term and the 1e-2 diagonal damping,
+ *   so both modes solve the same system. */
+typedef enum mvdr_mode {
+    MVDR_MODE_MATERIALIZED = 0,
+    MVDR_MODE_MATRIX_FREE = 1
+} mvdr_mode;
+
+/* Compatibility switches reproducing reference behaviour that this library
+ * corrects by default. */
+enum {
+    /* Sample each compacted pixel's maps by the cumulative per-view lookup of
+     * CalculateDensityMapCameraViewDpt (DenseDepthJacobianResidual.cu:14-22)
+     * instead of the pixel's own view tag. Only differs when num_views > 1. */
+    MVDR_COMPAT_REF_VIEW_LOOKUP = 1u << 0
+};
+
+typedef struct mvdr_float4 { float x, y, z, w; } mvdr_float4;
+
+/* Same memory layout as the reference DualQuaternion
+ * (math/DualQuaternion/DualQuaternion.h:99-102): two quaternions stored as
+ * float4 (x, y, z, w), real part q0 first. 32 bytes. */
+typedef struct mvdr_dual_quaternion { float q0[4]; float q1[4]; } mvdr_dual_quaternion;
+
+/* Same layout as the reference mat34 (math/MatUtils.h:19-20, 401-403): the
+ * rotation as three float3 COLUMNS, then the translation. 48 bytes. */
+typedef struct mvdr_mat34 { float rot[9]; float trans[3]; } mvdr_mat34;
+
+/* Same field order as the reference Intrinsic (base/CommonTypes.h:79-105). */
+typedef struct mvdr_intrinsic { float principal_x, principal_y, focal_x, focal_y; } mvdr_intrinsic;
+
+/* Term weights lambda (PenaltyConstants.h:9-46). The dense-depth weight is
+ * fixed at 1 as in the reference. */
+typedef struct mvdr_penalty {
+    float smooth;
+    float density;
+    float foreground;
+    float feature;
+    float cross_view;
+} mvdr_penalty;
+
+typedef struct mvdr_config {
+    uint32_t abi_version;        /* must be MVDR_ABI_VERSION                  */
+    /* capacities (the reference's compile-time maxima, made runtime) */
+    uint32_t max_nodes;          /* <= 65535                                   */
+    uint32_t max_views;          /* <= MVDR_MAX_VIEWS                          */
+    uint32_t image_width;
+    uint32_t image_height;
+    uint32_t max_surfels;
+    uint32_t max_feature_terms;
+    uint32_t max_cross_terms;
+    uint32_t max_dense_terms;    /* 0: max_views * width * height              */
+    uint32_t max_foreground_terms; /* 0: max_dense_terms                       */
+    uint32_t max_node_pairs;     /* unique unordered pairs; 0: 32 * max_nodes  */
+    uint32_t max_terms_per_node; /* 0: 16384                                   */
+    /* numerics */
+    float node_radius;           /* NODE_RADIUS (base/GlobalConfigs.h:85)      */
+    int32_t precision;           /* mvdr_precision                            */
+    int32_t mode;                /* mvdr_mode                                 */
+    int32_t use_foreground;      /* foreground-mask term                      */
+    int32_t use_feature;         /* sparse feature term                       */
+    int32_t use_cross_view;      /* cross-view correspondence term            */
+    int32_t use_elastic_penalty; /* global/local lambda schedule              */
+    int32_t num_global_iterations; /* GN iterations that use global lambdas   */
+    uint32_t compat_flags;       /* MVDR_COMPAT_*                             */
+    /* penalties used when use_elastic_penalty == 0; with the schedule on, the
+     * values of PenaltyConstants.cpp:25-51 are used instead. */
+    mvdr_penalty penalty;
+} mvdr_config;
+
+/* Per-view inputs: the rendered solver maps (Renderer::SolverMaps,
+ * render/Renderer.h:381-388), the camera observation maps
+ * (CameraObservation, base/CameraObservation.h:16-63) and the view's camera
+ * parameters. Maps are dense row-major image_height x image_width arrays with
+ * a row pitch of `pitch` elements (0 = image_width). */
+typedef struct mvdr_view_inputs {
+    const mvdr_float4* reference_vertex_map;   /* canonical vertex, this camera's frame */
+    const mvdr_float4* reference_normal_map;   /* canonical normal, this camera's frame */
+    const uint32_t* index_map;                 /* surfel index or MVDR_INVALID_INDEX   */
+    const mvdr_float4* vertex_confidence_map;  /* observed depth vertex                */
+    const mvdr_float4* normal_radius_map;      /* observed depth normal                */
+    const float* filtered_foreground_mask;     /* may be NULL if foreground is off     */
+    const float* foreground_mask_gradient;     /* float2 per pixel; may be NULL        */
+    uint32_t pitch;
+    mvdr_intrinsic intrinsic;                  /* ClipColorIntrinsic[v]                */
+    mvdr_mat34 world2camera;                   /* world2Camera[v] (canonical2Live)     */
+    mvdr_mat34 initial_camera_se3;             /* InitialCameraSE3[v]: camera v -> 0   */
+} mvdr_view_inputs;
+
+/* Correspondence terms after selection and compaction, as held by
+ * Point2PointICPTerm2Jacobian (core/NonRigidSolver/solver_types.h:150-160):
+ * target (observed, live frame 0), reference (canonical, frame 0), 4-NN. */
+typedef struct mvdr_correspondences {
+    uint32_t count;
+    const mvdr_float4* target_vertex;
+    const mvdr_float4* reference_vertex;
+    const uint16_t* knn;           /* ushort4 per term */
+    const mvdr_float4* knn_weight;
+} mvdr_correspondences;
+
+typedef struct mvdr_inputs {
+    uint32_t num_views;
+    uint32_t num_nodes;
+    uint32_t num_surfels;
+    uint32_t num_graph_edges;      /* entries of node_graph (8 * num_nodes)  */
+    mvdr_view_inputs views[MVDR_MAX_VIEWS];
+    /* SurfelGeometry::NonRigidSolverInput (SurfelGeometry.h:179-182) */
+    const uint16_t* surfel_knn;            /* ushort4 per surfel */
+    const mvdr_float4* surfel_knn_weight;
+    /* WarpField::NonRigidSolverInput (WarpField.h:157-161) */
+    const mvdr_dual_quaternion* node_se3;
+    const mvdr_float4* canonical_node_coords;
+    const uint16_t* node_graph;            /* ushort2 (i, j) per edge */
+    mvdr_correspondences feature;          /* SparseCorrespondenceHandler output */
+    mvdr_correspondences cross_view;       /* CrossViewCorrespondenceHandler output */
+} mvdr_inputs;
+
+/* Sizes produced by the index build (host-readable after a stream sync). */
+typedef struct mvdr_counts {
+    uint32_t dense_terms;       /* T_d: valid index-map pixels, all views   */
+    uint32_t smooth_terms;      /* T_s                                      */
+    uint32_t foreground_terms;  /* T_f                                      */
+    uint32_t feature_terms;     /* T_p                                      */
+    uint32_t cross_terms;       /* T_c                                      */
+    uint32_t node2term_entries; /* K1                                       */
+    uint32_t nodepair_entries;  /* K2 (valid entries)                       */
+    uint32_t half_pairs;        /* P                                        */
+    uint32_t num_bins;          /* bins of 32 scalar rows                   */
+    uint32_t binblock_nnz;      /* scalar slots of the bin-block CSR         */
+    uint32_t error_flags;       /* device-side capacity/timeout flags        */
+    uint32_t reserved;
+} mvdr_counts;
+
+typedef struct mvdr_solver mvdr_solver;
+typedef struct mvdr_batch mvdr_batch;
+
+/* ---- life cycle ------------------------------------------------------- */
+
+/* Fills *cfg with defaults for the given capacities. */
+void mvdr_config_default(mvdr_config* cfg, uint32_t max_nodes, uint32_t max_views,
+                         uint32_t image_width, uint32_t image_height);
+
+/* NonRigidSolver::NonRigidSolver + AllocateBuffer (NonRigidSolver.h:103,117). */
+int mvdr_create(const mvdr_config* cfg, mvdr_solver** out);
+/* ReleaseBuffer + destructor (NonRigidSolver.h:108,123). */
+int mvdr_destroy(mvdr_solver* solver);
+
+/* SetSolverInput (NonRigidSolver.cpp:77-97): binds the caller's device arrays
+ * and resets the iteration state to inputs->node_se3
+ * (SolverIterationData::SetWarpFieldInitialValue, SolverIterationData.cpp:37-50). */
+int mvdr_set_inputs(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
+
+/* As mvdr_set_inputs, but every array pointer is a HOST pointer; the data is
+ * copied into solver-owned device buffers on `stream` (pinned host memory
+ * makes the copies asynchronous). */
+int mvdr_set_inputs_host(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
+
+/* buildSolverIndexStreamed (NonRigidSolver.h:257, body not in the reference):
+ * pixel selection and compaction (ImageTermKNNFetcher.cu:19-137,
+ * DensityForegroundMapHandler.cu:34-146), node->term index
+ * (Node2TermsIndex.cu:8-187), node-pair->term index and bin-block CSR
+ * structure (NodePair2TermsIndex.cu:11-296, NodePairRowColumnIndex.cu:19-308).
+ * No host synchronisation. */
+int mvdr_build_index(mvdr_solver* solver, void* stream);
+
+/* One Gauss-Newton iteration (solverIteration{Global,Local}IterationStreamed,
+ * NonRigidSolver.h:258-259): term evaluation, preconditioner and RHS, JtJ
+ * materialisation (MATERIALIZED mode), block PCG with `pcg_iterations`
+ * iterations, warp-field update (SolverIterationData.cu:9-94). */
+int mvdr_gn_iteration(mvdr_solver* solver, uint32_t pcg_iterations, void* stream);
+
+/* SolveNonRigidAlignment (NonRigidSolver.h:254): build_index followed by
+ * `gn_iterations` Gauss-Newton iterations. */
+int mvdr_solve(mvdr_solver* solver, uint32_t gn_iterations, uint32_t pcg_iterations, void* stream);
+
+/* SolvedNodeSE3 (NonRigidSolver.h:214): copies the current node SE(3) array
+ * (num_nodes dual quaternions) to `dst`, which may be host or device memory. */
+int mvdr_get_node_se3(mvdr_solver* solver, mvdr_dual_quaternion* dst, void* stream);
+
+/* Synchronises `stream` and returns the sizes of the current index. */
+int mvdr_get_counts(mvdr_solver* solver, mvdr_counts* out, void* stream);
+
+/* Energy sum (lambda * r)^2 of the terms evaluated by the last Gauss-Newton
+ * iteration, accumulated in double (ResidualEvaluator.cu:71-226). */
+int mvdr_get_energy(mvdr_solver* solver, double* energy, void* stream);
+
+/* ---- intermediate products (for checks) --------------------------------
+ * `which` selects an array, `dst` receives it (host or device memory),
+ * `capacity_bytes` is the size of dst; *written_bytes returns the byte count.
+ * The call synchronises `stream`. */
+enum {
+    MVDR_ARRAY_DENSE_PIXELS = 0,        /* ushort4 (x, y, view, 0) per dense term          */
+    MVDR_ARRAY_DENSE_KNN = 1,           /* ushort4 per dense term                          */
+    MVDR_ARRAY_DENSE_KNN_WEIGHT = 2,    /* float4 per dense term                           */
+    MVDR_ARRAY_FOREGROUND_PIXELS = 3,   /* ushort4 per foreground term                     */
+    MVDR_ARRAY_NODE2TERM_OFFSET = 4,    /* uint32 [N+1]                                    */
+    MVDR_ARRAY_NODE2TERM_INDEX = 5,     /* uint32 [K1]                                     */
+    MVDR_ARRAY_HALF_NODEPAIR_KEY = 6,   /* uint32 [P]: i*4096+j for i<j (4096 -> 2^ceil(log2 N) past 4096) */
+    MVDR_ARRAY_NODEPAIR_TERM_INDEX = 7, /* uint32 [K2]                                     */
+    MVDR_ARRAY_NODEPAIR_KEY = 8,        /* uint32 [2P]: symmetric keys, sorted             */
+    MVDR_ARRAY_NODEPAIR_TERM_RANGE = 9, /* uint2  [2P]                                     */
+    MVDR_ARRAY_BLKROW_OFFSET = 10,      /* uint32 [N+1]                                    */
+    MVDR_ARRAY_BINBLOCK_ROWPTR = 11,    /* int32  [32*(nbins+1)]                           */
+    MVDR_ARRAY_BINBLOCK_COLPTR = 12,    /* int32  [binblock_nnz/6]                         */
+    MVDR_ARRAY_TERM_JACOBIAN = 13,      /* float [T_d+T_f][8]: twist gradient (6), residual, pad */
+    MVDR_ARRAY_SMOOTH_TERMS = 14,       /* float [T_s][8]: Ti_xj (3), Tj_xj (3), validity, pad */
+    MVDR_ARRAY_WARPED_CORRESPONDENCE = 15, /* float4 [T_p+T_c] warped reference vertex     */
+    MVDR_ARRAY_DIAG_BLOCKS = 16,        /* float [N][36] JtJ diagonal blocks incl. damping  */
+    MVDR_ARRAY_JTR = 17,                /* float [N][6]  b = -Jt r                          */
+    MVDR_ARRAY_PRECONDITIONER = 18,     /* float [N][36] inverse of the diagonal blocks      */
+    MVDR_ARRAY_OFFDIAG_BLOCKS = 19,     /* float [2P][36] in symmetric-key order, blk[6k+r] = A(r,k) */
+    MVDR_ARRAY_BINBLOCK_DATA = 20,      /* float [binblock_nnz] bin-block CSR values        */
+    MVDR_ARRAY_INCREMENT = 21,          /* float [6N] PCG solution of the last iteration     */
+    MVDR_ARRAY_NODE_SE3 = 22            /* dual quaternion [N] current warp field            */
+};
+int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t capacity_bytes,
+                   size_t* written_bytes, void* stream);
+
+/* y = JtJ x with the operator of the last Gauss-Newton iteration, in the
+ * current mode (bin-block/BSR SpMV or matrix-free adjoint pair). x and y are
+ * device arrays of 6*num_nodes floats. */
+int mvdr_apply_jtj(mvdr_solver* solver, const float* x, float* y, void* stream);
+
+/* ---- batched solves (many independent instances per launch) ------------- */
+
+/* All instances share the capacities of *cfg; their actual sizes may differ. */
+int mvdr_batch_create(const mvdr_config* cfg, uint32_t num_instances, mvdr_batch** out);
+int mvdr_batch_destroy(mvdr_batch* batch);
+int mvdr_batch_set_inputs(mvdr_batch* batch, uint32_t instance, const mvdr_inputs* inputs, void* stream);
+int mvdr_batch_set_inputs_host(mvdr_batch* batch, uint32_t instance, const mvdr_inputs* inputs, void* stream);
+/* Index build and `gn_iterations` Gauss-Newton iterations for every instance;
+ * each stage is one launch over all instances. When use_graph is non-zero the
+ * Gauss-Newton iterations are captured once as a CUDA graph and replayed. */
+int mvdr_batch_solve(mvdr_batch* batch, uint32_t gn_iterations, uint32_t pcg_iterations,
+                     int use_graph, void* stream);
+int mvdr_batch_get_node_se3(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst, void* stream);
+/* The single-instance view of one batch member (not owned; do not destroy). */
+int mvdr_batch_instance(mvdr_batch* batch, uint32_t instance, mvdr_solver** out);
+
+/* ---- diagnostics -------------------------------------------------------- */
+
+/* Text of the last error recorded on this host thread. */
+const char* mvdr_last_error_string(void);
+/* Number of kernel launches this library has enqueued since load. */
+uint64_t mvdr_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MVDR_H_ */

@@ -1,0 +1,216 @@
+"""Python binding of the CPU oracle - TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import
+this package. It restates the reference NonRigidSolver algorithm on the CPU
+(oracle/oracle.cpp) and is used as the checker, never as the product.
+
+Parity unpinned: the reference cannot be built here and ships no golden
+vectors; the restatement is pinned by known-answer tests instead
+(tests/test_oracle.py).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from multiviewdynrecon_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+                os.path.join(_HERE, "oracle.cpp")):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Inputs), C.c_int]
+        for name in ("orc_destroy", "orc_build_index", "orc_eval_terms", "orc_assemble", "orc_update",
+                     "orc_unfreeze"):
+            getattr(L, name).argtypes = [C.c_void_p]
+            getattr(L, name).restype = None
+        L.orc_pcg.argtypes = [C.c_void_p, C.c_uint32]
+        L.orc_gn_iteration.argtypes = [C.c_void_p, C.c_uint32]
+        L.orc_solve.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        L.orc_set_term_data.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_freeze_decisions.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_set_increment.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_energy.restype = C.c_double
+        L.orc_energy.argtypes = [C.c_void_p]
+        L.orc_energy_now.restype = C.c_double
+        L.orc_energy_now.argtypes = [C.c_void_p]
+        L.orc_counts.argtypes = [C.c_void_p, C.POINTER(abi.Counts)]
+        L.orc_get.restype = C.c_longlong
+        L.orc_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_int]
+        L.orc_apply_jtj.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_dq_to_mat34.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_mat34_to_dq.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_apply_twist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_gauss_jordan_inverse.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# element type and per-item width of each array id
+_ARRAY_SPEC = {
+    abi.ARRAY_DENSE_PIXELS: (np.uint16, 4), abi.ARRAY_DENSE_KNN: (np.uint16, 4),
+    abi.ARRAY_DENSE_KNN_WEIGHT: (np.float32, 4), abi.ARRAY_FOREGROUND_PIXELS: (np.uint16, 4),
+    abi.ARRAY_NODE2TERM_OFFSET: (np.uint32, 1), abi.ARRAY_NODE2TERM_INDEX: (np.uint32, 1),
+    abi.ARRAY_HALF_NODEPAIR_KEY: (np.uint32, 1), abi.ARRAY_NODEPAIR_TERM_INDEX: (np.uint32, 1),
+    abi.ARRAY_NODEPAIR_KEY: (np.uint32, 1), abi.ARRAY_NODEPAIR_TERM_RANGE: (np.uint32, 2),
+    abi.ARRAY_BLKROW_OFFSET: (np.uint32, 1), abi.ARRAY_BINBLOCK_ROWPTR: (np.int32, 1),
+    abi.ARRAY_BINBLOCK_COLPTR: (np.int32, 1), abi.ARRAY_TERM_JACOBIAN: (np.float32, 8),
+    abi.ARRAY_SMOOTH_TERMS: (np.float32, 8), abi.ARRAY_WARPED_CORRESPONDENCE: (np.float32, 4),
+    abi.ARRAY_DIAG_BLOCKS: (np.float32, 36), abi.ARRAY_JTR: (np.float32, 6),
+    abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
+    abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
+    abi.ARRAY_NODE_SE3: (np.float32, 8),
+}
+REAL_ARRAYS = {abi.ARRAY_DIAG_BLOCKS, abi.ARRAY_JTR, abi.ARRAY_PRECONDITIONER, abi.ARRAY_OFFDIAG_BLOCKS,
+               abi.ARRAY_BINBLOCK_DATA, abi.ARRAY_INCREMENT, abi.ARRAY_NODE_SE3}
+
+
+class Oracle:
+    """CPU restatement of one solve. `fp64` selects double arithmetic."""
+
+    def __init__(self, scene, config, fp64=False):
+        self.scene = scene
+        self.config = config
+        self._keep = []
+
+        def ptr(name, arr):
+            a = np.ascontiguousarray(arr)
+            self._keep.append(a)
+            return a.ctypes.data
+
+        self.inputs = abi.fill_inputs(scene, ptr)
+        self.h = lib().orc_create(C.byref(config), C.byref(self.inputs), int(fp64))
+        if not self.h:
+            raise ValueError("oracle rejected the inputs")
+        self.fp64 = fp64
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().orc_destroy(h)
+            self.h = None
+
+    # stages
+    def build_index(self):
+        lib().orc_build_index(self.h)
+
+    def eval_terms(self):
+        lib().orc_eval_terms(self.h)
+
+    def assemble(self):
+        lib().orc_assemble(self.h)
+
+    def pcg(self, iters):
+        lib().orc_pcg(self.h, iters)
+
+    def update(self):
+        lib().orc_update(self.h)
+
+    def gn_iteration(self, pcg):
+        lib().orc_gn_iteration(self.h, pcg)
+
+    def solve(self, gn, pcg):
+        lib().orc_solve(self.h, gn, pcg)
+
+    def set_term_data(self, term_jr=None, smooth=None, warped=None):
+        keep = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (term_jr, smooth, warped)]
+        lib().orc_set_term_data(self.h, *[None if a is None else _p(a) for a in keep])
+
+    def freeze(self, term_jr, smooth):
+        """Freeze projected pixels / validity from another run's term data."""
+        jr = np.ascontiguousarray(term_jr, np.float32).reshape(-1, 8)
+        pix = np.ascontiguousarray(jr[:, 7].view(np.uint32))
+        sv = np.ascontiguousarray((np.asarray(smooth, np.float32).reshape(-1, 8)[:, 6] != 0).astype(np.uint8))
+        lib().orc_freeze_decisions(self.h, _p(pix), _p(sv))
+
+    def unfreeze(self):
+        lib().orc_unfreeze(self.h)
+
+    def set_increment(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        lib().orc_set_increment(self.h, _p(x))
+
+    def energy(self):
+        return lib().orc_energy(self.h)
+
+    def counts(self):
+        c = abi.Counts()
+        lib().orc_counts(self.h, C.byref(c))
+        return c
+
+    def get(self, which, as_double=False):
+        dt, width = _ARRAY_SPEC[which]
+        if as_double and which in REAL_ARRAYS:
+            dt = np.float64
+        cap = 1 << 20
+        while True:
+            buf = np.empty(cap // np.dtype(dt).itemsize, dt)
+            n = lib().orc_get(self.h, which, _p(buf), buf.nbytes, int(as_double))
+            if n >= 0:
+                out = buf[: n // np.dtype(dt).itemsize]
+                return out.reshape(-1, width) if width > 1 else out
+            cap *= 4
+
+    def apply_jtj(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        lib().orc_apply_jtj(self.h, _p(x), _p(y))
+        return y
+
+
+# known-answer helpers over the restated math
+def dq_to_mat34(dq):
+    dq = np.ascontiguousarray(dq, np.float32)
+    out = np.empty(12, np.float32)
+    lib().orc_dq_to_mat34(_p(dq), _p(out))
+    return out
+
+
+def mat34_to_dq(m):
+    m = np.ascontiguousarray(m, np.float32)
+    out = np.empty(8, np.float32)
+    lib().orc_mat34_to_dq(_p(m), _p(out))
+    return out
+
+
+def apply_twist(dq, tw):
+    dq = np.ascontiguousarray(dq, np.float64)
+    tw = np.ascontiguousarray(tw, np.float64)
+    out = np.empty(8, np.float64)
+    lib().orc_apply_twist(_p(dq), _p(tw), _p(out))
+    return out
+
+
+def gauss_jordan_inverse(A):
+    A = np.ascontiguousarray(A, np.float64).reshape(36)
+    out = np.empty(36, np.float64)
+    lib().orc_gauss_jordan_inverse(_p(A), _p(out))
+    return out.reshape(6, 6)
+
+
+def cholesky_inverse(A):
+    A = np.ascontiguousarray(A, np.float64).reshape(36)
+    out = np.empty(36, np.float64)
+    lib().orc_cholesky_inverse(_p(A), _p(out))
+    return out.reshape(6, 6)
