@@ -1,0 +1,401 @@
+"""Benchmark: non-rigid Gauss-Newton solves per second on B200.
+
+Workload (one step): a batch of independent multi-view solves, each 3 views at
+640x480 around a torso-like ellipsoid, 4096 nodes, 8-NN graph, 4-NN skinning,
+all terms (dense depth, foreground mask, 1000 sparse feature pairs per view,
+2000 cross-view pairs per adjacent view pair), 5 Gauss-Newton x 15 PCG
+iterations, mixed precision (float bulk, double reductions and block Cholesky).
+Each instance shares the synthetic geometry and has its own random initial
+warp field. Every step re-binds the inputs (which resets each warp field) and
+runs the index build plus all Gauss-Newton iterations of every instance as one
+captured CUDA graph.
+
+Outputs one JSON line (rank 0). `value` uses inputs resident in HBM; `e2e`
+uploads every input from pinned host memory and reads every solved warp field
+back inside the timed region. `--impl reference` times the CPU restatement of
+the reference algorithm (the reference itself cannot be built here) on all
+host cores, one instance per thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+WORKLOAD = "torso_3view_640x480_4096nodes_5gn_15pcg"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=16, help="instances per GPU")
+    p.add_argument("--nodes", type=int, default=4096)
+    p.add_argument("--width", type=int, default=640)
+    p.add_argument("--height", type=int, default=480)
+    p.add_argument("--gn", type=int, default=5)
+    p.add_argument("--pcg", type=int, default=15)
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
+    p.add_argument("--mode", default="materialized", choices=["materialized", "matrix_free"])
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison leg")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def make_scenes(args, rank):
+    from multiviewdynrecon_b200 import synth
+    base = synth.torso_multi_view(seed=2, num_nodes=args.nodes, width=args.width, height=args.height)
+    scenes = [synth.perturb_warp_field(base, seed=1000 * rank + i) for i in range(args.batch)]
+    return base, scenes
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                return
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def algorithmic_bytes(counts, N):
+    """Compulsory HBM bytes per stage (each array read or written once)."""
+    Td, Ts, Tf, Tp, Tc = (counts.dense_terms, counts.smooth_terms, counts.foreground_terms, counts.feature_terms,
+                          counts.cross_terms)
+    P = counts.half_pairs
+    nnzb = N + 2 * P
+    term_data = 52 * (Td + Tf) + 29 * Ts + 88 * (Tp + Tc)
+    return {
+        "terms": 122 * Td + 86 * Tf + 29 * Ts + 72 * (Tp + Tc) + 32 * N,
+        "diag": term_data + 144 * N + 24 * N + 288 * N,
+        "offdiag": term_data + 148 * nnzb + 4 * (N + 1),
+        "spmv": 148 * nnzb + 4 * (N + 1) + 24 * N + 24 * N,
+        "pcg_update": 24 * N * 6 + 168 * N,
+        "update": 24 * N + 64 * N,
+    }
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from multiviewdynrecon_b200 import abi, lib
+    from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, NonRigidSolver
+
+    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
+    dev = torch.cuda.current_device()
+    base, scenes = make_scenes(args, rank)
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP32
+    mode = abi.MODE_MATERIALIZED if args.mode == "materialized" else abi.MODE_MATRIX_FREE
+    cfg = abi.make_config(base, precision=prec, mode=mode)
+    B = args.batch
+    batch = BatchSolver(cfg, B)
+    dev_scenes = [DeviceScene(s) for s in scenes]
+    stream = torch.cuda.Stream()
+
+    def bind_all():
+        for i, ds in enumerate(dev_scenes):
+            batch.set_input(i, ds, stream=stream)
+
+    def step():
+        bind_all()
+        batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+
+    # kernels per solve: one direct (non-graph) solve counted through the ABI
+    with torch.cuda.stream(stream):
+        bind_all()
+        k0 = lib().mvdr_kernel_launch_count()
+        batch.solve(args.gn, args.pcg, use_graph=False, stream=stream)
+        kernels_per_step = lib().mvdr_kernel_launch_count() - k0
+        stream.synchronize()
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with clocks, torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * B / (ms / 1e3)
+
+    # accuracy of instance 0 and counts
+    inst0 = batch.instance(0)
+    counts = inst0.counts()
+
+    # per-stage timing on the same stream (CUDA events), all instances
+    stages = {}
+    abytes = algorithmic_bytes(counts, base.num_nodes)
+    reps = 20
+    with torch.cuda.stream(stream):
+        bind_all()
+        batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+        stream.synchronize()
+        for name, sid in (("index", abi.STAGE_INDEX), ("terms", abi.STAGE_TERMS), ("diag", abi.STAGE_DIAG),
+                          ("offdiag", abi.STAGE_OFFDIAG), ("spmv", abi.STAGE_SPMV),
+                          ("pcg_update", abi.STAGE_PCG_UPDATE), ("update", abi.STAGE_UPDATE)):
+            if name == "offdiag" and mode != abi.MODE_MATERIALIZED:
+                continue
+            for _ in range(2):
+                lib().mvdr_batch_enqueue_stage(batch.h, sid, stream.cuda_stream)
+            a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                lib().mvdr_batch_enqueue_stage(batch.h, sid, stream.cuda_stream)
+            b2.record(stream)
+            b2.synchronize()
+            t_ms = a.elapsed_time(b2) / reps
+            entry = {"ms": round(t_ms, 5)}
+            if name in abytes:
+                gb = B * abytes[name] / 1e9
+                entry["GB_per_launch"] = round(gb, 6)
+                entry["GBps"] = round(gb / (t_ms / 1e3), 1)
+            stages[name] = entry
+    peak, peak_kind = load_peaks()
+    spmv = stages["spmv"]
+    spmv_bytes = B * abytes["spmv"]
+    roofline = {"kernel": "pcg_spmv_kernel", "bound": "hbm", "achieved": spmv["GBps"], "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": round(spmv["GBps"] / peak, 4),
+                "traffic": None, "algorithmic_bytes_per_launch": spmv_bytes,
+                "launch_ms": spmv["ms"]}
+
+    # e2e: host buffers -> device copies -> solve -> warp fields back to host
+    host_scenes = [DeviceScene(s, pin=True) for s in scenes]
+    out_host = [torch.empty((s.num_nodes, 8), dtype=torch.float32, pin_memory=True) for s in scenes]
+    h2d = sum(hs.nbytes for hs in host_scenes)
+    d2h = sum(o.numel() * 4 for o in out_host)
+
+    def e2e_step():
+        for i, hs in enumerate(host_scenes):
+            batch.set_input_host(i, hs, stream=stream)
+        batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+        for i in range(B):
+            batch.node_se3(i, out=out_host[i], stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        b2.record(stream)
+        b2.synchronize()
+    e2e_ms = a.elapsed_time(b2) / args.steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": round(world * B / (e2e_ms / 1e3), 3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)}
+
+    # plain FP32 form: one instance at a time, per-kernel launches, float dots
+    plain = None
+    if not args.no_plain:
+        pcfg = abi.make_config(base, precision=abi.PRECISION_FP32, mode=mode)
+        single = NonRigidSolver(pcfg)
+        n_plain = min(B, 4)
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                single.set_solver_input(dev_scenes[0], stream=stream)
+                single.solve_non_rigid_alignment(args.gn, args.pcg, stream=stream)
+            stream.synchronize()
+            a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for i in range(n_plain):
+                single.set_solver_input(dev_scenes[i], stream=stream)
+                single.solve_non_rigid_alignment(args.gn, args.pcg, stream=stream)
+            b2.record(stream)
+            b2.synchronize()
+        p_ms = a.elapsed_time(b2) / n_plain
+        plain = {"value": round(1e3 / p_ms, 3), "unit": "solves/s", "ms_per_solve": round(p_ms, 4),
+                 "form": "plain FP32, one instance per solve, no graph"}
+        single.close()
+
+    return dict(value=value, ms=ms, kernels_per_step=kernels_per_step, clocks=clocks.summary(), stages=stages,
+                roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base)
+
+
+def cpu_solve_instance(scene, gn, pcg):
+    import oracle
+    from multiviewdynrecon_b200 import abi
+    o = oracle.Oracle(scene, abi.make_config(scene), fp64=False)
+    o.solve(gn, pcg)
+    return o
+
+
+def run_cpu_baseline(args, scenes, threads, seconds):
+    """Time whole solves of the CPU restatement on `threads` host threads, one
+    instance per thread, for about `seconds`."""
+    from concurrent.futures import ThreadPoolExecutor
+    done = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while True:
+            futs = [ex.submit(cpu_solve_instance, scenes[(done + k) % len(scenes)], args.gn, args.pcg)
+                    for k in range(threads)]
+            for f in futs:
+                f.result()
+            done += threads
+            if time.perf_counter() - t0 >= seconds:
+                break
+    dt = time.perf_counter() - t0
+    return done / dt, done, dt
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        import oracle
+        oracle.lib()
+        base, scenes = make_scenes(args, 0)
+        threads = os.cpu_count() or 1
+        # warm-up steps, then timed steps; a step solves one instance per thread
+        for _ in range(args.warmup):
+            run_cpu_baseline(args, scenes, threads, 0.0)
+        vals = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            v, n, dt = run_cpu_baseline(args, scenes, threads, 0.0)
+            vals.append(dt)
+        total = time.perf_counter() - t0
+        value = args.steps * threads / total
+        line = {"metric": "non-rigid GN solves/s", "impl": "reference", "value": round(value, 4),
+                "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1e3 * total / args.steps, 2), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "instances_per_step": threads, "gn": args.gn, "pcg": args.pcg},
+                "cpu_baseline": {"value": round(value, 4), "unit": "solves/s", "cores": threads, "kind": "port",
+                                 "sample": f"{threads} whole solves per step, one per host thread"},
+                "e2e": {"value": round(value, 4), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        import datetime
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    r = run_ours(args, rank, world, dist)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        base, scenes = r["base"], make_scenes(args, 0)[1]
+        v, n, dt = run_cpu_baseline(args, scenes, 1, args.cpu_seconds)
+        cpu = {"value": round(v, 4), "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"{n} whole solves of the workload's instances on 1 thread in {dt:.1f} s"}
+    if rank == 0:
+        c = r["counts"]
+        line = {
+            "metric": "non-rigid GN solves/s (batched mixed vs plain FP32) at <=1e-4 rel err vs FP64",
+            "value": round(r["value"], 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "instances_per_gpu": args.batch, "views": 3,
+                       "image": [args.width, args.height], "nodes": args.nodes, "gn": args.gn, "pcg": args.pcg,
+                       "precision": args.precision, "mode": args.mode, "graph": True,
+                       "l2": "aggregate working set of the batch well above the 126 MB L2; no flush",
+                       "dense_terms": c.dense_terms, "half_pairs": c.half_pairs,
+                       "parallelism": f"independent instances, {world} GPU(s), no collective in the solve"},
+            "gpu_launches": int(r["kernels_per_step"] * args.steps),
+            "kernels_per_step": int(r["kernels_per_step"]),
+            "clocks": r["clocks"], "roofline": r["roofline"], "stages": r["stages"], "e2e": r["e2e"],
+            "plain_fp32": r["plain"],
+            "speedup_vs_plain_fp32": (round(r["value"] / r["plain"]["value"], 3) if r["plain"] else None),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -21,7 +21,9 @@
  *    (non-owning views, like the reference's DeviceArrayView). They must stay
  *    valid until the next mvdr_set_inputs on the same solver.
  *  - Every workspace buffer is allocated by mvdr_create / mvdr_batch_create.
- *    Nothing is allocated by set_inputs, build_index, gn_iteration or solve.
+ *    Nothing is allocated by mvdr_set_inputs, build_index, gn_iteration or
+ *    solve. (mvdr_set_inputs_host allocates its input copies once; the
+ *    diagnostic mvdr_get_array exports use a temporary buffer.)
  *  - Every call returns an mvdr_status. No call aborts the process; a CUDA
  *    error is returned as MVDR_ECUDA and its text is kept for
  *    mvdr_last_error_string.
@@ -33,6 +35,12 @@
 
 #include <stddef.h>
 #include <stdint.h>
+
+#if defined(_WIN32)
+#define MVDR_API __declspec(dllexport)
+#else
+#define MVDR_API __attribute__((visibility("default")))
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -125,8 +133,8 @@ typedef struct mvdr_config {
     uint32_t max_cross_terms;
     uint32_t max_dense_terms;    /* 0: max_views * width * height              */
     uint32_t max_foreground_terms; /* 0: max_dense_terms                       */
-    uint32_t max_node_pairs;     /* unique unordered pairs; 0: 32 * max_nodes  */
-    uint32_t max_terms_per_node; /* 0: 16384                                   */
+    uint32_t max_node_pairs;     /* unique unordered pairs; 0: 16 * max_nodes  */
+    uint32_t max_terms_per_node; /* terms touching one node; 0: 4096           */
     /* numerics */
     float node_radius;           /* NODE_RADIUS (base/GlobalConfigs.h:85)      */
     int32_t precision;           /* mvdr_precision                            */
@@ -211,23 +219,24 @@ typedef struct mvdr_batch mvdr_batch;
 /* ---- life cycle ------------------------------------------------------- */
 
 /* Fills *cfg with defaults for the given capacities. */
-void mvdr_config_default(mvdr_config* cfg, uint32_t max_nodes, uint32_t max_views,
+MVDR_API void mvdr_config_default(mvdr_config* cfg, uint32_t max_nodes, uint32_t max_views,
                          uint32_t image_width, uint32_t image_height);
 
 /* NonRigidSolver::NonRigidSolver + AllocateBuffer (NonRigidSolver.h:103,117). */
-int mvdr_create(const mvdr_config* cfg, mvdr_solver** out);
+MVDR_API int mvdr_create(const mvdr_config* cfg, mvdr_solver** out);
 /* ReleaseBuffer + destructor (NonRigidSolver.h:108,123). */
-int mvdr_destroy(mvdr_solver* solver);
+MVDR_API int mvdr_destroy(mvdr_solver* solver);
 
 /* SetSolverInput (NonRigidSolver.cpp:77-97): binds the caller's device arrays
  * and resets the iteration state to inputs->node_se3
  * (SolverIterationData::SetWarpFieldInitialValue, SolverIterationData.cpp:37-50). */
-int mvdr_set_inputs(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
+MVDR_API int mvdr_set_inputs(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
 
 /* As mvdr_set_inputs, but every array pointer is a HOST pointer; the data is
  * copied into solver-owned device buffers on `stream` (pinned host memory
- * makes the copies asynchronous). */
-int mvdr_set_inputs_host(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
+ * makes the copies asynchronous). The first call on an instance, or a call
+ * with larger inputs than before, allocates those device buffers. */
+MVDR_API int mvdr_set_inputs_host(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
 
 /* buildSolverIndexStreamed (NonRigidSolver.h:257, body not in the reference):
  * pixel selection and compaction (ImageTermKNNFetcher.cu:19-137,
@@ -235,28 +244,28 @@ int mvdr_set_inputs_host(mvdr_solver* solver, const mvdr_inputs* inputs, void* s
  * (Node2TermsIndex.cu:8-187), node-pair->term index and bin-block CSR
  * structure (NodePair2TermsIndex.cu:11-296, NodePairRowColumnIndex.cu:19-308).
  * No host synchronisation. */
-int mvdr_build_index(mvdr_solver* solver, void* stream);
+MVDR_API int mvdr_build_index(mvdr_solver* solver, void* stream);
 
 /* One Gauss-Newton iteration (solverIteration{Global,Local}IterationStreamed,
  * NonRigidSolver.h:258-259): term evaluation, preconditioner and RHS, JtJ
  * materialisation (MATERIALIZED mode), block PCG with `pcg_iterations`
  * iterations, warp-field update (SolverIterationData.cu:9-94). */
-int mvdr_gn_iteration(mvdr_solver* solver, uint32_t pcg_iterations, void* stream);
+MVDR_API int mvdr_gn_iteration(mvdr_solver* solver, uint32_t pcg_iterations, void* stream);
 
 /* SolveNonRigidAlignment (NonRigidSolver.h:254): build_index followed by
  * `gn_iterations` Gauss-Newton iterations. */
-int mvdr_solve(mvdr_solver* solver, uint32_t gn_iterations, uint32_t pcg_iterations, void* stream);
+MVDR_API int mvdr_solve(mvdr_solver* solver, uint32_t gn_iterations, uint32_t pcg_iterations, void* stream);
 
 /* SolvedNodeSE3 (NonRigidSolver.h:214): copies the current node SE(3) array
  * (num_nodes dual quaternions) to `dst`, which may be host or device memory. */
-int mvdr_get_node_se3(mvdr_solver* solver, mvdr_dual_quaternion* dst, void* stream);
+MVDR_API int mvdr_get_node_se3(mvdr_solver* solver, mvdr_dual_quaternion* dst, void* stream);
 
 /* Synchronises `stream` and returns the sizes of the current index. */
-int mvdr_get_counts(mvdr_solver* solver, mvdr_counts* out, void* stream);
+MVDR_API int mvdr_get_counts(mvdr_solver* solver, mvdr_counts* out, void* stream);
 
 /* Energy sum (lambda * r)^2 of the terms evaluated by the last Gauss-Newton
  * iteration, accumulated in double (ResidualEvaluator.cu:71-226). */
-int mvdr_get_energy(mvdr_solver* solver, double* energy, void* stream);
+MVDR_API int mvdr_get_energy(mvdr_solver* solver, double* energy, void* stream);
 
 /* ---- intermediate products (for checks) --------------------------------
  * `which` selects an array, `dst` receives it (host or device memory),
@@ -287,36 +296,56 @@ enum {
     MVDR_ARRAY_INCREMENT = 21,          /* float [6N] PCG solution of the last iteration     */
     MVDR_ARRAY_NODE_SE3 = 22            /* dual quaternion [N] current warp field            */
 };
-int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t capacity_bytes,
+MVDR_API int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t capacity_bytes,
                    size_t* written_bytes, void* stream);
 
 /* y = JtJ x with the operator of the last Gauss-Newton iteration, in the
  * current mode (bin-block/BSR SpMV or matrix-free adjoint pair). x and y are
  * device arrays of 6*num_nodes floats. */
-int mvdr_apply_jtj(mvdr_solver* solver, const float* x, float* y, void* stream);
+MVDR_API int mvdr_apply_jtj(mvdr_solver* solver, const float* x, float* y, void* stream);
 
 /* ---- batched solves (many independent instances per launch) ------------- */
 
 /* All instances share the capacities of *cfg; their actual sizes may differ. */
-int mvdr_batch_create(const mvdr_config* cfg, uint32_t num_instances, mvdr_batch** out);
-int mvdr_batch_destroy(mvdr_batch* batch);
-int mvdr_batch_set_inputs(mvdr_batch* batch, uint32_t instance, const mvdr_inputs* inputs, void* stream);
-int mvdr_batch_set_inputs_host(mvdr_batch* batch, uint32_t instance, const mvdr_inputs* inputs, void* stream);
+MVDR_API int mvdr_batch_create(const mvdr_config* cfg, uint32_t num_instances, mvdr_batch** out);
+MVDR_API int mvdr_batch_destroy(mvdr_batch* batch);
+MVDR_API int mvdr_batch_set_inputs(mvdr_batch* batch, uint32_t instance, const mvdr_inputs* inputs, void* stream);
+MVDR_API int mvdr_batch_set_inputs_host(mvdr_batch* batch, uint32_t instance, const mvdr_inputs* inputs, void* stream);
 /* Index build and `gn_iterations` Gauss-Newton iterations for every instance;
  * each stage is one launch over all instances. When use_graph is non-zero the
  * Gauss-Newton iterations are captured once as a CUDA graph and replayed. */
-int mvdr_batch_solve(mvdr_batch* batch, uint32_t gn_iterations, uint32_t pcg_iterations,
+MVDR_API int mvdr_batch_solve(mvdr_batch* batch, uint32_t gn_iterations, uint32_t pcg_iterations,
                      int use_graph, void* stream);
-int mvdr_batch_get_node_se3(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst, void* stream);
+MVDR_API int mvdr_batch_get_node_se3(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst, void* stream);
 /* The single-instance view of one batch member (not owned; do not destroy). */
-int mvdr_batch_instance(mvdr_batch* batch, uint32_t instance, mvdr_solver** out);
+MVDR_API int mvdr_batch_instance(mvdr_batch* batch, uint32_t instance, mvdr_solver** out);
 
 /* ---- diagnostics -------------------------------------------------------- */
 
+/* Stages of one Gauss-Newton iteration, for timing one stage in isolation. */
+enum {
+    MVDR_STAGE_INDEX = 0,      /* the whole index build                          */
+    MVDR_STAGE_TERMS = 1,      /* term evaluation                                */
+    MVDR_STAGE_DIAG = 2,       /* diagonal blocks, Jt r and the preconditioner   */
+    MVDR_STAGE_OFFDIAG = 3,    /* off-diagonal JtJ blocks (materialised mode)    */
+    MVDR_STAGE_SPMV = 4,       /* one PCG operator application (SpMV + d.q)      */
+    MVDR_STAGE_PCG_UPDATE = 5, /* one PCG vector update (x, r, s, r.s)           */
+    MVDR_STAGE_UPDATE = 6      /* warp-field update                              */
+};
+/* Enqueue the kernels of one stage for every instance of the batch, with the
+ * lambdas of Gauss-Newton iteration 0. The stage reads the state left by the
+ * previous solve and overwrites that stage's outputs, so a later solve must
+ * start again from mvdr_batch_set_inputs. No host synchronisation. */
+MVDR_API int mvdr_batch_enqueue_stage(mvdr_batch* batch, int stage, void* stream);
+
 /* Text of the last error recorded on this host thread. */
-const char* mvdr_last_error_string(void);
-/* Number of kernel launches this library has enqueued since load. */
-uint64_t mvdr_kernel_launch_count(void);
+MVDR_API const char* mvdr_last_error_string(void);
+/* Number of kernel launches this library has enqueued since load (a graph
+ * launch counts once). */
+MVDR_API uint64_t mvdr_kernel_launch_count(void);
+/* sizeof() of the public struct `name` ("mvdr_config", "mvdr_inputs", ...) as
+ * compiled into this library, so a binding can check its own layout. */
+MVDR_API int mvdr_abi_layout(const char* name, size_t* size);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,692 @@
+// Index build: pixel selection and compaction, node -> term index, node-pair
+// -> term index, symmetric block-row structure and the bin-block CSR layout.
+//
+// Reference: ImageTermKNNFetcher.cu:19-137, DensityForegroundMapHandler.cu:17-146,
+// Node2TermsIndex.cu:8-187, NodePair2TermsIndex.cu:11-296,
+// NodePairRowColumnIndex.cu:19-308.
+//
+// The reference sorts (node, term) and (pair, term) key/value arrays with
+// global CUB radix sorts and stable ordering. Both orders are the same as
+// sorting unique composite keys (node, term) and (pair, term), so here the
+// entries are counted and scattered into per-node segments with integer
+// atomics and each short segment is then sorted in shared memory. The result
+// is independent of the scatter order, hence bit-exact with the reference
+// order and reproducible run to run. No host synchronisation is needed: every
+// size lives in DeviceCounts.
+#include "kernels_common.cuh"
+
+namespace mvdr {
+
+constexpr uint32_t kChunk = 2048;  // pixels per compaction CTA (256 threads x 8)
+
+// ----------------------------------------------------- input checks -----
+// Node ids of the skinning, the node graph and the correspondences must be
+// below num_nodes and surfel ids below num_surfels; otherwise the instance is
+// flagged and every kernel that would index with them skips its work.
+__global__ void __launch_bounds__(256) input_check_kernel(const InstDesc* insts, uint32_t width, uint32_t height) {
+    const InstDesc& I = insts[blockIdx.y];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    for (uint32_t i = t0; i < I.S; i += stride) {
+        const ushort4 k = I.surfel_knn[i];
+        bad |= k.x >= I.N || k.y >= I.N || k.z >= I.N || k.w >= I.N;
+    }
+    for (uint32_t i = t0; i < I.E; i += stride) {
+        const ushort2 e = I.graph[i];
+        bad |= e.x >= I.N || e.y >= I.N;
+    }
+    for (uint32_t i = t0; i < I.Tp; i += stride) {
+        const ushort4 k = I.feat_knn[i];
+        bad |= k.x >= I.N || k.y >= I.N || k.z >= I.N || k.w >= I.N;
+    }
+    for (uint32_t i = t0; i < I.Tc; i += stride) {
+        const ushort4 k = I.cross_knn[i];
+        bad |= k.x >= I.N || k.y >= I.N || k.z >= I.N || k.w >= I.N;
+    }
+    const uint32_t npix = width * height;
+    for (uint32_t v = 0; v < I.num_views; ++v) {
+        const ViewDesc& V = I.views[v];
+        for (uint32_t p = t0; p < npix; p += stride) {
+            const uint32_t s = V.index[(size_t)(p / width) * V.pitch + p % width];
+            bad |= s != kInvalid && s >= I.S;
+        }
+    }
+    if (bad) set_error(I, kErrBadNodeIndex);
+}
+
+// ------------------------------------------------------- compaction -----
+
+// a surfel id past the surfel array marks the pixel invalid (and is reported
+// by input_check_kernel)
+struct DensePred {
+    __device__ static inline bool eval(const InstDesc& I, uint32_t v, uint32_t x, uint32_t y) {
+        const ViewDesc& V = I.views[v];
+        return V.index[(size_t)y * V.pitch + x] < I.S;
+    }
+};
+
+// markValidColorForegroundMapsPixelKernel (DensityForegroundMapHandler.cu:34-105):
+// project the initially warped surfel; keep it when it lands inside the image,
+// faces the camera (cos > 0.5) and the filtered mask there is non-zero.
+struct ForegroundPred {
+    __device__ static inline bool eval(const InstDesc& I, uint32_t v, uint32_t x, uint32_t y) {
+        const ViewDesc& V = I.views[v];
+        const size_t p = (size_t)y * V.pitch + x;
+        const uint32_t s = V.index[p];
+        if (!I.use_fg || s >= I.S || V.fg == nullptr || bad_inputs(I)) return false;
+        const float4 cv = V.ref_v[p], cn = V.ref_n[p];
+        const float3 cv0 = apply3(V.init, mk3(cv.x, cv.y, cv.z));
+        const float3 cn0 = rot3(V.init, mk3(cn.x, cn.y, cn.z));
+        const M34 se3 = dq_se3(blend_dq(I.se3, I.surfel_knn[s], I.surfel_w[s]));
+        const float3 wv = apply3(se3, cv0), wn = rot3(se3, cn0);
+        const float3 vc = apply3(V.init_inv, apply3(V.w2c, wv));
+        const float3 nc = rot3(V.init_inv, rot3(V.w2c, wn));
+        const float inv = rsqrtf(dot3(vc, vc));
+        const float cosang = -dot3(mul3(inv, vc), nc);
+        const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
+        const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
+        if (u < 0 || u >= (int)I.width || w < 0 || w >= (int)I.height || !(cosang > 0.5f)) return false;
+        return V.fg[(size_t)w * V.pitch + u] > 1e-5f;  // isValidForegroundMaskPixel
+    }
+};
+
+template <class Pred>
+__global__ void __launch_bounds__(256) compact_count_kernel(const InstDesc* insts, uint32_t width, uint32_t height,
+                                                            uint32_t cpv) {
+    const InstDesc& I = insts[blockIdx.y];
+    const uint32_t view = blockIdx.x / cpv, c = blockIdx.x % cpv;
+    uint32_t cnt = 0;
+    if (view < I.num_views) {
+        const uint32_t npix = width * height;
+        for (uint32_t k = 0; k < kChunk / 256; ++k) {
+            const uint32_t p = c * kChunk + k * 256 + threadIdx.x;
+            if (p < npix) cnt += Pred::eval(I, view, p % width, p / width) ? 1u : 0u;
+        }
+    }
+    cnt = warp_sum(cnt);
+    __shared__ uint32_t ws[8];
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < 8; ++i) t += ws[i];
+        I.chunk_count[blockIdx.x] = t;
+    }
+}
+
+// exclusive scan of the chunk counts; per-view totals; capacity check
+__global__ void __launch_bounds__(1024) compact_scan_kernel(const InstDesc* insts, uint32_t cpv, uint32_t max_views,
+                                                            int foreground) {
+    const InstDesc& I = insts[blockIdx.y];
+    DeviceCounts* C = I.counts;
+    // per-view totals before the scan
+    if (threadIdx.x < MVDR_MAX_VIEWS) {
+        uint32_t t = 0;
+        if (threadIdx.x < max_views)
+            for (uint32_t c = 0; c < cpv; ++c) t += I.chunk_count[threadIdx.x * cpv + c];
+        if (foreground) C->fg_view_count[threadIdx.x] = t;
+        else C->dense_view_count[threadIdx.x] = t;
+    }
+    __syncthreads();
+    uint32_t total = 0;
+    __shared__ uint32_t tot;
+    block_exclusive_scan_inplace(I.chunk_count, cpv * max_views, &tot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        total = tot;
+        const uint32_t cap = foreground ? I.cap_fg : I.cap_dense;
+        if (total > cap) {
+            atomicOr(&C->error_flags, foreground ? kErrForegroundCapacity : kErrDenseCapacity);
+            total = cap;
+        }
+        if (foreground) C->foreground_terms = total;
+        else C->dense_terms = total;
+    }
+}
+
+template <class Pred>
+__global__ void __launch_bounds__(256) compact_write_kernel(const InstDesc* insts, uint32_t width, uint32_t height,
+                                                            uint32_t cpv, int foreground) {
+    const InstDesc& I = insts[blockIdx.y];
+    const uint32_t view = blockIdx.x / cpv, c = blockIdx.x % cpv;
+    if (view >= I.num_views) return;
+    const uint32_t npix = width * height;
+    const uint32_t cap = foreground ? I.cap_fg : I.cap_dense;
+    __shared__ uint32_t wtot[8];
+    uint32_t carry = I.chunk_count[blockIdx.x];
+    for (uint32_t k = 0; k < kChunk / 256; ++k) {
+        const uint32_t p = c * kChunk + k * 256 + threadIdx.x;
+        const uint32_t x = p % width, y = p / width;
+        const bool ok = p < npix && Pred::eval(I, view, x, y);
+        const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+        const uint32_t lane_prefix = __popc(bal & ((1u << lane_id()) - 1u));
+        if (lane_id() == 0) wtot[threadIdx.x >> 5] = __popc(bal);
+        __syncthreads();
+        uint32_t wbase = 0, slice = 0;
+        for (uint32_t w = 0; w < 8; ++w) {
+            if (w < (threadIdx.x >> 5)) wbase += wtot[w];
+            slice += wtot[w];
+        }
+        if (ok) {
+            const uint32_t out = carry + wbase + lane_prefix;
+            if (out < cap) {
+                const ViewDesc& V = I.views[view];
+                const uint32_t s = V.index[(size_t)y * V.pitch + x];
+                if (s < I.S) {
+                    const ushort4 pix = make_ushort4((unsigned short)x, (unsigned short)y, (unsigned short)view, 0);
+                    if (foreground) {
+                        I.fg_pix[out] = pix;
+                        I.fg_knn[out] = I.surfel_knn[s];
+                        I.fg_w[out] = I.surfel_w[s];
+                    } else {
+                        I.dense_pix[out] = pix;
+                        I.dense_knn[out] = I.surfel_knn[s];
+                        I.dense_w[out] = I.surfel_w[s];
+                    }
+                } else {
+                    set_error(I, kErrBadNodeIndex);
+                }
+            }
+        }
+        carry += slice;
+        __syncthreads();
+    }
+}
+
+// view whose maps a compacted pixel samples: its own tag, or in compat mode
+// the reference's lookup that reads per-view counts as offsets
+// (DenseDepthJacobianResidual.cu:14-22)
+__device__ inline uint32_t sample_view(const InstDesc& I, ushort4 pix, uint32_t idx, const uint32_t* view_count) {
+    if (!(I.compat & MVDR_COMPAT_REF_VIEW_LOOKUP)) return pix.z;
+    for (uint32_t i = 0; i < I.num_views; ++i) {
+        if (i == I.num_views - 1) return i;
+        if (view_count[i] <= idx && idx < view_count[i + 1]) return i;
+    }
+    return I.num_views - 1;
+}
+
+// canonical vertex / normal of each compacted pixel in frame 0; constant over
+// the Gauss-Newton iterations, so computed once per index build
+__global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    const uint32_t Td = C->dense_terms, Tf = C->foreground_terms;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < Td + Tf; t += gridDim.x * blockDim.x) {
+        const bool fg = t >= Td;
+        const uint32_t k = fg ? t - Td : t;
+        const ushort4 pix = fg ? I.fg_pix[k] : I.dense_pix[k];
+        const uint32_t v = sample_view(I, pix, k, fg ? C->fg_view_count : C->dense_view_count);
+        const ViewDesc& V = I.views[v];
+        const size_t p = (size_t)pix.y * V.pitch + pix.x;
+        const float4 cv = V.ref_v[p];
+        const float3 a = apply3(V.init, mk3(cv.x, cv.y, cv.z));
+        if (fg) {
+            I.fg_cv[k] = make_float4(a.x, a.y, a.z, __uint_as_float(v));
+        } else {
+            const float4 cn = V.ref_n[p];
+            const float3 b = rot3(V.init, mk3(cn.x, cn.y, cn.z));
+            I.dense_cv[k] = make_float4(a.x, a.y, a.z, __uint_as_float(v));
+            I.dense_cn[k] = make_float4(b.x, b.y, b.z, 0.f);
+        }
+    }
+}
+
+// size2offset (term_offset_types.h:44-64) on the device
+__global__ void term_offsets_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (threadIdx.x != 0) return;
+    DeviceCounts* C = I.counts;
+    C->smooth_terms = I.E;
+    C->feature_terms = I.Tp;
+    C->cross_terms = I.Tc;
+    uint32_t o = C->dense_terms;
+    C->term_offset[0] = o;
+    o += I.E;
+    C->term_offset[1] = o;
+    o += C->foreground_terms;
+    C->term_offset[2] = o;
+    o += I.Tp;
+    C->term_offset[3] = o;
+    o += I.Tc;
+    C->term_offset[4] = o;
+}
+
+// ------------------------------------------------------ node -> term -----
+
+__global__ void __launch_bounds__(256) n2t_count_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (bad_inputs(I)) return;
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t T = off.o[4];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        uint32_t k;
+        const TermType ty = off.typed(t, k);
+        const ushort4 n = term_nodes(I, ty, k);
+        const uint32_t m = ty == kSmooth ? 2 : 4;
+        const unsigned short a[4] = {n.x, n.y, n.z, n.w};
+        for (uint32_t j = 0; j < m; ++j) {
+            if (a[j] < I.N) atomicAdd(&I.n2t_count[a[j]], 1u);
+            else set_error(I, kErrBadNodeIndex);
+        }
+    }
+}
+
+// single-CTA exclusive scans over per-node arrays
+enum ScanWhat : int { kScanN2T = 0, kScanRows = 1, kScanUpper = 2, kScanBlkRows = 3, kScanBins = 4 };
+
+__global__ void __launch_bounds__(1024) node_scan_kernel(const InstDesc* insts, int what) {
+    const InstDesc& I = insts[blockIdx.y];
+    DeviceCounts* C = I.counts;
+    __shared__ uint32_t total;
+    const uint32_t N = I.N;
+    switch (what) {
+        case kScanN2T: {
+            for (uint32_t i = threadIdx.x; i <= N; i += blockDim.x) {
+                I.n2t_offset[i] = i < N ? I.n2t_count[i] : 0u;
+                if (i < N) I.n2t_cursor[i] = 0;
+            }
+            __syncthreads();
+            block_exclusive_scan_inplace(I.n2t_offset, N + 1, &total);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                C->node2term_entries = total;
+                if (total > I.cap_k1) atomicOr(&C->error_flags, kErrNode2TermCapacity);
+            }
+            break;
+        }
+        case kScanRows: {
+            for (uint32_t i = threadIdx.x; i <= N; i += blockDim.x) I.row_offset[i] = i < N ? I.row_count[i] : 0u;
+            __syncthreads();
+            block_exclusive_scan_inplace(I.row_offset, N + 1, &total);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                C->nodepair_entries = total;
+                if (total > I.cap_k2) atomicOr(&C->error_flags, kErrNodePairEntryCapacity);
+            }
+            break;
+        }
+        case kScanUpper: {
+            for (uint32_t i = threadIdx.x; i <= N; i += blockDim.x) {
+                I.half_offset[i] = i < N ? I.upper_count[i] : 0u;
+                if (i < N) { I.lower_count[i] = 0; I.lower_cursor[i] = 0; }
+            }
+            __syncthreads();
+            block_exclusive_scan_inplace(I.half_offset, N + 1, &total);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                C->half_pairs = total;
+                if (total > I.cap_pairs) atomicOr(&C->error_flags, kErrHalfPairCapacity);
+            }
+            break;
+        }
+        case kScanBlkRows: {
+            for (uint32_t i = threadIdx.x; i <= N; i += blockDim.x)
+                I.blkrow_offset[i] = i < N ? I.lower_count[i] + I.upper_count[i] : 0u;
+            __syncthreads();
+            block_exclusive_scan_inplace(I.blkrow_offset, N + 1, &total);
+            break;
+        }
+        case kScanBins: {
+            const uint32_t nb = C->num_bins;
+            __syncthreads();
+            block_exclusive_scan_inplace(I.bin_scan, nb + 1, &total);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                C->binblock_nnz = I.bin_scan[nb];
+                if (I.bin_scan[nb] > I.cap_bb) atomicOr(&C->error_flags, kErrBinBlockCapacity);
+            }
+            break;
+        }
+        default: break;
+    }
+}
+
+__global__ void __launch_bounds__(256) n2t_scatter_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t T = off.o[4];
+    const uint32_t K1 = I.counts->node2term_entries;
+    if (K1 > I.cap_k1) return;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        uint32_t k;
+        const TermType ty = off.typed(t, k);
+        const ushort4 n = term_nodes(I, ty, k);
+        const uint32_t m = ty == kSmooth ? 2 : 4;
+        const unsigned short a[4] = {n.x, n.y, n.z, n.w};
+        for (uint32_t j = 0; j < m; ++j) {
+            if (a[j] >= I.N) continue;
+            const uint32_t pos = I.n2t_offset[a[j]] + atomicAdd(&I.n2t_cursor[a[j]], 1u);
+            I.n2t_index[pos] = t;
+        }
+    }
+}
+
+// sort each node's term segment ascending (one CTA per node)
+__global__ void __launch_bounds__(256) n2t_sort_kernel(const InstDesc* insts) {
+    extern __shared__ uint32_t s32[];
+    const InstDesc& I = insts[blockIdx.y];
+    if (I.counts->node2term_entries > I.cap_k1) return;
+    for (uint32_t node = blockIdx.x; node < I.N; node += gridDim.x) {
+        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        const uint32_t len = e - b;
+        if (len <= 1) continue;
+        if (len > I.cap_seg) {
+            if (threadIdx.x == 0) set_error(I, kErrSegmentTooLong);
+            continue;
+        }
+        const uint32_t n2 = next_pow2(len);
+        for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) s32[i] = i < len ? I.n2t_index[b + i] : 0xFFFFFFFFu;
+        __syncthreads();
+        block_bitonic_sort(s32, n2);
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) I.n2t_index[b + i] = s32[i];
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------ node pair -> term -----
+// Row i of the upper triangle holds the entries (j, t) for every term t of
+// node i and every other node j > i of t: the reference's half-pair keys
+// (computeKVNodePairKNN, NodePair2TermsIndex.cu:11-28; smooth pairs :71-81)
+// grouped by their smaller node.
+
+__device__ inline uint32_t upper_entries_of(const InstDesc& I, const TermOffsets& off, uint32_t node, uint32_t t,
+                                            uint32_t js[4]) {
+    uint32_t k;
+    const TermType ty = off.typed(t, k);
+    const ushort4 n = term_nodes(I, ty, k);
+    uint32_t c = 0;
+    if (ty == kSmooth) {
+        // the smooth term contributes one pair (min, max) to the row of min
+        const uint32_t a = n.x, b = n.y;
+        if (a == node && b > node && b < I.N) js[c++] = b;
+        else if (b == node && a > node && a < I.N) js[c++] = a;
+        // a node listed twice in the same smooth term (a == b) gives no pair
+        return c;
+    }
+    const unsigned short a[4] = {n.x, n.y, n.z, n.w};
+    for (int q = 0; q < 4; ++q)
+        if (a[q] > node && a[q] < I.N) js[c++] = a[q];
+    return c;
+}
+
+// warp per node: number of upper entries of the row
+__global__ void __launch_bounds__(256) np_row_count_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (I.counts->node2term_entries > I.cap_k1) return;
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        uint32_t c = 0;
+        for (uint32_t p = b + lane_id(); p < e; p += 32) {
+            uint32_t js[4];
+            c += upper_entries_of(I, off, node, I.n2t_index[p], js);
+        }
+        c = warp_sum(c);
+        if (lane_id() == 0) I.row_count[node] = c;
+    }
+}
+
+// CTA per node: gather (j, t) keys of the row, sort them, write the term
+// values of the row and the row's unique pairs (to a temporary per-row area)
+__global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts) {
+    extern __shared__ unsigned long long s64[];
+    __shared__ uint32_t fill;
+    __shared__ uint32_t wtot[8];
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->node2term_entries > I.cap_k1 || C->nodepair_entries > I.cap_k2) return;
+    TermOffsets off;
+    off.load(I.counts);
+    for (uint32_t node = blockIdx.x; node < I.N; node += gridDim.x) {
+        const uint32_t len = I.row_count[node];
+        const uint32_t out = I.row_offset[node];
+        if (len == 0) {
+            if (threadIdx.x == 0) I.upper_count[node] = 0;
+            continue;
+        }
+        if (len > I.cap_row) {
+            if (threadIdx.x == 0) { set_error(I, kErrRowTooLong); I.upper_count[node] = 0; }
+            continue;
+        }
+        if (threadIdx.x == 0) fill = 0;
+        __syncthreads();
+        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        for (uint32_t p = b + threadIdx.x; p < e; p += blockDim.x) {
+            const uint32_t t = I.n2t_index[p];
+            uint32_t js[4];
+            const uint32_t c = upper_entries_of(I, off, node, t, js);
+            if (c) {
+                const uint32_t base = atomicAdd(&fill, c);
+                for (uint32_t q = 0; q < c; ++q) s64[base + q] = ((unsigned long long)js[q] << 32) | t;
+            }
+        }
+        __syncthreads();
+        const uint32_t n2 = next_pow2(len);
+        for (uint32_t i = len + threadIdx.x; i < n2; i += blockDim.x) s64[i] = ~0ull;
+        __syncthreads();
+        block_bitonic_sort(s64, n2);
+        // values, and unique-j run starts (block scan over the row)
+        uint32_t carry = 0;
+        for (uint32_t base = 0; base < len; base += blockDim.x) {
+            const uint32_t i = base + threadIdx.x;
+            bool start = false;
+            uint32_t j = 0;
+            if (i < len) {
+                const unsigned long long key = s64[i];
+                I.np_index[out + i] = (uint32_t)key;
+                j = (uint32_t)(key >> 32);
+                start = (i == 0) || ((uint32_t)(s64[i - 1] >> 32) != j);
+            }
+            const uint32_t bal = __ballot_sync(0xffffffffu, start);
+            const uint32_t lp = __popc(bal & ((1u << lane_id()) - 1u));
+            if (lane_id() == 0) wtot[threadIdx.x >> 5] = __popc(bal);
+            __syncthreads();
+            uint32_t wb = 0, slice = 0;
+            for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+                if (w < (threadIdx.x >> 5)) wb += wtot[w];
+                slice += wtot[w];
+            }
+            if (start) {
+                const uint32_t u = carry + wb + lp;
+                I.tmp_key[out + u] = node * I.enc + j;
+                I.tmp_start[out + u] = out + i;
+            }
+            carry += slice;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) I.upper_count[node] = carry;
+        __syncthreads();
+    }
+}
+
+// warp per node: copy the row's unique pairs to the compact half-pair arrays
+// and count the lower-triangle entries of each column
+__global__ void __launch_bounds__(256) np_half_compact_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2 || C->node2term_entries > I.cap_k1) return;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        const uint32_t nu = I.upper_count[node];
+        const uint32_t ro = I.row_offset[node], re = I.row_offset[node + 1];
+        const uint32_t h0 = I.half_offset[node];
+        for (uint32_t u = lane_id(); u < nu; u += 32) {
+            const uint32_t key = I.tmp_key[ro + u];
+            const uint32_t start = I.tmp_start[ro + u];
+            const uint32_t end = (u + 1 < nu) ? I.tmp_start[ro + u + 1] : re;
+            I.half_key[h0 + u] = key;
+            I.half_range[h0 + u] = make_uint2(start, end);
+            atomicAdd(&I.lower_count[key % I.enc], 1u);
+        }
+    }
+}
+
+// warp per node: place the row's upper entries and scatter its pairs into the
+// lower part of each partner row (unordered there; sorted next)
+__global__ void __launch_bounds__(256) np_sym_scatter_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2 || C->node2term_entries > I.cap_k1) return;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        const uint32_t nu = I.upper_count[node];
+        const uint32_t h0 = I.half_offset[node];
+        const uint32_t up0 = I.blkrow_offset[node] + I.lower_count[node];
+        for (uint32_t u = lane_id(); u < nu; u += 32) {
+            const uint32_t h = h0 + u;
+            const uint32_t key = I.half_key[h];
+            const uint2 rg = I.half_range[h];
+            const uint32_t s = up0 + u;
+            I.sym_key[s] = key;
+            I.sym_range[s] = rg;
+            I.sym_half[s] = h;
+            I.upper_pos[h] = s;
+            const uint32_t j = key % I.enc;
+            const uint32_t pos = I.blkrow_offset[j] + atomicAdd(&I.lower_cursor[j], 1u);
+            I.sym_key[pos] = j * I.enc + node;
+            I.sym_range[pos] = rg;
+            I.sym_half[pos] = h;
+        }
+    }
+}
+
+// warp per row: sort the lower part by key (keys are unique) by ranking
+__global__ void __launch_bounds__(128) np_lower_sort_kernel(const InstDesc* insts) {
+    constexpr uint32_t kMaxLower = 256;
+    __shared__ uint32_t sk[4][kMaxLower];
+    __shared__ uint2 sr[4][kMaxLower];
+    __shared__ uint32_t sh[4][kMaxLower];
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2 || C->node2term_entries > I.cap_k1) return;
+    const uint32_t w = threadIdx.x >> 5;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + w; node < I.N; node += warps) {
+        const uint32_t nl = I.lower_count[node];
+        const uint32_t b = I.blkrow_offset[node];
+        if (nl > kMaxLower) {
+            if (lane_id() == 0) set_error(I, kErrRowTooLong);
+            continue;
+        }
+        for (uint32_t i = lane_id(); i < nl; i += 32) {
+            sk[w][i] = I.sym_key[b + i];
+            sr[w][i] = I.sym_range[b + i];
+            sh[w][i] = I.sym_half[b + i];
+        }
+        __syncwarp();
+        for (uint32_t i = lane_id(); i < nl; i += 32) {
+            const uint32_t key = sk[w][i];
+            uint32_t rank = 0;
+            for (uint32_t m = 0; m < nl; ++m) rank += sk[w][m] < key ? 1u : 0u;
+            I.sym_key[b + rank] = key;
+            I.sym_range[b + rank] = sr[w][i];
+            I.sym_half[b + rank] = sh[w][i];
+            I.lower_pos[sh[w][i]] = b + rank;
+        }
+        __syncwarp();
+    }
+}
+
+// --------------------------------------------------- bin-block CSR -------
+// computeBinLengthKernel (NodePairRowColumnIndex.cu:64-119), multi-CTA: the
+// bin width is 6 x the longest block row (diagonal included) among the block
+// rows that the bin's 32 scalar rows touch
+__global__ void __launch_bounds__(256) bin_length_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const uint32_t nb = (6 * I.N + 31) / 32;
+    if (blockIdx.x == 0 && threadIdx.x == 0) I.counts->num_bins = nb;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x) {
+        if (b == nb) { I.bin_scan[b] = 0; continue; }
+        const uint32_t r0 = 32 * b / 6;
+        uint32_t r1 = (32 * b + 31) / 6;
+        r1 = min(r1, I.N - 1);
+        uint32_t mx = 0;
+        for (uint32_t r = r0; r <= r1; ++r) mx = max(mx, 1 + I.blkrow_offset[r + 1] - I.blkrow_offset[r]);
+        I.bin_scan[b] = 32 * 6 * mx;
+    }
+}
+
+// computeBinBlockedCSRRowPtrKernel (NodePairRowColumnIndex.cu:122-132) and the
+// 0xFF fill of the column array (:273-281)
+__global__ void __launch_bounds__(256) bin_rowptr_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    const uint32_t nb = C->num_bins;
+    if (C->binblock_nnz > I.cap_bb) return;
+    const uint32_t ncol = C->binblock_nnz / 6;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 32 * (nb + 1); i += stride)
+        I.bb_rowptr[i] = (int32_t)(i % 32 + I.bin_scan[i / 32]);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncol; i += stride) I.bb_colptr[i] = -1;
+}
+
+// computeBinBlockedCSRColPtrKernel (NodePairRowColumnIndex.cu:136-179)
+__global__ void __launch_bounds__(256) bin_colptr_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->binblock_nnz > I.cap_bb || C->half_pairs > I.cap_pairs) return;
+    const uint32_t rows = 6 * I.N;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
+        const uint32_t br = row / 6, lane = row % 32;
+        const uint32_t data = (uint32_t)(row % 32) + I.bin_scan[row / 32];
+        uint32_t col = (data - lane) / 6 + lane;
+        I.bb_colptr[col] = (int32_t)(6 * br);
+        col += 32;
+        for (uint32_t s = I.blkrow_offset[br]; s < I.blkrow_offset[br + 1]; ++s, col += 32)
+            I.bb_colptr[col] = (int32_t)(6 * (I.sym_key[s] % I.enc));
+    }
+}
+
+// ------------------------------------------------------------ launch -----
+
+static inline dim3 grid2(uint32_t x, uint32_t B) { return dim3(x ? x : 1, B); }
+
+cudaError_t set_index_smem_limits(size_t seg_bytes, size_t row_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(n2t_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(np_row_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_bytes);
+}
+
+cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
+    const uint32_t B = lc.B;
+    const uint32_t cpv = lc.chunks_per_view;
+    const uint32_t spread = (uint32_t)lc.sm_count * 4;  // grid-stride kernels
+    MVDR_LAUNCH(input_check_kernel, grid2(spread, B), 256, 0, st, d, lc.width, lc.height);
+    // dense pixels
+    MVDR_LAUNCH(compact_count_kernel<DensePred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv);
+    MVDR_LAUNCH(compact_scan_kernel, grid2(1, B), 1024, 0, st, d, cpv, lc.max_views, 0);
+    MVDR_LAUNCH(compact_write_kernel<DensePred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv, 0);
+    // foreground pixels (the predicate is false when the term is off)
+    MVDR_LAUNCH(compact_count_kernel<ForegroundPred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv);
+    MVDR_LAUNCH(compact_scan_kernel, grid2(1, B), 1024, 0, st, d, cpv, lc.max_views, 1);
+    MVDR_LAUNCH(compact_write_kernel<ForegroundPred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv, 1);
+    MVDR_LAUNCH(prepare_pixels_kernel, grid2(spread, B), 256, 0, st, d);
+    MVDR_LAUNCH(term_offsets_kernel, grid2(1, B), 32, 0, st, d);
+    // node -> term
+    MVDR_LAUNCH(n2t_count_kernel, grid2(spread, B), 256, 0, st, d);
+    MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanN2T);
+    MVDR_LAUNCH(n2t_scatter_kernel, grid2(spread, B), 256, 0, st, d);
+    MVDR_LAUNCH(n2t_sort_kernel, grid2(lc.max_nodes, B), 256, (size_t)lc.cap_seg * 4, st, d);
+    // node pair -> term
+    MVDR_LAUNCH(np_row_count_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
+    MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanRows);
+    MVDR_LAUNCH(np_row_build_kernel, grid2(lc.max_nodes, B), 256, (size_t)lc.cap_row * 8, st, d);
+    MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanUpper);
+    MVDR_LAUNCH(np_half_compact_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
+    MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanBlkRows);
+    MVDR_LAUNCH(np_sym_scatter_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
+    MVDR_LAUNCH(np_lower_sort_kernel, grid2((lc.max_nodes + 3) / 4, B), 128, 0, st, d);
+    // bin-block CSR structure
+    MVDR_LAUNCH(bin_length_kernel, grid2((6 * lc.max_nodes / 32 + 256) / 256, B), 256, 0, st, d);
+    MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanBins);
+    MVDR_LAUNCH(bin_rowptr_kernel, grid2(spread, B), 256, 0, st, d);
+    MVDR_LAUNCH(bin_colptr_kernel, grid2((6 * lc.max_nodes + 255) / 256, B), 256, 0, st, d);
+    return cudaGetLastError();
+}
+
+}  // namespace mvdr

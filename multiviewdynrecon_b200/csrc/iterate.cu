@@ -1,0 +1,925 @@
+// Per Gauss-Newton iteration kernels: term evaluation, JtJ diagonal blocks /
+// Jt r / block preconditioner, off-diagonal JtJ blocks into BSR storage,
+// block-Jacobi PCG (materialised or matrix-free), warp-field update, energy.
+//
+// Reference: DenseDepthJacobianResidual.cu:24-104, NodeGraphSmoothHandler.cu:10-43,
+// DensityForegroundJacobianResidual.cu:93-142 with density_map_jacobian.cuh:12-79,
+// SparseCorrespondenceHandler.cu:202-220, PreconditionerBlocked.cu:172-284,
+// JtDotResidualIndexed.cu:116-224, BlockDiagonalPreconditionerInverse.cu:7-41,
+// JtJMaterializer.cu:270-365, BlockPCG.cuh:65-181,317-335,
+// ApplyJacobianDot.cu:127-198, ApplyJacobianTransposeDot.cu:29-155,
+// SolverIterationData.cu:9-57, ResidualEvaluator.cu:71-142.
+//
+// Accumulation: every per-node and per-pair sum is a warp-shuffle reduction
+// of lane partials; global reductions (dot products, energy) use per-CTA
+// partials summed in fixed order by the last CTA. No floating-point atomics,
+// so every result is reproducible run to run.
+#include <type_traits>
+
+#include "kernels_common.cuh"
+
+namespace mvdr {
+
+// ------------------------------------------------------- term evaluation --
+
+__global__ void __launch_bounds__(256) eval_terms_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (bad_inputs(I)) return;
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t Td = off.o[0];
+    const uint32_t T = off.o[4];
+    const float clip = 64.f * I.node_radius * I.node_radius;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        uint32_t k;
+        const TermType ty = off.typed(t, k);
+        if (ty == kDense) {
+            // computeDenseDepthJacobianKernel (DenseDepthJacobianResidual.cu:24-104)
+            const float4 cv = I.dense_cv[k], cn = I.dense_cn[k];
+            const uint32_t v = __float_as_uint(cv.w);
+            const ViewDesc& V = I.views[v];
+            const M34 se3 = dq_se3(blend_dq(I.se3, I.dense_knn[k], I.dense_w[k]));
+            const float3 wv = apply3(se3, mk3(cv.x, cv.y, cv.z));
+            const float3 wn = rot3(se3, mk3(cn.x, cn.y, cn.z));
+            const float3 vc = apply3(V.init_inv, apply3(V.w2c, wv));
+            const float3 nc = rot3(V.init_inv, rot3(V.w2c, wn));
+            const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
+            const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
+            float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
+            if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height) {
+                const size_t p = (size_t)w * V.pitch + u;
+                const float4 dv4 = V.obs_v[p], dn4 = V.obs_n[p];
+                const float3 dv = mk3(dv4.x, dv4.y, dv4.z), dn = mk3(dn4.x, dn4.y, dn4.z);
+                bool valid = true;
+                if (fabsf(dv4.x) < 1e-3f && fabsf(dv4.y) < 1e-3f && fabsf(dv4.z) < 1e-3f) valid = false;
+                if (dot3(dn, nc) < 0.7f) valid = false;
+                const float3 df = sub3(dv, vc);
+                if (dot3(df, df) > 0.075f * 0.075f) valid = false;
+                if (valid) {
+                    const float r = dot3(dn, sub3(vc, dv));
+                    const float3 tr = rotT3(V.w2c, rot3(V.init, dn));
+                    const float3 ro = cross3(wv, tr);
+                    o0 = make_float4(ro.x, ro.y, ro.z, tr.x);
+                    o1 = make_float4(tr.y, tr.z, r, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+                }
+            }
+            I.term_jr[2 * (size_t)k] = o0;
+            I.term_jr[2 * (size_t)k + 1] = o1;
+        } else if (ty == kSmooth) {
+            // forwardWarpSmootherNodeKernel (NodeGraphSmoothHandler.cu:10-43)
+            const ushort2 e = I.graph[k];
+            const float4 xi = I.nodes[e.x], xj = I.nodes[e.y];
+            const M34 Ti = dq_se3(load_dq(I.se3, e.x)), Tj = dq_se3(load_dq(I.se3, e.y));
+            const float3 a = apply3(Ti, mk3(xj.x, xj.y, xj.z)), b = apply3(Tj, mk3(xj.x, xj.y, xj.z));
+            const float3 dd = mk3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+            const float valid = dot3(dd, dd) > clip ? 0.f : 1.f;
+            I.smooth[2 * (size_t)k] = make_float4(a.x, a.y, a.z, b.x);
+            I.smooth[2 * (size_t)k + 1] = make_float4(b.y, b.z, valid, 0.f);
+        } else if (ty == kForeground) {
+            // computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual;
+            // the canonical vertex is taken to frame 0 first, as the dense term does
+            const float4 cv = I.fg_cv[k];
+            const uint32_t v = __float_as_uint(cv.w);
+            const ViewDesc& V = I.views[v];
+            const M34 se3 = dq_se3(blend_dq(I.se3, I.fg_knn[k], I.fg_w[k]));
+            const float3 wv = apply3(se3, mk3(cv.x, cv.y, cv.z));
+            const float3 vc = apply3(V.init_inv, apply3(V.w2c, wv));
+            const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
+            const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
+            float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
+            if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height && V.fg != nullptr) {
+                const size_t p = (size_t)w * V.pitch + u;
+                const float img = V.fg[p];
+                const float2 gr = V.fg_grad[p];
+                float3 g;
+                g.x = gr.x * V.fx / vc.z;
+                g.y = gr.y * V.fy / vc.z;
+                g.z = -1.0f / (vc.z * vc.z) * (V.fx * vc.x * gr.x + V.fy * vc.y * gr.y);
+                g = rotT3(V.w2c, rot3(V.init, g));
+                o0 = make_float4(-g.y * wv.z + g.z * wv.y, g.x * wv.z - g.z * wv.x, -g.x * wv.y + g.y * wv.x, g.x);
+                o1 = make_float4(g.y, g.z, img - 0.0f, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+            }
+            I.term_jr[2 * (size_t)(Td + k)] = o0;
+            I.term_jr[2 * (size_t)(Td + k) + 1] = o1;
+        } else if (ty == kFeature || ty == kCross) {
+            // forwardWarpFeatureVertexKernel (SparseCorrespondenceHandler.cu:202-220)
+            const bool f = ty == kFeature;
+            const float4 ref = f ? I.feat_ref[k] : I.cross_ref[k];
+            const M34 se3 = dq_se3(blend_dq(I.se3, f ? I.feat_knn[k] : I.cross_knn[k], f ? I.feat_w[k] : I.cross_w[k]));
+            const float3 wv = apply3(se3, mk3(ref.x, ref.y, ref.z));
+            I.warped[f ? k : I.Tp + k] = make_float4(wv.x, wv.y, wv.z, 1.0f);
+        }
+    }
+}
+
+// --------------------------------------------- per-term Jacobian rows -----
+// The weighted Jacobian rows that term t contributes to node `node`:
+// J[c][0..5] (rotation, translation), residual r[c]; returns the channel count
+// (0 when the term is invalid) and sets lam2 and the node's skinning weight.
+struct TermRows {
+    float J[3][6];
+    float r[3];
+    float lam2;
+    float w;
+};
+
+__device__ inline void skew_rows(float3 p, float sg, float hw[3], TermRows& o) {
+    // rows of [p]x^T (geometry_icp_jacobian.cuh:323-343, 91-120)
+    o.J[0][0] = 0.f;           o.J[0][1] = sg * hw[0] * p.z;  o.J[0][2] = -sg * hw[0] * p.y;
+    o.J[1][0] = -sg * hw[1] * p.z; o.J[1][1] = 0.f;           o.J[1][2] = sg * hw[1] * p.x;
+    o.J[2][0] = sg * hw[2] * p.y;  o.J[2][1] = -sg * hw[2] * p.x; o.J[2][2] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o.J[c][3 + i] = (c == i) ? sg * hw[c] : 0.f;
+}
+
+__device__ inline int term_rows(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
+                                uint32_t node, TermRows& o) {
+    uint32_t k;
+    const TermType ty = off.typed(t, k);
+    switch (ty) {
+        case kDense:
+        case kForeground: {
+            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+            const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+            o.J[0][0] = a.x; o.J[0][1] = a.y; o.J[0][2] = a.z; o.J[0][3] = a.w; o.J[0][4] = b.x; o.J[0][5] = b.y;
+            o.r[0] = b.z;
+            o.lam2 = ty == kDense ? 1.0f : lam.foreground * lam.foreground;
+            o.w = weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+            return 1;
+        }
+        case kSmooth: {
+            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            if (b.z == 0.f) return 0;
+            const bool is_i = node == I.graph[k].x;
+            const float3 ti = mk3(a.x, a.y, a.z), tj = mk3(a.w, b.x, b.y);
+            float one[3] = {1.f, 1.f, 1.f};
+            skew_rows(is_i ? ti : tj, is_i ? 1.f : -1.f, one, o);
+            o.r[0] = ti.x - tj.x; o.r[1] = ti.y - tj.y; o.r[2] = ti.z - tj.z;
+            o.lam2 = lam.smooth * lam.smooth;
+            o.w = 1.f;
+            return 3;
+        }
+        case kFeature:
+        case kCross: {
+            const bool f = ty == kFeature;
+            const float4 wv = I.warped[f ? k : I.Tp + k];
+            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+            float hw[3] = {huber_weight(raw[0]), huber_weight(raw[1]), huber_weight(raw[2])};
+            skew_rows(mk3(wv.x, wv.y, wv.z), 1.f, hw, o);
+            o.r[0] = hw[0] * raw[0]; o.r[1] = hw[1] * raw[1]; o.r[2] = hw[2] * raw[2];
+            o.lam2 = f ? lam.feature * lam.feature : lam.cross_view * lam.cross_view;
+            o.w = weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+            return 3;
+        }
+        default: return 0;
+    }
+}
+
+// ------------------------------------------ diagonal blocks, Jt r, M^-1 ----
+
+__device__ constexpr int upper_index(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }
+
+// DenseGaussian<6>::Inverse with partial pivoting (DenseGaussian.h:55-125)
+__device__ inline void gauss_jordan6(const float* Din, float* out) {
+    float m[36];
+#pragma unroll
+    for (int i = 0; i < 36; ++i) m[i] = Din[i];  // column-major, symmetric input
+    int perm[6] = {0, 1, 2, 3, 4, 5}, reloc[6];
+    for (int i = 0; i < 6; ++i) {
+        int piv = i;
+        float pv = fabsf(m[i + 6 * i]);
+        for (int j = i + 1; j < 6; ++j)
+            if (pv < fabsf(m[j + 6 * i])) { pv = fabsf(m[j + 6 * i]); piv = j; }
+        for (int k = 0; k < 6; ++k) { const float tmp = m[i + 6 * k]; m[i + 6 * k] = m[piv + 6 * k]; m[piv + 6 * k] = tmp; }
+        { const int tp = perm[i]; perm[i] = perm[piv]; perm[piv] = tp; }
+        reloc[i] = perm[i];
+        const float inv = 1.0f / m[i + 6 * i];
+        for (int k = 0; k < 6; ++k) m[i + 6 * k] *= inv;
+        m[i + 6 * i] = inv;
+        for (int r = 0; r < 6; ++r) {
+            if (r == i) continue;
+            const float a = m[r + 6 * i];
+            for (int k = 0; k < 6; ++k) m[r + 6 * k] -= a * m[i + 6 * k];
+            m[r + 6 * i] = -a * m[i + 6 * i];
+        }
+    }
+    for (int j = 0; j < 6; ++j)
+        for (int i = 0; i < 6; ++i) out[6 * reloc[j] + i] = m[i + 6 * j];
+}
+
+// 6x6 Cholesky in double; packed lower triangle L[i(i+1)/2 + j], j <= i
+__device__ inline void cholesky6(const float* A, double* L) {
+    for (int j = 0; j < 6; ++j) {
+        double s = A[6 * j + j];
+        for (int k = 0; k < j; ++k) s -= L[j * (j + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+        const double ljj = sqrt(s);
+        L[j * (j + 1) / 2 + j] = ljj;
+        for (int i = j + 1; i < 6; ++i) {
+            double t = A[6 * i + j];
+            for (int k = 0; k < j; ++k) t -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+            L[i * (i + 1) / 2 + j] = t / ljj;
+        }
+    }
+}
+
+__device__ inline void cholesky6_solve(const double* L, const double* b, double* x) {
+    double y[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double t = b[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) t -= L[i * (i + 1) / 2 + k] * y[k];
+        y[i] = t / L[i * (i + 1) / 2 + i];
+    }
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+        double t = y[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; ++k) t -= L[k * (k + 1) / 2 + i] * x[k];
+        x[i] = t / L[i * (i + 1) / 2 + i];
+    }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs) return;
+    TermOffsets off;
+    off.load(C);
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        float acc[27];
+#pragma unroll
+        for (int i = 0; i < 27; ++i) acc[i] = 0.f;
+        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        for (uint32_t p = b + lane_id(); p < e; p += 32) {
+            TermRows tr;
+            const int ch = term_rows(I, off, lam, I.n2t_index[p], node, tr);
+            const float sd = tr.lam2 * tr.w * tr.w;
+            const float sb = tr.lam2 * tr.w;
+            for (int c = 0; c < ch; ++c) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+#pragma unroll
+                    for (int j = i; j < 6; ++j) acc[upper_index(i, j)] += sd * tr.J[c][i] * tr.J[c][j];
+                    acc[21 + i] -= sb * tr.J[c][i] * tr.r[c];
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 27; ++i) acc[i] = warp_sum(acc[i]);
+        float D[36];
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int j = 0; j < 6; ++j) D[6 * i + j] = acc[i <= j ? upper_index(i, j) : upper_index(j, i)];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) D[7 * i] += 1e-2f;  // PreconditionerBlocked.cu:272-275
+        const uint32_t lane = lane_id();
+        // diagonal block: the parity copy and the block of the BSR row
+        float* bsr_blk = I.bsr + 36 * (size_t)(I.blkrow_offset[node] + node);
+        for (uint32_t i = lane; i < 36; i += 32) {
+            float v = 0.f;
+#pragma unroll
+            for (int q = 0; q < 36; ++q) v = (q == (int)i) ? D[q] : v;
+            I.diag[36 * (size_t)node + i] = v;
+            bsr_blk[i] = v;
+        }
+        if (lane < 6) {
+            float v = 0.f;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v = (q == (int)lane) ? acc[21 + q] : v;
+            I.jtr[6 * (size_t)node + lane] = v;
+        }
+        if (lane == 0) {
+            if (MIXED) {
+                double L[21];
+                cholesky6(D, L);
+#pragma unroll
+                for (int i = 0; i < 21; ++i) I.chol[21 * (size_t)node + i] = L[i];
+            } else {
+                float Mi[36];
+                gauss_jordan6(D, Mi);
+#pragma unroll
+                for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
+            }
+        }
+    }
+}
+
+// --------------------------------------------------- off-diagonal blocks --
+// warp per unordered pair (i < j): A_ij = sum_t lam^2 w_i w_j J_i J_j^T is
+// written to row i and its transpose to row j (the reference computes both
+// orderings separately, JtJMaterializer.cu:270-365)
+__global__ void __launch_bounds__(256) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2) return;
+    TermOffsets off;
+    off.load(C);
+    const uint32_t P = C->half_pairs;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t h = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < P; h += warps) {
+        const uint32_t key = I.half_key[h];
+        const uint32_t ni = key / I.enc, nj = key % I.enc;
+        const uint2 rg = I.half_range[h];
+        float acc[36];
+#pragma unroll
+        for (int i = 0; i < 36; ++i) acc[i] = 0.f;
+        for (uint32_t p = rg.x + lane_id(); p < rg.y; p += 32) {
+            const uint32_t t = I.np_index[p];
+            TermRows a, b;
+            const int ch = term_rows(I, off, lam, t, ni, a);
+            if (ch == 0) continue;
+            term_rows(I, off, lam, t, nj, b);
+            const float s = a.lam2 * a.w * b.w;
+            for (int c = 0; c < ch; ++c) {
+#pragma unroll
+                for (int r = 0; r < 6; ++r)
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) acc[6 * r + q] += s * a.J[c][r] * b.J[c][q];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 36; ++i) acc[i] = warp_sum(acc[i]);
+        const uint32_t up = I.upper_pos[h] + ni + 1;   // BSR block of (i, j)
+        const uint32_t lo = I.lower_pos[h] + nj + 1;   // BSR block of (j, i)
+        for (uint32_t e = lane_id(); e < 36; e += 32) {
+            float v = 0.f, vt = 0.f;
+            const uint32_t r = e / 6, q = e % 6;
+#pragma unroll
+            for (int z = 0; z < 36; ++z) {
+                v = (z == (int)e) ? acc[z] : v;
+                vt = (z == (int)(6 * q + r)) ? acc[z] : vt;
+            }
+            I.bsr[36 * (size_t)up + e] = v;
+            I.bsr[36 * (size_t)lo + e] = vt;
+        }
+    }
+}
+
+// ----------------------------------------------------------- reductions ---
+// Last-CTA reduction: every CTA of instance blockIdx.y stores a partial, the
+// last CTA to arrive sums them in index order. Returns true in that CTA.
+template <class T>
+__device__ inline bool block_partial_and_last(const InstDesc& I, T v, int ticket, T* total) {
+    __shared__ T ws[32];
+    __shared__ bool last;
+    v = warp_sum(v);
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T s = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += ws[w];
+        I.partials[blockIdx.x] = (double)s;
+        __threadfence();
+        const uint32_t prev = atomicAdd(&I.counts->reduce_ticket[ticket], 1u);
+        last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        T s = 0;
+        const volatile double* pp = I.partials;
+        for (uint32_t c = 0; c < gridDim.x; ++c) s += (T)pp[c];
+        *total = s;
+        I.counts->reduce_ticket[ticket] = 0;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------- PCG -----
+// Scalars per instance (double storage): [0] delta = r.s, [1] alpha,
+// [2] beta, [3] d.q. In FP32 mode they are computed in float.
+
+// blockPCGZeroInitKernel (BlockPCG.cuh:65-111): r = b, s = M^-1 b, x = 0,
+// delta = r.s; the first direction is d = s (beta = 0)
+template <bool MIXED>
+__global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    using T = typename std::conditional<MIXED, double, float>::type;
+    T part = 0;
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
+        float bv[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) bv[i] = I.jtr[6 * (size_t)node + i];
+        float sv[6];
+        if (MIXED) {
+            double bd[6], xd[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) bd[i] = bv[i];
+            cholesky6_solve(I.chol + 21 * (size_t)node, bd, xd);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) sv[i] = (float)xd[i];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                float a = 0.f;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) a += I.minv[36 * (size_t)node + 6 * j + i] * bv[i];
+                sv[j] = a;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const size_t e = 6 * (size_t)node + i;
+            I.r[e] = bv[i];
+            I.s[e] = sv[i];
+            I.d1[e] = 0.f;
+            I.x[e] = 0.f;
+            part += (T)bv[i] * (T)sv[i];
+        }
+    }
+    T tot;
+    if (block_partial_and_last<T>(I, part, 0, &tot) && threadIdx.x == 0) {
+        I.scalars[0] = (double)tot;
+        I.scalars[2] = 0.0;
+    }
+}
+
+// q = A d with d = s + beta d_prev formed on the fly (BlockPCG.cuh:167-181 fused
+// into the SpMV of the next iteration); d.q partial; alpha = delta / d.q.
+// Six threads per block row (one per scalar row), row-major 6x6 blocks.
+template <bool MIXED>
+__global__ void __launch_bounds__(192) pcg_spmv_kernel(const InstDesc* insts, int parity) {
+    const InstDesc& I = insts[blockIdx.y];
+    using T = typename std::conditional<MIXED, double, float>::type;
+    const float* dprev = parity ? I.d0 : I.d1;
+    float* dcur = parity ? I.d1 : I.d0;
+    const float beta = (float)I.scalars[2];
+    const uint32_t mask = I.enc - 1;
+    T part = 0;
+    const uint32_t rows_per_cta = blockDim.x / 6;
+    for (uint32_t base = blockIdx.x * rows_per_cta; base < I.N; base += gridDim.x * rows_per_cta) {
+        const uint32_t br = base + threadIdx.x / 6;
+        const uint32_t r = threadIdx.x % 6;
+        if (threadIdx.x < rows_per_cta * 6 && br < I.N) {
+            const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
+            const float* blk = I.bsr + 36 * (size_t)(so + br) + 6 * r;
+            float acc = 0.f;
+            // diagonal block
+            {
+                const float* xs = I.s + 6 * (size_t)br;
+                const float* xp = dprev + 6 * (size_t)br;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc += blk[k] * (xs[k] + beta * xp[k]);
+            }
+            blk += 36;
+            for (uint32_t s = so; s < se; ++s, blk += 36) {
+                const uint32_t col = I.sym_key[s] & mask;
+                const float* xs = I.s + 6 * (size_t)col;
+                const float* xp = dprev + 6 * (size_t)col;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc += blk[k] * (xs[k] + beta * xp[k]);
+            }
+            const size_t e = 6 * (size_t)br + r;
+            const float dv = I.s[e] + beta * dprev[e];
+            dcur[e] = dv;
+            I.q[e] = acc;
+            part += (T)dv * (T)acc;
+        }
+    }
+    T tot;
+    if (block_partial_and_last<T>(I, part, 1, &tot) && threadIdx.x == 0) {
+        I.scalars[3] = (double)tot;
+        if (MIXED) I.scalars[1] = I.scalars[0] / (double)tot;
+        else I.scalars[1] = (double)((float)I.scalars[0] / (float)tot);
+    }
+}
+
+// blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): x += alpha d, r -= alpha q,
+// s = M^-1 r, delta_new = r.s, beta = delta_new / delta
+template <bool MIXED>
+__global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity) {
+    const InstDesc& I = insts[blockIdx.y];
+    using T = typename std::conditional<MIXED, double, float>::type;
+    const float* d = parity ? I.d1 : I.d0;
+    const float alpha = (float)I.scalars[1];
+    T part = 0;
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
+        float rv[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const size_t e = 6 * (size_t)node + i;
+            I.x[e] += alpha * d[e];
+            rv[i] = I.r[e] - alpha * I.q[e];
+            I.r[e] = rv[i];
+        }
+        float sv[6];
+        if (MIXED) {
+            double bd[6], xd[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) bd[i] = rv[i];
+            cholesky6_solve(I.chol + 21 * (size_t)node, bd, xd);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) sv[i] = (float)xd[i];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                float a = 0.f;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) a += I.minv[36 * (size_t)node + 6 * j + i] * rv[i];
+                sv[j] = a;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            I.s[6 * (size_t)node + i] = sv[i];
+            part += (T)rv[i] * (T)sv[i];
+        }
+    }
+    T tot;
+    if (block_partial_and_last<T>(I, part, 2, &tot) && threadIdx.x == 0) {
+        if (MIXED) {
+            I.scalars[2] = (double)tot / I.scalars[0];
+        } else {
+            I.scalars[2] = (double)((float)tot / (float)I.scalars[0]);
+        }
+        I.scalars[0] = (double)tot;
+    }
+}
+
+// ------------------------------------------------------ matrix-free JtJ ---
+// J.p per term (ApplyJacobianDot.cu:127-198): jp[3t + c] for each channel,
+// with p = s + beta * d_prev formed on the fly when `fused` is set
+__global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
+                                                      mvdr_penalty lam) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (bad_inputs(I)) return;
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t T = off.o[4];
+    const float beta = fused ? (float)I.scalars[2] : 0.f;
+    const float* s = fused ? I.s : xin;
+    const float* dp = parity ? I.d0 : I.d1;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        uint32_t k;
+        const TermType ty = off.typed(t, k);
+        const ushort4 nn = term_nodes(I, ty, k);
+        const unsigned short nodes[4] = {nn.x, nn.y, nn.z, nn.w};
+        const int m = ty == kSmooth ? 2 : 4;
+        float out[3] = {0.f, 0.f, 0.f};
+        for (int q = 0; q < m; ++q) {
+            const uint32_t node = nodes[q];
+            if (node >= I.N) continue;
+            TermRows tr;
+            const int ch = term_rows(I, off, lam, t, node, tr);
+            float p[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const size_t e = 6 * (size_t)node + i;
+                p[i] = fused ? s[e] + beta * dp[e] : s[e];
+            }
+            for (int c = 0; c < ch; ++c) {
+                float a = 0.f;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) a += tr.J[c][i] * p[i];
+                out[c] += tr.w * a;
+            }
+        }
+        I.jp[3 * (size_t)t] = out[0];
+        I.jp[3 * (size_t)t + 1] = out[1];
+        I.jp[3 * (size_t)t + 2] = out[2];
+    }
+}
+
+// Jt.y per node (ApplyJacobianTransposeDot.cu:29-155) plus the 1e-2 damping;
+// warp per node. With `pcg` set it also forms this node's direction d, stores
+// q and the d.q partial, like pcg_spmv_kernel.
+template <bool MIXED>
+__global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
+                                                       int parity, mvdr_penalty lam) {
+    const InstDesc& I = insts[blockIdx.y];
+    using T = typename std::conditional<MIXED, double, float>::type;
+    TermOffsets off;
+    off.load(I.counts);
+    const float* dprev = parity ? I.d0 : I.d1;
+    float* dcur = parity ? I.d1 : I.d0;
+    const float beta = pcg ? (float)I.scalars[2] : 0.f;
+    T part = 0;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        for (uint32_t p = b + lane_id(); p < e; p += 32) {
+            const uint32_t t = I.n2t_index[p];
+            TermRows tr;
+            const int ch = term_rows(I, off, lam, t, node, tr);
+            const float sc = tr.lam2 * tr.w;
+            for (int c = 0; c < ch; ++c) {
+                const float y = I.jp[3 * (size_t)t + c];
+#pragma unroll
+                for (int i = 0; i < 6; ++i) acc[i] += sc * tr.J[c][i] * y;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) acc[i] = warp_sum(acc[i]);
+        const uint32_t lane = lane_id();
+        if (lane < 6) {
+            float a = 0.f;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a = (q == (int)lane) ? acc[q] : a;
+            const size_t el = 6 * (size_t)node + lane;
+            float dv;
+            if (pcg) dv = I.s[el] + beta * dprev[el];
+            else dv = xin[el];
+            const float qv = a + 1e-2f * dv;
+            if (pcg) {
+                dcur[el] = dv;
+                I.q[el] = qv;
+                part += (T)dv * (T)qv;
+            } else {
+                yout[el] = qv;
+            }
+        }
+    }
+    if (pcg) {
+        T tot;
+        if (block_partial_and_last<T>(I, part, 1, &tot) && threadIdx.x == 0) {
+            I.scalars[3] = (double)tot;
+            if (MIXED) I.scalars[1] = I.scalars[0] / (double)tot;
+            else I.scalars[1] = (double)((float)I.scalars[0] / (float)tot);
+        }
+    }
+}
+
+// y = A x with the materialised operator (no PCG side effects)
+__global__ void __launch_bounds__(192) bsr_apply_kernel(const InstDesc* insts, const float* xin, float* yout) {
+    const InstDesc& I = insts[blockIdx.y];
+    const uint32_t mask = I.enc - 1;
+    const uint32_t rows_per_cta = blockDim.x / 6;
+    for (uint32_t base = blockIdx.x * rows_per_cta; base < I.N; base += gridDim.x * rows_per_cta) {
+        const uint32_t br = base + threadIdx.x / 6;
+        const uint32_t r = threadIdx.x % 6;
+        if (threadIdx.x >= rows_per_cta * 6 || br >= I.N) continue;
+        const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
+        const float* blk = I.bsr + 36 * (size_t)(so + br) + 6 * r;
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc += blk[k] * xin[6 * (size_t)br + k];
+        blk += 36;
+        for (uint32_t s = so; s < se; ++s, blk += 36) {
+            const uint32_t col = I.sym_key[s] & mask;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) acc += blk[k] * xin[6 * (size_t)col + k];
+        }
+        yout[6 * (size_t)br + r] = acc;
+    }
+}
+
+// ----------------------------------------------------------- update -------
+// applyWarpFieldUpdateKernel (SolverIterationData.cu:9-57)
+__global__ void __launch_bounds__(128) update_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
+        float tw[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) tw[i] = I.x[6 * (size_t)node + i];
+        M34 se3;
+        const float3 w = mk3(tw[0], tw[1], tw[2]);
+        if (fabsf(w.x) + fabsf(w.y) + fabsf(w.z) < 1e-4f) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) se3.r[i] = (i % 4 == 0) ? 1.f : 0.f;
+        } else {
+            const float angle = sqrtf(dot3(w, w));
+            const float3 ax = mul3(1.0f / angle, w);
+            const float c = cosf(angle), s = sinf(angle), t = 1.0f - c;
+            se3.r[0] = t * ax.x * ax.x + c;
+            se3.r[1] = t * ax.x * ax.y - ax.z * s;
+            se3.r[2] = t * ax.x * ax.z + ax.y * s;
+            se3.r[3] = t * ax.x * ax.y + ax.z * s;
+            se3.r[4] = t * ax.y * ax.y + c;
+            se3.r[5] = t * ax.y * ax.z - ax.x * s;
+            se3.r[6] = t * ax.x * ax.z - ax.y * s;
+            se3.r[7] = t * ax.y * ax.z + ax.x * s;
+            se3.r[8] = t * ax.z * ax.z + c;
+        }
+        se3.t[0] = tw[3]; se3.t[1] = tw[4]; se3.t[2] = tw[5];
+        const M34 p = dq_to_mat34(load_dq(I.se3, node));
+        M34 n;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                n.r[3 * r + c] = se3.r[3 * r] * p.r[c] + se3.r[3 * r + 1] * p.r[3 + c] + se3.r[3 * r + 2] * p.r[6 + c];
+            n.t[r] = se3.r[3 * r] * p.t[0] + se3.r[3 * r + 1] * p.t[1] + se3.r[3 * r + 2] * p.t[2] + se3.t[r];
+        }
+        // DualQuaternion(mat34) (DualQuaternion.h:123-130) via Quaternion(mat33) (Quaternion.h:46-77)
+        const float* m = n.r;
+        float4 q;
+        const float tr = m[0] + m[4] + m[8];
+        if (tr > 0) {
+            const float s = sqrtf(tr + 1.0f) * 2;
+            q.w = s * 0.25f; q.x = (m[7] - m[5]) / s; q.y = (m[2] - m[6]) / s; q.z = (m[3] - m[1]) / s;
+        } else if ((m[0] > m[4]) && (m[0] > m[8])) {
+            const float s = sqrtf(1.0f + m[0] - m[4] - m[8]) * 2;
+            q.w = (m[7] - m[5]) / s; q.x = 0.25f * s; q.y = (m[1] + m[3]) / s; q.z = (m[2] + m[6]) / s;
+        } else if (m[4] > m[8]) {
+            const float s = sqrtf(1.0f + m[4] - m[0] - m[8]) * 2;
+            q.w = (m[2] - m[6]) / s; q.x = (m[1] + m[3]) / s; q.y = 0.25f * s; q.z = (m[5] + m[7]) / s;
+        } else {
+            const float s = sqrtf(1.0f + m[8] - m[0] - m[4]) * 2;
+            q.w = (m[3] - m[1]) / s; q.x = (m[2] + m[6]) / s; q.y = (m[5] + m[7]) / s; q.z = 0.25f * s;
+        }
+        const float4 tq = make_float4(0.5f * n.t[0], 0.5f * n.t[1], 0.5f * n.t[2], 0.f);
+        float4 q1;  // tq * q
+        q1.w = tq.w * q.w - tq.x * q.x - tq.y * q.y - tq.z * q.z;
+        q1.x = tq.w * q.x + tq.x * q.w + tq.y * q.z - tq.z * q.y;
+        q1.y = tq.w * q.y - tq.x * q.z + tq.y * q.w + tq.z * q.x;
+        q1.z = tq.w * q.z + tq.x * q.y - tq.y * q.x + tq.z * q.w;
+        float4* out = reinterpret_cast<float4*>(I.se3 + node);
+        out[0] = q;
+        out[1] = q1;
+    }
+}
+
+// ------------------------------------------------------------- energy -----
+// computeTermResidualKernel (ResidualEvaluator.cu:71-142): sum (lambda r)^2
+__global__ void __launch_bounds__(256) energy_kernel(const InstDesc* insts, mvdr_penalty lam, uint32_t slot) {
+    const InstDesc& I = insts[blockIdx.y];
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t T = off.o[4];
+    double part = 0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        uint32_t k;
+        const TermType ty = off.typed(t, k);
+        if (ty == kDense || ty == kForeground) {
+            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+            const float l = ty == kDense ? 1.0f : lam.foreground;
+            const float v = l * I.term_jr[2 * (size_t)idx + 1].z;
+            part += (double)v * v;
+        } else if (ty == kSmooth) {
+            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            if (b.z != 0.f) {
+                const float r0 = lam.smooth * (a.x - a.w), r1 = lam.smooth * (a.y - b.x), r2 = lam.smooth * (a.z - b.y);
+                part += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+            }
+        } else if (ty == kFeature || ty == kCross) {
+            const bool f = ty == kFeature;
+            const float4 wv = I.warped[f ? k : I.Tp + k];
+            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const float l = f ? lam.feature : lam.cross_view;
+            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float v = l * (huber_weight(raw[c]) * raw[c]);
+                part += (double)v * v;
+            }
+        }
+    }
+    double tot;
+    if (block_partial_and_last<double>(I, part, 3, &tot) && threadIdx.x == 0) I.energy[slot] = tot;
+}
+
+// --------------------------------------------------------- exports -------
+// symmetric-key order, reference layout blk[6k + r] = A(r, k)
+__global__ void export_offdiag_kernel(const InstDesc* insts, uint32_t inst, float* out) {
+    const InstDesc& I = insts[inst];
+    const uint32_t P2 = 2 * I.counts->half_pairs;
+    const uint32_t mask = I.enc - 1;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 36 * P2; i += gridDim.x * blockDim.x) {
+        const uint32_t s = i / 36, e = i % 36;
+        const uint32_t row = I.sym_key[s] / I.enc;
+        (void)mask;
+        const uint32_t k = e / 6, r = e % 6;
+        out[i] = I.bsr[36 * (size_t)(s + row + 1) + 6 * r + k];
+    }
+}
+
+__global__ void export_preconditioner_kernel(const InstDesc* insts, uint32_t inst, float* out, int mixed) {
+    const InstDesc& I = insts[inst];
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
+        if (!mixed) {
+            for (int i = 0; i < 36; ++i) out[36 * (size_t)node + i] = I.minv[36 * (size_t)node + i];
+            continue;
+        }
+        for (int c = 0; c < 6; ++c) {
+            double e[6] = {0, 0, 0, 0, 0, 0}, x[6];
+            e[c] = 1.0;
+            cholesky6_solve(I.chol + 21 * (size_t)node, e, x);
+            for (int r = 0; r < 6; ++r) out[36 * (size_t)node + 6 * r + c] = (float)x[r];
+        }
+    }
+}
+
+// ------------------------------------------------------------- launch -----
+
+static inline dim3 grid2(uint32_t x, uint32_t B) { return dim3(x ? x : 1, B); }
+
+cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
+    const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
+    MVDR_LAUNCH(eval_terms_kernel, grid2(g, lc.B), 256, 0, st, d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, bool materialize,
+                            cudaStream_t st) {
+    const uint32_t gn = (lc.max_nodes + 7) / 8;
+    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 256, 0, st, d, lam);
+    else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 256, 0, st, d, lam);
+    if (materialize) {
+        const uint32_t gp = min((lc.cap_pairs + 7) / 8, (uint32_t)lc.sm_count * 16);
+        MVDR_LAUNCH(offdiag_kernel, grid2(gp, lc.B), 256, 0, st, d, lam);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t slot, cudaStream_t st) {
+    const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 4);
+    MVDR_LAUNCH(energy_kernel, grid2(g, lc.B), 256, 0, st, d, lam, slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
+    const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
+    const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
+    const uint32_t gspmv = min((lc.max_nodes + 31) / 32, (uint32_t)lc.sm_count * 8);
+    const uint32_t gwarp = (lc.max_nodes + 7) / 8;
+    const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
+    if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d);
+    else MVDR_LAUNCH(pcg_init_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d);
+    for (uint32_t it = 0; it < iters; ++it) {
+        const int parity = (int)(it & 1u);
+        if (lc.mode == MVDR_MODE_MATRIX_FREE) {
+            // J.(s + beta d_prev) per term, then Jt per node (+ damping, d, q, d.q)
+            MVDR_LAUNCH(apply_j_kernel, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
+            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
+            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
+        } else {
+            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gspmv, lc.B), 192, 0, st, d, parity);
+            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gspmv, lc.B), 192, 0, st, d, parity);
+        }
+        if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity);
+        else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, int stage, cudaStream_t st) {
+    const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
+    const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
+    const uint32_t gspmv = min((lc.max_nodes + 31) / 32, (uint32_t)lc.sm_count * 8);
+    const uint32_t gn = (lc.max_nodes + 7) / 8;
+    switch (stage) {
+        case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
+        case MVDR_STAGE_DIAG:
+            if (mixed) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 256, 0, st, d, lam);
+            else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 256, 0, st, d, lam);
+            break;
+        case MVDR_STAGE_OFFDIAG: {
+            const uint32_t gp = min((lc.cap_pairs + 7) / 8, (uint32_t)lc.sm_count * 16);
+            MVDR_LAUNCH(offdiag_kernel, grid2(gp, lc.B), 256, 0, st, d, lam);
+            break;
+        }
+        case MVDR_STAGE_SPMV:
+            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gspmv, lc.B), 192, 0, st, d, 0);
+            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gspmv, lc.B), 192, 0, st, d, 0);
+            break;
+        case MVDR_STAGE_PCG_UPDATE:
+            if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0);
+            else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, 0);
+            break;
+        case MVDR_STAGE_UPDATE: return launch_update(lc, d, st);
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
+    const uint32_t g = (lc.max_nodes + 127) / 128;
+    MVDR_LAUNCH(update_kernel, grid2(g, lc.B), 128, 0, st, d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_jtj(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, const float* x, float* y,
+                             cudaStream_t st) {
+    // single instance view: d points at the instance's descriptor, B = 1
+    if (lc.mode == MVDR_MODE_MATRIX_FREE) {
+        const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
+        MVDR_LAUNCH(apply_j_kernel, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
+        MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
+    } else {
+        MVDR_LAUNCH(bsr_apply_kernel, grid2((lc.max_nodes + 31) / 32, 1), 192, 0, st, d, x, y);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_offdiag(const LaunchCfg& lc, InstDesc* d, uint32_t inst, float* out, cudaStream_t st) {
+    MVDR_LAUNCH(export_offdiag_kernel, dim3(lc.sm_count * 4), 256, 0, st, d, inst, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_preconditioner(const LaunchCfg& lc, InstDesc* d, uint32_t inst, float* out,
+                                         cudaStream_t st) {
+    MVDR_LAUNCH(export_preconditioner_kernel, dim3((lc.max_nodes + 127) / 128), 128, 0, st, d, inst, out,
+                lc.precision == MVDR_PRECISION_MIXED ? 1 : 0);
+    return cudaGetLastError();
+}
+
+}  // namespace mvdr

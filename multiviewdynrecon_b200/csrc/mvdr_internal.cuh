@@ -1,0 +1,310 @@
+// Internal declarations of the B200 non-rigid solver: device math, the
+// per-instance descriptor that every kernel reads, and the kernel launchers.
+//
+// Batching: every kernel takes the descriptor array of all instances and uses
+// blockIdx.y as the instance index. Grid sizes come from the capacities fixed
+// at create time, and data-dependent sizes (dense-term count, node pairs, ...)
+// are read from device memory, so a whole solve runs without a host
+// synchronisation and can be captured once as a CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mvdr.h"
+
+namespace mvdr {
+
+constexpr int kWarp = 32;
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+
+// error flag bits (DeviceCounts::error_flags)
+enum : uint32_t {
+    kErrDenseCapacity = 1u << 0,
+    kErrForegroundCapacity = 1u << 1,
+    kErrNode2TermCapacity = 1u << 2,
+    kErrNodePairEntryCapacity = 1u << 3,
+    kErrHalfPairCapacity = 1u << 4,
+    kErrSegmentTooLong = 1u << 5,
+    kErrRowTooLong = 1u << 6,
+    kErrBinBlockCapacity = 1u << 7,
+    kErrNonFinite = 1u << 8,
+    kErrBadNodeIndex = 1u << 9,
+};
+
+// ------------------------------------------------------------- math ----
+
+struct M34 {  // row-major rotation + translation
+    float r[9];
+    float t[3];
+};
+
+__host__ __device__ inline float3 mk3(float x, float y, float z) { return make_float3(x, y, z); }
+__host__ __device__ inline float3 add3(float3 a, float3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ inline float3 sub3(float3 a, float3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ inline float3 mul3(float s, float3 a) { return mk3(s * a.x, s * a.y, s * a.z); }
+__host__ __device__ inline float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ inline float3 cross3(float3 a, float3 b) {
+    return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ inline float3 rot3(const M34& m, float3 v) {
+    return mk3(m.r[0] * v.x + m.r[1] * v.y + m.r[2] * v.z, m.r[3] * v.x + m.r[4] * v.y + m.r[5] * v.z,
+               m.r[6] * v.x + m.r[7] * v.y + m.r[8] * v.z);
+}
+__host__ __device__ inline float3 rotT3(const M34& m, float3 v) {
+    return mk3(m.r[0] * v.x + m.r[3] * v.y + m.r[6] * v.z, m.r[1] * v.x + m.r[4] * v.y + m.r[7] * v.z,
+               m.r[2] * v.x + m.r[5] * v.y + m.r[8] * v.z);
+}
+__host__ __device__ inline float3 apply3(const M34& m, float3 v) {
+    float3 a = rot3(m, v);
+    return mk3(a.x + m.t[0], a.y + m.t[1], a.z + m.t[2]);
+}
+
+// dual quaternion: q0 = (x, y, z, w) real part, q1 dual part
+struct DQ {
+    float4 q0, q1;
+};
+
+__device__ inline DQ load_dq(const DQ* field, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(field + i);
+    DQ d;
+    d.q0 = __ldg(p);
+    d.q1 = __ldg(p + 1);
+    return d;
+}
+
+// averageDualQuaternion (DualQuaternion.h:381-393): linear blend of 4 nodes
+__device__ inline DQ blend_dq(const DQ* field, ushort4 knn, float4 w) {
+    const DQ a = load_dq(field, knn.x), b = load_dq(field, knn.y), c = load_dq(field, knn.z),
+             d = load_dq(field, knn.w);
+    DQ o;
+    o.q0.x = w.x * a.q0.x; o.q0.y = w.x * a.q0.y; o.q0.z = w.x * a.q0.z; o.q0.w = w.x * a.q0.w;
+    o.q1.x = w.x * a.q1.x; o.q1.y = w.x * a.q1.y; o.q1.z = w.x * a.q1.z; o.q1.w = w.x * a.q1.w;
+    o.q0.x += w.y * b.q0.x; o.q0.y += w.y * b.q0.y; o.q0.z += w.y * b.q0.z; o.q0.w += w.y * b.q0.w;
+    o.q1.x += w.y * b.q1.x; o.q1.y += w.y * b.q1.y; o.q1.z += w.y * b.q1.z; o.q1.w += w.y * b.q1.w;
+    o.q0.x += w.z * c.q0.x; o.q0.y += w.z * c.q0.y; o.q0.z += w.z * c.q0.z; o.q0.w += w.z * c.q0.w;
+    o.q1.x += w.z * c.q1.x; o.q1.y += w.z * c.q1.y; o.q1.z += w.z * c.q1.z; o.q1.w += w.z * c.q1.w;
+    o.q0.x += w.w * d.q0.x; o.q0.y += w.w * d.q0.y; o.q0.z += w.w * d.q0.z; o.q0.w += w.w * d.q0.w;
+    o.q1.x += w.w * d.q1.x; o.q1.y += w.w * d.q1.y; o.q1.z += w.w * d.q1.z; o.q1.w += w.w * d.q1.w;
+    return o;
+}
+
+__device__ inline float qdot(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+
+// q1 * conj(q0) * 2, vector part (translation of a unit dual quaternion)
+__device__ inline float3 dq_translation(float4 q0, float4 q1) {
+    const float4 a = make_float4(2.f * q1.x, 2.f * q1.y, 2.f * q1.z, 2.f * q1.w);
+    const float4 b = make_float4(-q0.x, -q0.y, -q0.z, q0.w);
+    // Hamilton product a*b, vector part
+    return mk3(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+               a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w);
+}
+
+__device__ inline void quat_rotation(float4 q, float* r) {
+    r[0] = 1.f - 2.f * q.y * q.y - 2.f * q.z * q.z;
+    r[1] = 2.f * q.x * q.y - 2.f * q.z * q.w;
+    r[2] = 2.f * q.x * q.z + 2.f * q.y * q.w;
+    r[3] = 2.f * q.x * q.y + 2.f * q.z * q.w;
+    r[4] = 1.f - 2.f * q.x * q.x - 2.f * q.z * q.z;
+    r[5] = 2.f * q.y * q.z - 2.f * q.x * q.w;
+    r[6] = 2.f * q.x * q.z - 2.f * q.y * q.w;
+    r[7] = 2.f * q.y * q.z + 2.f * q.x * q.w;
+    r[8] = 1.f - 2.f * q.x * q.x - 2.f * q.y * q.y;
+}
+
+// DualQuaternion::normalize (DualQuaternion.h:281-287)
+__device__ inline DQ dq_normalize(DQ d) {
+    const float inv = rsqrtf(qdot(d.q0, d.q0));
+    d.q0 = make_float4(inv * d.q0.x, inv * d.q0.y, inv * d.q0.z, inv * d.q0.w);
+    d.q1 = make_float4(inv * d.q1.x, inv * d.q1.y, inv * d.q1.z, inv * d.q1.w);
+    const float dd = qdot(d.q0, d.q1);
+    d.q1 = make_float4(d.q1.x - dd * d.q0.x, d.q1.y - dd * d.q0.y, d.q1.z - dd * d.q0.z, d.q1.w - dd * d.q0.w);
+    return d;
+}
+
+// DualQuaternion::se3_matrix (DualQuaternion.h:326-332)
+__device__ inline M34 dq_se3(DQ d) {
+    d = dq_normalize(d);
+    M34 m;
+    quat_rotation(d.q0, m.r);
+    const float3 t = dq_translation(d.q0, d.q1);
+    m.t[0] = t.x; m.t[1] = t.y; m.t[2] = t.z;
+    return m;
+}
+
+// DualQuaternion::operator mat34 (DualQuaternion.h:309-319): normalised, then
+// Quaternion::matrix() which normalises the rotation quaternion once more
+__device__ inline M34 dq_to_mat34(DQ d) {
+    d = dq_normalize(d);
+    float4 q = d.q0;
+    const float inv2 = rsqrtf(qdot(q, q));
+    q = make_float4(inv2 * q.x, inv2 * q.y, inv2 * q.z, inv2 * q.w);
+    M34 m;
+    quat_rotation(q, m.r);
+    const float3 t = dq_translation(d.q0, d.q1);
+    m.t[0] = t.x; m.t[1] = t.y; m.t[2] = t.z;
+    return m;
+}
+
+// ------------------------------------------------------- descriptor ----
+
+struct ViewDesc {
+    const float4* ref_v;
+    const float4* ref_n;
+    const uint32_t* index;
+    const float4* obs_v;
+    const float4* obs_n;
+    const float* fg;
+    const float2* fg_grad;
+    uint32_t pitch;
+    float cx, cy, fx, fy;
+    M34 w2c, init, init_inv;
+};
+
+// device-resident sizes of one instance (written by the index build)
+struct DeviceCounts {
+    uint32_t dense_terms;
+    uint32_t smooth_terms;
+    uint32_t foreground_terms;
+    uint32_t feature_terms;
+    uint32_t cross_terms;
+    uint32_t node2term_entries;
+    uint32_t nodepair_entries;
+    uint32_t half_pairs;
+    uint32_t num_bins;
+    uint32_t binblock_nnz;
+    uint32_t error_flags;
+    uint32_t reserved;
+    uint32_t term_offset[5];  // prefix ends of Dense, Smooth, Foreground, Feature, Cross
+    uint32_t dense_view_count[MVDR_MAX_VIEWS];
+    uint32_t fg_view_count[MVDR_MAX_VIEWS];
+    uint32_t reduce_ticket[4];  // last-block reduction counters
+};
+
+struct InstDesc {
+    // host-known sizes (set_inputs)
+    uint32_t num_views, N, S, E, Tp, Tc;
+    uint32_t width, height;
+    uint32_t enc;         // node-pair key multiplier (4096, or 2^k >= N)
+    uint32_t compat;
+    uint32_t use_fg;
+    float node_radius;
+    ViewDesc views[MVDR_MAX_VIEWS];
+    const ushort4* surfel_knn;
+    const float4* surfel_w;
+    const float4* nodes;
+    const ushort2* graph;
+    const float4* feat_target;
+    const float4* feat_ref;
+    const ushort4* feat_knn;
+    const float4* feat_w;
+    const float4* cross_target;
+    const float4* cross_ref;
+    const ushort4* cross_knn;
+    const float4* cross_w;
+
+    // ---- workspace (solver-owned) ----
+    DeviceCounts* counts;
+    DQ* se3;                // current warp field
+    // compaction: per dense/foreground term
+    uint32_t* chunk_count;  // [num chunk slots]
+    ushort4* dense_pix;     // (x, y, view, 0)
+    ushort4* dense_knn;
+    float4* dense_w;
+    float4* dense_cv;       // canonical vertex in frame 0
+    float4* dense_cn;       // canonical normal in frame 0
+    ushort4* fg_pix;
+    ushort4* fg_knn;
+    float4* fg_w;
+    float4* fg_cv;
+    // node -> term
+    uint32_t* n2t_count;    // [N+1]
+    uint32_t* n2t_offset;   // [N+1]
+    uint32_t* n2t_cursor;   // [N]
+    uint32_t* n2t_index;    // [K1 cap]
+    // node pair -> term
+    uint32_t* row_count;    // [N+1] entries (j, t) with j > i per row
+    uint32_t* row_offset;   // [N+1]
+    uint32_t* np_index;     // [K2 cap]
+    uint32_t* upper_count;  // [N+1]
+    uint32_t* half_offset;  // [N+1]
+    uint32_t* tmp_key;      // [K2 cap] per-row unique pairs before compaction
+    uint32_t* tmp_start;    // [K2 cap]
+    uint32_t* half_key;     // [P cap]
+    uint2* half_range;      // [P cap]
+    uint32_t* lower_count;  // [N+1]
+    uint32_t* lower_cursor; // [N]
+    uint32_t* blkrow_offset;// [N+1]
+    uint32_t* sym_key;      // [2P cap]
+    uint2* sym_range;       // [2P cap]
+    uint32_t* sym_half;     // [2P cap] half pair of each symmetric entry
+    uint32_t* upper_pos;    // [P cap] symmetric position of (i, j)
+    uint32_t* lower_pos;    // [P cap] symmetric position of (j, i)
+    // bin-block CSR structure (reference layout, for checks and the bin-block SpMV)
+    uint32_t* bin_scan;     // [nbins+1]
+    int32_t* bb_rowptr;     // [32 (nbins+1)]
+    int32_t* bb_colptr;     // [bb cap / 6]
+    float* bb_data;         // [bb cap]
+    // per-iteration term data
+    float4* term_jr;        // 2 float4 per dense+fg term: J(6), r, pixel bits
+    float4* smooth;         // 2 float4 per smooth term: Ti_xj(3), Tj_xj(3), valid, 0
+    float4* warped;         // per feature+cross term
+    // assembly
+    float* diag;            // [36N] JtJ diagonal blocks incl. damping
+    float* minv;            // [36N] preconditioner (inverse diagonal), float
+    double* chol;           // [21N] Cholesky factors (mixed precision)
+    float* jtr;             // [6N]
+    float* bsr;             // [(N + 2P cap) * 36] row-major blocks, diagonal first per row
+    // pcg vectors [6N each]
+    float* x;
+    float* r;
+    float* s;
+    float* q;
+    float* d0;
+    float* d1;
+    float* jp;              // matrix-free scratch: J.p per scalar term
+    double* scalars;        // PCG scalars: [0] delta, [1] alpha, [2] beta, [3] dq
+    double* partials;       // per-CTA partial sums
+    double* energy;         // [max GN iterations + 1]
+
+    // capacities
+    uint32_t cap_dense, cap_fg, cap_k1, cap_k2, cap_pairs, cap_seg, cap_row, cap_bb;
+    uint32_t chunks_per_view;
+};
+
+struct LaunchCfg {
+    uint32_t B;            // instances
+    uint32_t max_nodes, max_views, width, height;
+    uint32_t cap_dense, cap_fg, cap_terms, cap_k1, cap_k2, cap_pairs, cap_seg, cap_row, cap_bb;
+    uint32_t max_edges, max_tp, max_tc;
+    uint32_t chunks_per_view;
+    int precision, mode;
+    int sm_count;
+};
+
+// ----------------------------------------------------------- launchers --
+// Each launcher enqueues kernels on `st` for all instances. They return
+// cudaGetLastError() of the last launch.
+void count_launch();
+
+// raise the dynamic shared-memory limit of the segment-sort kernels
+cudaError_t set_index_smem_limits(size_t seg_bytes, size_t row_bytes);
+
+cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
+cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
+cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, bool materialize,
+                            cudaStream_t st);
+cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t slot,
+                          cudaStream_t st);
+cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t iters,
+                       cudaStream_t st);
+cudaError_t launch_update(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
+cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, int stage, cudaStream_t st);
+cudaError_t launch_apply_jtj(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, const float* x,
+                             float* y, cudaStream_t st);
+cudaError_t launch_export_offdiag(const LaunchCfg& lc, InstDesc* d_inst, uint32_t inst, float* out,
+                                  cudaStream_t st);
+cudaError_t launch_export_preconditioner(const LaunchCfg& lc, InstDesc* d_inst, uint32_t inst, float* out,
+                                         cudaStream_t st);
+
+}  // namespace mvdr

@@ -1,0 +1,864 @@
+// Host side of the solver: the NonRigidSolver-shaped batch object, its
+// workspace arena, the Gauss-Newton orchestration (buildSolverIndexStreamed /
+// solverIteration*Streamed, whose bodies are missing from the reference), the
+// CUDA-graph capture of whole solves, and the extern "C" layer of mvdr.h.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kernels_common.cuh"
+
+namespace mvdr {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CU(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e__ = (call);                                                                 \
+        if (e__ != cudaSuccess)                                                                   \
+            return fail(MVDR_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e__));        \
+    } while (0)
+
+// bin-block CSR values for the diagnostic export (diagnostic path only)
+__global__ void export_binblock_fill_kernel(const InstDesc* insts, uint32_t inst, float* out) {
+    // assembleBinBlockCSRKernel (JtJMaterializerBinBlockCSR.cu:8-37)
+    const InstDesc& I = insts[inst];
+    const uint32_t rows = 6 * I.N;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
+        uint32_t off = (uint32_t)I.bb_rowptr[row];
+        const uint32_t br = row / 6, in = row % 6;
+        for (int k = 0; k < 6; ++k, off += 32) out[off] = I.diag[36 * (size_t)br + in + 6 * k];
+        for (uint32_t s = I.blkrow_offset[br]; s < I.blkrow_offset[br + 1]; ++s)
+            for (int k = 0; k < 6; ++k, off += 32) out[off] = I.bsr[36 * (size_t)(s + br + 1) + 6 * in + k];
+    }
+}
+
+struct Arena {
+    char* base = nullptr;
+    size_t off = 0, size = 0;
+    template <class T> T* take(size_t n) {
+        const size_t bytes = ((n * sizeof(T)) + 255) & ~(size_t)255;
+        T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+        off += bytes;
+        return p;
+    }
+};
+
+// per-instance owned device copies of the inputs (mvdr_set_inputs_host)
+struct OwnedInputs {
+    void* mem = nullptr;
+    size_t bytes = 0;
+};
+
+struct Batch {
+    mvdr_config cfg{};
+    LaunchCfg lc{};
+    uint32_t B = 0;
+    uint32_t cap_edges = 0;
+    std::vector<InstDesc> host;
+    InstDesc* d_inst = nullptr;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    size_t per_inst_bytes = 0;
+    std::vector<OwnedInputs> owned;
+    std::vector<uint8_t> has_inputs;
+    uint32_t gn_iter = 0;
+    // graph cache: (gn, pcg) -> exec
+    std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;
+    std::vector<struct SolverView*> views;
+
+    ~Batch();
+};
+
+}  // namespace mvdr
+
+struct mvdr_solver {
+    mvdr::Batch* batch;
+    uint32_t inst;
+    bool owns;
+};
+struct mvdr_batch {
+    mvdr::Batch* batch;
+};
+
+namespace mvdr {
+
+struct SolverView {
+    mvdr_solver s;
+};
+
+Batch::~Batch() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& o : owned)
+        if (o.mem) cudaFree(o.mem);
+    if (d_inst) cudaFree(d_inst);
+    if (arena) cudaFree(arena);
+    for (auto* v : views) delete v;
+}
+
+static mvdr_penalty penalty_for(const mvdr_config& c, uint32_t iter) {
+    mvdr_penalty p{};
+    if (!c.use_elastic_penalty) return c.penalty;
+    if ((int64_t)iter < (int64_t)c.num_global_iterations) {  // PenaltyConstants.cpp:25-37
+        p.smooth = 5.0f;
+        p.density = 0.0f;
+        p.foreground = c.use_foreground ? 2e-3f : 0.0f;
+        p.feature = 1.0f;
+        p.cross_view = c.use_cross_view ? 1.0f : 0.0f;
+    } else {  // PenaltyConstants.cpp:39-51
+        p.smooth = 5.0f;
+        p.density = 0.0f;
+        p.foreground = 0.0f;
+        p.feature = 0.0f;
+        p.cross_view = c.use_cross_view ? 1.0f : 0.0f;
+    }
+    return p;
+}
+
+static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32_t cap_edges, uint32_t max_tp,
+                              uint32_t max_tc, uint32_t partial_slots) {
+    const size_t N = lc.max_nodes;
+    I.counts = a.take<DeviceCounts>(1);
+    I.se3 = a.take<DQ>(N);
+    I.chunk_count = a.take<uint32_t>((size_t)lc.chunks_per_view * lc.max_views + 1);
+    I.dense_pix = a.take<ushort4>(lc.cap_dense);
+    I.dense_knn = a.take<ushort4>(lc.cap_dense);
+    I.dense_w = a.take<float4>(lc.cap_dense);
+    I.dense_cv = a.take<float4>(lc.cap_dense);
+    I.dense_cn = a.take<float4>(lc.cap_dense);
+    I.fg_pix = a.take<ushort4>(lc.cap_fg);
+    I.fg_knn = a.take<ushort4>(lc.cap_fg);
+    I.fg_w = a.take<float4>(lc.cap_fg);
+    I.fg_cv = a.take<float4>(lc.cap_fg);
+    I.n2t_count = a.take<uint32_t>(N + 1);
+    I.n2t_offset = a.take<uint32_t>(N + 1);
+    I.n2t_cursor = a.take<uint32_t>(N + 1);
+    I.n2t_index = a.take<uint32_t>(lc.cap_k1);
+    I.row_count = a.take<uint32_t>(N + 1);
+    I.row_offset = a.take<uint32_t>(N + 1);
+    I.np_index = a.take<uint32_t>(lc.cap_k2);
+    I.upper_count = a.take<uint32_t>(N + 1);
+    I.half_offset = a.take<uint32_t>(N + 1);
+    I.tmp_key = a.take<uint32_t>(lc.cap_k2);
+    I.tmp_start = a.take<uint32_t>(lc.cap_k2);
+    I.half_key = a.take<uint32_t>(lc.cap_pairs);
+    I.half_range = a.take<uint2>(lc.cap_pairs);
+    I.lower_count = a.take<uint32_t>(N + 1);
+    I.lower_cursor = a.take<uint32_t>(N + 1);
+    I.blkrow_offset = a.take<uint32_t>(N + 1);
+    I.sym_key = a.take<uint32_t>(2 * (size_t)lc.cap_pairs);
+    I.sym_range = a.take<uint2>(2 * (size_t)lc.cap_pairs);
+    I.sym_half = a.take<uint32_t>(2 * (size_t)lc.cap_pairs);
+    I.upper_pos = a.take<uint32_t>(lc.cap_pairs);
+    I.lower_pos = a.take<uint32_t>(lc.cap_pairs);
+    const size_t nbins = (6 * N + 31) / 32;
+    I.bin_scan = a.take<uint32_t>(nbins + 2);
+    I.bb_rowptr = a.take<int32_t>(32 * (nbins + 1));
+    I.bb_colptr = a.take<int32_t>(lc.cap_bb / 6 + 1);
+    I.bb_data = nullptr;
+    I.term_jr = a.take<float4>(2 * ((size_t)lc.cap_dense + lc.cap_fg));
+    I.smooth = a.take<float4>(2 * (size_t)cap_edges);
+    I.warped = a.take<float4>((size_t)max_tp + max_tc + 1);
+    I.diag = a.take<float>(36 * N);
+    I.minv = a.take<float>(36 * N);
+    I.chol = a.take<double>(21 * N);
+    I.jtr = a.take<float>(6 * N);
+    I.bsr = a.take<float>(36 * (N + 2 * (size_t)lc.cap_pairs));
+    I.x = a.take<float>(6 * N);
+    I.r = a.take<float>(6 * N);
+    I.s = a.take<float>(6 * N);
+    I.q = a.take<float>(6 * N);
+    I.d0 = a.take<float>(6 * N);
+    I.d1 = a.take<float>(6 * N);
+    I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(3 * (size_t)lc.cap_terms) : nullptr;
+    I.scalars = a.take<double>(8);
+    I.partials = a.take<double>(partial_slots);
+    I.energy = a.take<double>(64);
+    I.cap_dense = lc.cap_dense;
+    I.cap_fg = lc.cap_fg;
+    I.cap_k1 = lc.cap_k1;
+    I.cap_k2 = lc.cap_k2;
+    I.cap_pairs = lc.cap_pairs;
+    I.cap_seg = lc.cap_seg;
+    I.cap_row = lc.cap_row;
+    I.cap_bb = lc.cap_bb;
+    I.chunks_per_view = lc.chunks_per_view;
+    return a.off;
+}
+
+static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
+    if (!cfg || !out || B == 0) return fail(MVDR_EINVAL, "null argument or zero instances");
+    if (cfg->abi_version != MVDR_ABI_VERSION) return fail(MVDR_EINVAL, "abi_version mismatch");
+    if (cfg->max_nodes == 0 || cfg->max_nodes > 65535) return fail(MVDR_EINVAL, "max_nodes must be in [1, 65535]");
+    if (cfg->max_views == 0 || cfg->max_views > MVDR_MAX_VIEWS) return fail(MVDR_EINVAL, "max_views out of range");
+    if (cfg->image_width == 0 || cfg->image_height == 0 || cfg->image_width > 65535 || cfg->image_height > 65535)
+        return fail(MVDR_EINVAL, "image size out of range");
+    if (cfg->precision != MVDR_PRECISION_FP32 && cfg->precision != MVDR_PRECISION_MIXED)
+        return fail(MVDR_EINVAL, "unknown precision");
+    if (cfg->mode != MVDR_MODE_MATERIALIZED && cfg->mode != MVDR_MODE_MATRIX_FREE)
+        return fail(MVDR_EINVAL, "unknown mode");
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, dev));
+
+    Batch* b = new Batch();
+    b->cfg = *cfg;
+    b->B = B;
+    LaunchCfg& lc = b->lc;
+    lc.B = B;
+    lc.max_nodes = cfg->max_nodes;
+    lc.max_views = cfg->max_views;
+    lc.width = cfg->image_width;
+    lc.height = cfg->image_height;
+    const uint64_t pix = (uint64_t)cfg->max_views * cfg->image_width * cfg->image_height;
+    lc.cap_dense = cfg->max_dense_terms ? cfg->max_dense_terms : (uint32_t)std::min<uint64_t>(pix, 0x7fffffffu);
+    lc.cap_fg = cfg->use_foreground ? (cfg->max_foreground_terms ? cfg->max_foreground_terms : lc.cap_dense) : 0;
+    lc.max_tp = cfg->use_feature ? cfg->max_feature_terms : 0;
+    lc.max_tc = cfg->use_cross_view ? cfg->max_cross_terms : 0;
+    b->cap_edges = 8 * cfg->max_nodes;
+    lc.max_edges = b->cap_edges;
+    const uint64_t four = (uint64_t)lc.cap_dense + lc.cap_fg + lc.max_tp + lc.max_tc;
+    const uint64_t k1 = 4 * four + 2 * (uint64_t)b->cap_edges;
+    const uint64_t k2 = 6 * four + (uint64_t)b->cap_edges;
+    if (k2 > 0x7fffffffull) {
+        delete b;
+        return fail(MVDR_ECAPACITY, "term capacities exceed 2^31 index entries");
+    }
+    lc.cap_terms = (uint32_t)(four + b->cap_edges);
+    lc.cap_k1 = (uint32_t)k1;
+    lc.cap_k2 = (uint32_t)k2;
+    lc.cap_pairs = cfg->max_node_pairs ? cfg->max_node_pairs : 16 * cfg->max_nodes;
+    // shared-memory sort capacities are powers of two: the bitonic sort pads
+    // a segment up to the next power of two
+    auto pow2 = [](uint32_t v) { uint32_t p = 1; while (p < v) p <<= 1; return p; };
+    lc.cap_seg = std::min<uint32_t>(pow2(cfg->max_terms_per_node ? cfg->max_terms_per_node : 4096), 16384);
+    lc.cap_row = std::min<uint32_t>(pow2(2 * lc.cap_seg), 16384);
+    lc.cap_bb = 36 * (cfg->max_nodes + 2 * lc.cap_pairs);
+    lc.chunks_per_view = (cfg->image_width * cfg->image_height + 2047) / 2048;
+    lc.precision = cfg->precision;
+    lc.mode = cfg->mode;
+    lc.sm_count = prop.multiProcessorCount;
+
+    const size_t smem_seg = (size_t)lc.cap_seg * 4, smem_row = (size_t)lc.cap_row * 8;
+    if (smem_seg > (size_t)prop.sharedMemPerBlockOptin || smem_row > (size_t)prop.sharedMemPerBlockOptin) {
+        delete b;
+        return fail(MVDR_EINVAL, "max_terms_per_node too large for shared memory");
+    }
+    if (set_index_smem_limits(smem_seg, smem_row) != cudaSuccess) {
+        delete b;
+        return fail(MVDR_ECUDA, "cudaFuncSetAttribute failed");
+    }
+
+    const uint32_t gmax = std::max<uint32_t>({(lc.max_nodes + 255) / 256, (lc.max_nodes + 31) / 32,
+                                              (lc.max_nodes + 7) / 8, (uint32_t)lc.sm_count * 8}) + 8;
+    // size one instance, then allocate all
+    Arena sizing;
+    InstDesc tmp{};
+    const size_t per = layout_instance(sizing, tmp, lc, b->cap_edges, lc.max_tp, lc.max_tc, gmax);
+    b->per_inst_bytes = per;
+    b->arena_bytes = per * B;
+    cudaError_t e = cudaMalloc(&b->arena, b->arena_bytes);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(MVDR_ECUDA, std::string("workspace allocation failed: ") + cudaGetErrorString(e));
+    }
+    e = cudaMemset(b->arena, 0, b->arena_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_inst, sizeof(InstDesc) * B);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(MVDR_ECUDA, std::string("workspace setup failed: ") + cudaGetErrorString(e));
+    }
+    b->host.resize(B);
+    for (uint32_t i = 0; i < B; ++i) {
+        Arena a;
+        a.base = static_cast<char*>(b->arena) + per * i;
+        InstDesc& I = b->host[i];
+        std::memset(&I, 0, sizeof(I));
+        layout_instance(a, I, lc, b->cap_edges, lc.max_tp, lc.max_tc, gmax);
+    }
+    b->owned.resize(B);
+    b->has_inputs.assign(B, 0);
+    e = cudaMemcpy(b->d_inst, b->host.data(), sizeof(InstDesc) * B, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(MVDR_ECUDA, std::string("descriptor upload failed: ") + cudaGetErrorString(e));
+    }
+    b->views.resize(B);
+    for (uint32_t i = 0; i < B; ++i) {
+        b->views[i] = new SolverView();
+        b->views[i]->s = mvdr_solver{b, i, false};
+    }
+    *out = b;
+    return MVDR_OK;
+}
+
+static M34 load34(const mvdr_mat34& a) {
+    M34 m;
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) m.r[3 * r + c] = a.rot[3 * c + r];
+    for (int r = 0; r < 3; ++r) m.t[r] = a.trans[r];
+    return m;
+}
+
+// mat34::inverse (math/MatUtils.h:585-590) in float
+static M34 inverse34(const M34& a) {
+    M34 o;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) o.r[3 * r + c] = a.r[3 * c + r];
+    for (int r = 0; r < 3; ++r) o.t[r] = -(o.r[3 * r] * a.t[0] + o.r[3 * r + 1] * a.t[1] + o.r[3 * r + 2] * a.t[2]);
+    return o;
+}
+
+static int check_inputs(const Batch& b, const mvdr_inputs* in) {
+    const mvdr_config& c = b.cfg;
+    if (!in) return fail(MVDR_EINVAL, "inputs is null");
+    if (in->num_views == 0 || in->num_views > c.max_views) return fail(MVDR_ECAPACITY, "num_views exceeds max_views");
+    if (in->num_nodes == 0 || in->num_nodes > c.max_nodes) return fail(MVDR_ECAPACITY, "num_nodes exceeds max_nodes");
+    if (in->num_surfels > c.max_surfels && c.max_surfels) return fail(MVDR_ECAPACITY, "num_surfels exceeds max_surfels");
+    if (in->num_graph_edges > b.cap_edges) return fail(MVDR_ECAPACITY, "node graph larger than 8 * max_nodes");
+    if (c.use_feature && in->feature.count > c.max_feature_terms)
+        return fail(MVDR_ECAPACITY, "feature terms exceed max_feature_terms");
+    if (c.use_cross_view && in->cross_view.count > c.max_cross_terms)
+        return fail(MVDR_ECAPACITY, "cross-view terms exceed max_cross_terms");
+    if (!in->node_se3 || !in->canonical_node_coords || (in->num_graph_edges && !in->node_graph) ||
+        (in->num_surfels && (!in->surfel_knn || !in->surfel_knn_weight)))
+        return fail(MVDR_EINVAL, "missing node or surfel arrays");
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        const mvdr_view_inputs& V = in->views[v];
+        if (!V.reference_vertex_map || !V.reference_normal_map || !V.index_map || !V.vertex_confidence_map ||
+            !V.normal_radius_map)
+            return fail(MVDR_EINVAL, "missing view maps");
+        if (V.pitch && V.pitch < c.image_width) return fail(MVDR_EINVAL, "pitch smaller than image width");
+        if (c.use_foreground && (!V.filtered_foreground_mask || !V.foreground_mask_gradient))
+            return fail(MVDR_EINVAL, "foreground term on but mask maps missing");
+    }
+    if (c.use_feature && in->feature.count &&
+        (!in->feature.target_vertex || !in->feature.reference_vertex || !in->feature.knn || !in->feature.knn_weight))
+        return fail(MVDR_EINVAL, "missing feature arrays");
+    if (c.use_cross_view && in->cross_view.count &&
+        (!in->cross_view.target_vertex || !in->cross_view.reference_vertex || !in->cross_view.knn ||
+         !in->cross_view.knn_weight))
+        return fail(MVDR_EINVAL, "missing cross-view arrays");
+    return MVDR_OK;
+}
+
+static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st) {
+    int rc = check_inputs(b, in);
+    if (rc != MVDR_OK) return rc;
+    const mvdr_config& c = b.cfg;
+    InstDesc& I = b.host[inst];
+    I.num_views = in->num_views;
+    I.N = in->num_nodes;
+    I.S = in->num_surfels;
+    I.E = in->num_graph_edges;
+    I.Tp = c.use_feature ? in->feature.count : 0;
+    I.Tc = c.use_cross_view ? in->cross_view.count : 0;
+    I.width = c.image_width;
+    I.height = c.image_height;
+    uint32_t enc = 4096;  // EncodeUtils.h:187-204, widened past 4096 nodes
+    while (enc < I.N) enc <<= 1;
+    I.enc = enc;
+    I.compat = c.compat_flags;
+    I.use_fg = c.use_foreground ? 1u : 0u;
+    I.node_radius = c.node_radius;
+    for (uint32_t v = 0; v < MVDR_MAX_VIEWS; ++v) {
+        ViewDesc& V = I.views[v];
+        std::memset(&V, 0, sizeof(V));
+        if (v >= in->num_views) continue;
+        const mvdr_view_inputs& S = in->views[v];
+        V.ref_v = reinterpret_cast<const float4*>(S.reference_vertex_map);
+        V.ref_n = reinterpret_cast<const float4*>(S.reference_normal_map);
+        V.index = S.index_map;
+        V.obs_v = reinterpret_cast<const float4*>(S.vertex_confidence_map);
+        V.obs_n = reinterpret_cast<const float4*>(S.normal_radius_map);
+        V.fg = c.use_foreground ? S.filtered_foreground_mask : nullptr;
+        V.fg_grad = c.use_foreground ? reinterpret_cast<const float2*>(S.foreground_mask_gradient) : nullptr;
+        V.pitch = S.pitch ? S.pitch : c.image_width;
+        V.cx = S.intrinsic.principal_x;
+        V.cy = S.intrinsic.principal_y;
+        V.fx = S.intrinsic.focal_x;
+        V.fy = S.intrinsic.focal_y;
+        V.w2c = load34(S.world2camera);
+        V.init = load34(S.initial_camera_se3);
+        V.init_inv = inverse34(V.init);
+    }
+    I.surfel_knn = reinterpret_cast<const ushort4*>(in->surfel_knn);
+    I.surfel_w = reinterpret_cast<const float4*>(in->surfel_knn_weight);
+    I.nodes = reinterpret_cast<const float4*>(in->canonical_node_coords);
+    I.graph = reinterpret_cast<const ushort2*>(in->node_graph);
+    I.feat_target = reinterpret_cast<const float4*>(in->feature.target_vertex);
+    I.feat_ref = reinterpret_cast<const float4*>(in->feature.reference_vertex);
+    I.feat_knn = reinterpret_cast<const ushort4*>(in->feature.knn);
+    I.feat_w = reinterpret_cast<const float4*>(in->feature.knn_weight);
+    I.cross_target = reinterpret_cast<const float4*>(in->cross_view.target_vertex);
+    I.cross_ref = reinterpret_cast<const float4*>(in->cross_view.reference_vertex);
+    I.cross_knn = reinterpret_cast<const ushort4*>(in->cross_view.knn);
+    I.cross_w = reinterpret_cast<const float4*>(in->cross_view.knn_weight);
+    // SolverIterationData::SetWarpFieldInitialValue (SolverIterationData.cpp:37-50)
+    CU(cudaMemcpyAsync(I.se3, in->node_se3, sizeof(DQ) * I.N, cudaMemcpyDefault, st));
+    CU(cudaMemsetAsync(I.counts, 0, sizeof(DeviceCounts), st));
+    CU(cudaMemcpyAsync(b.d_inst + inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice, st));
+    b.has_inputs[inst] = 1;
+    b.gn_iter = 0;
+    return MVDR_OK;
+}
+
+// copy host arrays into owned device buffers, then bind them
+static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st) {
+    int rc = check_inputs(b, in);
+    if (rc != MVDR_OK) return rc;
+    const mvdr_config& c = b.cfg;
+    const size_t W = c.image_width, H = c.image_height;
+    struct Item { const void* src; size_t bytes; };
+    std::vector<Item> items;
+    mvdr_inputs dev = *in;
+    auto add = [&](const void* src, size_t bytes) { items.push_back({src, bytes}); };
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        const mvdr_view_inputs& V = in->views[v];
+        const size_t pitch = V.pitch ? V.pitch : W;
+        const size_t np = pitch * H;
+        add(V.reference_vertex_map, 16 * np);
+        add(V.reference_normal_map, 16 * np);
+        add(V.index_map, 4 * np);
+        add(V.vertex_confidence_map, 16 * np);
+        add(V.normal_radius_map, 16 * np);
+        add(c.use_foreground ? V.filtered_foreground_mask : nullptr, c.use_foreground ? 4 * np : 0);
+        add(c.use_foreground ? V.foreground_mask_gradient : nullptr, c.use_foreground ? 8 * np : 0);
+    }
+    add(in->surfel_knn, 8 * (size_t)in->num_surfels);
+    add(in->surfel_knn_weight, 16 * (size_t)in->num_surfels);
+    add(in->node_se3, 32 * (size_t)in->num_nodes);
+    add(in->canonical_node_coords, 16 * (size_t)in->num_nodes);
+    add(in->node_graph, 4 * (size_t)in->num_graph_edges);
+    const uint32_t tp = c.use_feature ? in->feature.count : 0, tc = c.use_cross_view ? in->cross_view.count : 0;
+    add(in->feature.target_vertex, 16 * (size_t)tp);
+    add(in->feature.reference_vertex, 16 * (size_t)tp);
+    add(in->feature.knn, 8 * (size_t)tp);
+    add(in->feature.knn_weight, 16 * (size_t)tp);
+    add(in->cross_view.target_vertex, 16 * (size_t)tc);
+    add(in->cross_view.reference_vertex, 16 * (size_t)tc);
+    add(in->cross_view.knn, 8 * (size_t)tc);
+    add(in->cross_view.knn_weight, 16 * (size_t)tc);
+    size_t total = 0;
+    for (auto& it : items) total += (it.bytes + 255) & ~(size_t)255;
+    OwnedInputs& o = b.owned[inst];
+    if (o.bytes < total) {
+        // first call (or larger inputs): allocate the device copies once
+        if (o.mem) CU(cudaFree(o.mem));
+        o.mem = nullptr;
+        o.bytes = 0;
+        CU(cudaMalloc(&o.mem, total));
+        o.bytes = total;
+    }
+    std::vector<void*> dst(items.size(), nullptr);
+    size_t off = 0;
+    for (size_t i = 0; i < items.size(); ++i) {
+        if (items[i].bytes && items[i].src) {
+            dst[i] = static_cast<char*>(o.mem) + off;
+            CU(cudaMemcpyAsync(dst[i], items[i].src, items[i].bytes, cudaMemcpyHostToDevice, st));
+        }
+        off += (items[i].bytes + 255) & ~(size_t)255;
+    }
+    size_t k = 0;
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        mvdr_view_inputs& V = dev.views[v];
+        V.reference_vertex_map = (const mvdr_float4*)dst[k++];
+        V.reference_normal_map = (const mvdr_float4*)dst[k++];
+        V.index_map = (const uint32_t*)dst[k++];
+        V.vertex_confidence_map = (const mvdr_float4*)dst[k++];
+        V.normal_radius_map = (const mvdr_float4*)dst[k++];
+        V.filtered_foreground_mask = (const float*)dst[k++];
+        V.foreground_mask_gradient = (const float*)dst[k++];
+    }
+    dev.surfel_knn = (const uint16_t*)dst[k++];
+    dev.surfel_knn_weight = (const mvdr_float4*)dst[k++];
+    dev.node_se3 = (const mvdr_dual_quaternion*)dst[k++];
+    dev.canonical_node_coords = (const mvdr_float4*)dst[k++];
+    dev.node_graph = (const uint16_t*)dst[k++];
+    dev.feature.target_vertex = (const mvdr_float4*)dst[k++];
+    dev.feature.reference_vertex = (const mvdr_float4*)dst[k++];
+    dev.feature.knn = (const uint16_t*)dst[k++];
+    dev.feature.knn_weight = (const mvdr_float4*)dst[k++];
+    dev.cross_view.target_vertex = (const mvdr_float4*)dst[k++];
+    dev.cross_view.reference_vertex = (const mvdr_float4*)dst[k++];
+    dev.cross_view.knn = (const uint16_t*)dst[k++];
+    dev.cross_view.knn_weight = (const mvdr_float4*)dst[k++];
+    return bind_inputs(b, inst, &dev, st);
+}
+
+static int all_bound(const Batch& b) {
+    for (uint32_t i = 0; i < b.B; ++i)
+        if (!b.has_inputs[i]) return fail(MVDR_ESTATE, "inputs not set for every instance");
+    return MVDR_OK;
+}
+
+static int enqueue_index(Batch& b, cudaStream_t st) {
+    // zero the per-build counters of every instance
+    for (uint32_t i = 0; i < b.B; ++i) {
+        const InstDesc& I = b.host[i];
+        CU(cudaMemsetAsync(I.counts, 0, sizeof(DeviceCounts), st));
+        CU(cudaMemsetAsync(I.n2t_count, 0, sizeof(uint32_t) * (b.lc.max_nodes + 1), st));
+    }
+    CU(launch_build_index(b.lc, b.d_inst, st));
+    return MVDR_OK;
+}
+
+static int enqueue_iteration(Batch& b, uint32_t iter, uint32_t pcg, cudaStream_t st) {
+    const mvdr_penalty lam = penalty_for(b.cfg, iter);
+    CU(launch_eval_terms(b.lc, b.d_inst, st));
+    CU(launch_energy(b.lc, b.d_inst, lam, std::min<uint32_t>(iter, 63), st));
+    CU(launch_assemble(b.lc, b.d_inst, lam, b.cfg.mode == MVDR_MODE_MATERIALIZED, st));
+    CU(launch_pcg(b.lc, b.d_inst, lam, pcg, st));
+    CU(launch_update(b.lc, b.d_inst, st));
+    return MVDR_OK;
+}
+
+static int solve_batch(Batch& b, uint32_t gn, uint32_t pcg, bool graph, cudaStream_t st) {
+    int rc = all_bound(b);
+    if (rc != MVDR_OK) return rc;
+    if (gn > 63) return fail(MVDR_EINVAL, "at most 63 Gauss-Newton iterations per solve");
+    if (!graph) {
+        rc = enqueue_index(b, st);
+        if (rc != MVDR_OK) return rc;
+        for (uint32_t k = 0; k < gn; ++k) {
+            rc = enqueue_iteration(b, k, pcg, st);
+            if (rc != MVDR_OK) return rc;
+        }
+        b.gn_iter = gn;
+        return MVDR_OK;
+    }
+    auto key = std::make_pair(gn, pcg);
+    auto it = b.graphs.find(key);
+    if (it == b.graphs.end()) {
+        // capture the whole solve once; the descriptors are read from device
+        // memory, so the graph stays valid across set_inputs calls
+        cudaStream_t cap;
+        CU(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            cudaStreamDestroy(cap);
+            return fail(MVDR_ECUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+        }
+        rc = enqueue_index(b, cap);
+        for (uint32_t k = 0; rc == MVDR_OK && k < gn; ++k) rc = enqueue_iteration(b, k, pcg, cap);
+        e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc != MVDR_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(MVDR_ECUDA, std::string("end capture: ") + cudaGetErrorString(e));
+        cudaGraphExec_t ex = nullptr;
+        e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(MVDR_ECUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+        it = b.graphs.emplace(key, ex).first;
+    }
+    CU(cudaGraphLaunch(it->second, st));
+    count_launch();
+    b.gn_iter = gn;
+    return MVDR_OK;
+}
+
+static int read_counts(Batch& b, uint32_t inst, DeviceCounts& c, cudaStream_t st) {
+    CU(cudaStreamSynchronize(st));
+    CU(cudaMemcpy(&c, b.host[inst].counts, sizeof(DeviceCounts), cudaMemcpyDeviceToHost));
+    return MVDR_OK;
+}
+
+static int check_flags(const DeviceCounts& c) {
+    if (c.error_flags & (kErrDenseCapacity | kErrForegroundCapacity | kErrNode2TermCapacity |
+                         kErrNodePairEntryCapacity | kErrHalfPairCapacity | kErrSegmentTooLong | kErrRowTooLong |
+                         kErrBinBlockCapacity)) {
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "device capacity exceeded (flags 0x%x)", c.error_flags);
+        return fail(MVDR_ECAPACITY, buf);
+    }
+    if (c.error_flags & kErrBadNodeIndex) return fail(MVDR_EINVAL, "node or surfel index out of range in inputs");
+    return MVDR_OK;
+}
+
+static int copy_out(void* dst, const void* src, size_t bytes, size_t cap, size_t* written) {
+    if (written) *written = bytes;
+    if (bytes > cap) return fail(MVDR_ECAPACITY, "destination buffer too small");
+    if (bytes) CU(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+    return MVDR_OK;
+}
+
+static int get_array(Batch& b, uint32_t inst, int which, void* dst, size_t cap, size_t* written, cudaStream_t st) {
+    DeviceCounts c;
+    int rc = read_counts(b, inst, c, st);
+    if (rc != MVDR_OK) return rc;
+    const InstDesc& I = b.host[inst];
+    const size_t N = I.N, P = c.half_pairs;
+    switch (which) {
+        case MVDR_ARRAY_DENSE_PIXELS: return copy_out(dst, I.dense_pix, 8 * (size_t)c.dense_terms, cap, written);
+        case MVDR_ARRAY_DENSE_KNN: return copy_out(dst, I.dense_knn, 8 * (size_t)c.dense_terms, cap, written);
+        case MVDR_ARRAY_DENSE_KNN_WEIGHT: return copy_out(dst, I.dense_w, 16 * (size_t)c.dense_terms, cap, written);
+        case MVDR_ARRAY_FOREGROUND_PIXELS: return copy_out(dst, I.fg_pix, 8 * (size_t)c.foreground_terms, cap, written);
+        case MVDR_ARRAY_NODE2TERM_OFFSET: return copy_out(dst, I.n2t_offset, 4 * (N + 1), cap, written);
+        case MVDR_ARRAY_NODE2TERM_INDEX: return copy_out(dst, I.n2t_index, 4 * (size_t)c.node2term_entries, cap, written);
+        case MVDR_ARRAY_HALF_NODEPAIR_KEY: return copy_out(dst, I.half_key, 4 * P, cap, written);
+        case MVDR_ARRAY_NODEPAIR_TERM_INDEX: return copy_out(dst, I.np_index, 4 * (size_t)c.nodepair_entries, cap, written);
+        case MVDR_ARRAY_NODEPAIR_KEY: return copy_out(dst, I.sym_key, 8 * P, cap, written);
+        case MVDR_ARRAY_NODEPAIR_TERM_RANGE: return copy_out(dst, I.sym_range, 16 * P, cap, written);
+        case MVDR_ARRAY_BLKROW_OFFSET: return copy_out(dst, I.blkrow_offset, 4 * (N + 1), cap, written);
+        case MVDR_ARRAY_BINBLOCK_ROWPTR:
+            return copy_out(dst, I.bb_rowptr, 4 * 32 * ((size_t)c.num_bins + 1), cap, written);
+        case MVDR_ARRAY_BINBLOCK_COLPTR: return copy_out(dst, I.bb_colptr, 4 * ((size_t)c.binblock_nnz / 6), cap, written);
+        case MVDR_ARRAY_TERM_JACOBIAN:
+            return copy_out(dst, I.term_jr, 32 * ((size_t)c.dense_terms + c.foreground_terms), cap, written);
+        case MVDR_ARRAY_SMOOTH_TERMS: return copy_out(dst, I.smooth, 32 * (size_t)I.E, cap, written);
+        case MVDR_ARRAY_WARPED_CORRESPONDENCE:
+            return copy_out(dst, I.warped, 16 * ((size_t)I.Tp + I.Tc), cap, written);
+        case MVDR_ARRAY_DIAG_BLOCKS: return copy_out(dst, I.diag, 4 * 36 * N, cap, written);
+        case MVDR_ARRAY_JTR: return copy_out(dst, I.jtr, 4 * 6 * N, cap, written);
+        case MVDR_ARRAY_INCREMENT: return copy_out(dst, I.x, 4 * 6 * N, cap, written);
+        case MVDR_ARRAY_NODE_SE3: return copy_out(dst, I.se3, 32 * N, cap, written);
+        case MVDR_ARRAY_PRECONDITIONER:
+        case MVDR_ARRAY_OFFDIAG_BLOCKS:
+        case MVDR_ARRAY_BINBLOCK_DATA: {
+            size_t bytes = which == MVDR_ARRAY_PRECONDITIONER ? 4 * 36 * N
+                           : which == MVDR_ARRAY_OFFDIAG_BLOCKS ? 4 * 36 * 2 * P
+                                                                 : 4 * (size_t)c.binblock_nnz;
+            if (written) *written = bytes;
+            if (bytes > cap) return fail(MVDR_ECAPACITY, "destination buffer too small");
+            if (bytes == 0) return MVDR_OK;
+            // diagnostic path: a temporary device buffer for the reformatted array
+            float* tmp = nullptr;
+            CU(cudaMalloc(&tmp, bytes));
+            cudaError_t e;
+            if (which == MVDR_ARRAY_PRECONDITIONER) e = launch_export_preconditioner(b.lc, b.d_inst, inst, tmp, st);
+            else if (which == MVDR_ARRAY_OFFDIAG_BLOCKS) e = launch_export_offdiag(b.lc, b.d_inst, inst, tmp, st);
+            else {
+                e = cudaMemsetAsync(tmp, 0, bytes, st);
+                if (e == cudaSuccess) {
+                    export_binblock_fill_kernel<<<b.lc.sm_count * 4, 256, 0, st>>>(b.d_inst, inst, tmp);
+                    count_launch();
+                    e = cudaGetLastError();
+                }
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess) e = cudaMemcpy(dst, tmp, bytes, cudaMemcpyDefault);
+            cudaFree(tmp);
+            if (e != cudaSuccess) return fail(MVDR_ECUDA, std::string("export: ") + cudaGetErrorString(e));
+            return MVDR_OK;
+        }
+        default: return fail(MVDR_EINVAL, "unknown array id");
+    }
+}
+
+}  // namespace mvdr
+
+using namespace mvdr;
+
+// ------------------------------------------------------------- C ABI -----
+extern "C" {
+
+void mvdr_config_default(mvdr_config* cfg, uint32_t max_nodes, uint32_t max_views, uint32_t image_width,
+                         uint32_t image_height) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->abi_version = MVDR_ABI_VERSION;
+    cfg->max_nodes = max_nodes;
+    cfg->max_views = max_views;
+    cfg->image_width = image_width;
+    cfg->image_height = image_height;
+    cfg->max_surfels = max_views * image_width * image_height;
+    cfg->node_radius = 0.025f;
+    cfg->precision = MVDR_PRECISION_MIXED;
+    cfg->mode = MVDR_MODE_MATERIALIZED;
+    cfg->use_elastic_penalty = 1;
+    cfg->num_global_iterations = 3;
+    cfg->penalty = mvdr_penalty{2.5f, 0.0f, 0.0f, 0.7f, 0.1f};  // PenaltyConstants::setDefaultValue
+}
+
+int mvdr_create(const mvdr_config* cfg, mvdr_solver** out) {
+    if (!out) return fail(MVDR_EINVAL, "out is null");
+    Batch* b = nullptr;
+    int rc = create_batch(cfg, 1, &b);
+    if (rc != MVDR_OK) return rc;
+    *out = new mvdr_solver{b, 0, true};
+    return MVDR_OK;
+}
+
+int mvdr_destroy(mvdr_solver* s) {
+    if (!s) return MVDR_OK;
+    if (!s->owns) return fail(MVDR_EINVAL, "solver belongs to a batch; destroy the batch");
+    delete s->batch;
+    delete s;
+    return MVDR_OK;
+}
+
+int mvdr_set_inputs(mvdr_solver* s, const mvdr_inputs* in, void* stream) {
+    if (!s) return fail(MVDR_EINVAL, "solver is null");
+    return bind_inputs(*s->batch, s->inst, in, (cudaStream_t)stream);
+}
+
+int mvdr_set_inputs_host(mvdr_solver* s, const mvdr_inputs* in, void* stream) {
+    if (!s) return fail(MVDR_EINVAL, "solver is null");
+    return bind_inputs_host(*s->batch, s->inst, in, (cudaStream_t)stream);
+}
+
+int mvdr_build_index(mvdr_solver* s, void* stream) {
+    if (!s) return fail(MVDR_EINVAL, "solver is null");
+    if (!s->owns) return fail(MVDR_EINVAL, "use mvdr_batch_solve for batch members");
+    int rc = all_bound(*s->batch);
+    if (rc != MVDR_OK) return rc;
+    rc = enqueue_index(*s->batch, (cudaStream_t)stream);
+    if (rc == MVDR_OK) s->batch->gn_iter = 0;
+    return rc;
+}
+
+int mvdr_gn_iteration(mvdr_solver* s, uint32_t pcg_iterations, void* stream) {
+    if (!s) return fail(MVDR_EINVAL, "solver is null");
+    if (!s->owns) return fail(MVDR_EINVAL, "use mvdr_batch_solve for batch members");
+    Batch& b = *s->batch;
+    int rc = all_bound(b);
+    if (rc != MVDR_OK) return rc;
+    if (b.gn_iter >= 63) return fail(MVDR_EINVAL, "too many Gauss-Newton iterations");
+    rc = enqueue_iteration(b, b.gn_iter, pcg_iterations, (cudaStream_t)stream);
+    if (rc == MVDR_OK) b.gn_iter++;
+    return rc;
+}
+
+int mvdr_solve(mvdr_solver* s, uint32_t gn, uint32_t pcg, void* stream) {
+    if (!s) return fail(MVDR_EINVAL, "solver is null");
+    if (!s->owns) return fail(MVDR_EINVAL, "use mvdr_batch_solve for batch members");
+    return solve_batch(*s->batch, gn, pcg, false, (cudaStream_t)stream);
+}
+
+int mvdr_get_node_se3(mvdr_solver* s, mvdr_dual_quaternion* dst, void* stream) {
+    if (!s || !dst) return fail(MVDR_EINVAL, "null argument");
+    Batch& b = *s->batch;
+    DeviceCounts c;
+    int rc = read_counts(b, s->inst, c, (cudaStream_t)stream);
+    if (rc != MVDR_OK) return rc;
+    rc = check_flags(c);
+    if (rc != MVDR_OK) return rc;
+    CU(cudaMemcpy(dst, b.host[s->inst].se3, sizeof(DQ) * b.host[s->inst].N, cudaMemcpyDefault));
+    return MVDR_OK;
+}
+
+int mvdr_get_counts(mvdr_solver* s, mvdr_counts* out, void* stream) {
+    if (!s || !out) return fail(MVDR_EINVAL, "null argument");
+    DeviceCounts c;
+    int rc = read_counts(*s->batch, s->inst, c, (cudaStream_t)stream);
+    if (rc != MVDR_OK) return rc;
+    std::memcpy(out, &c, sizeof(mvdr_counts));
+    return MVDR_OK;
+}
+
+int mvdr_get_energy(mvdr_solver* s, double* energy, void* stream) {
+    if (!s || !energy) return fail(MVDR_EINVAL, "null argument");
+    Batch& b = *s->batch;
+    if (b.gn_iter == 0) return fail(MVDR_ESTATE, "no Gauss-Newton iteration has run");
+    CU(cudaStreamSynchronize((cudaStream_t)stream));
+    const uint32_t slot = std::min<uint32_t>(b.gn_iter - 1, 63);
+    CU(cudaMemcpy(energy, b.host[s->inst].energy + slot, sizeof(double), cudaMemcpyDeviceToHost));
+    return MVDR_OK;
+}
+
+int mvdr_get_array(mvdr_solver* s, int which, void* dst, size_t cap, size_t* written, void* stream) {
+    if (!s || !dst) return fail(MVDR_EINVAL, "null argument");
+    return get_array(*s->batch, s->inst, which, dst, cap, written, (cudaStream_t)stream);
+}
+
+int mvdr_apply_jtj(mvdr_solver* s, const float* x, float* y, void* stream) {
+    if (!s || !x || !y) return fail(MVDR_EINVAL, "null argument");
+    Batch& b = *s->batch;
+    if (b.gn_iter == 0) return fail(MVDR_ESTATE, "no Gauss-Newton iteration has run");
+    LaunchCfg lc = b.lc;
+    lc.B = 1;
+    const mvdr_penalty lam = penalty_for(b.cfg, b.gn_iter - 1);
+    CU(launch_apply_jtj(lc, b.d_inst + s->inst, lam, x, y, (cudaStream_t)stream));
+    return MVDR_OK;
+}
+
+int mvdr_batch_create(const mvdr_config* cfg, uint32_t n, mvdr_batch** out) {
+    if (!out) return fail(MVDR_EINVAL, "out is null");
+    Batch* b = nullptr;
+    int rc = create_batch(cfg, n, &b);
+    if (rc != MVDR_OK) return rc;
+    *out = new mvdr_batch{b};
+    return MVDR_OK;
+}
+
+int mvdr_batch_destroy(mvdr_batch* b) {
+    if (!b) return MVDR_OK;
+    delete b->batch;
+    delete b;
+    return MVDR_OK;
+}
+
+int mvdr_batch_set_inputs(mvdr_batch* b, uint32_t i, const mvdr_inputs* in, void* stream) {
+    if (!b || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
+    return bind_inputs(*b->batch, i, in, (cudaStream_t)stream);
+}
+
+int mvdr_batch_set_inputs_host(mvdr_batch* b, uint32_t i, const mvdr_inputs* in, void* stream) {
+    if (!b || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
+    return bind_inputs_host(*b->batch, i, in, (cudaStream_t)stream);
+}
+
+int mvdr_batch_solve(mvdr_batch* b, uint32_t gn, uint32_t pcg, int use_graph, void* stream) {
+    if (!b) return fail(MVDR_EINVAL, "batch is null");
+    return solve_batch(*b->batch, gn, pcg, use_graph != 0, (cudaStream_t)stream);
+}
+
+int mvdr_batch_get_node_se3(mvdr_batch* b, uint32_t i, mvdr_dual_quaternion* dst, void* stream) {
+    if (!b || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
+    return mvdr_get_node_se3(&b->batch->views[i]->s, dst, stream);
+}
+
+int mvdr_batch_instance(mvdr_batch* b, uint32_t i, mvdr_solver** out) {
+    if (!b || !out || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
+    *out = &b->batch->views[i]->s;
+    return MVDR_OK;
+}
+
+int mvdr_batch_enqueue_stage(mvdr_batch* b, int stage, void* stream) {
+    if (!b) return fail(MVDR_EINVAL, "batch is null");
+    Batch& bb = *b->batch;
+    int rc = all_bound(bb);
+    if (rc != MVDR_OK) return rc;
+    if (stage == MVDR_STAGE_INDEX) return enqueue_index(bb, (cudaStream_t)stream);
+    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_UPDATE) return fail(MVDR_EINVAL, "unknown stage");
+    CU(launch_stage(bb.lc, bb.d_inst, penalty_for(bb.cfg, 0), stage, (cudaStream_t)stream));
+    return MVDR_OK;
+}
+
+const char* mvdr_last_error_string(void) { return g_last_error.c_str(); }
+
+uint64_t mvdr_kernel_launch_count(void) { return g_launches.load(); }
+
+/* Layout report for the binding's self-check: sizes of the public structs. */
+int mvdr_abi_layout(const char* name, size_t* size) {
+    if (!name || !size) return MVDR_EINVAL;
+    const struct { const char* n; size_t s; } table[] = {
+        {"mvdr_float4", sizeof(mvdr_float4)}, {"mvdr_dual_quaternion", sizeof(mvdr_dual_quaternion)},
+        {"mvdr_mat34", sizeof(mvdr_mat34)}, {"mvdr_intrinsic", sizeof(mvdr_intrinsic)},
+        {"mvdr_penalty", sizeof(mvdr_penalty)}, {"mvdr_config", sizeof(mvdr_config)},
+        {"mvdr_view_inputs", sizeof(mvdr_view_inputs)}, {"mvdr_correspondences", sizeof(mvdr_correspondences)},
+        {"mvdr_inputs", sizeof(mvdr_inputs)}, {"mvdr_counts", sizeof(mvdr_counts)}};
+    for (const auto& t : table)
+        if (std::strcmp(t.n, name) == 0) { *size = t.s; return MVDR_OK; }
+    return MVDR_EINVAL;
+}
+
+}  // extern "C"

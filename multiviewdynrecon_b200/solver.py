@@ -1,0 +1,216 @@
+"""Python mirror of the reference NonRigidSolver interface over the C ABI.
+
+    NonRigidSolver.SetSolverInput(...)      -> NonRigidSolver.set_solver_input(scene)
+    NonRigidSolver.SolveNonRigidAlignment() -> NonRigidSolver.solve_non_rigid_alignment(gn, pcg)
+    NonRigidSolver.SolvedNodeSE3()          -> NonRigidSolver.solved_node_se3()
+
+(core/NonRigidSolver/NonRigidSolver.h:133-140, 254, 214.) Device memory and
+streams come from torch; every computation runs in libmvdr.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi, check, lib
+
+_NP_TO_TORCH = {np.dtype(np.float32): torch.float32, np.dtype(np.uint16): torch.int16,
+                np.dtype(np.uint32): torch.int32, np.dtype(np.float64): torch.float64,
+                np.dtype(np.int32): torch.int32}
+
+# element type and per-item width of each exported array
+ARRAY_SPEC = {
+    abi.ARRAY_DENSE_PIXELS: (np.uint16, 4), abi.ARRAY_DENSE_KNN: (np.uint16, 4),
+    abi.ARRAY_DENSE_KNN_WEIGHT: (np.float32, 4), abi.ARRAY_FOREGROUND_PIXELS: (np.uint16, 4),
+    abi.ARRAY_NODE2TERM_OFFSET: (np.uint32, 1), abi.ARRAY_NODE2TERM_INDEX: (np.uint32, 1),
+    abi.ARRAY_HALF_NODEPAIR_KEY: (np.uint32, 1), abi.ARRAY_NODEPAIR_TERM_INDEX: (np.uint32, 1),
+    abi.ARRAY_NODEPAIR_KEY: (np.uint32, 1), abi.ARRAY_NODEPAIR_TERM_RANGE: (np.uint32, 2),
+    abi.ARRAY_BLKROW_OFFSET: (np.uint32, 1), abi.ARRAY_BINBLOCK_ROWPTR: (np.int32, 1),
+    abi.ARRAY_BINBLOCK_COLPTR: (np.int32, 1), abi.ARRAY_TERM_JACOBIAN: (np.float32, 8),
+    abi.ARRAY_SMOOTH_TERMS: (np.float32, 8), abi.ARRAY_WARPED_CORRESPONDENCE: (np.float32, 4),
+    abi.ARRAY_DIAG_BLOCKS: (np.float32, 36), abi.ARRAY_JTR: (np.float32, 6),
+    abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
+    abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
+    abi.ARRAY_NODE_SE3: (np.float32, 8),
+}
+
+
+def _stream_handle(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+class DeviceScene:
+    """Device copies (torch tensors) of every array of a synthetic scene."""
+
+    def __init__(self, scene, device="cuda", pin=False):
+        self.tensors = {}
+        self.device = device
+        self.pin = pin
+
+        def ptr(name, arr):
+            a = np.ascontiguousarray(arr)
+            if a.size == 0:
+                return None
+            t = torch.from_numpy(a.view(np.uint8).reshape(-1).copy())
+            if pin:
+                t = t.pin_memory()
+            else:
+                t = t.to(device)
+            self.tensors[name] = t
+            return t.data_ptr()
+
+        self.inputs = abi.fill_inputs(scene, ptr)
+
+    @property
+    def nbytes(self):
+        return sum(t.numel() for t in self.tensors.values())
+
+
+class NonRigidSolver:
+    def __init__(self, config):
+        self.config = config
+        h = C.c_void_p()
+        check(lib().mvdr_create(C.byref(config), C.byref(h)))
+        self.h = h
+        self._inputs = None
+        self.num_nodes = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mvdr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # SetSolverInput
+    def set_solver_input(self, scene, stream=None):
+        ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene)
+        self._inputs = ds
+        self.num_nodes = ds.inputs.num_nodes
+        check(lib().mvdr_set_inputs(self.h, C.byref(ds.inputs), _stream_handle(stream)))
+        return ds
+
+    def set_solver_input_host(self, host_scene, stream=None):
+        """`host_scene`: a DeviceScene built with pin=True (host pointers)."""
+        self._inputs = host_scene
+        self.num_nodes = host_scene.inputs.num_nodes
+        check(lib().mvdr_set_inputs_host(self.h, C.byref(host_scene.inputs), _stream_handle(stream)))
+
+    def build_index(self, stream=None):
+        check(lib().mvdr_build_index(self.h, _stream_handle(stream)))
+
+    def gn_iteration(self, pcg_iterations, stream=None):
+        check(lib().mvdr_gn_iteration(self.h, pcg_iterations, _stream_handle(stream)))
+
+    # SolveNonRigidAlignment
+    def solve_non_rigid_alignment(self, gn_iterations, pcg_iterations, stream=None):
+        check(lib().mvdr_solve(self.h, gn_iterations, pcg_iterations, _stream_handle(stream)))
+
+    # SolvedNodeSE3
+    def solved_node_se3(self, stream=None):
+        out = torch.empty((self.num_nodes, 8), dtype=torch.float32, device="cuda")
+        check(lib().mvdr_get_node_se3(self.h, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
+        return out
+
+    def counts(self, stream=None):
+        c = abi.Counts()
+        check(lib().mvdr_get_counts(self.h, C.byref(c), _stream_handle(stream)))
+        return c
+
+    def energy(self, stream=None):
+        e = C.c_double()
+        check(lib().mvdr_get_energy(self.h, C.byref(e), _stream_handle(stream)))
+        return e.value
+
+    def get_array(self, which, stream=None):
+        dt, width = ARRAY_SPEC[which]
+        cap = 1 << 22
+        while True:
+            buf = np.empty(cap // np.dtype(dt).itemsize, dt)
+            written = C.c_size_t()
+            st = lib().mvdr_get_array(self.h, which, buf.ctypes.data_as(C.c_void_p), buf.nbytes, C.byref(written),
+                                      _stream_handle(stream))
+            if st == abi.MVDR_ECAPACITY and written.value > buf.nbytes:
+                cap = written.value
+                continue
+            check(st)
+            out = buf[: written.value // np.dtype(dt).itemsize]
+            return out.reshape(-1, width) if width > 1 else out
+
+    def apply_jtj(self, x, stream=None):
+        x = x.contiguous().float()
+        y = torch.empty_like(x)
+        check(lib().mvdr_apply_jtj(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                   _stream_handle(stream)))
+        return y
+
+
+class BatchSolver:
+    """Many independent solves of uneven sizes, one launch per stage."""
+
+    def __init__(self, config, count):
+        self.config = config
+        self.count = count
+        h = C.c_void_p()
+        check(lib().mvdr_batch_create(C.byref(config), count, C.byref(h)))
+        self.h = h
+        self._inputs = [None] * count
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mvdr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_input(self, i, scene, stream=None):
+        ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene)
+        self._inputs[i] = ds
+        check(lib().mvdr_batch_set_inputs(self.h, i, C.byref(ds.inputs), _stream_handle(stream)))
+        return ds
+
+    def set_input_host(self, i, host_scene, stream=None):
+        self._inputs[i] = host_scene
+        check(lib().mvdr_batch_set_inputs_host(self.h, i, C.byref(host_scene.inputs), _stream_handle(stream)))
+
+    def solve(self, gn, pcg, use_graph=True, stream=None):
+        check(lib().mvdr_batch_solve(self.h, gn, pcg, int(use_graph), _stream_handle(stream)))
+
+    def node_se3(self, i, out=None, stream=None):
+        n = self._inputs[i].inputs.num_nodes
+        if out is None:
+            out = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+        check(lib().mvdr_batch_get_node_se3(self.h, i, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
+        return out
+
+    def instance(self, i):
+        """NonRigidSolver-like view of one member (for checks); not owned."""
+        h = C.c_void_p()
+        check(lib().mvdr_batch_instance(self.h, i, C.byref(h)))
+        n = self._inputs[i].inputs.num_nodes if self._inputs[i] else 0
+        return _InstanceView(h, n, self.config)
+
+
+class _InstanceView(NonRigidSolver):
+    """A batch member seen through the single-solver interface. Its handle
+    belongs to the batch, so closing the view releases nothing."""
+
+    def __init__(self, h, num_nodes, config):
+        self.h = h
+        self.num_nodes = num_nodes
+        self.config = config
+        self._inputs = None
+
+    def close(self):
+        self.h = None

@@ -1,0 +1,57 @@
+"""The C-ABI library loads without a GPU, exports every function declared in
+include/mvdr.h, and its struct layouts match the ctypes mirror."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import multiviewdynrecon_b200 as m
+from multiviewdynrecon_b200 import abi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "mvdr.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mvdr_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    if not os.path.exists(m.LIB_PATH):
+        m.build()
+    return m.lib()
+
+
+def test_exports_every_declared_symbol(L):
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_struct_layouts_match(L):
+    for name, cls in abi.STRUCTS.items():
+        size = C.c_size_t()
+        assert L.mvdr_abi_layout(name.encode(), C.byref(size)) == abi.MVDR_OK, name
+        assert size.value == C.sizeof(cls), (name, size.value, C.sizeof(cls))
+
+
+def test_config_default_and_errors_without_gpu(L):
+    cfg = abi.Config()
+    L.mvdr_config_default(C.byref(cfg), 4096, 3, 640, 480)
+    assert cfg.abi_version == abi.MVDR_ABI_VERSION
+    assert cfg.precision == abi.PRECISION_MIXED and cfg.max_nodes == 4096
+    # invalid configurations are rejected on the host before any CUDA call
+    bad = abi.Config()
+    L.mvdr_config_default(C.byref(bad), 70000, 3, 640, 480)
+    h = C.c_void_p()
+    assert L.mvdr_create(C.byref(bad), C.byref(h)) == abi.MVDR_EINVAL
+    assert b"max_nodes" in L.mvdr_last_error_string()
+    bad.max_nodes = 10
+    bad.abi_version = 99
+    assert L.mvdr_create(C.byref(bad), C.byref(h)) == abi.MVDR_EINVAL
+    assert L.mvdr_destroy(None) == abi.MVDR_OK
+    assert L.mvdr_set_inputs(None, None, None) == abi.MVDR_EINVAL

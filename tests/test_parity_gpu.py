@@ -1,0 +1,266 @@
+"""Parity of the CUDA solver (through the C ABI) with the CPU oracle.
+
+Bars:
+* index and bin-block CSR structure: bit-exact;
+* per-term Jacobians / residuals: maxRelativeError (sanity_check.cpp:50-73)
+  below 1e-4 with a small cutoff; projected-pixel choices that differ because
+  of FMA rounding at a threshold are counted and must stay below 0.1 %;
+* JtJ diagonal / off-diagonal blocks and Jt r built from the same term data:
+  below 1e-4;
+* PCG increment: relative 2-norm error against the FP64 oracle below 1e-4 in
+  mixed precision (2e-3 in plain FP32);
+* warp-field update from the same increment: below 1e-4.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import max_relative_error, rel_norm_error, small_scene
+from multiviewdynrecon_b200 import abi
+from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, NonRigidSolver
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["sphere", "sphere_rigid", "torso", "torso_rigid", "body"]
+INDEX_ARRAYS = [abi.ARRAY_DENSE_PIXELS, abi.ARRAY_DENSE_KNN, abi.ARRAY_DENSE_KNN_WEIGHT,
+                abi.ARRAY_FOREGROUND_PIXELS, abi.ARRAY_NODE2TERM_OFFSET, abi.ARRAY_NODE2TERM_INDEX,
+                abi.ARRAY_HALF_NODEPAIR_KEY, abi.ARRAY_NODEPAIR_TERM_INDEX, abi.ARRAY_NODEPAIR_KEY,
+                abi.ARRAY_NODEPAIR_TERM_RANGE, abi.ARRAY_BLKROW_OFFSET, abi.ARRAY_BINBLOCK_ROWPTR,
+                abi.ARRAY_BINBLOCK_COLPTR]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import multiviewdynrecon_b200 as m
+    m.lib()
+
+
+def make_gpu(scene, precision=abi.PRECISION_MIXED, mode=abi.MODE_MATERIALIZED, **kw):
+    cfg = abi.make_config(scene, precision=precision, mode=mode, **kw)
+    s = NonRigidSolver(cfg)
+    s.set_solver_input(scene)
+    return s, cfg
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint8)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_index_bit_exact(oracle_mod, kind):
+    scene = small_scene(kind)
+    g, cfg = make_gpu(scene)
+    g.build_index()
+    o = oracle_mod.Oracle(scene, cfg)
+    o.build_index()
+    gc, oc = g.counts(), o.counts()
+    assert gc.error_flags == 0
+    for f in ("dense_terms", "smooth_terms", "foreground_terms", "feature_terms", "cross_terms",
+              "node2term_entries", "nodepair_entries", "half_pairs", "num_bins", "binblock_nnz"):
+        assert getattr(gc, f) == getattr(oc, f), f
+    for which in INDEX_ARRAYS:
+        a, b = g.get_array(which), o.get(which)
+        assert a.shape == b.shape, which
+        assert np.array_equal(bits(a), bits(b)), which
+
+
+def _stage_compare(oracle_mod, scene, precision):
+    g, cfg = make_gpu(scene, precision=precision)
+    g.build_index()
+    g.gn_iteration(scene.pcg_iterations)
+    torch.cuda.synchronize()
+    o = oracle_mod.Oracle(scene, cfg)
+    o.build_index()
+    o.eval_terms()
+    return g, o, cfg
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_term_evaluation(oracle_mod, kind):
+    scene = small_scene(kind)
+    g, o, _ = _stage_compare(oracle_mod, scene, abi.PRECISION_MIXED)
+    gj, oj = g.get_array(abi.ARRAY_TERM_JACOBIAN), o.get(abi.ARRAY_TERM_JACOBIAN)
+    assert gj.shape == oj.shape
+    same = gj[:, 7].view(np.uint32) == oj[:, 7].view(np.uint32)
+    assert (~same).sum() <= max(2, int(1e-3 * len(same)))
+    scale = np.abs(oj[same, :7]).max() if same.any() else 1.0
+    assert max_relative_error(gj[same, :7], oj[same, :7], 1e-6 * scale) < 1e-4
+    gs, os_ = g.get_array(abi.ARRAY_SMOOTH_TERMS), o.get(abi.ARRAY_SMOOTH_TERMS)
+    assert np.array_equal(gs[:, 6], os_[:, 6])
+    assert max_relative_error(gs[:, :6], os_[:, :6], 1e-6) < 1e-4
+    gw, ow = g.get_array(abi.ARRAY_WARPED_CORRESPONDENCE), o.get(abi.ARRAY_WARPED_CORRESPONDENCE)
+    assert max_relative_error(gw, ow, 1e-6) < 1e-4
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_FP32])
+def test_assembly_and_pcg(oracle_mod, kind, precision):
+    scene = small_scene(kind)
+    g, o, cfg = _stage_compare(oracle_mod, scene, precision)
+    # the oracle assembles from the GPU's own term data
+    o.set_term_data(g.get_array(abi.ARRAY_TERM_JACOBIAN), g.get_array(abi.ARRAY_SMOOTH_TERMS),
+                    g.get_array(abi.ARRAY_WARPED_CORRESPONDENCE))
+    o.assemble()
+    for which in (abi.ARRAY_DIAG_BLOCKS, abi.ARRAY_JTR, abi.ARRAY_OFFDIAG_BLOCKS):
+        a, b = g.get_array(which), o.get(which, as_double=True)
+        assert a.shape == b.shape, which
+        assert max_relative_error(a, b, 1e-6 * np.abs(b).max()) < 1e-4, which
+    bb_g, bb_o = g.get_array(abi.ARRAY_BINBLOCK_DATA), o.get(abi.ARRAY_BINBLOCK_DATA, as_double=True)
+    assert max_relative_error(bb_g, bb_o, 1e-6 * np.abs(bb_o).max()) < 1e-4
+    # preconditioner: M^-1 D = I per block
+    D = g.get_array(abi.ARRAY_DIAG_BLOCKS).reshape(-1, 6, 6).astype(np.float64)
+    M = g.get_array(abi.ARRAY_PRECONDITIONER).reshape(-1, 6, 6).astype(np.float64)
+    eye_err = np.abs(M @ D - np.eye(6)).max()
+    assert eye_err < (1e-3 if precision == abi.PRECISION_FP32 else 1e-4)
+    # PCG increment vs the FP64 oracle on the same system
+    o64 = oracle_mod.Oracle(scene, cfg, fp64=True)
+    o64.build_index()
+    o64.eval_terms()
+    o64.set_term_data(g.get_array(abi.ARRAY_TERM_JACOBIAN), g.get_array(abi.ARRAY_SMOOTH_TERMS),
+                      g.get_array(abi.ARRAY_WARPED_CORRESPONDENCE))
+    o64.assemble()
+    o64.pcg(scene.pcg_iterations)
+    x64 = o64.get(abi.ARRAY_INCREMENT, as_double=True)
+    xg = g.get_array(abi.ARRAY_INCREMENT)
+    tol = 1e-4 if precision == abi.PRECISION_MIXED else 2e-3
+    assert rel_norm_error(xg, x64) < tol
+    # update from the GPU's increment
+    o.set_increment(xg.reshape(-1))
+    o.update()
+    assert max_relative_error(g.get_array(abi.ARRAY_NODE_SE3), o.get(abi.ARRAY_NODE_SE3), 1e-6) < 1e-4
+
+
+@pytest.mark.parametrize("kind", ["sphere", "torso", "body"])
+def test_solve_vs_fp64_oracle(oracle_mod, kind):
+    """Every Gauss-Newton increment of the mixed-precision solve against the
+    FP64 oracle run from the same warp field, with the discrete projection and
+    validity choices taken from the GPU run."""
+    scene = small_scene(kind)
+    g, cfg = make_gpu(scene, precision=abi.PRECISION_MIXED)
+    g.build_index()
+    o64 = oracle_mod.Oracle(scene, cfg, fp64=True)
+    o64.build_index()
+    energies = []
+    for it in range(scene.gn_iterations):
+        g.gn_iteration(scene.pcg_iterations)
+        torch.cuda.synchronize()
+        jr, sm = g.get_array(abi.ARRAY_TERM_JACOBIAN), g.get_array(abi.ARRAY_SMOOTH_TERMS)
+        o64.freeze(jr, sm)
+        o64.eval_terms()
+        o64.assemble()
+        energies.append((g.energy(), o64.energy()))
+        o64.pcg(scene.pcg_iterations)
+        x64 = o64.get(abi.ARRAY_INCREMENT, as_double=True)
+        xg = g.get_array(abi.ARRAY_INCREMENT)
+        assert rel_norm_error(xg, x64) < 1e-4, it
+        o64.update()
+    for eg, eo in energies:
+        assert abs(eg - eo) <= 1e-4 * abs(eo)
+    assert energies[-1][0] < energies[0][0]
+
+
+@pytest.mark.parametrize("kind", ["sphere", "torso"])
+def test_matrix_free_equals_materialized(oracle_mod, kind):
+    scene = small_scene(kind)
+    a, _ = make_gpu(scene, mode=abi.MODE_MATERIALIZED)
+    b, _ = make_gpu(scene, mode=abi.MODE_MATRIX_FREE)
+    for s in (a, b):
+        s.build_index()
+        s.gn_iteration(scene.pcg_iterations)
+    torch.cuda.synchronize()
+    x = torch.randn(6 * scene.num_nodes, device="cuda")
+    ya, yb = a.apply_jtj(x), b.apply_jtj(x)
+    assert rel_norm_error(yb.cpu().numpy(), ya.cpu().numpy()) < 1e-5
+    assert rel_norm_error(b.get_array(abi.ARRAY_INCREMENT), a.get_array(abi.ARRAY_INCREMENT)) < 1e-4
+    # and both equal the oracle's assembled operator
+    o = oracle_mod.Oracle(scene, abi.make_config(scene), fp64=True)
+    o.build_index()
+    o.eval_terms()
+    o.set_term_data(a.get_array(abi.ARRAY_TERM_JACOBIAN), a.get_array(abi.ARRAY_SMOOTH_TERMS),
+                    a.get_array(abi.ARRAY_WARPED_CORRESPONDENCE))
+    o.assemble()
+    yo = o.apply_jtj(x.cpu().numpy().astype(np.float64))
+    assert rel_norm_error(ya.cpu().numpy(), yo) < 1e-5
+
+
+def test_batch_graph_and_determinism():
+    """Uneven instances in one batch give bit-identical results to solving them
+    one by one; the graph replay equals direct launches; reruns are identical."""
+    scenes = [small_scene("torso"), small_scene("sphere"), small_scene("body")]
+    n = max(s.num_nodes for s in scenes)
+    caps = dict(max_nodes=n, max_views=3, width=192, height=120, use_foreground=True, use_feature=True,
+                use_cross_view=True, max_surfels=max(s.num_surfels for s in scenes),
+                max_feature_terms=max(s.feature.count for s in scenes),
+                max_cross_terms=max(s.cross_view.count for s in scenes))
+
+    def pad(scene):
+        # bring every scene to the batch image size (zero / invalid padding)
+        from copy import copy
+        s2 = copy(scene)
+        views = []
+        for v in scene.views:
+            def p(a, fill):
+                out = np.full((120, 192) + a.shape[2:], fill, a.dtype)
+                out[:a.shape[0], :a.shape[1]] = a
+                return out
+            from dataclasses import replace
+            views.append(replace(v, reference_vertex_map=p(v.reference_vertex_map, 0),
+                                 reference_normal_map=p(v.reference_normal_map, 0),
+                                 index_map=p(v.index_map, 0xFFFFFFFF),
+                                 vertex_confidence_map=p(v.vertex_confidence_map, 0),
+                                 normal_radius_map=p(v.normal_radius_map, 0),
+                                 filtered_foreground_mask=p(v.filtered_foreground_mask, 0),
+                                 foreground_mask_gradient=p(v.foreground_mask_gradient, 0)))
+        s2.views = views
+        s2.width, s2.height = 192, 120
+        return s2
+
+    padded = [pad(s) for s in scenes]
+    cfg = abi.make_config(None, **caps)
+    batch = BatchSolver(cfg, len(padded))
+    for i, s in enumerate(padded):
+        batch.set_input(i, s)
+    batch.solve(3, 10, use_graph=False)
+    direct = [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
+    batch.solve(3, 10, use_graph=True)
+    graph = [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
+    batch.solve(3, 10, use_graph=True)
+    again = [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
+    for i, s in enumerate(padded):
+        single = NonRigidSolver(cfg)
+        single.set_solver_input(s)
+        single.solve_non_rigid_alignment(3, 10)
+        ref = single.solved_node_se3().cpu().numpy()
+        assert np.array_equal(bits(direct[i]), bits(ref)), i
+        assert np.array_equal(bits(graph[i]), bits(ref)), i
+        assert np.array_equal(bits(again[i]), bits(ref)), i
+
+
+def test_host_inputs_match_device_inputs():
+    scene = small_scene("torso")
+    a, cfg = make_gpu(scene)
+    a.solve_non_rigid_alignment(2, 10)
+    b = NonRigidSolver(cfg)
+    b.set_solver_input_host(DeviceScene(scene, pin=True))
+    b.solve_non_rigid_alignment(2, 10)
+    assert np.array_equal(bits(a.solved_node_se3().cpu().numpy()), bits(b.solved_node_se3().cpu().numpy()))
+
+
+def test_capacity_overflow_is_reported():
+    from multiviewdynrecon_b200 import MvdrError
+    scene = small_scene("sphere")
+    cfg = abi.make_config(scene)
+    cfg.max_terms_per_node = 16  # far below the real per-node term count
+    s = NonRigidSolver(cfg)
+    s.set_solver_input(scene)
+    s.solve_non_rigid_alignment(1, 2)
+    with pytest.raises(MvdrError) as e:
+        s.solved_node_se3()
+    assert e.value.status == abi.MVDR_ECAPACITY
+    # the context stays usable
+    ok, _ = make_gpu(scene)
+    ok.solve_non_rigid_alignment(1, 2)
+    ok.solved_node_se3()
