@@ -211,7 +211,7 @@ __device__ inline void gauss_jordan6(const float* Din, float* out) {
 }
 
 // 6x6 Cholesky in double; packed lower triangle L[i(i+1)/2 + j], j <= i
-__device__ inline void cholesky6(const float* A, double* L) {
+template <class T> __device__ inline void cholesky6(const T* A, double* L) {
     for (int j = 0; j < 6; ++j) {
         double s = A[6 * j + j];
         for (int k = 0; k < j; ++k) s -= L[j * (j + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
@@ -243,8 +243,25 @@ __device__ inline void cholesky6_solve(const double* L, const double* b, double*
     }
 }
 
+// Compensated block storage of mixed precision: a block element a is kept as
+// hi = fl32(a) and a 16-bit correction s with a = hi (1 + s 2^-24), so the
+// SpMV sees the operator to about 35 significant bits for 6 extra bytes per
+// element (rounding the assembled JtJ to float alone moves the PCG increment
+// by ~1e-4 on these blocks, whose condition numbers reach 1e5).
+constexpr double kLoScale = 16777216.0;            // 2^24
+constexpr double kLoUnscale = 5.9604644775390625e-8;  // 2^-24
+
+__device__ inline void store_split(double a, float* hi, __half* lo) {
+    const float h = (float)a;
+    float sc = 0.f;
+    if (h != 0.f) sc = (float)((a - (double)h) / (double)h * kLoScale);
+    *hi = h;
+    *lo = __float2half_rn(sc);
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
+    using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs) return;
@@ -252,48 +269,49 @@ __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mv
     off.load(C);
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
-        float acc[27];
+        Acc acc[27];
 #pragma unroll
-        for (int i = 0; i < 27; ++i) acc[i] = 0.f;
+        for (int i = 0; i < 27; ++i) acc[i] = 0;
         const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
         for (uint32_t p = b + lane_id(); p < e; p += 32) {
             TermRows tr;
             const int ch = term_rows(I, off, lam, I.n2t_index[p], node, tr);
-            const float sd = tr.lam2 * tr.w * tr.w;
-            const float sb = tr.lam2 * tr.w;
+            const Acc sd = (Acc)tr.lam2 * (Acc)tr.w * (Acc)tr.w;
+            const Acc sb = (Acc)tr.lam2 * (Acc)tr.w;
             for (int c = 0; c < ch; ++c) {
 #pragma unroll
                 for (int i = 0; i < 6; ++i) {
 #pragma unroll
-                    for (int j = i; j < 6; ++j) acc[upper_index(i, j)] += sd * tr.J[c][i] * tr.J[c][j];
-                    acc[21 + i] -= sb * tr.J[c][i] * tr.r[c];
+                    for (int j = i; j < 6; ++j) acc[upper_index(i, j)] += sd * (Acc)tr.J[c][i] * (Acc)tr.J[c][j];
+                    acc[21 + i] -= sb * (Acc)tr.J[c][i] * (Acc)tr.r[c];
                 }
             }
         }
 #pragma unroll
         for (int i = 0; i < 27; ++i) acc[i] = warp_sum(acc[i]);
-        float D[36];
+        Acc D[36];
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
             for (int j = 0; j < 6; ++j) D[6 * i + j] = acc[i <= j ? upper_index(i, j) : upper_index(j, i)];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) D[7 * i] += 1e-2f;  // PreconditionerBlocked.cu:272-275
+        for (int i = 0; i < 6; ++i) D[7 * i] += (Acc)1e-2f;  // PreconditionerBlocked.cu:272-275
         const uint32_t lane = lane_id();
         // diagonal block: the parity copy and the block of the BSR row
-        float* bsr_blk = I.bsr + 36 * (size_t)(I.blkrow_offset[node] + node);
+        const size_t blk = 36 * (size_t)(I.blkrow_offset[node] + node);
         for (uint32_t i = lane; i < 36; i += 32) {
-            float v = 0.f;
+            Acc v = 0;
 #pragma unroll
             for (int q = 0; q < 36; ++q) v = (q == (int)i) ? D[q] : v;
-            I.diag[36 * (size_t)node + i] = v;
-            bsr_blk[i] = v;
+            I.diag[36 * (size_t)node + i] = (float)v;
+            if (MIXED) store_split((double)v, I.bsr + blk + i, I.bsr_lo + blk + i);
+            else I.bsr[blk + i] = (float)v;
         }
         if (lane < 6) {
-            float v = 0.f;
+            Acc v = 0;
 #pragma unroll
             for (int q = 0; q < 6; ++q) v = (q == (int)lane) ? acc[21 + q] : v;
-            I.jtr[6 * (size_t)node + lane] = v;
+            I.jtr[6 * (size_t)node + lane] = (float)v;
         }
         if (lane == 0) {
             if (MIXED) {
@@ -302,8 +320,10 @@ __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mv
 #pragma unroll
                 for (int i = 0; i < 21; ++i) I.chol[21 * (size_t)node + i] = L[i];
             } else {
-                float Mi[36];
-                gauss_jordan6(D, Mi);
+                float Df[36], Mi[36];
+#pragma unroll
+                for (int i = 0; i < 36; ++i) Df[i] = (float)D[i];
+                gauss_jordan6(Df, Mi);
 #pragma unroll
                 for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
             }
@@ -315,7 +335,9 @@ __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mv
 // warp per unordered pair (i < j): A_ij = sum_t lam^2 w_i w_j J_i J_j^T is
 // written to row i and its transpose to row j (the reference computes both
 // orderings separately, JtJMaterializer.cu:270-365)
+template <bool MIXED>
 __global__ void __launch_bounds__(256) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
+    using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2) return;
@@ -327,37 +349,42 @@ __global__ void __launch_bounds__(256) offdiag_kernel(const InstDesc* insts, mvd
         const uint32_t key = I.half_key[h];
         const uint32_t ni = key / I.enc, nj = key % I.enc;
         const uint2 rg = I.half_range[h];
-        float acc[36];
+        Acc acc[36];
 #pragma unroll
-        for (int i = 0; i < 36; ++i) acc[i] = 0.f;
+        for (int i = 0; i < 36; ++i) acc[i] = 0;
         for (uint32_t p = rg.x + lane_id(); p < rg.y; p += 32) {
             const uint32_t t = I.np_index[p];
             TermRows a, b;
             const int ch = term_rows(I, off, lam, t, ni, a);
             if (ch == 0) continue;
             term_rows(I, off, lam, t, nj, b);
-            const float s = a.lam2 * a.w * b.w;
+            const Acc s = (Acc)a.lam2 * (Acc)a.w * (Acc)b.w;
             for (int c = 0; c < ch; ++c) {
 #pragma unroll
                 for (int r = 0; r < 6; ++r)
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) acc[6 * r + q] += s * a.J[c][r] * b.J[c][q];
+                    for (int q = 0; q < 6; ++q) acc[6 * r + q] += s * (Acc)a.J[c][r] * (Acc)b.J[c][q];
             }
         }
 #pragma unroll
         for (int i = 0; i < 36; ++i) acc[i] = warp_sum(acc[i]);
-        const uint32_t up = I.upper_pos[h] + ni + 1;   // BSR block of (i, j)
-        const uint32_t lo = I.lower_pos[h] + nj + 1;   // BSR block of (j, i)
+        const size_t up = 36 * (size_t)(I.upper_pos[h] + ni + 1);  // BSR block of (i, j)
+        const size_t lo = 36 * (size_t)(I.lower_pos[h] + nj + 1);  // BSR block of (j, i)
         for (uint32_t e = lane_id(); e < 36; e += 32) {
-            float v = 0.f, vt = 0.f;
+            Acc v = 0, vt = 0;
             const uint32_t r = e / 6, q = e % 6;
 #pragma unroll
             for (int z = 0; z < 36; ++z) {
                 v = (z == (int)e) ? acc[z] : v;
                 vt = (z == (int)(6 * q + r)) ? acc[z] : vt;
             }
-            I.bsr[36 * (size_t)up + e] = v;
-            I.bsr[36 * (size_t)lo + e] = vt;
+            if (MIXED) {
+                store_split((double)v, I.bsr + up + e, I.bsr_lo + up + e);
+                store_split((double)vt, I.bsr + lo + e, I.bsr_lo + lo + e);
+            } else {
+                I.bsr[up + e] = (float)v;
+                I.bsr[lo + e] = (float)vt;
+            }
         }
     }
 }
@@ -442,6 +469,46 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
     }
 }
 
+// One scalar row of y = A x over the row-major 6x6 BSR blocks of block row
+// `br`; x[c] = xs[c] + beta xp[c] (xp may be null). Mixed precision reads the
+// compensated blocks and accumulates in double.
+template <bool MIXED>
+__device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, const float* xs, const float* xp,
+                                float beta) {
+    const uint32_t mask = I.enc - 1;
+    const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
+    size_t blk = 36 * (size_t)(so + br) + 6 * r;
+    typename std::conditional<MIXED, double, float>::type acc = 0;
+    for (uint32_t s = so; s <= se; ++s, blk += 36) {
+        const uint32_t col = (s == so) ? br : (I.sym_key[s - 1] & mask);
+        const float* a = I.bsr + blk;
+        const float2 a01 = *reinterpret_cast<const float2*>(a);
+        const float2 a23 = *reinterpret_cast<const float2*>(a + 2);
+        const float2 a45 = *reinterpret_cast<const float2*>(a + 4);
+        const float av[6] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y};
+        float xv[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const size_t e = 6 * (size_t)col + k;
+            xv[k] = xp ? xs[e] + beta * xp[e] : xs[e];
+        }
+        if (MIXED) {
+            const __half2* l = reinterpret_cast<const __half2*>(I.bsr_lo + blk);
+            const float2 l01 = __half22float2(l[0]), l23 = __half22float2(l[1]), l45 = __half22float2(l[2]);
+            const float lv[6] = {l01.x, l01.y, l23.x, l23.y, l45.x, l45.y};
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const double ak = (double)av[k] * (1.0 + (double)lv[k] * kLoUnscale);
+                acc += ak * (double)xv[k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
+        }
+    }
+    return (float)acc;
+}
+
 // q = A d with d = s + beta d_prev formed on the fly (BlockPCG.cuh:167-181 fused
 // into the SpMV of the next iteration); d.q partial; alpha = delta / d.q.
 // Six threads per block row (one per scalar row), row-major 6x6 blocks.
@@ -452,31 +519,13 @@ __global__ void __launch_bounds__(192) pcg_spmv_kernel(const InstDesc* insts, in
     const float* dprev = parity ? I.d0 : I.d1;
     float* dcur = parity ? I.d1 : I.d0;
     const float beta = (float)I.scalars[2];
-    const uint32_t mask = I.enc - 1;
     T part = 0;
     const uint32_t rows_per_cta = blockDim.x / 6;
     for (uint32_t base = blockIdx.x * rows_per_cta; base < I.N; base += gridDim.x * rows_per_cta) {
         const uint32_t br = base + threadIdx.x / 6;
         const uint32_t r = threadIdx.x % 6;
         if (threadIdx.x < rows_per_cta * 6 && br < I.N) {
-            const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
-            const float* blk = I.bsr + 36 * (size_t)(so + br) + 6 * r;
-            float acc = 0.f;
-            // diagonal block
-            {
-                const float* xs = I.s + 6 * (size_t)br;
-                const float* xp = dprev + 6 * (size_t)br;
-#pragma unroll
-                for (int k = 0; k < 6; ++k) acc += blk[k] * (xs[k] + beta * xp[k]);
-            }
-            blk += 36;
-            for (uint32_t s = so; s < se; ++s, blk += 36) {
-                const uint32_t col = I.sym_key[s] & mask;
-                const float* xs = I.s + 6 * (size_t)col;
-                const float* xp = dprev + 6 * (size_t)col;
-#pragma unroll
-                for (int k = 0; k < 6; ++k) acc += blk[k] * (xs[k] + beta * xp[k]);
-            }
+            const float acc = bsr_row<MIXED>(I, br, r, I.s, dprev, beta);
             const size_t e = 6 * (size_t)br + r;
             const float dv = I.s[e] + beta * dprev[e];
             dcur[e] = dv;
@@ -547,8 +596,10 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
 // ------------------------------------------------------ matrix-free JtJ ---
 // J.p per term (ApplyJacobianDot.cu:127-198): jp[3t + c] for each channel,
 // with p = s + beta * d_prev formed on the fly when `fused` is set
+template <bool MIXED>
 __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
                                                       mvdr_penalty lam) {
+    using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
     if (bad_inputs(I)) return;
     TermOffsets off;
@@ -563,7 +614,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
         const ushort4 nn = term_nodes(I, ty, k);
         const unsigned short nodes[4] = {nn.x, nn.y, nn.z, nn.w};
         const int m = ty == kSmooth ? 2 : 4;
-        float out[3] = {0.f, 0.f, 0.f};
+        Acc out[3] = {0, 0, 0};
         for (int q = 0; q < m; ++q) {
             const uint32_t node = nodes[q];
             if (node >= I.N) continue;
@@ -576,15 +627,23 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
                 p[i] = fused ? s[e] + beta * dp[e] : s[e];
             }
             for (int c = 0; c < ch; ++c) {
-                float a = 0.f;
+                Acc a = 0;
 #pragma unroll
-                for (int i = 0; i < 6; ++i) a += tr.J[c][i] * p[i];
-                out[c] += tr.w * a;
+                for (int i = 0; i < 6; ++i) a += (Acc)tr.J[c][i] * (Acc)p[i];
+                out[c] += (Acc)tr.w * a;
             }
         }
-        I.jp[3 * (size_t)t] = out[0];
-        I.jp[3 * (size_t)t + 1] = out[1];
-        I.jp[3 * (size_t)t + 2] = out[2];
+        // mixed precision keeps J.p in double (jp holds 3 doubles per term)
+        if (MIXED) {
+            double* jp = reinterpret_cast<double*>(I.jp);
+            jp[3 * (size_t)t] = out[0];
+            jp[3 * (size_t)t + 1] = out[1];
+            jp[3 * (size_t)t + 2] = out[2];
+        } else {
+            I.jp[3 * (size_t)t] = (float)out[0];
+            I.jp[3 * (size_t)t + 1] = (float)out[1];
+            I.jp[3 * (size_t)t + 2] = (float)out[2];
+        }
     }
 }
 
@@ -604,31 +663,32 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
     T part = 0;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
-        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        T acc[6] = {0, 0, 0, 0, 0, 0};
         const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        const double* jpd = reinterpret_cast<const double*>(I.jp);
         for (uint32_t p = b + lane_id(); p < e; p += 32) {
             const uint32_t t = I.n2t_index[p];
             TermRows tr;
             const int ch = term_rows(I, off, lam, t, node, tr);
-            const float sc = tr.lam2 * tr.w;
+            const T sc = (T)tr.lam2 * (T)tr.w;
             for (int c = 0; c < ch; ++c) {
-                const float y = I.jp[3 * (size_t)t + c];
+                const T y = MIXED ? (T)jpd[3 * (size_t)t + c] : (T)I.jp[3 * (size_t)t + c];
 #pragma unroll
-                for (int i = 0; i < 6; ++i) acc[i] += sc * tr.J[c][i] * y;
+                for (int i = 0; i < 6; ++i) acc[i] += sc * (T)tr.J[c][i] * y;
             }
         }
 #pragma unroll
         for (int i = 0; i < 6; ++i) acc[i] = warp_sum(acc[i]);
         const uint32_t lane = lane_id();
         if (lane < 6) {
-            float a = 0.f;
+            T a = 0;
 #pragma unroll
             for (int q = 0; q < 6; ++q) a = (q == (int)lane) ? acc[q] : a;
             const size_t el = 6 * (size_t)node + lane;
             float dv;
             if (pcg) dv = I.s[el] + beta * dprev[el];
             else dv = xin[el];
-            const float qv = a + 1e-2f * dv;
+            const float qv = (float)(a + (T)1e-2f * (T)dv);
             if (pcg) {
                 dcur[el] = dv;
                 I.q[el] = qv;
@@ -649,26 +709,15 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
 }
 
 // y = A x with the materialised operator (no PCG side effects)
+template <bool MIXED>
 __global__ void __launch_bounds__(192) bsr_apply_kernel(const InstDesc* insts, const float* xin, float* yout) {
     const InstDesc& I = insts[blockIdx.y];
-    const uint32_t mask = I.enc - 1;
     const uint32_t rows_per_cta = blockDim.x / 6;
     for (uint32_t base = blockIdx.x * rows_per_cta; base < I.N; base += gridDim.x * rows_per_cta) {
         const uint32_t br = base + threadIdx.x / 6;
         const uint32_t r = threadIdx.x % 6;
         if (threadIdx.x >= rows_per_cta * 6 || br >= I.N) continue;
-        const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
-        const float* blk = I.bsr + 36 * (size_t)(so + br) + 6 * r;
-        float acc = 0.f;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) acc += blk[k] * xin[6 * (size_t)br + k];
-        blk += 36;
-        for (uint32_t s = so; s < se; ++s, blk += 36) {
-            const uint32_t col = I.sym_key[s] & mask;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) acc += blk[k] * xin[6 * (size_t)col + k];
-        }
-        yout[6 * (size_t)br + r] = acc;
+        yout[6 * (size_t)br + r] = bsr_row<MIXED>(I, br, r, xin, nullptr, 0.f);
     }
 }
 
@@ -825,7 +874,8 @@ cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty
     else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 256, 0, st, d, lam);
     if (materialize) {
         const uint32_t gp = min((lc.cap_pairs + 7) / 8, (uint32_t)lc.sm_count * 16);
-        MVDR_LAUNCH(offdiag_kernel, grid2(gp, lc.B), 256, 0, st, d, lam);
+        if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 256, 0, st, d, lam);
+        else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 256, 0, st, d, lam);
     }
     return cudaGetLastError();
 }
@@ -848,7 +898,8 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
         const int parity = (int)(it & 1u);
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
             // J.(s + beta d_prev) per term, then Jt per node (+ damping, d, q, d.q)
-            MVDR_LAUNCH(apply_j_kernel, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
+            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
+            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
             if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
         } else {
@@ -874,7 +925,8 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             break;
         case MVDR_STAGE_OFFDIAG: {
             const uint32_t gp = min((lc.cap_pairs + 7) / 8, (uint32_t)lc.sm_count * 16);
-            MVDR_LAUNCH(offdiag_kernel, grid2(gp, lc.B), 256, 0, st, d, lam);
+            if (mixed) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 256, 0, st, d, lam);
+            else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 256, 0, st, d, lam);
             break;
         }
         case MVDR_STAGE_SPMV:
@@ -902,10 +954,18 @@ cudaError_t launch_apply_jtj(const LaunchCfg& lc, InstDesc* d, const mvdr_penalt
     // single instance view: d points at the instance's descriptor, B = 1
     if (lc.mode == MVDR_MODE_MATRIX_FREE) {
         const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-        MVDR_LAUNCH(apply_j_kernel, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
-        MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
+        if (lc.precision == MVDR_PRECISION_MIXED) {
+            MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
+            MVDR_LAUNCH(apply_jt_kernel<true>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
+        } else {
+            MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
+            MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
+        }
     } else {
-        MVDR_LAUNCH(bsr_apply_kernel, grid2((lc.max_nodes + 31) / 32, 1), 192, 0, st, d, x, y);
+        if (lc.precision == MVDR_PRECISION_MIXED)
+            MVDR_LAUNCH(bsr_apply_kernel<true>, grid2((lc.max_nodes + 31) / 32, 1), 192, 0, st, d, x, y);
+        else
+            MVDR_LAUNCH(bsr_apply_kernel<false>, grid2((lc.max_nodes + 31) / 32, 1), 192, 0, st, d, x, y);
     }
     return cudaGetLastError();
 }

@@ -8,6 +8,7 @@
 // synchronisation and can be captured once as a CUDA graph.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -255,6 +256,7 @@ struct InstDesc {
     double* chol;           // [21N] Cholesky factors (mixed precision)
     float* jtr;             // [6N]
     float* bsr;             // [(N + 2P cap) * 36] row-major blocks, diagonal first per row
+    __half* bsr_lo;         // mixed precision: per-element correction, a = hi (1 + lo 2^-24)
     // pcg vectors [6N each]
     float* x;
     float* r;

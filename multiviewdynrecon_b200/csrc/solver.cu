@@ -177,13 +177,15 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.chol = a.take<double>(21 * N);
     I.jtr = a.take<float>(6 * N);
     I.bsr = a.take<float>(36 * (N + 2 * (size_t)lc.cap_pairs));
+    I.bsr_lo = lc.precision == MVDR_PRECISION_MIXED ? a.take<__half>(36 * (N + 2 * (size_t)lc.cap_pairs)) : nullptr;
     I.x = a.take<float>(6 * N);
     I.r = a.take<float>(6 * N);
     I.s = a.take<float>(6 * N);
     I.q = a.take<float>(6 * N);
     I.d0 = a.take<float>(6 * N);
     I.d1 = a.take<float>(6 * N);
-    I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(3 * (size_t)lc.cap_terms) : nullptr;
+    // J.p per scalar term of the matrix-free operator (double in mixed precision)
+    I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
     I.scalars = a.take<double>(8);
     I.partials = a.take<double>(partial_slots);
     I.energy = a.take<double>(64);

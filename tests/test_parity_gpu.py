@@ -110,11 +110,15 @@ def test_assembly_and_pcg(oracle_mod, kind, precision):
         assert max_relative_error(a, b, 1e-6 * np.abs(b).max()) < 1e-4, which
     bb_g, bb_o = g.get_array(abi.ARRAY_BINBLOCK_DATA), o.get(abi.ARRAY_BINBLOCK_DATA, as_double=True)
     assert max_relative_error(bb_g, bb_o, 1e-6 * np.abs(bb_o).max()) < 1e-4
-    # preconditioner: M^-1 D = I per block
+    # preconditioner: M D = I per block, to the accuracy the block's condition
+    # number allows in the arithmetic used (float Gauss-Jordan or double
+    # Cholesky rounded to float for the export)
     D = g.get_array(abi.ARRAY_DIAG_BLOCKS).reshape(-1, 6, 6).astype(np.float64)
     M = g.get_array(abi.ARRAY_PRECONDITIONER).reshape(-1, 6, 6).astype(np.float64)
-    eye_err = np.abs(M @ D - np.eye(6)).max()
-    assert eye_err < (1e-3 if precision == abi.PRECISION_FP32 else 1e-4)
+    eye_err = np.abs(M @ D - np.eye(6)).max(axis=(1, 2))
+    cond = np.linalg.cond(D)
+    bound = (200.0 if precision == abi.PRECISION_FP32 else 20.0) * cond * 2.0 ** -24 + 1e-6
+    assert (eye_err <= bound).all(), (eye_err / bound).max()
     # PCG increment vs the FP64 oracle on the same system
     o64 = oracle_mod.Oracle(scene, cfg, fp64=True)
     o64.build_index()
@@ -221,14 +225,18 @@ def test_batch_graph_and_determinism():
     padded = [pad(s) for s in scenes]
     cfg = abi.make_config(None, **caps)
     batch = BatchSolver(cfg, len(padded))
-    for i, s in enumerate(padded):
-        batch.set_input(i, s)
-    batch.solve(3, 10, use_graph=False)
-    direct = [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
-    batch.solve(3, 10, use_graph=True)
-    graph = [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
-    batch.solve(3, 10, use_graph=True)
-    again = [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
+    dev = [DeviceScene(s) for s in padded]
+
+    def run(use_graph):
+        # binding the inputs resets every warp field to its initial value
+        for i, ds in enumerate(dev):
+            batch.set_input(i, ds)
+        batch.solve(3, 10, use_graph=use_graph)
+        return [batch.node_se3(i).cpu().numpy() for i in range(len(padded))]
+
+    direct = run(False)
+    graph = run(True)
+    again = run(True)
     for i, s in enumerate(padded):
         single = NonRigidSolver(cfg)
         single.set_solver_input(s)
