@@ -259,61 +259,205 @@ __device__ inline void store_split(double a, float* hi, __half* lo) {
     *lo = __float2half_rn(sc);
 }
 
+// ------------------------------- element-parallel block accumulation -----
+// A warp stages up to 32 terms of one node (diagonal block) or one node pair
+// (off-diagonal block) in shared memory as compact descriptors, then each
+// lane accumulates the block element(s) it owns over the staged terms. The
+// per-lane state is one or two accumulators, so occupancy stays high, and the
+// kind of the staged term is the same for every lane, so the inner loop does
+// not diverge.
+//
+// Twist Jacobian row of a point-to-point or smooth residual at point p
+// (geometry_icp_jacobian.cuh:91-120, 323-343): f_c(p) = [row c of [p]x^T ; e_c].
+// f_c(p)[r] = coef * P[sel] with P = (p.x, p.y, p.z, 1).
+struct RowSel {
+    int sel[3];
+    float coef[3];
+};
+
+__device__ inline RowSel make_rowsel(int r) {
+    RowSel o;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (r >= 3) {
+            o.sel[c] = 3;
+            o.coef[c] = (r - 3 == c) ? 1.f : 0.f;
+        } else {
+            const int d = (r - c + 3) % 3;
+            o.sel[c] = d == 1 ? (c + 2) % 3 : (c + 1) % 3;
+            o.coef[c] = d == 0 ? 0.f : (d == 1 ? 1.f : -1.f);
+        }
+    }
+    return o;
+}
+
+enum : uint32_t { kStageNone = 0, kStageScalar = 1, kStageP2P = 2, kStageSmooth = 3 };
+constexpr int kStageFloats = 16;
+
+// Stage descriptor of term t as seen from node `ni` (and `nj` for a pair):
+//  [0] kind  [1] s1  [2] s2  [3..8] six values  [9..11] three values
+//  scalar : s1 = lam^2 w_i w_j (pair) or lam^2 w^2 (diag), s2 = lam^2 w, [3..8] J, [9] r
+//  p2p    : s1 as scalar, s2 = lam^2 w, [3..5] p, [6..8] huber weights, [9..11] raw residual
+//  smooth : s1 = lam^2, pair: [3..5] p_i, [6..8] p_j; diag: [3..5] p, [6] sign, [9..11] r
+__device__ inline void stage_term(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
+                                  uint32_t ni, uint32_t nj, bool pair, float* o) {
+    uint32_t k;
+    const TermType ty = off.typed(t, k);
+    o[0] = __uint_as_float(kStageNone);
+    o[1] = 0.f;
+    switch (ty) {
+        case kDense:
+        case kForeground: {
+            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+            const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+            const ushort4 kn = term_nodes(I, ty, k);
+            const float4 w4 = term_weights(I, ty, k);
+            const float l2 = ty == kDense ? 1.0f : lam.foreground * lam.foreground;
+            const float wi = weight_of(kn, w4, ni);
+            const float wj = pair ? weight_of(kn, w4, nj) : wi;
+            o[0] = __uint_as_float(kStageScalar);
+            o[1] = l2 * wi * wj;
+            o[2] = l2 * wi;
+            o[3] = a.x; o[4] = a.y; o[5] = a.z; o[6] = a.w; o[7] = b.x; o[8] = b.y;
+            o[9] = b.z;
+            break;
+        }
+        case kSmooth: {
+            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            if (b.z == 0.f) break;
+            const bool is_i = ni == I.graph[k].x;
+            const float ti[3] = {a.x, a.y, a.z}, tj[3] = {a.w, b.x, b.y};
+            o[0] = __uint_as_float(kStageSmooth);
+            o[1] = lam.smooth * lam.smooth;
+            if (pair) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    o[3 + q] = is_i ? ti[q] : tj[q];
+                    o[6 + q] = is_i ? tj[q] : ti[q];
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    o[3 + q] = is_i ? ti[q] : tj[q];
+                    o[9 + q] = ti[q] - tj[q];
+                }
+                o[6] = is_i ? 1.f : -1.f;
+            }
+            break;
+        }
+        case kFeature:
+        case kCross: {
+            const bool f = ty == kFeature;
+            const float4 wv = I.warped[f ? k : I.Tp + k];
+            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const ushort4 kn = term_nodes(I, ty, k);
+            const float4 w4 = term_weights(I, ty, k);
+            const float l2 = f ? lam.feature * lam.feature : lam.cross_view * lam.cross_view;
+            const float wi = weight_of(kn, w4, ni);
+            const float wj = pair ? weight_of(kn, w4, nj) : wi;
+            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+            o[0] = __uint_as_float(kStageP2P);
+            o[1] = l2 * wi * wj;
+            o[2] = l2 * wi;
+            o[3] = wv.x; o[4] = wv.y; o[5] = wv.z;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                o[6 + q] = huber_weight(raw[q]);
+                o[9 + q] = raw[q];
+            }
+            break;
+        }
+        default: break;
+    }
+}
+
+// f_c(P)[row] for the lane's row selection
+__device__ inline float frow(const RowSel& rs, int c, const float* p) {
+    const int sl = rs.sel[c];
+    return rs.coef[c] * (sl == 3 ? 1.f : p[sl]);
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
+    __shared__ float stage[8][32][kStageFloats];
+    __shared__ Acc blockv[8][28];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs) return;
     TermOffsets off;
     off.load(C);
+    const uint32_t w = threadIdx.x >> 5, lane = lane_id();
+    // lane -> element: lanes 0..20 the upper triangle (r <= k) of D, 21..26 b
+    int er = 0, ek = 0;
+    {
+        int e = 0;
+        for (int r = 0; r < 6; ++r)
+            for (int k2 = r; k2 < 6; ++k2, ++e)
+                if (e == (int)lane) { er = r; ek = k2; }
+        if (lane >= 21 && lane < 27) { er = lane - 21; ek = er; }
+    }
+    const bool is_d = lane < 21, is_b = lane >= 21 && lane < 27;
+    const RowSel rr = make_rowsel(er), rk = make_rowsel(ek);
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
-        Acc acc[27];
-#pragma unroll
-        for (int i = 0; i < 27; ++i) acc[i] = 0;
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + w; node < I.N; node += warps) {
+        Acc acc = 0;
         const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
-        for (uint32_t p = b + lane_id(); p < e; p += 32) {
-            TermRows tr;
-            const int ch = term_rows(I, off, lam, I.n2t_index[p], node, tr);
-            const Acc sd = (Acc)tr.lam2 * (Acc)tr.w * (Acc)tr.w;
-            const Acc sb = (Acc)tr.lam2 * (Acc)tr.w;
-            for (int c = 0; c < ch; ++c) {
+        for (uint32_t base = b; base < e; base += 32) {
+            const uint32_t p = base + lane;
+            float* my = stage[w][lane];
+            if (p < e) stage_term(I, off, lam, I.n2t_index[p], node, node, false, my);
+            else my[0] = __uint_as_float(kStageNone);
+            __syncwarp();
+            const uint32_t n = min(32u, e - base);
+            for (uint32_t q = 0; q < n; ++q) {
+                const float* d = stage[w][q];
+                const uint32_t kind = __float_as_uint(d[0]);
+                if (kind == kStageScalar) {
+                    if (is_d) acc += (Acc)d[1] * (Acc)d[3 + er] * (Acc)d[3 + ek];
+                    else if (is_b) acc -= (Acc)d[2] * (Acc)d[3 + er] * (Acc)d[9];
+                } else if (kind == kStageP2P) {
+                    const float* pp = d + 3;
 #pragma unroll
-                for (int i = 0; i < 6; ++i) {
+                    for (int c = 0; c < 3; ++c) {
+                        const Acc h2 = (Acc)d[6 + c] * (Acc)d[6 + c];
+                        if (is_d) acc += (Acc)d[1] * h2 * (Acc)frow(rr, c, pp) * (Acc)frow(rk, c, pp);
+                        else if (is_b) acc -= (Acc)d[2] * h2 * (Acc)d[9 + c] * (Acc)frow(rr, c, pp);
+                    }
+                } else if (kind == kStageSmooth) {
+                    const float* pp = d + 3;
 #pragma unroll
-                    for (int j = i; j < 6; ++j) acc[upper_index(i, j)] += sd * (Acc)tr.J[c][i] * (Acc)tr.J[c][j];
-                    acc[21 + i] -= sb * (Acc)tr.J[c][i] * (Acc)tr.r[c];
+                    for (int c = 0; c < 3; ++c) {
+                        if (is_d) acc += (Acc)d[1] * (Acc)frow(rr, c, pp) * (Acc)frow(rk, c, pp);
+                        else if (is_b) acc -= (Acc)d[1] * (Acc)d[6] * (Acc)frow(rr, c, pp) * (Acc)d[9 + c];
+                    }
                 }
             }
+            __syncwarp();
         }
-#pragma unroll
-        for (int i = 0; i < 27; ++i) acc[i] = warp_sum(acc[i]);
-        Acc D[36];
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-            for (int j = 0; j < 6; ++j) D[6 * i + j] = acc[i <= j ? upper_index(i, j) : upper_index(j, i)];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) D[7 * i] += (Acc)1e-2f;  // PreconditionerBlocked.cu:272-275
-        const uint32_t lane = lane_id();
+        if (is_d && er == ek) acc += (Acc)1e-2f;  // PreconditionerBlocked.cu:272-275
+        if (lane < 27) blockv[w][lane] = acc;
+        __syncwarp();
         // diagonal block: the parity copy and the block of the BSR row
         const size_t blk = 36 * (size_t)(I.blkrow_offset[node] + node);
         for (uint32_t i = lane; i < 36; i += 32) {
-            Acc v = 0;
-#pragma unroll
-            for (int q = 0; q < 36; ++q) v = (q == (int)i) ? D[q] : v;
+            const int r = i / 6, k2 = i % 6;
+            const int lo = min(r, k2), hi = max(r, k2);
+            const Acc v = blockv[w][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
             I.diag[36 * (size_t)node + i] = (float)v;
             if (MIXED) store_split((double)v, I.bsr + blk + i, I.bsr_lo + blk + i);
             else I.bsr[blk + i] = (float)v;
         }
-        if (lane < 6) {
-            Acc v = 0;
-#pragma unroll
-            for (int q = 0; q < 6; ++q) v = (q == (int)lane) ? acc[21 + q] : v;
-            I.jtr[6 * (size_t)node + lane] = (float)v;
-        }
+        if (is_b) I.jtr[6 * (size_t)node + er] = (float)acc;
         if (lane == 0) {
+            Acc D[36];
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+#pragma unroll
+                for (int k2 = 0; k2 < 6; ++k2) {
+                    const int lo = r < k2 ? r : k2, hi = r < k2 ? k2 : r;
+                    D[6 * r + k2] = blockv[w][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
+                }
             if (MIXED) {
                 double L[21];
                 cholesky6(D, L);
@@ -328,62 +472,86 @@ __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mv
                 for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
             }
         }
+        __syncwarp();
     }
 }
 
 // --------------------------------------------------- off-diagonal blocks --
-// warp per unordered pair (i < j): A_ij = sum_t lam^2 w_i w_j J_i J_j^T is
-// written to row i and its transpose to row j (the reference computes both
-// orderings separately, JtJMaterializer.cu:270-365)
+// warp per unordered pair (i < j): A_ij(r, k) = sum_t sum_c J_i,c[r] J_j,c[k]
+// with the term weights, written to row i and, transposed, to row j (the
+// reference computes both orderings separately, JtJMaterializer.cu:270-365)
 template <bool MIXED>
 __global__ void __launch_bounds__(256) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
+    __shared__ float stage[8][32][kStageFloats];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2) return;
     TermOffsets off;
     off.load(C);
     const uint32_t P = C->half_pairs;
+    const uint32_t w = threadIdx.x >> 5, lane = lane_id();
+    // lane owns element e0 = lane and, for lanes 0..3, e1 = lane + 32
+    const int r0 = lane / 6, k0 = lane % 6;
+    const int r1 = (lane + 32) / 6, k1 = (lane + 32) % 6;
+    const bool two = lane < 4;
+    const RowSel rr0 = make_rowsel(r0), rk0 = make_rowsel(k0), rr1 = make_rowsel(r1), rk1 = make_rowsel(k1);
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t h = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < P; h += warps) {
+    for (uint32_t h = blockIdx.x * (blockDim.x >> 5) + w; h < P; h += warps) {
         const uint32_t key = I.half_key[h];
         const uint32_t ni = key / I.enc, nj = key % I.enc;
         const uint2 rg = I.half_range[h];
-        Acc acc[36];
+        Acc a0 = 0, a1 = 0;
+        for (uint32_t base = rg.x; base < rg.y; base += 32) {
+            const uint32_t p = base + lane;
+            float* my = stage[w][lane];
+            if (p < rg.y) stage_term(I, off, lam, I.np_index[p], ni, nj, true, my);
+            else my[0] = __uint_as_float(kStageNone);
+            __syncwarp();
+            const uint32_t n = min(32u, rg.y - base);
+            for (uint32_t q = 0; q < n; ++q) {
+                const float* d = stage[w][q];
+                const uint32_t kind = __float_as_uint(d[0]);
+                if (kind == kStageScalar) {
+                    a0 += (Acc)d[1] * (Acc)d[3 + r0] * (Acc)d[3 + k0];
+                    if (two) a1 += (Acc)d[1] * (Acc)d[3 + r1] * (Acc)d[3 + k1];
+                } else if (kind == kStageP2P) {
+                    const float* pp = d + 3;
 #pragma unroll
-        for (int i = 0; i < 36; ++i) acc[i] = 0;
-        for (uint32_t p = rg.x + lane_id(); p < rg.y; p += 32) {
-            const uint32_t t = I.np_index[p];
-            TermRows a, b;
-            const int ch = term_rows(I, off, lam, t, ni, a);
-            if (ch == 0) continue;
-            term_rows(I, off, lam, t, nj, b);
-            const Acc s = (Acc)a.lam2 * (Acc)a.w * (Acc)b.w;
-            for (int c = 0; c < ch; ++c) {
+                    for (int c = 0; c < 3; ++c) {
+                        const Acc h2 = (Acc)d[1] * (Acc)d[6 + c] * (Acc)d[6 + c];
+                        a0 += h2 * (Acc)frow(rr0, c, pp) * (Acc)frow(rk0, c, pp);
+                        if (two) a1 += h2 * (Acc)frow(rr1, c, pp) * (Acc)frow(rk1, c, pp);
+                    }
+                } else if (kind == kStageSmooth) {
+                    // J_i,c = +-f_c(p_i), J_j,c = -+f_c(p_j): the product is negative
+                    const float* pi = d + 3;
+                    const float* pj = d + 6;
 #pragma unroll
-                for (int r = 0; r < 6; ++r)
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) acc[6 * r + q] += s * (Acc)a.J[c][r] * (Acc)b.J[c][q];
+                    for (int c = 0; c < 3; ++c) {
+                        a0 -= (Acc)d[1] * (Acc)frow(rr0, c, pi) * (Acc)frow(rk0, c, pj);
+                        if (two) a1 -= (Acc)d[1] * (Acc)frow(rr1, c, pi) * (Acc)frow(rk1, c, pj);
+                    }
+                }
             }
+            __syncwarp();
         }
-#pragma unroll
-        for (int i = 0; i < 36; ++i) acc[i] = warp_sum(acc[i]);
         const size_t up = 36 * (size_t)(I.upper_pos[h] + ni + 1);  // BSR block of (i, j)
         const size_t lo = 36 * (size_t)(I.lower_pos[h] + nj + 1);  // BSR block of (j, i)
-        for (uint32_t e = lane_id(); e < 36; e += 32) {
-            Acc v = 0, vt = 0;
-            const uint32_t r = e / 6, q = e % 6;
-#pragma unroll
-            for (int z = 0; z < 36; ++z) {
-                v = (z == (int)e) ? acc[z] : v;
-                vt = (z == (int)(6 * q + r)) ? acc[z] : vt;
+        // element (r, k) of A_ij is element (k, r) of A_ji
+        if (MIXED) {
+            store_split((double)a0, I.bsr + up + lane, I.bsr_lo + up + lane);
+            store_split((double)a0, I.bsr + lo + 6 * k0 + r0, I.bsr_lo + lo + 6 * k0 + r0);
+            if (two) {
+                store_split((double)a1, I.bsr + up + lane + 32, I.bsr_lo + up + lane + 32);
+                store_split((double)a1, I.bsr + lo + 6 * k1 + r1, I.bsr_lo + lo + 6 * k1 + r1);
             }
-            if (MIXED) {
-                store_split((double)v, I.bsr + up + e, I.bsr_lo + up + e);
-                store_split((double)vt, I.bsr + lo + e, I.bsr_lo + lo + e);
-            } else {
-                I.bsr[up + e] = (float)v;
-                I.bsr[lo + e] = (float)vt;
+        } else {
+            I.bsr[up + lane] = (float)a0;
+            I.bsr[lo + 6 * k0 + r0] = (float)a0;
+            if (two) {
+                I.bsr[up + lane + 32] = (float)a1;
+                I.bsr[lo + 6 * k1 + r1] = (float)a1;
             }
         }
     }

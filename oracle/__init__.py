@@ -46,6 +46,7 @@ def lib():
         L.orc_set_term_data.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_freeze_decisions.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_set_increment.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_set_node_se3.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_energy.restype = C.c_double
         L.orc_energy.argtypes = [C.c_void_p]
         L.orc_energy_now.restype = C.c_double
@@ -150,6 +151,11 @@ class Oracle:
     def set_increment(self, x):
         x = np.ascontiguousarray(x, np.float32)
         lib().orc_set_increment(self.h, _p(x))
+
+    def set_node_se3(self, dq):
+        """Continue from another run's warp field (N x 8 float)."""
+        dq = np.ascontiguousarray(dq, np.float32)
+        lib().orc_set_node_se3(self.h, _p(dq))
 
     def energy(self):
         return lib().orc_energy(self.h)

@@ -1147,6 +1147,15 @@ void orc_set_increment(void* h, const float* x) {
 }
 void orc_update(void* h) { ((Oracle*)h)->update(); }
 
+/* Replace the current warp field (num_nodes dual quaternions, float). */
+void orc_set_node_se3(void* h, const float* dq) {
+    Oracle* o = (Oracle*)h;
+    for (uint32_t i = 0; i < o->N; ++i) {
+        const float* d = dq + 8 * (size_t)i;
+        o->se3d[i] = {{d[0], d[1], d[2], d[3]}, {d[4], d[5], d[6], d[7]}};
+    }
+}
+
 /* One full Gauss-Newton iteration. */
 void orc_gn_iteration(void* h, uint32_t pcg) {
     Oracle* o = (Oracle*)h;
