@@ -260,51 +260,35 @@ __device__ inline void store_split(double a, float* hi, __half* lo) {
 }
 
 // ------------------------------- element-parallel block accumulation -----
-// A warp stages up to 32 terms of one node (diagonal block) or one node pair
-// (off-diagonal block) in shared memory as compact descriptors, then each
-// lane accumulates the block element(s) it owns over the staged terms. The
-// per-lane state is one or two accumulators, so occupancy stays high, and the
-// kind of the staged term is the same for every lane, so the inner loop does
-// not diverge.
+// A group of 8 lanes owns one node (diagonal block) or one node pair
+// (off-diagonal block); a warp holds 4 groups. The group stages 8 of its terms
+// at a time in shared memory, each as weighted twist-Jacobian rows already in
+// the accumulation precision, then every lane accumulates the 4-5 block
+// elements it owns over the staged terms. The inner loop is shared loads and
+// fused multiply-adds only: no type conversions, no cross-lane reduction, and
+// all 8 lanes of a group busy.
 //
 // Twist Jacobian row of a point-to-point or smooth residual at point p
 // (geometry_icp_jacobian.cuh:91-120, 323-343): f_c(p) = [row c of [p]x^T ; e_c].
-// f_c(p)[r] = coef * P[sel] with P = (p.x, p.y, p.z, 1).
-struct RowSel {
-    int sel[3];
-    float coef[3];
-};
-
-__device__ inline RowSel make_rowsel(int r) {
-    RowSel o;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        if (r >= 3) {
-            o.sel[c] = 3;
-            o.coef[c] = (r - 3 == c) ? 1.f : 0.f;
-        } else {
-            const int d = (r - c + 3) % 3;
-            o.sel[c] = d == 1 ? (c + 2) % 3 : (c + 1) % 3;
-            o.coef[c] = d == 0 ? 0.f : (d == 1 ? 1.f : -1.f);
-        }
-    }
-    return o;
+template <class T> __device__ inline void twist_rows(T px, T py, T pz, T f[3][6]) {
+    f[0][0] = 0;   f[0][1] = pz;  f[0][2] = -py; f[0][3] = 1; f[0][4] = 0; f[0][5] = 0;
+    f[1][0] = -pz; f[1][1] = 0;   f[1][2] = px;  f[1][3] = 0; f[1][4] = 1; f[1][5] = 0;
+    f[2][0] = py;  f[2][1] = -px; f[2][2] = 0;   f[2][3] = 0; f[2][4] = 0; f[2][5] = 1;
 }
 
-enum : uint32_t { kStageNone = 0, kStageScalar = 1, kStageP2P = 2, kStageSmooth = 3 };
-constexpr int kStageFloats = 16;
+constexpr int kGroupLanes = 8;
+constexpr int kPairStride = 37;  // u[3][6], v[3][6], channel count (odd stride: no bank conflicts)
+constexpr int kDiagStride = 23;  // u[3][6], lambda^2, rb[3], channel count
 
-// Stage descriptor of term t as seen from node `ni` (and `nj` for a pair):
-//  [0] kind  [1] s1  [2] s2  [3..8] six values  [9..11] three values
-//  scalar : s1 = lam^2 w_i w_j (pair) or lam^2 w^2 (diag), s2 = lam^2 w, [3..8] J, [9] r
-//  p2p    : s1 as scalar, s2 = lam^2 w, [3..5] p, [6..8] huber weights, [9..11] raw residual
-//  smooth : s1 = lam^2, pair: [3..5] p_i, [6..8] p_j; diag: [3..5] p, [6] sign, [9..11] r
-__device__ inline void stage_term(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
-                                  uint32_t ni, uint32_t nj, bool pair, float* o) {
+// Off-diagonal descriptor of term t for the pair (ni, nj): the block is
+// sum_c u_c v_c^T with u_c = J_i,c-side rows and v_c the lambda^2-weighted
+// J_j,c-side rows; returns the channel count.
+template <class T>
+__device__ inline void stage_pair(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
+                                  uint32_t ni, uint32_t nj, T* o) {
     uint32_t k;
     const TermType ty = off.typed(t, k);
-    o[0] = __uint_as_float(kStageNone);
-    o[1] = 0.f;
+    T nch = 0;
     switch (ty) {
         case kDense:
         case kForeground: {
@@ -312,37 +296,36 @@ __device__ inline void stage_term(const InstDesc& I, const TermOffsets& off, con
             const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
             const ushort4 kn = term_nodes(I, ty, k);
             const float4 w4 = term_weights(I, ty, k);
-            const float l2 = ty == kDense ? 1.0f : lam.foreground * lam.foreground;
-            const float wi = weight_of(kn, w4, ni);
-            const float wj = pair ? weight_of(kn, w4, nj) : wi;
-            o[0] = __uint_as_float(kStageScalar);
-            o[1] = l2 * wi * wj;
-            o[2] = l2 * wi;
-            o[3] = a.x; o[4] = a.y; o[5] = a.z; o[6] = a.w; o[7] = b.x; o[8] = b.y;
-            o[9] = b.z;
+            const T l2 = ty == kDense ? (T)1 : (T)(lam.foreground * lam.foreground);
+            const T wi = (T)weight_of(kn, w4, ni), wj = l2 * (T)weight_of(kn, w4, nj);
+            const T J[6] = {(T)a.x, (T)a.y, (T)a.z, (T)a.w, (T)b.x, (T)b.y};
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                o[q] = wi * J[q];
+                o[18 + q] = wj * J[q];
+            }
+            nch = 1;
             break;
         }
         case kSmooth: {
             const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
             if (b.z == 0.f) break;
             const bool is_i = ni == I.graph[k].x;
-            const float ti[3] = {a.x, a.y, a.z}, tj[3] = {a.w, b.x, b.y};
-            o[0] = __uint_as_float(kStageSmooth);
-            o[1] = lam.smooth * lam.smooth;
-            if (pair) {
+            const float4 pi = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
+            const float4 pj = is_i ? make_float4(a.w, b.x, b.y, 0.f) : a;
+            T fi[3][6], fj[3][6];
+            twist_rows<T>((T)pi.x, (T)pi.y, (T)pi.z, fi);
+            twist_rows<T>((T)pj.x, (T)pj.y, (T)pj.z, fj);
+            // J_i,c = +-f_c(p_i), J_j,c = -+f_c(p_j): their product carries a minus
+            const T l2 = -(T)(lam.smooth * lam.smooth);
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    o[3 + q] = is_i ? ti[q] : tj[q];
-                    o[6 + q] = is_i ? tj[q] : ti[q];
-                }
-            } else {
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    o[3 + q] = is_i ? ti[q] : tj[q];
-                    o[9 + q] = ti[q] - tj[q];
+                for (int q = 0; q < 6; ++q) {
+                    o[6 * c + q] = fi[c][q];
+                    o[18 + 6 * c + q] = l2 * fj[c][q];
                 }
-                o[6] = is_i ? 1.f : -1.f;
-            }
+            nch = 3;
             break;
         }
         case kFeature:
@@ -352,124 +335,194 @@ __device__ inline void stage_term(const InstDesc& I, const TermOffsets& off, con
             const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
             const ushort4 kn = term_nodes(I, ty, k);
             const float4 w4 = term_weights(I, ty, k);
-            const float l2 = f ? lam.feature * lam.feature : lam.cross_view * lam.cross_view;
-            const float wi = weight_of(kn, w4, ni);
-            const float wj = pair ? weight_of(kn, w4, nj) : wi;
-            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
-            o[0] = __uint_as_float(kStageP2P);
-            o[1] = l2 * wi * wj;
-            o[2] = l2 * wi;
-            o[3] = wv.x; o[4] = wv.y; o[5] = wv.z;
+            const T l2 = f ? (T)(lam.feature * lam.feature) : (T)(lam.cross_view * lam.cross_view);
+            const T wi = (T)weight_of(kn, w4, ni), wj = l2 * (T)weight_of(kn, w4, nj);
+            const float hw[3] = {huber_weight(wv.x - tg.x), huber_weight(wv.y - tg.y), huber_weight(wv.z - tg.z)};
+            T fr[3][6];
+            twist_rows<T>((T)wv.x, (T)wv.y, (T)wv.z, fr);
 #pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                o[6 + q] = huber_weight(raw[q]);
-                o[9 + q] = raw[q];
-            }
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    const T jv = (T)hw[c] * fr[c][q];
+                    o[6 * c + q] = wi * jv;
+                    o[18 + 6 * c + q] = wj * jv;
+                }
+            nch = 3;
             break;
         }
         default: break;
     }
+    o[36] = nch;
 }
 
-// f_c(P)[row] for the lane's row selection
-__device__ inline float frow(const RowSel& rs, int c, const float* p) {
-    const int sl = rs.sel[c];
-    return rs.coef[c] * (sl == 3 ? 1.f : p[sl]);
+// Diagonal descriptor of term t for node n: D += lambda^2 sum_c u_c u_c^T,
+// b += sum_c u_c rb_c.
+template <class T>
+__device__ inline void stage_diag(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
+                                  uint32_t n, T* o) {
+    uint32_t k;
+    const TermType ty = off.typed(t, k);
+    T nch = 0;
+    switch (ty) {
+        case kDense:
+        case kForeground: {
+            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+            const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+            const T l2 = ty == kDense ? (T)1 : (T)(lam.foreground * lam.foreground);
+            const T w = (T)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n);
+            const T J[6] = {(T)a.x, (T)a.y, (T)a.z, (T)a.w, (T)b.x, (T)b.y};
+#pragma unroll
+            for (int q = 0; q < 6; ++q) o[q] = w * J[q];
+            o[18] = l2;
+            o[19] = -l2 * (T)b.z;
+            nch = 1;
+            break;
+        }
+        case kSmooth: {
+            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            if (b.z == 0.f) break;
+            const bool is_i = n == I.graph[k].x;
+            const float4 p = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
+            T fr[3][6];
+            twist_rows<T>((T)p.x, (T)p.y, (T)p.z, fr);
+            const T l2 = (T)(lam.smooth * lam.smooth);
+            const T sg = is_i ? (T)1 : (T)-1;
+            const T rc[3] = {(T)a.x - (T)a.w, (T)a.y - (T)b.x, (T)a.z - (T)b.y};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                for (int q = 0; q < 6; ++q) o[6 * c + q] = fr[c][q];
+                o[19 + c] = -l2 * sg * rc[c];
+            }
+            o[18] = l2;
+            nch = 3;
+            break;
+        }
+        case kFeature:
+        case kCross: {
+            const bool f = ty == kFeature;
+            const float4 wv = I.warped[f ? k : I.Tp + k];
+            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const T l2 = f ? (T)(lam.feature * lam.feature) : (T)(lam.cross_view * lam.cross_view);
+            const T w = (T)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n);
+            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+            T fr[3][6];
+            twist_rows<T>((T)wv.x, (T)wv.y, (T)wv.z, fr);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T hw = (T)huber_weight(raw[c]);
+#pragma unroll
+                for (int q = 0; q < 6; ++q) o[6 * c + q] = w * hw * fr[c][q];
+                o[19 + c] = -l2 * hw * (T)raw[c];
+            }
+            o[18] = l2;
+            nch = 3;
+            break;
+        }
+        default: break;
+    }
+    o[22] = nch;
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
+__global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
-    __shared__ float stage[8][32][kStageFloats];
-    __shared__ Acc blockv[8][28];
+    constexpr int kWarps = 4;
+    __shared__ Acc stage[kWarps][32][kDiagStride];
+    __shared__ Acc vals[kWarps][4][28];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs) return;
     TermOffsets off;
     off.load(C);
     const uint32_t w = threadIdx.x >> 5, lane = lane_id();
-    // lane -> element: lanes 0..20 the upper triangle (r <= k) of D, 21..26 b
-    int er = 0, ek = 0;
-    {
-        int e = 0;
+    const uint32_t g = lane / kGroupLanes, l8 = lane % kGroupLanes;
+    // lane-owned elements e = l8 + 8 m: 0..20 the upper triangle of D, 21..26 b
+    int er[4], ek[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int e = (int)l8 + 8 * m;
+        er[m] = 0;
+        ek[m] = 0;
+        int c = 0;
         for (int r = 0; r < 6; ++r)
-            for (int k2 = r; k2 < 6; ++k2, ++e)
-                if (e == (int)lane) { er = r; ek = k2; }
-        if (lane >= 21 && lane < 27) { er = lane - 21; ek = er; }
+            for (int k2 = r; k2 < 6; ++k2, ++c)
+                if (c == e) { er[m] = r; ek[m] = k2; }
+        if (e >= 21) { er[m] = e - 21; ek[m] = -1; }
+        if (e >= 27) { er[m] = 0; ek[m] = -2; }
     }
-    const bool is_d = lane < 21, is_b = lane >= 21 && lane < 27;
-    const RowSel rr = make_rowsel(er), rk = make_rowsel(ek);
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + w; node < I.N; node += warps) {
-        Acc acc = 0;
-        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
-        for (uint32_t base = b; base < e; base += 32) {
-            const uint32_t p = base + lane;
-            float* my = stage[w][lane];
-            if (p < e) stage_term(I, off, lam, I.n2t_index[p], node, node, false, my);
-            else my[0] = __uint_as_float(kStageNone);
+    const uint32_t groups = gridDim.x * kWarps * 4;
+    const uint32_t first = (blockIdx.x * kWarps + w) * 4;
+    for (uint32_t gbase = first; gbase < I.N + 0u; gbase += groups) {
+        const uint32_t node = gbase + g;
+        const bool active = node < I.N;
+        const uint32_t b = active ? I.n2t_offset[node] : 0, e = active ? I.n2t_offset[node + 1] : 0;
+        // chunks of this warp: the longest group decides
+        uint32_t nchunks = (e - b + kGroupLanes - 1) / kGroupLanes;
+        for (int o = 8; o <= 16; o <<= 1) nchunks = max(nchunks, __shfl_xor_sync(0xffffffffu, nchunks, o));
+        Acc acc[4] = {0, 0, 0, 0};
+        for (uint32_t ch = 0; ch < nchunks; ++ch) {
+            const uint32_t p = b + ch * kGroupLanes + l8;
+            Acc* my = stage[w][lane];
+            if (p < e) stage_diag<Acc>(I, off, lam, I.n2t_index[p], node, my);
+            else my[22] = 0;
             __syncwarp();
-            const uint32_t n = min(32u, e - base);
-            for (uint32_t q = 0; q < n; ++q) {
-                const float* d = stage[w][q];
-                const uint32_t kind = __float_as_uint(d[0]);
-                if (kind == kStageScalar) {
-                    if (is_d) acc += (Acc)d[1] * (Acc)d[3 + er] * (Acc)d[3 + ek];
-                    else if (is_b) acc -= (Acc)d[2] * (Acc)d[3 + er] * (Acc)d[9];
-                } else if (kind == kStageP2P) {
-                    const float* pp = d + 3;
+#pragma unroll 2
+            for (int q = 0; q < kGroupLanes; ++q) {
+                const Acc* d = stage[w][g * kGroupLanes + q];
+                const int nch = (int)d[22];
+                for (int c = 0; c < nch; ++c) {
+                    const Acc* u = d + 6 * c;
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const Acc h2 = (Acc)d[6 + c] * (Acc)d[6 + c];
-                        if (is_d) acc += (Acc)d[1] * h2 * (Acc)frow(rr, c, pp) * (Acc)frow(rk, c, pp);
-                        else if (is_b) acc -= (Acc)d[2] * h2 * (Acc)d[9 + c] * (Acc)frow(rr, c, pp);
-                    }
-                } else if (kind == kStageSmooth) {
-                    const float* pp = d + 3;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        if (is_d) acc += (Acc)d[1] * (Acc)frow(rr, c, pp) * (Acc)frow(rk, c, pp);
-                        else if (is_b) acc -= (Acc)d[1] * (Acc)d[6] * (Acc)frow(rr, c, pp) * (Acc)d[9 + c];
+                    for (int m = 0; m < 4; ++m) {
+                        if (ek[m] >= 0) acc[m] += d[18] * u[er[m]] * u[ek[m]];
+                        else if (ek[m] == -1) acc[m] += u[er[m]] * d[19 + c];
                     }
                 }
             }
             __syncwarp();
         }
-        if (is_d && er == ek) acc += (Acc)1e-2f;  // PreconditionerBlocked.cu:272-275
-        if (lane < 27) blockv[w][lane] = acc;
-        __syncwarp();
-        // diagonal block: the parity copy and the block of the BSR row
-        const size_t blk = 36 * (size_t)(I.blkrow_offset[node] + node);
-        for (uint32_t i = lane; i < 36; i += 32) {
-            const int r = i / 6, k2 = i % 6;
-            const int lo = min(r, k2), hi = max(r, k2);
-            const Acc v = blockv[w][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
-            I.diag[36 * (size_t)node + i] = (float)v;
-            if (MIXED) store_split((double)v, I.bsr + blk + i, I.bsr_lo + blk + i);
-            else I.bsr[blk + i] = (float)v;
+        // gather the 27 values of each group, damping on the diagonal
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int el = (int)l8 + 8 * m;
+            if (el < 27) vals[w][g][el] = acc[m] + ((ek[m] >= 0 && er[m] == ek[m]) ? (Acc)1e-2f : (Acc)0);
         }
-        if (is_b) I.jtr[6 * (size_t)node + er] = (float)acc;
-        if (lane == 0) {
-            Acc D[36];
+        __syncwarp();
+        if (active) {
+            const size_t blk = 36 * (size_t)(I.blkrow_offset[node] + node);
+            for (uint32_t i = l8; i < 36; i += kGroupLanes) {
+                const int r = i / 6, k2 = i % 6;
+                const int lo = min(r, k2), hi = max(r, k2);
+                const Acc v = vals[w][g][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
+                I.diag[36 * (size_t)node + i] = (float)v;
+                if (MIXED) store_split((double)v, I.bsr + blk + i, I.bsr_lo + blk + i);
+                else I.bsr[blk + i] = (float)v;
+            }
+            if (l8 < 6) I.jtr[6 * (size_t)node + l8] = (float)vals[w][g][21 + l8];
+            if (l8 == 0) {
+                Acc D[36];
 #pragma unroll
-            for (int r = 0; r < 6; ++r)
+                for (int r = 0; r < 6; ++r)
 #pragma unroll
-                for (int k2 = 0; k2 < 6; ++k2) {
-                    const int lo = r < k2 ? r : k2, hi = r < k2 ? k2 : r;
-                    D[6 * r + k2] = blockv[w][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
+                    for (int k2 = 0; k2 < 6; ++k2) {
+                        const int lo = r < k2 ? r : k2, hi = r < k2 ? k2 : r;
+                        D[6 * r + k2] = vals[w][g][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
+                    }
+                if (MIXED) {
+                    double L[21];
+                    cholesky6(D, L);
+#pragma unroll
+                    for (int i = 0; i < 21; ++i) I.chol[21 * (size_t)node + i] = L[i];
+                } else {
+                    float Df[36], Mi[36];
+#pragma unroll
+                    for (int i = 0; i < 36; ++i) Df[i] = (float)D[i];
+                    gauss_jordan6(Df, Mi);
+#pragma unroll
+                    for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
                 }
-            if (MIXED) {
-                double L[21];
-                cholesky6(D, L);
-#pragma unroll
-                for (int i = 0; i < 21; ++i) I.chol[21 * (size_t)node + i] = L[i];
-            } else {
-                float Df[36], Mi[36];
-#pragma unroll
-                for (int i = 0; i < 36; ++i) Df[i] = (float)D[i];
-                gauss_jordan6(Df, Mi);
-#pragma unroll
-                for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
             }
         }
         __syncwarp();
@@ -477,13 +530,14 @@ __global__ void __launch_bounds__(256) diag_rhs_kernel(const InstDesc* insts, mv
 }
 
 // --------------------------------------------------- off-diagonal blocks --
-// warp per unordered pair (i < j): A_ij(r, k) = sum_t sum_c J_i,c[r] J_j,c[k]
-// with the term weights, written to row i and, transposed, to row j (the
-// reference computes both orderings separately, JtJMaterializer.cu:270-365)
+// 8 lanes per unordered pair (i < j): A_ij(r, k) = sum_t sum_c u_c[r] v_c[k],
+// written to row i and, transposed, to row j (the reference computes both
+// orderings separately, JtJMaterializer.cu:270-365)
 template <bool MIXED>
-__global__ void __launch_bounds__(256) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
+__global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
-    __shared__ float stage[8][32][kStageFloats];
+    constexpr int kWarps = 4;
+    __shared__ Acc stage[kWarps][32][kPairStride];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2) return;
@@ -491,67 +545,65 @@ __global__ void __launch_bounds__(256) offdiag_kernel(const InstDesc* insts, mvd
     off.load(C);
     const uint32_t P = C->half_pairs;
     const uint32_t w = threadIdx.x >> 5, lane = lane_id();
-    // lane owns element e0 = lane and, for lanes 0..3, e1 = lane + 32
-    const int r0 = lane / 6, k0 = lane % 6;
-    const int r1 = (lane + 32) / 6, k1 = (lane + 32) % 6;
-    const bool two = lane < 4;
-    const RowSel rr0 = make_rowsel(r0), rk0 = make_rowsel(k0), rr1 = make_rowsel(r1), rk1 = make_rowsel(k1);
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t h = blockIdx.x * (blockDim.x >> 5) + w; h < P; h += warps) {
-        const uint32_t key = I.half_key[h];
-        const uint32_t ni = key / I.enc, nj = key % I.enc;
-        const uint2 rg = I.half_range[h];
-        Acc a0 = 0, a1 = 0;
-        for (uint32_t base = rg.x; base < rg.y; base += 32) {
-            const uint32_t p = base + lane;
-            float* my = stage[w][lane];
-            if (p < rg.y) stage_term(I, off, lam, I.np_index[p], ni, nj, true, my);
-            else my[0] = __uint_as_float(kStageNone);
+    const uint32_t g = lane / kGroupLanes, l8 = lane % kGroupLanes;
+    // lane-owned elements e = l8 + 8 m (m < 5, e < 36)
+    int er[5], ek[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const int e = (int)l8 + 8 * m;
+        er[m] = e < 36 ? e / 6 : -1;
+        ek[m] = e < 36 ? e % 6 : 0;
+    }
+    const uint32_t groups = gridDim.x * kWarps * 4;
+    const uint32_t first = (blockIdx.x * kWarps + w) * 4;
+    for (uint32_t hbase = first; hbase < P; hbase += groups) {
+        const uint32_t h = hbase + g;
+        const bool active = h < P;
+        uint32_t ni = 0, nj = 0;
+        uint2 rg = make_uint2(0, 0);
+        if (active) {
+            const uint32_t key = I.half_key[h];
+            ni = key / I.enc;
+            nj = key % I.enc;
+            rg = I.half_range[h];
+        }
+        uint32_t nchunks = (rg.y - rg.x + kGroupLanes - 1) / kGroupLanes;
+        for (int o = 8; o <= 16; o <<= 1) nchunks = max(nchunks, __shfl_xor_sync(0xffffffffu, nchunks, o));
+        Acc acc[5] = {0, 0, 0, 0, 0};
+        for (uint32_t ch = 0; ch < nchunks; ++ch) {
+            const uint32_t p = rg.x + ch * kGroupLanes + l8;
+            Acc* my = stage[w][lane];
+            if (p < rg.y) stage_pair<Acc>(I, off, lam, I.np_index[p], ni, nj, my);
+            else my[36] = 0;
             __syncwarp();
-            const uint32_t n = min(32u, rg.y - base);
-            for (uint32_t q = 0; q < n; ++q) {
-                const float* d = stage[w][q];
-                const uint32_t kind = __float_as_uint(d[0]);
-                if (kind == kStageScalar) {
-                    a0 += (Acc)d[1] * (Acc)d[3 + r0] * (Acc)d[3 + k0];
-                    if (two) a1 += (Acc)d[1] * (Acc)d[3 + r1] * (Acc)d[3 + k1];
-                } else if (kind == kStageP2P) {
-                    const float* pp = d + 3;
+#pragma unroll 2
+            for (int q = 0; q < kGroupLanes; ++q) {
+                const Acc* d = stage[w][g * kGroupLanes + q];
+                const int nch = (int)d[36];
+                for (int c = 0; c < nch; ++c) {
+                    const Acc* u = d + 6 * c;
+                    const Acc* v = d + 18 + 6 * c;
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const Acc h2 = (Acc)d[1] * (Acc)d[6 + c] * (Acc)d[6 + c];
-                        a0 += h2 * (Acc)frow(rr0, c, pp) * (Acc)frow(rk0, c, pp);
-                        if (two) a1 += h2 * (Acc)frow(rr1, c, pp) * (Acc)frow(rk1, c, pp);
-                    }
-                } else if (kind == kStageSmooth) {
-                    // J_i,c = +-f_c(p_i), J_j,c = -+f_c(p_j): the product is negative
-                    const float* pi = d + 3;
-                    const float* pj = d + 6;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        a0 -= (Acc)d[1] * (Acc)frow(rr0, c, pi) * (Acc)frow(rk0, c, pj);
-                        if (two) a1 -= (Acc)d[1] * (Acc)frow(rr1, c, pi) * (Acc)frow(rk1, c, pj);
-                    }
+                    for (int m = 0; m < 5; ++m)
+                        if (er[m] >= 0) acc[m] += u[er[m]] * v[ek[m]];
                 }
             }
             __syncwarp();
         }
-        const size_t up = 36 * (size_t)(I.upper_pos[h] + ni + 1);  // BSR block of (i, j)
-        const size_t lo = 36 * (size_t)(I.lower_pos[h] + nj + 1);  // BSR block of (j, i)
-        // element (r, k) of A_ij is element (k, r) of A_ji
-        if (MIXED) {
-            store_split((double)a0, I.bsr + up + lane, I.bsr_lo + up + lane);
-            store_split((double)a0, I.bsr + lo + 6 * k0 + r0, I.bsr_lo + lo + 6 * k0 + r0);
-            if (two) {
-                store_split((double)a1, I.bsr + up + lane + 32, I.bsr_lo + up + lane + 32);
-                store_split((double)a1, I.bsr + lo + 6 * k1 + r1, I.bsr_lo + lo + 6 * k1 + r1);
-            }
-        } else {
-            I.bsr[up + lane] = (float)a0;
-            I.bsr[lo + 6 * k0 + r0] = (float)a0;
-            if (two) {
-                I.bsr[up + lane + 32] = (float)a1;
-                I.bsr[lo + 6 * k1 + r1] = (float)a1;
+        if (active) {
+            const size_t up = 36 * (size_t)(I.upper_pos[h] + ni + 1);  // BSR block of (i, j)
+            const size_t lo = 36 * (size_t)(I.lower_pos[h] + nj + 1);  // BSR block of (j, i)
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                if (er[m] < 0) continue;
+                const uint32_t e = 6 * er[m] + ek[m], et = 6 * ek[m] + er[m];
+                if (MIXED) {
+                    store_split((double)acc[m], I.bsr + up + e, I.bsr_lo + up + e);
+                    store_split((double)acc[m], I.bsr + lo + et, I.bsr_lo + lo + et);
+                } else {
+                    I.bsr[up + e] = (float)acc[m];
+                    I.bsr[lo + et] = (float)acc[m];
+                }
             }
         }
     }
@@ -1037,13 +1089,13 @@ cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, cudaStream_t st)
 
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, bool materialize,
                             cudaStream_t st) {
-    const uint32_t gn = (lc.max_nodes + 7) / 8;
-    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 256, 0, st, d, lam);
-    else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 256, 0, st, d, lam);
+    const uint32_t gn = (lc.max_nodes + 15) / 16;
+    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 128, 0, st, d, lam);
+    else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
     if (materialize) {
-        const uint32_t gp = min((lc.cap_pairs + 7) / 8, (uint32_t)lc.sm_count * 16);
-        if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 256, 0, st, d, lam);
-        else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 256, 0, st, d, lam);
+        const uint32_t gp = min((lc.cap_pairs + 15) / 16, (uint32_t)lc.sm_count * 16);
+        if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, st, d, lam);
+        else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, st, d, lam);
     }
     return cudaGetLastError();
 }
@@ -1084,17 +1136,17 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gspmv = min((lc.max_nodes + 31) / 32, (uint32_t)lc.sm_count * 8);
-    const uint32_t gn = (lc.max_nodes + 7) / 8;
+    const uint32_t gn = (lc.max_nodes + 15) / 16;
     switch (stage) {
         case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
         case MVDR_STAGE_DIAG:
-            if (mixed) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 256, 0, st, d, lam);
-            else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 256, 0, st, d, lam);
+            if (mixed) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 128, 0, st, d, lam);
+            else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
             break;
         case MVDR_STAGE_OFFDIAG: {
-            const uint32_t gp = min((lc.cap_pairs + 7) / 8, (uint32_t)lc.sm_count * 16);
-            if (mixed) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 256, 0, st, d, lam);
-            else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 256, 0, st, d, lam);
+            const uint32_t gp = min((lc.cap_pairs + 15) / 16, (uint32_t)lc.sm_count * 16);
+            if (mixed) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, st, d, lam);
+            else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, st, d, lam);
             break;
         }
         case MVDR_STAGE_SPMV:
