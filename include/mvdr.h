@@ -67,9 +67,13 @@ typedef enum mvdr_status {
  * FP32:  everything in float; Gauss-Jordan 6x6 inverse; float dot products
  *        (the reference's arithmetic, BlockPCG.cuh:187-458,
  *        BlockDiagonalPreconditionerInverse.cu:7-41).
- * MIXED: residuals, Jacobians, BSR blocks and SpMV in float; PCG dot products
- *        and norms in double; 6x6 block Cholesky of the preconditioner in
- *        double. */
+ * MIXED: Jacobians, stored residuals and PCG vectors in float. Double is used
+ *        where float rounding would move the increment by more than 1e-4:
+ *        the warped-point / residual chain of each term (positions of about
+ *        1 m give residuals of about 1 mm), the accumulation of the JtJ blocks
+ *        and Jt r (stored as float plus a 16-bit correction), the SpMV row
+ *        sums, the PCG dot products and norms, and the 6x6 block Cholesky of
+ *        the preconditioner. */
 typedef enum mvdr_precision {
     MVDR_PRECISION_FP32 = 0,
     MVDR_PRECISION_MIXED = 1
@@ -286,8 +290,10 @@ enum {
     MVDR_ARRAY_BINBLOCK_ROWPTR = 11,    /* int32  [32*(nbins+1)]                           */
     MVDR_ARRAY_BINBLOCK_COLPTR = 12,    /* int32  [binblock_nnz/6]                         */
     MVDR_ARRAY_TERM_JACOBIAN = 13,      /* float [T_d+T_f][8]: twist gradient (6), residual, pad */
-    MVDR_ARRAY_SMOOTH_TERMS = 14,       /* float [T_s][8]: Ti_xj (3), Tj_xj (3), validity, pad */
-    MVDR_ARRAY_WARPED_CORRESPONDENCE = 15, /* float4 [T_p+T_c] warped reference vertex     */
+    MVDR_ARRAY_SMOOTH_TERMS = 14,       /* float [T_s][12]: Ti_xj (3), Tj_xj (3), validity, pad,
+                                           residual Ti_xj - Tj_xj (3), pad                     */
+    MVDR_ARRAY_WARPED_CORRESPONDENCE = 15, /* float [T_p+T_c][8]: warped reference vertex (3),
+                                              1, residual warped - target (3), pad            */
     MVDR_ARRAY_DIAG_BLOCKS = 16,        /* float [N][36] JtJ diagonal blocks incl. damping  */
     MVDR_ARRAY_JTR = 17,                /* float [N][6]  b = -Jt r                          */
     MVDR_ARRAY_PRECONDITIONER = 18,     /* float [N][36] inverse of the diagonal blocks      */

@@ -21,16 +21,104 @@
 namespace mvdr {
 
 // ------------------------------------------------------- term evaluation --
+// The position chain of every term (blend, normalise, warp, camera
+// transforms, projection, residual) runs in T: float reproduces the reference
+// arithmetic (FP32 mode); double keeps the millimetre residuals of metre-scale
+// positions accurate (mixed mode). Jacobians are stored in float either way.
 
+template <class T> struct V3T { T x, y, z; };
+template <class T> __device__ inline V3T<T> v3t(T x, T y, T z) { return {x, y, z}; }
+template <class T> __device__ inline V3T<T> sub(V3T<T> a, V3T<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> __device__ inline T dotv(V3T<T> a, V3T<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> struct R34T { T r[9]; T t[3]; };
+template <class T> __device__ inline V3T<T> rotv(const R34T<T>& m, V3T<T> v) {
+    return {m.r[0] * v.x + m.r[1] * v.y + m.r[2] * v.z, m.r[3] * v.x + m.r[4] * v.y + m.r[5] * v.z,
+            m.r[6] * v.x + m.r[7] * v.y + m.r[8] * v.z};
+}
+template <class T> __device__ inline V3T<T> appv(const R34T<T>& m, V3T<T> v) {
+    const V3T<T> a = rotv(m, v);
+    return {a.x + m.t[0], a.y + m.t[1], a.z + m.t[2]};
+}
+
+// float -> double by bit manipulation (integer pipe; the FP64 conversion
+// instruction is a narrow pipe on this part). Exact for zero and normal
+// floats; float subnormals become signed zero.
+__device__ inline double f2d(float f) {
+    const uint32_t b = __float_as_uint(f);
+    const uint32_t em = b & 0x7fffffffu, sign = b & 0x80000000u;
+    const bool normal = em >= 0x00800000u;
+    const uint32_t hi = normal ? (sign | ((em >> 3) + (896u << 20))) : sign;
+    const uint32_t lo = normal ? (em << 29) : 0u;
+    return __hiloint2double((int)hi, (int)lo);
+}
+template <class T> __device__ inline T cvt(float x);
+template <> __device__ inline float cvt<float>(float x) { return x; }
+template <> __device__ inline double cvt<double>(float x) { return f2d(x); }
+template <class T> __device__ inline T rsqrt_t(T x);
+template <> __device__ inline float rsqrt_t<float>(float x) { return rsqrtf(x); }
+template <> __device__ inline double rsqrt_t<double>(double x) { return rsqrt(x); }
+
+template <class T> __device__ inline R34T<T> view_mat(const ViewDesc& V, int which);
+template <> __device__ inline R34T<float> view_mat<float>(const ViewDesc& V, int which) {
+    const M34& m = which == 0 ? V.w2c : (which == 1 ? V.init : V.init_inv);
+    R34T<float> o;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) o.r[q] = m.r[q];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) o.t[q] = m.t[q];
+    return o;
+}
+template <> __device__ inline R34T<double> view_mat<double>(const ViewDesc& V, int which) {
+    const double* m = which == 0 ? V.w2c_d : (which == 1 ? V.init_d : V.init_inv_d);
+    R34T<double> o;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) o.r[q] = m[q];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) o.t[q] = m[9 + q];
+    return o;
+}
+
+// averageDualQuaternion + DualQuaternion::se3_matrix (DualQuaternion.h:281-393)
+// in T; `n` nodes (1 for a single node's own transform)
+template <class T>
+__device__ inline R34T<T> blended_se3(const DQ* field, const unsigned short* nodes, const float* w, int n) {
+    T q0[4] = {0, 0, 0, 0}, q1[4] = {0, 0, 0, 0};
+    for (int k = 0; k < n; ++k) {
+        const DQ d = load_dq(field, nodes[k]);
+        const T s = cvt<T>(w[k]);
+        q0[0] += s * cvt<T>(d.q0.x); q0[1] += s * cvt<T>(d.q0.y); q0[2] += s * cvt<T>(d.q0.z); q0[3] += s * cvt<T>(d.q0.w);
+        q1[0] += s * cvt<T>(d.q1.x); q1[1] += s * cvt<T>(d.q1.y); q1[2] += s * cvt<T>(d.q1.z); q1[3] += s * cvt<T>(d.q1.w);
+    }
+    const T inv = rsqrt_t<T>(q0[0] * q0[0] + q0[1] * q0[1] + q0[2] * q0[2] + q0[3] * q0[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { q0[i] *= inv; q1[i] *= inv; }
+    const T dd = q0[0] * q1[0] + q0[1] * q1[1] + q0[2] * q1[2] + q0[3] * q1[3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q1[i] -= dd * q0[i];
+    const T x = q0[0], y = q0[1], z = q0[2], ww = q0[3];
+    R34T<T> m;
+    m.r[0] = 1 - 2 * y * y - 2 * z * z; m.r[1] = 2 * x * y - 2 * z * ww; m.r[2] = 2 * x * z + 2 * y * ww;
+    m.r[3] = 2 * x * y + 2 * z * ww; m.r[4] = 1 - 2 * x * x - 2 * z * z; m.r[5] = 2 * y * z - 2 * x * ww;
+    m.r[6] = 2 * x * z - 2 * y * ww; m.r[7] = 2 * y * z + 2 * x * ww; m.r[8] = 1 - 2 * x * x - 2 * y * y;
+    // 2 q1 conj(q0), vector part
+    const T a0 = 2 * q1[0], a1 = 2 * q1[1], a2 = 2 * q1[2], a3 = 2 * q1[3];
+    const T b0 = -x, b1 = -y, b2 = -z, b3 = ww;
+    m.t[0] = a3 * b0 + a0 * b3 + a1 * b2 - a2 * b1;
+    m.t[1] = a3 * b1 - a0 * b2 + a1 * b3 + a2 * b0;
+    m.t[2] = a3 * b2 + a0 * b1 - a1 * b0 + a2 * b3;
+    return m;
+}
+
+template <class T>
 __global__ void __launch_bounds__(256) eval_terms_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     if (bad_inputs(I)) return;
     TermOffsets off;
     off.load(I.counts);
     const uint32_t Td = off.o[0];
-    const uint32_t T = off.o[4];
+    const uint32_t T_all = off.o[4];
     const float clip = 64.f * I.node_radius * I.node_radius;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T_all; t += gridDim.x * blockDim.x) {
         uint32_t k;
         const TermType ty = off.typed(t, k);
         if (ty == kDense) {
@@ -38,27 +126,34 @@ __global__ void __launch_bounds__(256) eval_terms_kernel(const InstDesc* insts) 
             const float4 cv = I.dense_cv[k], cn = I.dense_cn[k];
             const uint32_t v = __float_as_uint(cv.w);
             const ViewDesc& V = I.views[v];
-            const M34 se3 = dq_se3(blend_dq(I.se3, I.dense_knn[k], I.dense_w[k]));
-            const float3 wv = apply3(se3, mk3(cv.x, cv.y, cv.z));
-            const float3 wn = rot3(se3, mk3(cn.x, cn.y, cn.z));
-            const float3 vc = apply3(V.init_inv, apply3(V.w2c, wv));
-            const float3 nc = rot3(V.init_inv, rot3(V.w2c, wn));
-            const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
-            const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
+            const ushort4 kn = I.dense_knn[k];
+            const float4 w4 = I.dense_w[k];
+            const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
+            const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
+            const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
+            const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
+            const V3T<T> wv = appv(se3, v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z)));
+            const V3T<T> wn = rotv(se3, v3t(cvt<T>(cn.x), cvt<T>(cn.y), cvt<T>(cn.z)));
+            const V3T<T> vc = appv(iinv, appv(w2c, wv));
+            const V3T<T> nc = rotv(iinv, rotv(w2c, wn));
+            const int u = project_coord((float)vc.x, (float)vc.z, V.fx, V.cx);
+            const int w = project_coord((float)vc.y, (float)vc.z, V.fy, V.cy);
             float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
             if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height) {
                 const size_t p = (size_t)w * V.pitch + u;
                 const float4 dv4 = V.obs_v[p], dn4 = V.obs_n[p];
-                const float3 dv = mk3(dv4.x, dv4.y, dv4.z), dn = mk3(dn4.x, dn4.y, dn4.z);
+                const V3T<T> dv = v3t(cvt<T>(dv4.x), cvt<T>(dv4.y), cvt<T>(dv4.z));
+                const V3T<T> dn = v3t(cvt<T>(dn4.x), cvt<T>(dn4.y), cvt<T>(dn4.z));
                 bool valid = true;
                 if (fabsf(dv4.x) < 1e-3f && fabsf(dv4.y) < 1e-3f && fabsf(dv4.z) < 1e-3f) valid = false;
-                if (dot3(dn, nc) < 0.7f) valid = false;
-                const float3 df = sub3(dv, vc);
-                if (dot3(df, df) > 0.075f * 0.075f) valid = false;
+                if (dotv(dn, nc) < (T)0.7f) valid = false;
+                const V3T<T> df = sub(dv, vc);
+                if (dotv(df, df) > (T)(0.075f * 0.075f)) valid = false;
                 if (valid) {
-                    const float r = dot3(dn, sub3(vc, dv));
-                    const float3 tr = rotT3(V.w2c, rot3(V.init, dn));
-                    const float3 ro = cross3(wv, tr);
+                    const float r = (float)dotv(dn, sub(vc, dv));
+                    const float3 dnf = mk3(dn4.x, dn4.y, dn4.z);
+                    const float3 tr = rotT3(V.w2c, rot3(V.init, dnf));
+                    const float3 ro = cross3(mk3((float)wv.x, (float)wv.y, (float)wv.z), tr);
                     o0 = make_float4(ro.x, ro.y, ro.z, tr.x);
                     o1 = make_float4(tr.y, tr.z, r, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
                 }
@@ -69,21 +164,31 @@ __global__ void __launch_bounds__(256) eval_terms_kernel(const InstDesc* insts) 
             // forwardWarpSmootherNodeKernel (NodeGraphSmoothHandler.cu:10-43)
             const ushort2 e = I.graph[k];
             const float4 xi = I.nodes[e.x], xj = I.nodes[e.y];
-            const M34 Ti = dq_se3(load_dq(I.se3, e.x)), Tj = dq_se3(load_dq(I.se3, e.y));
-            const float3 a = apply3(Ti, mk3(xj.x, xj.y, xj.z)), b = apply3(Tj, mk3(xj.x, xj.y, xj.z));
+            const float one = 1.f;
+            const R34T<T> Ti = blended_se3<T>(I.se3, &e.x, &one, 1), Tj = blended_se3<T>(I.se3, &e.y, &one, 1);
+            const V3T<T> xjt = v3t(cvt<T>(xj.x), cvt<T>(xj.y), cvt<T>(xj.z));
+            const V3T<T> a = appv(Ti, xjt), b = appv(Tj, xjt);
             const float3 dd = mk3(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
             const float valid = dot3(dd, dd) > clip ? 0.f : 1.f;
-            I.smooth[2 * (size_t)k] = make_float4(a.x, a.y, a.z, b.x);
-            I.smooth[2 * (size_t)k + 1] = make_float4(b.y, b.z, valid, 0.f);
+            I.smooth[3 * (size_t)k] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)b.x);
+            I.smooth[3 * (size_t)k + 1] = make_float4((float)b.y, (float)b.z, valid, 0.f);
+            I.smooth[3 * (size_t)k + 2] = make_float4((float)(a.x - b.x), (float)(a.y - b.y), (float)(a.z - b.z), 0.f);
         } else if (ty == kForeground) {
             // computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual;
             // the canonical vertex is taken to frame 0 first, as the dense term does
             const float4 cv = I.fg_cv[k];
             const uint32_t v = __float_as_uint(cv.w);
             const ViewDesc& V = I.views[v];
-            const M34 se3 = dq_se3(blend_dq(I.se3, I.fg_knn[k], I.fg_w[k]));
-            const float3 wv = apply3(se3, mk3(cv.x, cv.y, cv.z));
-            const float3 vc = apply3(V.init_inv, apply3(V.w2c, wv));
+            const ushort4 kn = I.fg_knn[k];
+            const float4 w4 = I.fg_w[k];
+            const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
+            const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
+            const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
+            const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
+            const V3T<T> wvt = appv(se3, v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z)));
+            const V3T<T> vct = appv(iinv, appv(w2c, wvt));
+            const float3 wv = mk3((float)wvt.x, (float)wvt.y, (float)wvt.z);
+            const float3 vc = mk3((float)vct.x, (float)vct.y, (float)vct.z);
             const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
             const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
             float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
@@ -105,9 +210,17 @@ __global__ void __launch_bounds__(256) eval_terms_kernel(const InstDesc* insts) 
             // forwardWarpFeatureVertexKernel (SparseCorrespondenceHandler.cu:202-220)
             const bool f = ty == kFeature;
             const float4 ref = f ? I.feat_ref[k] : I.cross_ref[k];
-            const M34 se3 = dq_se3(blend_dq(I.se3, f ? I.feat_knn[k] : I.cross_knn[k], f ? I.feat_w[k] : I.cross_w[k]));
-            const float3 wv = apply3(se3, mk3(ref.x, ref.y, ref.z));
-            I.warped[f ? k : I.Tp + k] = make_float4(wv.x, wv.y, wv.z, 1.0f);
+            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const ushort4 kn = f ? I.feat_knn[k] : I.cross_knn[k];
+            const float4 w4 = f ? I.feat_w[k] : I.cross_w[k];
+            const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
+            const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
+            const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
+            const V3T<T> wv = appv(se3, v3t(cvt<T>(ref.x), cvt<T>(ref.y), cvt<T>(ref.z)));
+            const V3T<T> raw = sub(wv, v3t(cvt<T>(tg.x), cvt<T>(tg.y), cvt<T>(tg.z)));
+            const size_t o = 2 * (size_t)(f ? k : I.Tp + k);
+            I.warped[o] = make_float4((float)wv.x, (float)wv.y, (float)wv.z, 1.0f);
+            I.warped[o + 1] = make_float4((float)raw.x, (float)raw.y, (float)raw.z, 0.0f);
         }
     }
 }
@@ -150,13 +263,14 @@ __device__ inline int term_rows(const InstDesc& I, const TermOffsets& off, const
             return 1;
         }
         case kSmooth: {
-            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
             if (b.z == 0.f) return 0;
+            const float4 rr = I.smooth[3 * (size_t)k + 2];
             const bool is_i = node == I.graph[k].x;
             const float3 ti = mk3(a.x, a.y, a.z), tj = mk3(a.w, b.x, b.y);
             float one[3] = {1.f, 1.f, 1.f};
             skew_rows(is_i ? ti : tj, is_i ? 1.f : -1.f, one, o);
-            o.r[0] = ti.x - tj.x; o.r[1] = ti.y - tj.y; o.r[2] = ti.z - tj.z;
+            o.r[0] = rr.x; o.r[1] = rr.y; o.r[2] = rr.z;
             o.lam2 = lam.smooth * lam.smooth;
             o.w = 1.f;
             return 3;
@@ -164,9 +278,9 @@ __device__ inline int term_rows(const InstDesc& I, const TermOffsets& off, const
         case kFeature:
         case kCross: {
             const bool f = ty == kFeature;
-            const float4 wv = I.warped[f ? k : I.Tp + k];
-            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
-            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+            const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
+            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
+            const float raw[3] = {rw.x, rw.y, rw.z};
             float hw[3] = {huber_weight(raw[0]), huber_weight(raw[1]), huber_weight(raw[2])};
             skew_rows(mk3(wv.x, wv.y, wv.z), 1.f, hw, o);
             o.r[0] = hw[0] * raw[0]; o.r[1] = hw[1] * raw[1]; o.r[2] = hw[2] * raw[2];
@@ -210,17 +324,19 @@ __device__ inline void gauss_jordan6(const float* Din, float* out) {
         for (int i = 0; i < 6; ++i) out[6 * reloc[j] + i] = m[i + 6 * j];
 }
 
-// 6x6 Cholesky in double; packed lower triangle L[i(i+1)/2 + j], j <= i
+// 6x6 Cholesky in double; packed lower triangle L[i(i+1)/2 + j], j <= i, with
+// the RECIPROCALS of the diagonal stored on the diagonal so that the solves
+// applied every PCG iteration only multiply
 template <class T> __device__ inline void cholesky6(const T* A, double* L) {
     for (int j = 0; j < 6; ++j) {
         double s = A[6 * j + j];
         for (int k = 0; k < j; ++k) s -= L[j * (j + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
-        const double ljj = sqrt(s);
-        L[j * (j + 1) / 2 + j] = ljj;
+        const double inv = 1.0 / sqrt(s);
+        L[j * (j + 1) / 2 + j] = inv;
         for (int i = j + 1; i < 6; ++i) {
             double t = A[6 * i + j];
             for (int k = 0; k < j; ++k) t -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
-            L[i * (i + 1) / 2 + j] = t / ljj;
+            L[i * (i + 1) / 2 + j] = t * inv;
         }
     }
 }
@@ -232,14 +348,14 @@ __device__ inline void cholesky6_solve(const double* L, const double* b, double*
         double t = b[i];
 #pragma unroll
         for (int k = 0; k < i; ++k) t -= L[i * (i + 1) / 2 + k] * y[k];
-        y[i] = t / L[i * (i + 1) / 2 + i];
+        y[i] = t * L[i * (i + 1) / 2 + i];
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
         double t = y[i];
 #pragma unroll
         for (int k = i + 1; k < 6; ++k) t -= L[k * (k + 1) / 2 + i] * x[k];
-        x[i] = t / L[i * (i + 1) / 2 + i];
+        x[i] = t * L[i * (i + 1) / 2 + i];
     }
 }
 
@@ -284,11 +400,11 @@ constexpr int kDiagStride = 23;  // u[3][6], lambda^2, rb[3], channel count
 // sum_c u_c v_c^T with u_c = J_i,c-side rows and v_c the lambda^2-weighted
 // J_j,c-side rows; returns the channel count.
 template <class T>
-__device__ inline void stage_pair(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
+__device__ inline int stage_pair(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
                                   uint32_t ni, uint32_t nj, T* o) {
     uint32_t k;
     const TermType ty = off.typed(t, k);
-    T nch = 0;
+    int nch = 0;
     switch (ty) {
         case kDense:
         case kForeground: {
@@ -296,9 +412,9 @@ __device__ inline void stage_pair(const InstDesc& I, const TermOffsets& off, con
             const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
             const ushort4 kn = term_nodes(I, ty, k);
             const float4 w4 = term_weights(I, ty, k);
-            const T l2 = ty == kDense ? (T)1 : (T)(lam.foreground * lam.foreground);
-            const T wi = (T)weight_of(kn, w4, ni), wj = l2 * (T)weight_of(kn, w4, nj);
-            const T J[6] = {(T)a.x, (T)a.y, (T)a.z, (T)a.w, (T)b.x, (T)b.y};
+            const T l2 = ty == kDense ? (T)1 : cvt<T>(lam.foreground * lam.foreground);
+            const T wi = cvt<T>(weight_of(kn, w4, ni)), wj = l2 * cvt<T>(weight_of(kn, w4, nj));
+            const T J[6] = {cvt<T>(a.x), cvt<T>(a.y), cvt<T>(a.z), cvt<T>(a.w), cvt<T>(b.x), cvt<T>(b.y)};
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
                 o[q] = wi * J[q];
@@ -308,16 +424,16 @@ __device__ inline void stage_pair(const InstDesc& I, const TermOffsets& off, con
             break;
         }
         case kSmooth: {
-            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
             if (b.z == 0.f) break;
             const bool is_i = ni == I.graph[k].x;
             const float4 pi = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
             const float4 pj = is_i ? make_float4(a.w, b.x, b.y, 0.f) : a;
             T fi[3][6], fj[3][6];
-            twist_rows<T>((T)pi.x, (T)pi.y, (T)pi.z, fi);
-            twist_rows<T>((T)pj.x, (T)pj.y, (T)pj.z, fj);
+            twist_rows<T>(cvt<T>(pi.x), cvt<T>(pi.y), cvt<T>(pi.z), fi);
+            twist_rows<T>(cvt<T>(pj.x), cvt<T>(pj.y), cvt<T>(pj.z), fj);
             // J_i,c = +-f_c(p_i), J_j,c = -+f_c(p_j): their product carries a minus
-            const T l2 = -(T)(lam.smooth * lam.smooth);
+            const T l2 = -cvt<T>(lam.smooth * lam.smooth);
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -331,20 +447,20 @@ __device__ inline void stage_pair(const InstDesc& I, const TermOffsets& off, con
         case kFeature:
         case kCross: {
             const bool f = ty == kFeature;
-            const float4 wv = I.warped[f ? k : I.Tp + k];
-            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
+            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
             const ushort4 kn = term_nodes(I, ty, k);
             const float4 w4 = term_weights(I, ty, k);
-            const T l2 = f ? (T)(lam.feature * lam.feature) : (T)(lam.cross_view * lam.cross_view);
-            const T wi = (T)weight_of(kn, w4, ni), wj = l2 * (T)weight_of(kn, w4, nj);
-            const float hw[3] = {huber_weight(wv.x - tg.x), huber_weight(wv.y - tg.y), huber_weight(wv.z - tg.z)};
+            const T l2 = f ? cvt<T>(lam.feature * lam.feature) : cvt<T>(lam.cross_view * lam.cross_view);
+            const T wi = cvt<T>(weight_of(kn, w4, ni)), wj = l2 * cvt<T>(weight_of(kn, w4, nj));
+            const float hw[3] = {huber_weight(rw.x), huber_weight(rw.y), huber_weight(rw.z)};
             T fr[3][6];
-            twist_rows<T>((T)wv.x, (T)wv.y, (T)wv.z, fr);
+            twist_rows<T>(cvt<T>(wv.x), cvt<T>(wv.y), cvt<T>(wv.z), fr);
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
                 for (int q = 0; q < 6; ++q) {
-                    const T jv = (T)hw[c] * fr[c][q];
+                    const T jv = cvt<T>(hw[c]) * fr[c][q];
                     o[6 * c + q] = wi * jv;
                     o[18 + 6 * c + q] = wj * jv;
                 }
@@ -353,42 +469,43 @@ __device__ inline void stage_pair(const InstDesc& I, const TermOffsets& off, con
         }
         default: break;
     }
-    o[36] = nch;
+    return nch;
 }
 
 // Diagonal descriptor of term t for node n: D += lambda^2 sum_c u_c u_c^T,
 // b += sum_c u_c rb_c.
 template <class T>
-__device__ inline void stage_diag(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
+__device__ inline int stage_diag(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
                                   uint32_t n, T* o) {
     uint32_t k;
     const TermType ty = off.typed(t, k);
-    T nch = 0;
+    int nch = 0;
     switch (ty) {
         case kDense:
         case kForeground: {
             const uint32_t idx = ty == kDense ? k : off.o[0] + k;
             const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
-            const T l2 = ty == kDense ? (T)1 : (T)(lam.foreground * lam.foreground);
-            const T w = (T)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n);
-            const T J[6] = {(T)a.x, (T)a.y, (T)a.z, (T)a.w, (T)b.x, (T)b.y};
+            const T l2 = ty == kDense ? (T)1 : cvt<T>(lam.foreground * lam.foreground);
+            const T w = cvt<T>(weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n));
+            const T J[6] = {cvt<T>(a.x), cvt<T>(a.y), cvt<T>(a.z), cvt<T>(a.w), cvt<T>(b.x), cvt<T>(b.y)};
 #pragma unroll
             for (int q = 0; q < 6; ++q) o[q] = w * J[q];
             o[18] = l2;
-            o[19] = -l2 * (T)b.z;
+            o[19] = -l2 * cvt<T>(b.z);
             nch = 1;
             break;
         }
         case kSmooth: {
-            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
             if (b.z == 0.f) break;
+            const float4 rr = I.smooth[3 * (size_t)k + 2];
             const bool is_i = n == I.graph[k].x;
             const float4 p = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
             T fr[3][6];
-            twist_rows<T>((T)p.x, (T)p.y, (T)p.z, fr);
-            const T l2 = (T)(lam.smooth * lam.smooth);
+            twist_rows<T>(cvt<T>(p.x), cvt<T>(p.y), cvt<T>(p.z), fr);
+            const T l2 = cvt<T>(lam.smooth * lam.smooth);
             const T sg = is_i ? (T)1 : (T)-1;
-            const T rc[3] = {(T)a.x - (T)a.w, (T)a.y - (T)b.x, (T)a.z - (T)b.y};
+            const T rc[3] = {cvt<T>(rr.x), cvt<T>(rr.y), cvt<T>(rr.z)};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -402,19 +519,19 @@ __device__ inline void stage_diag(const InstDesc& I, const TermOffsets& off, con
         case kFeature:
         case kCross: {
             const bool f = ty == kFeature;
-            const float4 wv = I.warped[f ? k : I.Tp + k];
-            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
-            const T l2 = f ? (T)(lam.feature * lam.feature) : (T)(lam.cross_view * lam.cross_view);
-            const T w = (T)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n);
-            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+            const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
+            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
+            const T l2 = f ? cvt<T>(lam.feature * lam.feature) : cvt<T>(lam.cross_view * lam.cross_view);
+            const T w = cvt<T>(weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n));
+            const float raw[3] = {rw.x, rw.y, rw.z};
             T fr[3][6];
-            twist_rows<T>((T)wv.x, (T)wv.y, (T)wv.z, fr);
+            twist_rows<T>(cvt<T>(wv.x), cvt<T>(wv.y), cvt<T>(wv.z), fr);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const T hw = (T)huber_weight(raw[c]);
+                const T hw = cvt<T>(huber_weight(raw[c]));
 #pragma unroll
                 for (int q = 0; q < 6; ++q) o[6 * c + q] = w * hw * fr[c][q];
-                o[19 + c] = -l2 * hw * (T)raw[c];
+                o[19 + c] = -l2 * hw * cvt<T>(raw[c]);
             }
             o[18] = l2;
             nch = 3;
@@ -422,7 +539,7 @@ __device__ inline void stage_diag(const InstDesc& I, const TermOffsets& off, con
         }
         default: break;
     }
-    o[22] = nch;
+    return nch;
 }
 
 template <bool MIXED>
@@ -430,6 +547,7 @@ __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mv
     using Acc = typename std::conditional<MIXED, double, float>::type;
     constexpr int kWarps = 4;
     __shared__ Acc stage[kWarps][32][kDiagStride];
+    __shared__ int nchs[kWarps][32];
     __shared__ Acc vals[kWarps][4][28];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
@@ -464,14 +582,12 @@ __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mv
         Acc acc[4] = {0, 0, 0, 0};
         for (uint32_t ch = 0; ch < nchunks; ++ch) {
             const uint32_t p = b + ch * kGroupLanes + l8;
-            Acc* my = stage[w][lane];
-            if (p < e) stage_diag<Acc>(I, off, lam, I.n2t_index[p], node, my);
-            else my[22] = 0;
+            nchs[w][lane] = p < e ? stage_diag<Acc>(I, off, lam, I.n2t_index[p], node, stage[w][lane]) : 0;
             __syncwarp();
 #pragma unroll 2
             for (int q = 0; q < kGroupLanes; ++q) {
                 const Acc* d = stage[w][g * kGroupLanes + q];
-                const int nch = (int)d[22];
+                const int nch = nchs[w][g * kGroupLanes + q];
                 for (int c = 0; c < nch; ++c) {
                     const Acc* u = d + 6 * c;
 #pragma unroll
@@ -538,6 +654,7 @@ __global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvd
     using Acc = typename std::conditional<MIXED, double, float>::type;
     constexpr int kWarps = 4;
     __shared__ Acc stage[kWarps][32][kPairStride];
+    __shared__ int nchs[kWarps][32];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2) return;
@@ -572,14 +689,12 @@ __global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvd
         Acc acc[5] = {0, 0, 0, 0, 0};
         for (uint32_t ch = 0; ch < nchunks; ++ch) {
             const uint32_t p = rg.x + ch * kGroupLanes + l8;
-            Acc* my = stage[w][lane];
-            if (p < rg.y) stage_pair<Acc>(I, off, lam, I.np_index[p], ni, nj, my);
-            else my[36] = 0;
+            nchs[w][lane] = p < rg.y ? stage_pair<Acc>(I, off, lam, I.np_index[p], ni, nj, stage[w][lane]) : 0;
             __syncwarp();
 #pragma unroll 2
             for (int q = 0; q < kGroupLanes; ++q) {
                 const Acc* d = stage[w][g * kGroupLanes + q];
-                const int nch = (int)d[36];
+                const int nch = nchs[w][g * kGroupLanes + q];
                 for (int c = 0; c < nch; ++c) {
                     const Acc* u = d + 6 * c;
                     const Acc* v = d + 18 + 6 * c;
@@ -699,6 +814,7 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
     const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
     size_t blk = 36 * (size_t)(so + br) + 6 * r;
     typename std::conditional<MIXED, double, float>::type acc = 0;
+    float corr = 0.f;
     for (uint32_t s = so; s <= se; ++s, blk += 36) {
         const uint32_t col = (s == so) ? br : (I.sym_key[s - 1] & mask);
         const float* a = I.bsr + blk;
@@ -713,19 +829,22 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
             xv[k] = xp ? xs[e] + beta * xp[e] : xs[e];
         }
         if (MIXED) {
+            // a = hi (1 + lo 2^-24): hi x in double, the correction hi lo x in
+            // float (it is 2^-24 of the term, so float accuracy is plenty)
             const __half2* l = reinterpret_cast<const __half2*>(I.bsr_lo + blk);
             const float2 l01 = __half22float2(l[0]), l23 = __half22float2(l[1]), l45 = __half22float2(l[2]);
             const float lv[6] = {l01.x, l01.y, l23.x, l23.y, l45.x, l45.y};
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                const double ak = (double)av[k] * (1.0 + (double)lv[k] * kLoUnscale);
-                acc += ak * (double)xv[k];
+                acc += f2d(av[k]) * f2d(xv[k]);
+                corr += (av[k] * lv[k]) * xv[k];
             }
         } else {
 #pragma unroll
             for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
         }
     }
+    if (MIXED) return (float)(acc + f2d(corr) * kLoUnscale);
     return (float)acc;
 }
 
@@ -1024,17 +1143,16 @@ __global__ void __launch_bounds__(256) energy_kernel(const InstDesc* insts, mvdr
             const float v = l * I.term_jr[2 * (size_t)idx + 1].z;
             part += (double)v * v;
         } else if (ty == kSmooth) {
-            const float4 a = I.smooth[2 * (size_t)k], b = I.smooth[2 * (size_t)k + 1];
+            const float4 b = I.smooth[3 * (size_t)k + 1], rr = I.smooth[3 * (size_t)k + 2];
             if (b.z != 0.f) {
-                const float r0 = lam.smooth * (a.x - a.w), r1 = lam.smooth * (a.y - b.x), r2 = lam.smooth * (a.z - b.y);
+                const float r0 = lam.smooth * rr.x, r1 = lam.smooth * rr.y, r2 = lam.smooth * rr.z;
                 part += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
             }
         } else if (ty == kFeature || ty == kCross) {
             const bool f = ty == kFeature;
-            const float4 wv = I.warped[f ? k : I.Tp + k];
-            const float4 tg = f ? I.feat_target[k] : I.cross_target[k];
+            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
             const float l = f ? lam.feature : lam.cross_view;
-            const float raw[3] = {wv.x - tg.x, wv.y - tg.y, wv.z - tg.z};
+            const float raw[3] = {rw.x, rw.y, rw.z};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const float v = l * (huber_weight(raw[c]) * raw[c]);
@@ -1083,7 +1201,8 @@ static inline dim3 grid2(uint32_t x, uint32_t B) { return dim3(x ? x : 1, B); }
 
 cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
     const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-    MVDR_LAUNCH(eval_terms_kernel, grid2(g, lc.B), 256, 0, st, d);
+    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(eval_terms_kernel<double>, grid2(g, lc.B), 256, 0, st, d);
+    else MVDR_LAUNCH(eval_terms_kernel<float>, grid2(g, lc.B), 256, 0, st, d);
     return cudaGetLastError();
 }
 

@@ -160,6 +160,8 @@ struct ViewDesc {
     uint32_t pitch;
     float cx, cy, fx, fy;
     M34 w2c, init, init_inv;
+    // the same transforms in double, for the mixed-precision residual chain
+    double w2c_d[12], init_d[12], init_inv_d[12];  // row-major rotation, then translation
 };
 
 // device-resident sizes of one instance (written by the index build)
@@ -248,8 +250,8 @@ struct InstDesc {
     float* bb_data;         // [bb cap]
     // per-iteration term data
     float4* term_jr;        // 2 float4 per dense+fg term: J(6), r, pixel bits
-    float4* smooth;         // 2 float4 per smooth term: Ti_xj(3), Tj_xj(3), valid, 0
-    float4* warped;         // per feature+cross term
+    float4* smooth;         // 3 float4 per smooth term: Ti_xj(3), Tj_xj(3), valid, 0, r(3), 0
+    float4* warped;         // 2 float4 per feature+cross term: warped(3), 1, raw residual(3), 0
     // assembly
     float* diag;            // [36N] JtJ diagonal blocks incl. damping
     float* minv;            // [36N] preconditioner (inverse diagonal), float

@@ -170,8 +170,8 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.bb_colptr = a.take<int32_t>(lc.cap_bb / 6 + 1);
     I.bb_data = nullptr;
     I.term_jr = a.take<float4>(2 * ((size_t)lc.cap_dense + lc.cap_fg));
-    I.smooth = a.take<float4>(2 * (size_t)cap_edges);
-    I.warped = a.take<float4>((size_t)max_tp + max_tc + 1);
+    I.smooth = a.take<float4>(3 * (size_t)cap_edges);
+    I.warped = a.take<float4>(2 * ((size_t)max_tp + max_tc + 1));
     I.diag = a.take<float>(36 * N);
     I.minv = a.take<float>(36 * N);
     I.chol = a.take<double>(21 * N);
@@ -397,6 +397,13 @@ static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStrea
         V.w2c = load34(S.world2camera);
         V.init = load34(S.initial_camera_se3);
         V.init_inv = inverse34(V.init);
+        // double copies for the mixed-precision residual chain
+        const M34* src[3] = {&V.w2c, &V.init, &V.init_inv};
+        double* dst[3] = {V.w2c_d, V.init_d, V.init_inv_d};
+        for (int m = 0; m < 3; ++m) {
+            for (int q = 0; q < 9; ++q) dst[m][q] = (double)src[m]->r[q];
+            for (int q = 0; q < 3; ++q) dst[m][9 + q] = (double)src[m]->t[q];
+        }
     }
     I.surfel_knn = reinterpret_cast<const ushort4*>(in->surfel_knn);
     I.surfel_w = reinterpret_cast<const float4*>(in->surfel_knn_weight);
@@ -625,9 +632,9 @@ static int get_array(Batch& b, uint32_t inst, int which, void* dst, size_t cap, 
         case MVDR_ARRAY_BINBLOCK_COLPTR: return copy_out(dst, I.bb_colptr, 4 * ((size_t)c.binblock_nnz / 6), cap, written);
         case MVDR_ARRAY_TERM_JACOBIAN:
             return copy_out(dst, I.term_jr, 32 * ((size_t)c.dense_terms + c.foreground_terms), cap, written);
-        case MVDR_ARRAY_SMOOTH_TERMS: return copy_out(dst, I.smooth, 32 * (size_t)I.E, cap, written);
+        case MVDR_ARRAY_SMOOTH_TERMS: return copy_out(dst, I.smooth, 48 * (size_t)I.E, cap, written);
         case MVDR_ARRAY_WARPED_CORRESPONDENCE:
-            return copy_out(dst, I.warped, 16 * ((size_t)I.Tp + I.Tc), cap, written);
+            return copy_out(dst, I.warped, 32 * ((size_t)I.Tp + I.Tc), cap, written);
         case MVDR_ARRAY_DIAG_BLOCKS: return copy_out(dst, I.diag, 4 * 36 * N, cap, written);
         case MVDR_ARRAY_JTR: return copy_out(dst, I.jtr, 4 * 6 * N, cap, written);
         case MVDR_ARRAY_INCREMENT: return copy_out(dst, I.x, 4 * 6 * N, cap, written);

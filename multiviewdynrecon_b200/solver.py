@@ -29,7 +29,7 @@ ARRAY_SPEC = {
     abi.ARRAY_NODEPAIR_KEY: (np.uint32, 1), abi.ARRAY_NODEPAIR_TERM_RANGE: (np.uint32, 2),
     abi.ARRAY_BLKROW_OFFSET: (np.uint32, 1), abi.ARRAY_BINBLOCK_ROWPTR: (np.int32, 1),
     abi.ARRAY_BINBLOCK_COLPTR: (np.int32, 1), abi.ARRAY_TERM_JACOBIAN: (np.float32, 8),
-    abi.ARRAY_SMOOTH_TERMS: (np.float32, 8), abi.ARRAY_WARPED_CORRESPONDENCE: (np.float32, 4),
+    abi.ARRAY_SMOOTH_TERMS: (np.float32, 12), abi.ARRAY_WARPED_CORRESPONDENCE: (np.float32, 8),
     abi.ARRAY_DIAG_BLOCKS: (np.float32, 36), abi.ARRAY_JTR: (np.float32, 6),
     abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
     abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),

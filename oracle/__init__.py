@@ -77,7 +77,7 @@ _ARRAY_SPEC = {
     abi.ARRAY_NODEPAIR_KEY: (np.uint32, 1), abi.ARRAY_NODEPAIR_TERM_RANGE: (np.uint32, 2),
     abi.ARRAY_BLKROW_OFFSET: (np.uint32, 1), abi.ARRAY_BINBLOCK_ROWPTR: (np.int32, 1),
     abi.ARRAY_BINBLOCK_COLPTR: (np.int32, 1), abi.ARRAY_TERM_JACOBIAN: (np.float32, 8),
-    abi.ARRAY_SMOOTH_TERMS: (np.float32, 8), abi.ARRAY_WARPED_CORRESPONDENCE: (np.float32, 4),
+    abi.ARRAY_SMOOTH_TERMS: (np.float32, 12), abi.ARRAY_WARPED_CORRESPONDENCE: (np.float32, 8),
     abi.ARRAY_DIAG_BLOCKS: (np.float32, 36), abi.ARRAY_JTR: (np.float32, 6),
     abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
     abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
@@ -142,7 +142,7 @@ class Oracle:
         """Freeze projected pixels / validity from another run's term data."""
         jr = np.ascontiguousarray(term_jr, np.float32).reshape(-1, 8)
         pix = np.ascontiguousarray(jr[:, 7].view(np.uint32))
-        sv = np.ascontiguousarray((np.asarray(smooth, np.float32).reshape(-1, 8)[:, 6] != 0).astype(np.uint8))
+        sv = np.ascontiguousarray((np.asarray(smooth, np.float32).reshape(-1, 12)[:, 6] != 0).astype(np.uint8))
         lib().orc_freeze_decisions(self.h, _p(pix), _p(sv))
 
     def unfreeze(self):

@@ -664,8 +664,8 @@ struct Oracle {
     template <class R> void eval_terms_t() {
         const auto f = field<R>();
         term_jr.assign(8 * (size_t)(Td + Tf), 0.0f);
-        smooth.assign(8 * (size_t)Ts, 0.0f);
-        warped.assign(4 * (size_t)(Tp + Tc), 0.0f);
+        smooth.assign(12 * (size_t)Ts, 0.0f);
+        warped.assign(8 * (size_t)(Tp + Tc), 0.0f);
         std::vector<M34<R>> init(V), inv(V), w2c(V);
         for (u32 v = 0; v < V; ++v) {
             const M34<float> i32 = load_mat34<float>(views[v].init);
@@ -743,11 +743,14 @@ struct Oracle {
             const V3<R> dd = xi - xj;
             float valid = dot(dd, dd) > clip ? 0.0f : 1.0f;
             if (frozen) valid = frozen_smooth[k] ? 1.0f : 0.0f;
-            float* o = &smooth[8 * (size_t)k];
+            // record: Ti xj, Tj xj, validity, 0, residual Ti xj - Tj xj (in R), 0
+            float* o = &smooth[12 * (size_t)k];
             o[0] = (float)a.x; o[1] = (float)a.y; o[2] = (float)a.z;
             o[3] = (float)bq.x; o[4] = (float)bq.y; o[5] = (float)bq.z;
             o[6] = valid;
             o[7] = 0;
+            o[8] = (float)(a.x - bq.x); o[9] = (float)(a.y - bq.y); o[10] = (float)(a.z - bq.z);
+            o[11] = 0;
         }
         // foreground: computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual
         // (DensityForegroundJacobianResidual.cu:93-142, density_map_jacobian.cuh:12-79).
@@ -793,12 +796,17 @@ struct Oracle {
         }
         // sparse feature / cross view: forwardWarpFeatureVertexKernel
         // (SparseCorrespondenceHandler.cu:202-220)
+        // record: warped vertex, 1, raw residual warped - target (in R), 0
         auto warp_corr = [&](const Corr& c, u32 count, u32 base) {
             for (u32 k = 0; k < count; ++k) {
                 const M34<R> se3 = se3_matrix(blend(f, &c.knn[4 * (size_t)k], &c.w[k].x));
                 const V3<R> w = se3.apply(V3<R>{(R)c.ref[k].x, (R)c.ref[k].y, (R)c.ref[k].z});
-                float* o = &warped[4 * (size_t)(base + k)];
+                float* o = &warped[8 * (size_t)(base + k)];
                 o[0] = (float)w.x; o[1] = (float)w.y; o[2] = (float)w.z; o[3] = 1.0f;
+                o[4] = (float)(w.x - (R)c.target[k].x);
+                o[5] = (float)(w.y - (R)c.target[k].y);
+                o[6] = (float)(w.z - (R)c.target[k].z);
+                o[7] = 0.0f;
             }
         };
         warp_corr(feat, Tp, 0);
@@ -825,7 +833,7 @@ struct Oracle {
                 return 1;
             }
             case kSmooth: {
-                const float* s = &smooth[8 * (size_t)k];
+                const float* s = &smooth[12 * (size_t)k];
                 lam2 = (double)lambda.smooth * lambda.smooth;
                 wnode = 1.0;
                 if (s[6] == 0.0f) return 0;
@@ -838,20 +846,20 @@ struct Oracle {
                 for (int c = 0; c < 3; ++c) {
                     for (int i = 0; i < 3; ++i) J[c][i] = sg * rot[c][i];
                     for (int i = 0; i < 3; ++i) J[c][3 + i] = (c == i) ? sg : 0.0;
-                    r[c] = a[c] - bq[c];
+                    r[c] = s[8 + c];
                 }
                 return 3;
             }
             case kFeature:
             case kCross: {
                 const Corr& c = t == kFeature ? feat : cross;
-                const float* wv = &warped[4 * (size_t)(t == kFeature ? k : Tp + k)];
-                const mvdr_float4 tg = c.target[k];
+                const float* wv = &warped[8 * (size_t)(t == kFeature ? k : Tp + k)];
+                (void)c;
                 lam2 = t == kFeature ? (double)lambda.feature * lambda.feature
                                      : (double)lambda.cross_view * lambda.cross_view;
                 wnode = weight_of(knn_of(t, k), w_of(t, k));
                 // computePointToPointICPTermJacobian / residual (geometry_icp_jacobian.cuh:50-120)
-                const float raw[3] = {wv[0] - tg.x, wv[1] - tg.y, wv[2] - tg.z};
+                const float raw[3] = {wv[4], wv[5], wv[6]};
                 const double rot[3][3] = {{0, wv[2], -wv[1]}, {-wv[2], 0, wv[0]}, {wv[1], -wv[0], 0}};
                 for (int ch = 0; ch < 3; ++ch) {
                     const double hw = huber<float>(raw[ch]);
@@ -1064,9 +1072,9 @@ struct Oracle {
         double e = 0;
         for (u32 k = 0; k < Td; ++k) { const double r = term_jr[8 * (size_t)k + 6]; e += r * r; }
         for (u32 k = 0; k < Ts; ++k) {
-            const float* s = &smooth[8 * (size_t)k];
+            const float* s = &smooth[12 * (size_t)k];
             if (s[6] == 0.0f) continue;
-            for (int c = 0; c < 3; ++c) { const double r = (double)lambda.smooth * (s[c] - s[3 + c]); e += r * r; }
+            for (int c = 0; c < 3; ++c) { const double r = (double)lambda.smooth * s[8 + c]; e += r * r; }
         }
         for (u32 k = 0; k < Tf; ++k) {
             const double r = (double)lambda.foreground * term_jr[8 * (size_t)(Td + k) + 6];
@@ -1074,8 +1082,9 @@ struct Oracle {
         }
         auto p2p = [&](const Corr& c, u32 count, u32 base, float lam) {
             for (u32 k = 0; k < count; ++k) {
-                const float* wv = &warped[4 * (size_t)(base + k)];
-                const float raw[3] = {wv[0] - c.target[k].x, wv[1] - c.target[k].y, wv[2] - c.target[k].z};
+                const float* wv = &warped[8 * (size_t)(base + k)];
+                (void)c;
+                const float raw[3] = {wv[4], wv[5], wv[6]};
                 for (int ch = 0; ch < 3; ++ch) {
                     const double r = (double)lam * (huber<float>(raw[ch]) * raw[ch]);
                     e += r * r;

@@ -198,7 +198,7 @@ def _sparse_jacobian(scene, o):
         for ch in range(3):
             Ji = np.concatenate([Si[ch], np.eye(3)[ch]])
             Jj = -np.concatenate([Sj[ch], np.eye(3)[ch]])
-            add_row([(int(i), Ji), (int(j), Jj)], lam[0] ** 2, a[ch] - b[ch])
+            add_row([(int(i), Ji), (int(j), Jj)], lam[0] ** 2, s[8 + ch])
     for f in range(c.foreground_terms):
         x, y, v, _ = fg_pix[f]
         s_id = scene.views[v].index_map[y, x]
@@ -211,7 +211,7 @@ def _sparse_jacobian(scene, o):
             continue
         for k in range(corr.count):
             p = wv[base + k, :3].astype(np.float32)
-            raw = (p - corr.target_vertex[k, :3]).astype(np.float32)
+            raw = wv[base + k, 4:7].astype(np.float32)
             hw = np.where(np.abs(raw) < np.float32(7.5e-2), np.float32(1.0),
                           np.float32(7.5e-2) / np.abs(raw)).astype(np.float32).astype(np.float64)
             S = skew_rows(p.astype(np.float64))
