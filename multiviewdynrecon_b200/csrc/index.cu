@@ -208,7 +208,7 @@ __device__ inline uint32_t sample_view(const InstDesc& I, ushort4 pix, uint32_t 
 
 // canonical vertex / normal of each compacted pixel in frame 0; constant over
 // the Gauss-Newton iterations, so computed once per index build
-__global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* insts) {
+__global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* insts, bool mixed) {
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     const uint32_t Td = C->dense_terms, Tf = C->foreground_terms;
@@ -220,7 +220,21 @@ __global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* ins
         const ViewDesc& V = I.views[v];
         const size_t p = (size_t)pix.y * V.pitch + pix.x;
         const float4 cv = V.ref_v[p];
-        const float3 a = apply3(V.init, mk3(cv.x, cv.y, cv.z));
+        float3 a = apply3(V.init, mk3(cv.x, cv.y, cv.z));
+        if (!fg && mixed) {
+            // The point-to-plane residual subtracts two ~1 m positions, and
+            // near convergence Jt r cancels by orders of magnitude more, so
+            // the FP32 rounding of this transform (~1e-7 m) would dominate
+            // the increment. Keep the transform in double as hi + lo floats.
+            const double* m = V.init_d;
+            double ad[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                ad[r] = m[3 * r] * (double)cv.x + m[3 * r + 1] * (double)cv.y + m[3 * r + 2] * (double)cv.z + m[9 + r];
+            a = mk3((float)ad[0], (float)ad[1], (float)ad[2]);
+            I.dense_cv_lo[k] = make_float4((float)(ad[0] - (double)a.x), (float)(ad[1] - (double)a.y),
+                                           (float)(ad[2] - (double)a.z), 0.f);
+        }
         if (fg) {
             I.fg_cv[k] = make_float4(a.x, a.y, a.z, __uint_as_float(v));
         } else {
@@ -665,7 +679,7 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     MVDR_LAUNCH(compact_count_kernel<ForegroundPred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv);
     MVDR_LAUNCH(compact_scan_kernel, grid2(1, B), 1024, 0, st, d, cpv, lc.max_views, 1);
     MVDR_LAUNCH(compact_write_kernel<ForegroundPred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv, 1);
-    MVDR_LAUNCH(prepare_pixels_kernel, grid2(spread, B), 256, 0, st, d);
+    MVDR_LAUNCH(prepare_pixels_kernel, grid2(spread, B), 256, 0, st, d, lc.precision == MVDR_PRECISION_MIXED);
     MVDR_LAUNCH(term_offsets_kernel, grid2(1, B), 32, 0, st, d);
     // node -> term
     MVDR_LAUNCH(n2t_count_kernel, grid2(spread, B), 256, 0, st, d);

@@ -132,7 +132,12 @@ __global__ void __launch_bounds__(256) eval_terms_kernel(const InstDesc* insts) 
             const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
             const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
             const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
-            const V3T<T> wv = appv(se3, v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z)));
+            V3T<T> cvt3 = v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z));
+            if constexpr (sizeof(T) == 8) {
+                const float4 lo = I.dense_cv_lo[k];
+                cvt3 = v3t(cvt3.x + cvt<T>(lo.x), cvt3.y + cvt<T>(lo.y), cvt3.z + cvt<T>(lo.z));
+            }
+            const V3T<T> wv = appv(se3, cvt3);
             const V3T<T> wn = rotv(se3, v3t(cvt<T>(cn.x), cvt<T>(cn.y), cvt<T>(cn.z)));
             const V3T<T> vc = appv(iinv, appv(w2c, wv));
             const V3T<T> nc = rotv(iinv, rotv(w2c, wn));

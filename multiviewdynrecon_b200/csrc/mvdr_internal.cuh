@@ -215,6 +215,7 @@ struct InstDesc {
     ushort4* dense_knn;
     float4* dense_w;
     float4* dense_cv;       // canonical vertex in frame 0
+    float4* dense_cv_lo;    // mixed precision: double transform minus dense_cv (x, y, z)
     float4* dense_cn;       // canonical normal in frame 0
     ushort4* fg_pix;
     ushort4* fg_knn;

@@ -138,6 +138,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.dense_knn = a.take<ushort4>(lc.cap_dense);
     I.dense_w = a.take<float4>(lc.cap_dense);
     I.dense_cv = a.take<float4>(lc.cap_dense);
+    I.dense_cv_lo = a.take<float4>(lc.cap_dense);
     I.dense_cn = a.take<float4>(lc.cap_dense);
     I.fg_pix = a.take<ushort4>(lc.cap_fg);
     I.fg_knn = a.take<ushort4>(lc.cap_fg);
