@@ -310,6 +310,36 @@ MVDR_API int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t ca
  * device arrays of 6*num_nodes floats. */
 MVDR_API int mvdr_apply_jtj(mvdr_solver* solver, const float* x, float* y, void* stream);
 
+/* ---- block SpMV without device allocation -------------------------------
+ * No counterpart in the reference. Every other entry point works on a solver
+ * handle whose workspaces mvdr_create allocates with cudaMalloc. This one is
+ * for callers that cannot allocate device memory: a host application whose
+ * GPU memory is owned by another allocator, or a real-time loop that forbids
+ * cudaMalloc after start-up because it may synchronise the device.
+ *
+ * y = A x and *x_dot_y = x.y (summed in double) for a 6x6 block-sparse matrix
+ * in block-CSR form: block row i holds stored blocks rowptr[i] ..
+ * rowptr[i+1]-1, block s sits in block column colidx[s] with
+ * blocks[36 s + 6 r + k] = A(r, k). x and y hold 6*num_block_rows floats;
+ * every pointer is device memory on the current device. This is the operator
+ * step of the PCG (the SpMV with its fused dot product) on a matrix the caller
+ * owns; mvdr_apply_jtj computes the same product on a solver's own matrix.
+ *
+ * It calls no cudaMalloc, cudaFree or allocating library routine. Its scratch
+ * (per-CTA partial sums, a completion ticket and an error flag, 64 KiB) is a
+ * static device array that each GPU loading the library holds until the
+ * process exits. The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress), so make the first call on each device before any
+ * stream capture. All calls share the array: calls whose work overlaps on the
+ * GPU (on different streams, or from several host threads) race and give wrong
+ * results; serialise them. num_block_rows above MVDR_NOALLOC_MAX_BLOCK_ROWS is
+ * rejected with MVDR_ECAPACITY. A column index outside [0, num_block_rows)
+ * skips its block and sets *x_dot_y to NaN. */
+#define MVDR_NOALLOC_MAX_BLOCK_ROWS 262144u
+MVDR_API int mvdr_bsr6_spmv_dot_noalloc(uint32_t num_block_rows, uint32_t num_blocks, const int32_t* rowptr,
+                                        const int32_t* colidx, const float* blocks, const float* x, float* y,
+                                        double* x_dot_y, void* stream);
+
 /* ---- batched solves (many independent instances per launch) ------------- */
 
 /* All instances share the capacities of *cfg; their actual sizes may differ. */

@@ -49,6 +49,7 @@ def _declare(L):
         "mvdr_get_energy": (i32, [vp, P(C.c_double), vp]),
         "mvdr_get_array": (i32, [vp, i32, vp, C.c_size_t, P(C.c_size_t), vp]),
         "mvdr_apply_jtj": (i32, [vp, vp, vp, vp]),
+        "mvdr_bsr6_spmv_dot_noalloc": (i32, [u32, u32, vp, vp, vp, vp, vp, vp, vp]),
         "mvdr_batch_create": (i32, [P(abi.Config), u32, P(vp)]),
         "mvdr_batch_destroy": (i32, [vp]),
         "mvdr_batch_set_inputs": (i32, [vp, u32, P(abi.Inputs), vp]),

@@ -25,6 +25,9 @@ static int fail(int code, const std::string& msg) {
     return code;
 }
 
+// the same error record for entry points defined in other files
+int record_failure(int code, const std::string& msg) { return fail(code, msg); }
+
 #define CU(call)                                                                                  \
     do {                                                                                          \
         cudaError_t e__ = (call);                                                                 \
