@@ -125,19 +125,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def algorithmic_bytes(counts, N):
-    """Compulsory HBM bytes per stage (each array read or written once)."""
+def algorithmic_bytes(counts, N, mixed=True):
+    """Compulsory HBM bytes per stage and instance (each array read or written
+    once). JtJ is kept as half storage: N diagonal + P upper 6x6 blocks, in
+    double (mixed precision) or float; the full block-row layout has N + 2P
+    entries of (column, position)."""
     Td, Ts, Tf, Tp, Tc = (counts.dense_terms, counts.smooth_terms, counts.foreground_terms, counts.feature_terms,
                           counts.cross_terms)
     P = counts.half_pairs
-    nnzb = N + 2 * P
+    elem = 8 if mixed else 4
+    blocks = 36 * elem * (N + P)
+    entries = 8 * (N + 2 * P)
     term_data = 52 * (Td + Tf) + 29 * Ts + 88 * (Tp + Tc)
+    precond = 168 * N if mixed else 144 * N
     return {
         "terms": 122 * Td + 86 * Tf + 29 * Ts + 72 * (Tp + Tc) + 32 * N,
-        "diag": term_data + 144 * N + 24 * N + 288 * N,
-        "offdiag": term_data + 148 * nnzb + 4 * (N + 1),
-        "spmv": 148 * nnzb + 4 * (N + 1) + 24 * N + 24 * N,
-        "pcg_update": 24 * N * 6 + 168 * N,
+        "diag": term_data + 4 * counts.node2term_entries + 144 * N + 36 * elem * N + 24 * N + precond,
+        "offdiag": term_data + 4 * counts.nodepair_entries + 12 * P + 36 * elem * P,
+        "spmv": blocks + entries + 4 * (N + 1) + 4 * 24 * N,
+        "pcg_update": 24 * N * 6 + precond,
         "update": 24 * N + 64 * N,
     }
 
@@ -202,7 +208,7 @@ def run_ours(args, rank, world, dist):
 
     # per-stage timing on the same stream (CUDA events), all instances
     stages = {}
-    abytes = algorithmic_bytes(counts, base.num_nodes)
+    abytes = algorithmic_bytes(counts, base.num_nodes, mixed=args.precision == "mixed")
     reps = 20
     with torch.cuda.stream(stream):
         bind_all()

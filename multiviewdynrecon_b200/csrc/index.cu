@@ -559,7 +559,6 @@ __global__ void __launch_bounds__(256) np_sym_scatter_kernel(const InstDesc* ins
             I.sym_key[s] = key;
             I.sym_range[s] = rg;
             I.sym_half[s] = h;
-            I.upper_pos[h] = s;
             const uint32_t j = key % I.enc;
             const uint32_t pos = I.blkrow_offset[j] + atomicAdd(&I.lower_cursor[j], 1u);
             I.sym_key[pos] = j * I.enc + node;
@@ -600,7 +599,22 @@ __global__ void __launch_bounds__(128) np_lower_sort_kernel(const InstDesc* inst
             I.sym_key[b + rank] = key;
             I.sym_range[b + rank] = sr[w][i];
             I.sym_half[b + rank] = sh[w][i];
-            I.lower_pos[sh[w][i]] = b + rank;
+        }
+        __syncwarp();
+        // column and half-storage position of every entry of this block row:
+        // the diagonal first, then the row's symmetric keys (lower part sorted
+        // above, upper part written by np_sym_scatter_kernel); pair h sits in
+        // row min(i, j) at h + min(i, j) + 1
+        const uint32_t ne = I.blkrow_offset[node + 1] - b, mask = I.enc - 1;
+        for (uint32_t i = lane_id(); i <= ne; i += 32) {
+            uint32_t col = node, pos = I.half_offset[node] + node;
+            if (i > 0) {
+                col = I.sym_key[b + i - 1] & mask;
+                pos = I.sym_half[b + i - 1] + min(node, col) + 1;
+                if (col < node) pos |= kTransposedBlock;
+            }
+            I.bsr_col[b + node + i] = col;
+            I.bsr_pos[b + node + i] = pos;
         }
         __syncwarp();
     }

@@ -364,21 +364,23 @@ __device__ inline void cholesky6_solve(const double* L, const double* b, double*
     }
 }
 
-// Compensated block storage of mixed precision: a block element a is kept as
-// hi = fl32(a) and a 16-bit correction s with a = hi (1 + s 2^-24), so the
-// SpMV sees the operator to about 35 significant bits for 6 extra bytes per
-// element (rounding the assembled JtJ to float alone moves the PCG increment
-// by ~1e-4 on these blocks, whose condition numbers reach 1e5).
-constexpr double kLoScale = 16777216.0;            // 2^24
-constexpr double kLoUnscale = 5.9604644775390625e-8;  // 2^-24
-
-__device__ inline void store_split(double a, float* hi, __half* lo) {
-    const float h = (float)a;
-    float sc = 0.f;
-    if (h != 0.f) sc = (float)((a - (double)h) / (double)h * kLoScale);
-    *hi = h;
-    *lo = __float2half_rn(sc);
-}
+// Mixed precision keeps the assembled JtJ blocks in double: rounding them to
+// float moves the PCG increment by 1.3e-4 to 5e-4 on these blocks, whose
+// condition numbers reach 1e5, and rounding only the off-diagonal blocks still
+// moves it by up to 1.5e-4. Double storage also spares the SpMV every
+// float-to-double conversion (B200 runs FP64 FMAs at half the FP32 rate, but
+// conversions go through a much slower pipe). The half storage (diagonal and
+// upper blocks) keeps the bytes per SpMV below those of full float storage
+// with a 16-bit correction.
+template <bool MIXED> struct BlockStore;
+template <> struct BlockStore<true> {
+    using V = double;
+    __device__ static V* ptr(const InstDesc& I) { return I.bsr_d; }
+};
+template <> struct BlockStore<false> {
+    using V = float;
+    __device__ static V* ptr(const InstDesc& I) { return I.bsr; }
+};
 
 // ------------------------------- element-parallel block accumulation -----
 // A group of 8 lanes owns one node (diagonal block) or one node pair
@@ -612,14 +614,13 @@ __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mv
         }
         __syncwarp();
         if (active) {
-            const size_t blk = 36 * (size_t)(I.blkrow_offset[node] + node);
+            const size_t blk = 36 * (size_t)(I.half_offset[node] + node);
             for (uint32_t i = l8; i < 36; i += kGroupLanes) {
                 const int r = i / 6, k2 = i % 6;
                 const int lo = min(r, k2), hi = max(r, k2);
                 const Acc v = vals[w][g][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
                 I.diag[36 * (size_t)node + i] = (float)v;
-                if (MIXED) store_split((double)v, I.bsr + blk + i, I.bsr_lo + blk + i);
-                else I.bsr[blk + i] = (float)v;
+                BlockStore<MIXED>::ptr(I)[blk + blk_idx(r, k2)] = v;
             }
             if (l8 < 6) I.jtr[6 * (size_t)node + l8] = (float)vals[w][g][21 + l8];
             if (l8 == 0) {
@@ -711,37 +712,32 @@ __global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvd
             __syncwarp();
         }
         if (active) {
-            const size_t up = 36 * (size_t)(I.upper_pos[h] + ni + 1);  // BSR block of (i, j)
-            const size_t lo = 36 * (size_t)(I.lower_pos[h] + nj + 1);  // BSR block of (j, i)
+            // the upper block (i, j); (j, i) is read as its transpose
+            const size_t up = 36 * (size_t)(h + ni + 1);
 #pragma unroll
-            for (int m = 0; m < 5; ++m) {
-                if (er[m] < 0) continue;
-                const uint32_t e = 6 * er[m] + ek[m], et = 6 * ek[m] + er[m];
-                if (MIXED) {
-                    store_split((double)acc[m], I.bsr + up + e, I.bsr_lo + up + e);
-                    store_split((double)acc[m], I.bsr + lo + et, I.bsr_lo + lo + et);
-                } else {
-                    I.bsr[up + e] = (float)acc[m];
-                    I.bsr[lo + et] = (float)acc[m];
-                }
-            }
+            for (int m = 0; m < 5; ++m)
+                if (er[m] >= 0) BlockStore<MIXED>::ptr(I)[up + blk_idx(er[m], ek[m])] = acc[m];
         }
     }
 }
 
 // ----------------------------------------------------------- reductions ---
-// Last-CTA reduction: every CTA of instance blockIdx.y stores a partial, the
-// last CTA to arrive sums them in index order. Returns true in that CTA.
+// Last-CTA reduction: every CTA of instance blockIdx.y stores a partial; the
+// last CTA to arrive sums them with all its threads in a fixed order (thread t
+// takes partials t, t + blockDim.x, ..., then a fixed tree), so the result is
+// reproducible. Returns true in every thread of that CTA; *total is valid in
+// thread 0. blockDim.x must be a multiple of 32.
 template <class T>
 __device__ inline bool block_partial_and_last(const InstDesc& I, T v, int ticket, T* total) {
     __shared__ T ws[32];
     __shared__ bool last;
+    const uint32_t nw = blockDim.x >> 5;
     v = warp_sum(v);
     if (lane_id() == 0) ws[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
         T s = 0;
-        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += ws[w];
+        for (uint32_t w = 0; w < nw; ++w) s += ws[w];
         I.partials[blockIdx.x] = (double)s;
         __threadfence();
         const uint32_t prev = atomicAdd(&I.counts->reduce_ticket[ticket], 1u);
@@ -749,12 +745,17 @@ __device__ inline bool block_partial_and_last(const InstDesc& I, T v, int ticket
     }
     __syncthreads();
     if (!last) return false;
+    __threadfence();
+    T s = 0;
+    for (uint32_t c = threadIdx.x; c < gridDim.x; c += blockDim.x) s += (T)__ldcg(I.partials + c);
+    s = warp_sum(s);
+    __syncthreads();  // every thread has read ws above
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        T s = 0;
-        const volatile double* pp = I.partials;
-        for (uint32_t c = 0; c < gridDim.x; ++c) s += (T)pp[c];
-        *total = s;
+        T tsum = 0;
+        for (uint32_t w = 0; w < nw; ++w) tsum += ws[w];
+        *total = tsum;
         I.counts->reduce_ticket[ticket] = 0;
     }
     return true;
@@ -809,72 +810,134 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
     }
 }
 
-// One scalar row of y = A x over the row-major 6x6 BSR blocks of block row
-// `br`; x[c] = xs[c] + beta xp[c] (xp may be null). Mixed precision reads the
-// compensated blocks and accumulates in double.
+// One scalar row r of y = A x for block row br, walking the full block-row
+// layout over the half storage; accumulates in the storage precision.
 template <bool MIXED>
-__device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, const float* xs, const float* xp,
-                                float beta) {
-    const uint32_t mask = I.enc - 1;
-    const uint32_t so = I.blkrow_offset[br], se = I.blkrow_offset[br + 1];
-    size_t blk = 36 * (size_t)(so + br) + 6 * r;
-    typename std::conditional<MIXED, double, float>::type acc = 0;
-    float corr = 0.f;
-    for (uint32_t s = so; s <= se; ++s, blk += 36) {
-        const uint32_t col = (s == so) ? br : (I.sym_key[s - 1] & mask);
-        const float* a = I.bsr + blk;
-        const float2 a01 = *reinterpret_cast<const float2*>(a);
-        const float2 a23 = *reinterpret_cast<const float2*>(a + 2);
-        const float2 a45 = *reinterpret_cast<const float2*>(a + 4);
-        const float av[6] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y};
-        float xv[6];
+__device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, const float* x) {
+    using V = typename BlockStore<MIXED>::V;
+    const V* store = BlockStore<MIXED>::ptr(I);
+    const uint32_t e0 = I.blkrow_offset[br] + br, e1 = I.blkrow_offset[br + 1] + br + 1;
+    V acc = 0;
+    for (uint32_t e = e0; e < e1; ++e) {
+        const uint32_t pos = I.bsr_pos[e];
+        const V* blk = store + 36 * (size_t)(pos & ~kTransposedBlock);
+        const bool tr = (pos & kTransposedBlock) != 0;
+        const float* xc = x + 6 * (size_t)I.bsr_col[e];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const size_t e = 6 * (size_t)col + k;
-            xv[k] = xp ? xs[e] + beta * xp[e] : xs[e];
-        }
-        if (MIXED) {
-            // a = hi (1 + lo 2^-24): hi x in double, the correction hi lo x in
-            // float (it is 2^-24 of the term, so float accuracy is plenty)
-            const __half2* l = reinterpret_cast<const __half2*>(I.bsr_lo + blk);
-            const float2 l01 = __half22float2(l[0]), l23 = __half22float2(l[1]), l45 = __half22float2(l[2]);
-            const float lv[6] = {l01.x, l01.y, l23.x, l23.y, l45.x, l45.y};
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                acc += f2d(av[k]) * f2d(xv[k]);
-                corr += (av[k] * lv[k]) * xv[k];
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
-        }
+        for (int k = 0; k < 6; ++k) acc += blk[tr ? blk_idx(k, r) : blk_idx(r, k)] * (V)xc[k];
     }
-    if (MIXED) return (float)(acc + f2d(corr) * kLoUnscale);
     return (float)acc;
 }
 
+// ------------------------------------------------------- tiled SpMV -----
+// A CTA owns kTileRows consecutive block rows. It first gathers x = s + beta
+// d_prev, in the storage precision, for every entry of those rows (bsr_col
+// gives the block column) into shared memory; the entries of consecutive rows
+// are contiguous, so this is one coalesced sweep of bsr_col. After that no
+// block address depends on a load, and the row loop streams the blocks from
+// HBM with many loads in flight (the block positions are staged in shared
+// memory with x, so a block load waits on no global load). Six threads per
+// block row: thread r reads row r of each stored block (three pair loads; the
+// six threads together sweep the block contiguously, see blk_idx). For an
+// upper or diagonal block that row
+// gives y_r directly; for a lower block, stored as its transpose, it is column
+// r of the needed block and adds x_r times it to all six rows, which the row's
+// threads sum through shared memory at the end. The stored transpose of a
+// lower block belongs to a row of this or an earlier tile, so it is usually
+// still in L2. Tiles with more than kTileMaxBlocks entries go in pieces.
+constexpr uint32_t kTileRows = 16;
+constexpr uint32_t kTileSplit = 2;  // threads per scalar row, taking alternate blocks
+constexpr uint32_t kTileThreads = 6 * kTileSplit * kTileRows;
+constexpr uint32_t kTileMaxBlocks = 384;
+
+template <class V> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
 // q = A d with d = s + beta d_prev formed on the fly (BlockPCG.cuh:167-181 fused
 // into the SpMV of the next iteration); d.q partial; alpha = delta / d.q.
-// Six threads per block row (one per scalar row), row-major 6x6 blocks.
 template <bool MIXED>
-__global__ void __launch_bounds__(192) pcg_spmv_kernel(const InstDesc* insts, int parity) {
+__global__ void __launch_bounds__(kTileThreads) pcg_spmv_kernel(const InstDesc* insts, int parity) {
+    using V = typename BlockStore<MIXED>::V;
+    using V2 = typename Pair<V>::type;
+    __shared__ __align__(16) V s_x[kTileMaxBlocks * 6];
+    __shared__ uint32_t s_pos[kTileMaxBlocks];
+    __shared__ V s_cols[kTileRows][kTileSplit * 6][7];
     const InstDesc& I = insts[blockIdx.y];
     using T = typename std::conditional<MIXED, double, float>::type;
+    const V* store = BlockStore<MIXED>::ptr(I);
     const float* dprev = parity ? I.d0 : I.d1;
     float* dcur = parity ? I.d1 : I.d0;
     const float beta = (float)I.scalars[2];
+    const uint32_t t = threadIdx.x;
     T part = 0;
-    const uint32_t rows_per_cta = blockDim.x / 6;
-    for (uint32_t base = blockIdx.x * rows_per_cta; base < I.N; base += gridDim.x * rows_per_cta) {
-        const uint32_t br = base + threadIdx.x / 6;
-        const uint32_t r = threadIdx.x % 6;
-        if (threadIdx.x < rows_per_cta * 6 && br < I.N) {
-            const float acc = bsr_row<MIXED>(I, br, r, I.s, dprev, beta);
-            const size_t e = 6 * (size_t)br + r;
+    const uint32_t r0 = blockIdx.x * kTileRows;
+    if (r0 < I.N) {
+        const uint32_t r1 = min(r0 + kTileRows, I.N);
+        const uint32_t b_begin = I.blkrow_offset[r0] + r0, b_end = I.blkrow_offset[r1] + r1;
+        const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
+        const bool computes = row < r1;
+        uint32_t rb = 0, re = 0;
+        if (computes) {
+            rb = I.blkrow_offset[row] + row;
+            re = I.blkrow_offset[row + 1] + row + 1;
+        }
+        V acc = 0;
+        V col_acc[6] = {0, 0, 0, 0, 0, 0};
+        for (uint32_t pb = b_begin; pb < b_end; pb += kTileMaxBlocks) {
+            const uint32_t pe = min(pb + kTileMaxBlocks, b_end), nb = pe - pb;
+            for (uint32_t i = t; i < nb; i += kTileThreads) s_pos[i] = I.bsr_pos[pb + i];
+#pragma unroll 4
+            for (uint32_t i = t; i < nb * 6; i += kTileThreads) {
+                const size_t e = 6 * (size_t)I.bsr_col[pb + i / 6] + i % 6;
+                s_x[i] = (V)(I.s[e] + beta * dprev[e]);
+            }
+            __syncthreads();
+            if (computes) {
+                // blocks rb + half, rb + half + kTileSplit, ... that lie in this piece
+                uint32_t mb = max(rb, pb);
+                mb += (rb + half + kTileSplit - mb % kTileSplit) % kTileSplit;
+                const uint32_t me = min(re, pe);
+#pragma unroll 4
+                for (uint32_t b = mb; b < me; b += kTileSplit) {
+                    const uint32_t pos = s_pos[b - pb];
+                    const V2* blk = reinterpret_cast<const V2*>(store + 36 * (size_t)(pos & ~kTransposedBlock));
+                    const V2 a01 = blk[rr], a23 = blk[6 + rr], a45 = blk[12 + rr];
+                    const V av[6] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y};
+                    const V* xv = s_x + 6 * (b - pb);
+                    if (pos & kTransposedBlock) {
+                        const V xr = xv[rr];
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) col_acc[k] += av[k] * xr;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
+                    }
+                }
+            }
+            __syncthreads();  // the next piece overwrites s_x
+        }
+        // slot 6 of a thread's row-sum entry holds its direct (row) sum
+        if (computes) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s_cols[lr][6 * half + rr][k] = col_acc[k];
+            s_cols[lr][6 * half + rr][6] = acc;
+        }
+        __syncthreads();
+        if (computes && half == 0) {
+            acc = 0;
+#pragma unroll
+            for (uint32_t h = 0; h < kTileSplit; ++h) {
+                acc += s_cols[lr][6 * h + rr][6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) acc += s_cols[lr][6 * h + c][rr];
+            }
+            const float qv = (float)acc;
+            const size_t e = 6 * (size_t)row + rr;
             const float dv = I.s[e] + beta * dprev[e];
             dcur[e] = dv;
-            I.q[e] = acc;
-            part += (T)dv * (T)acc;
+            I.q[e] = qv;
+            part += (T)dv * (T)qv;
         }
     }
     T tot;
@@ -1061,7 +1124,7 @@ __global__ void __launch_bounds__(192) bsr_apply_kernel(const InstDesc* insts, c
         const uint32_t br = base + threadIdx.x / 6;
         const uint32_t r = threadIdx.x % 6;
         if (threadIdx.x >= rows_per_cta * 6 || br >= I.N) continue;
-        yout[6 * (size_t)br + r] = bsr_row<MIXED>(I, br, r, xin, nullptr, 0.f);
+        yout[6 * (size_t)br + r] = bsr_row<MIXED>(I, br, r, xin);
     }
 }
 
@@ -1179,8 +1242,7 @@ __global__ void export_offdiag_kernel(const InstDesc* insts, uint32_t inst, floa
         const uint32_t s = i / 36, e = i % 36;
         const uint32_t row = I.sym_key[s] / I.enc;
         (void)mask;
-        const uint32_t k = e / 6, r = e % 6;
-        out[i] = I.bsr[36 * (size_t)(s + row + 1) + 6 * r + k];
+        out[i] = stored_block_element(I, s + row + 1, e % 6, e / 6);
     }
 }
 
@@ -1233,7 +1295,7 @@ cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& 
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
-    const uint32_t gspmv = min((lc.max_nodes + 31) / 32, (uint32_t)lc.sm_count * 8);
+    const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
     const uint32_t gwarp = (lc.max_nodes + 7) / 8;
     const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
     if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d);
@@ -1247,8 +1309,8 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
             if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
         } else {
-            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gspmv, lc.B), 192, 0, st, d, parity);
-            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gspmv, lc.B), 192, 0, st, d, parity);
+            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
+            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
         }
         if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity);
         else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity);
@@ -1259,7 +1321,7 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
 cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, int stage, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
-    const uint32_t gspmv = min((lc.max_nodes + 31) / 32, (uint32_t)lc.sm_count * 8);
+    const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
     const uint32_t gn = (lc.max_nodes + 15) / 16;
     switch (stage) {
         case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
@@ -1274,8 +1336,8 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             break;
         }
         case MVDR_STAGE_SPMV:
-            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gspmv, lc.B), 192, 0, st, d, 0);
-            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gspmv, lc.B), 192, 0, st, d, 0);
+            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
+            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
             break;
         case MVDR_STAGE_PCG_UPDATE:
             if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0);

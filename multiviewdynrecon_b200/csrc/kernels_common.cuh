@@ -175,6 +175,14 @@ __device__ inline float weight_of(ushort4 knn, float4 w, uint32_t node) {
 
 __device__ inline void set_error(const InstDesc& I, uint32_t bit) { atomicOr(&I.counts->error_flags, bit); }
 
+// A(r, k) of entry e of the full block-row layout, read from the half storage
+__device__ inline float stored_block_element(const InstDesc& I, uint32_t e, uint32_t r, uint32_t k) {
+    const uint32_t pos = I.bsr_pos[e];
+    const size_t blk = 36 * (size_t)(pos & ~kTransposedBlock);
+    const uint32_t idx = (pos & kTransposedBlock) ? blk_idx(k, r) : blk_idx(r, k);
+    return I.bsr_d ? (float)I.bsr_d[blk + idx] : I.bsr[blk + idx];
+}
+
 // true when the input check found an out-of-range node or surfel id
 __device__ inline bool bad_inputs(const InstDesc& I) {
     return (*(volatile const uint32_t*)&I.counts->error_flags & kErrBadNodeIndex) != 0;

@@ -18,6 +18,14 @@ namespace mvdr {
 
 constexpr int kWarp = 32;
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr uint32_t kTransposedBlock = 0x80000000u;
+
+// Element (r, k) of a stored 6x6 JtJ block. The layout keeps row r as three
+// pairs (k = 0-1, 2-3, 4-5) at pair slots r, 6 + r, 12 + r, so six threads that
+// each read one row with three pair loads cover the block in three
+// contiguous, non-overlapping sweeps (a row read never shares a sector with
+// another instruction's read).
+__host__ __device__ constexpr uint32_t blk_idx(uint32_t r, uint32_t k) { return 12 * (k >> 1) + 2 * r + (k & 1); }
 
 // error flag bits (DeviceCounts::error_flags)
 enum : uint32_t {
@@ -242,8 +250,6 @@ struct InstDesc {
     uint32_t* sym_key;      // [2P cap]
     uint2* sym_range;       // [2P cap]
     uint32_t* sym_half;     // [2P cap] half pair of each symmetric entry
-    uint32_t* upper_pos;    // [P cap] symmetric position of (i, j)
-    uint32_t* lower_pos;    // [P cap] symmetric position of (j, i)
     // bin-block CSR structure (reference layout, for checks and the bin-block SpMV)
     uint32_t* bin_scan;     // [nbins+1]
     int32_t* bb_rowptr;     // [32 (nbins+1)]
@@ -258,8 +264,16 @@ struct InstDesc {
     float* minv;            // [36N] preconditioner (inverse diagonal), float
     double* chol;           // [21N] Cholesky factors (mixed precision)
     float* jtr;             // [6N]
-    float* bsr;             // [(N + 2P cap) * 36] row-major blocks, diagonal first per row
-    __half* bsr_lo;         // mixed precision: per-element correction, a = hi (1 + lo 2^-24)
+    // JtJ in half storage: per block row i its diagonal block at
+    // half_offset[i] + i, then the upper blocks of its half pairs h at h + i + 1
+    // (element order blk_idx). A lower block (i, j), j < i, is the transpose
+    // of the stored block of pair (j, i).
+    float* bsr;             // FP32: [(N + P cap) * 36]
+    double* bsr_d;          // mixed precision: the same blocks in double
+    // per entry of the full (symmetric) block-row layout, row i: the diagonal,
+    // then its symmetric keys in order [N + 2P cap]
+    uint32_t* bsr_col;      // block column
+    uint32_t* bsr_pos;      // half-storage block | kTransposedBlock when read transposed
     // pcg vectors [6N each]
     float* x;
     float* r;

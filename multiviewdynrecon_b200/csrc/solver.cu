@@ -45,7 +45,7 @@ __global__ void export_binblock_fill_kernel(const InstDesc* insts, uint32_t inst
         const uint32_t br = row / 6, in = row % 6;
         for (int k = 0; k < 6; ++k, off += 32) out[off] = I.diag[36 * (size_t)br + in + 6 * k];
         for (uint32_t s = I.blkrow_offset[br]; s < I.blkrow_offset[br + 1]; ++s)
-            for (int k = 0; k < 6; ++k, off += 32) out[off] = I.bsr[36 * (size_t)(s + br + 1) + 6 * in + k];
+            for (int k = 0; k < 6; ++k, off += 32) out[off] = stored_block_element(I, s + br + 1, in, k);
     }
 }
 
@@ -166,8 +166,6 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.sym_key = a.take<uint32_t>(2 * (size_t)lc.cap_pairs);
     I.sym_range = a.take<uint2>(2 * (size_t)lc.cap_pairs);
     I.sym_half = a.take<uint32_t>(2 * (size_t)lc.cap_pairs);
-    I.upper_pos = a.take<uint32_t>(lc.cap_pairs);
-    I.lower_pos = a.take<uint32_t>(lc.cap_pairs);
     const size_t nbins = (6 * N + 31) / 32;
     I.bin_scan = a.take<uint32_t>(nbins + 2);
     I.bb_rowptr = a.take<int32_t>(32 * (nbins + 1));
@@ -180,8 +178,11 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.minv = a.take<float>(36 * N);
     I.chol = a.take<double>(21 * N);
     I.jtr = a.take<float>(6 * N);
-    I.bsr = a.take<float>(36 * (N + 2 * (size_t)lc.cap_pairs));
-    I.bsr_lo = lc.precision == MVDR_PRECISION_MIXED ? a.take<__half>(36 * (N + 2 * (size_t)lc.cap_pairs)) : nullptr;
+    const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
+    I.bsr = mixed ? nullptr : a.take<float>(36 * (N + (size_t)lc.cap_pairs));
+    I.bsr_d = mixed ? a.take<double>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
+    I.bsr_col = a.take<uint32_t>(N + 2 * (size_t)lc.cap_pairs);
+    I.bsr_pos = a.take<uint32_t>(N + 2 * (size_t)lc.cap_pairs);
     I.x = a.take<float>(6 * N);
     I.r = a.take<float>(6 * N);
     I.s = a.take<float>(6 * N);
