@@ -36,6 +36,7 @@ if ROOT not in sys.path:
 
 HBM_FALLBACK_GBS = 6650.0
 WORKLOAD = "torso_3view_640x480_4096nodes_5gn_15pcg"
+METRIC = "non-rigid GN solves/s (batched mixed vs plain FP32) at <=1e-4 rel err vs FP64"
 
 
 def parse():
@@ -351,11 +352,13 @@ def main():
             vals.append(dt)
         total = time.perf_counter() - t0
         value = args.steps * threads / total
-        line = {"metric": "non-rigid GN solves/s", "impl": "reference", "value": round(value, 4),
+        line = {"metric": METRIC, "impl": "reference", "value": round(value, 4),
                 "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(1e3 * total / args.steps, 2), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "instances_per_step": threads, "gn": args.gn, "pcg": args.pcg},
+                "config": {"workload": WORKLOAD, "instances_per_step": threads, "views": 3,
+                           "image": [args.width, args.height], "nodes": args.nodes, "gn": args.gn,
+                           "pcg": args.pcg, "precision": "fp32 terms, double sums (CPU restatement)"},
                 "cpu_baseline": {"value": round(value, 4), "unit": "solves/s", "cores": threads, "kind": "port",
                                  "sample": f"{threads} whole solves per step, one per host thread"},
                 "e2e": {"value": round(value, 4), "unit": "solves/s", "h2d_bytes_per_step": 0,
@@ -379,7 +382,7 @@ def main():
     if rank == 0:
         c = r["counts"]
         line = {
-            "metric": "non-rigid GN solves/s (batched mixed vs plain FP32) at <=1e-4 rel err vs FP64",
+            "metric": METRIC,
             "value": round(r["value"], 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f32", "data": "synthetic",
