@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(1024) node_scan_kernel(const InstDesc* insts, 
                 I.half_offset[i] = i < N ? I.upper_count[i] : 0u;
                 if (i < N) { I.lower_count[i] = 0; I.lower_cursor[i] = 0; }
             }
+            for (uint32_t i = threadIdx.x; i < kLenBuckets; i += blockDim.x) I.len_bucket[i] = 0;
             __syncthreads();
             block_exclusive_scan_inplace(I.half_offset, N + 1, &total);
             __syncthreads();
@@ -340,6 +341,14 @@ __global__ void __launch_bounds__(1024) node_scan_kernel(const InstDesc* insts, 
                 I.blkrow_offset[i] = i < N ? I.lower_count[i] + I.upper_count[i] : 0u;
             __syncthreads();
             block_exclusive_scan_inplace(I.blkrow_offset, N + 1, &total);
+            // start of every entry-count bucket in pair_order (a cursor per bucket)
+            if (threadIdx.x == 0) {
+                uint32_t acc = 0;
+                for (uint32_t b = 0; b < kLenBuckets; ++b) {
+                    I.len_bucket[kLenBuckets + b] = acc;
+                    acc += I.len_bucket[b];
+                }
+            }
             break;
         }
         case kScanBins: {
@@ -536,6 +545,7 @@ __global__ void __launch_bounds__(256) np_half_compact_kernel(const InstDesc* in
             I.half_key[h0 + u] = key;
             I.half_range[h0 + u] = make_uint2(start, end);
             atomicAdd(&I.lower_count[key % I.enc], 1u);
+            atomicAdd(&I.len_bucket[len_bucket_of(end - start)], 1u);
         }
     }
 }
@@ -559,6 +569,9 @@ __global__ void __launch_bounds__(256) np_sym_scatter_kernel(const InstDesc* ins
             I.sym_key[s] = key;
             I.sym_range[s] = rg;
             I.sym_half[s] = h;
+            // the order in which the off-diagonal kernel takes the pairs; each
+            // pair is summed by one thread, so the order leaves results unchanged
+            I.pair_order[atomicAdd(&I.len_bucket[kLenBuckets + len_bucket_of(rg.y - rg.x)], 1u)] = h;
             const uint32_t j = key % I.enc;
             const uint32_t pos = I.blkrow_offset[j] + atomicAdd(&I.lower_cursor[j], 1u);
             I.sym_key[pos] = j * I.enc + node;

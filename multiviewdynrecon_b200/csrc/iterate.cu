@@ -383,8 +383,8 @@ template <> struct BlockStore<false> {
 };
 
 // ------------------------------- element-parallel block accumulation -----
-// A group of 8 lanes owns one node (diagonal block) or one node pair
-// (off-diagonal block); a warp holds 4 groups. The group stages 8 of its terms
+// Diagonal blocks: a group of 8 lanes owns one node; a warp holds 4 groups.
+// The group stages 8 of its terms
 // at a time in shared memory, each as weighted twist-Jacobian rows already in
 // the accumulation precision, then every lane accumulates the 4-5 block
 // elements it owns over the staged terms. The inner loop is shared loads and
@@ -399,85 +399,23 @@ template <class T> __device__ inline void twist_rows(T px, T py, T pz, T f[3][6]
     f[2][0] = py;  f[2][1] = -px; f[2][2] = 0;   f[2][3] = 0; f[2][4] = 0; f[2][5] = 1;
 }
 
-constexpr int kGroupLanes = 8;
-constexpr int kPairStride = 37;  // u[3][6], v[3][6], channel count (odd stride: no bank conflicts)
-constexpr int kDiagStride = 23;  // u[3][6], lambda^2, rb[3], channel count
-
-// Off-diagonal descriptor of term t for the pair (ni, nj): the block is
-// sum_c u_c v_c^T with u_c = J_i,c-side rows and v_c the lambda^2-weighted
-// J_j,c-side rows; returns the channel count.
-template <class T>
-__device__ inline int stage_pair(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
-                                  uint32_t ni, uint32_t nj, T* o) {
-    uint32_t k;
-    const TermType ty = off.typed(t, k);
-    int nch = 0;
-    switch (ty) {
-        case kDense:
-        case kForeground: {
-            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
-            const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
-            const ushort4 kn = term_nodes(I, ty, k);
-            const float4 w4 = term_weights(I, ty, k);
-            const T l2 = ty == kDense ? (T)1 : cvt<T>(lam.foreground * lam.foreground);
-            const T wi = cvt<T>(weight_of(kn, w4, ni)), wj = l2 * cvt<T>(weight_of(kn, w4, nj));
-            const T J[6] = {cvt<T>(a.x), cvt<T>(a.y), cvt<T>(a.z), cvt<T>(a.w), cvt<T>(b.x), cvt<T>(b.y)};
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                o[q] = wi * J[q];
-                o[18 + q] = wj * J[q];
-            }
-            nch = 1;
-            break;
-        }
-        case kSmooth: {
-            const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
-            if (b.z == 0.f) break;
-            const bool is_i = ni == I.graph[k].x;
-            const float4 pi = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
-            const float4 pj = is_i ? make_float4(a.w, b.x, b.y, 0.f) : a;
-            T fi[3][6], fj[3][6];
-            twist_rows<T>(cvt<T>(pi.x), cvt<T>(pi.y), cvt<T>(pi.z), fi);
-            twist_rows<T>(cvt<T>(pj.x), cvt<T>(pj.y), cvt<T>(pj.z), fj);
-            // J_i,c = +-f_c(p_i), J_j,c = -+f_c(p_j): their product carries a minus
-            const T l2 = -cvt<T>(lam.smooth * lam.smooth);
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    o[6 * c + q] = fi[c][q];
-                    o[18 + 6 * c + q] = l2 * fj[c][q];
-                }
-            nch = 3;
-            break;
-        }
-        case kFeature:
-        case kCross: {
-            const bool f = ty == kFeature;
-            const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
-            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
-            const ushort4 kn = term_nodes(I, ty, k);
-            const float4 w4 = term_weights(I, ty, k);
-            const T l2 = f ? cvt<T>(lam.feature * lam.feature) : cvt<T>(lam.cross_view * lam.cross_view);
-            const T wi = cvt<T>(weight_of(kn, w4, ni)), wj = l2 * cvt<T>(weight_of(kn, w4, nj));
-            const float hw[3] = {huber_weight(rw.x), huber_weight(rw.y), huber_weight(rw.z)};
-            T fr[3][6];
-            twist_rows<T>(cvt<T>(wv.x), cvt<T>(wv.y), cvt<T>(wv.z), fr);
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    const T jv = cvt<T>(hw[c]) * fr[c][q];
-                    o[6 * c + q] = wi * jv;
-                    o[18 + 6 * c + q] = wj * jv;
-                }
-            nch = 3;
-            break;
-        }
-        default: break;
-    }
-    return nch;
+// (sum_c f_c(p) f_c(q)^T)(r, k) for the twist rows above; with r and k known
+// at compile time this folds to at most three products
+template <class T> __device__ inline T twist_rows_product(const T p[3], const T q[3], int r, int k) {
+    // f_c(p)[r] for r < 3: the rows of [p]x^T
+    auto sk = [](const T v[3], int c, int rr) -> T {
+        if (c == 0) return rr == 0 ? (T)0 : (rr == 1 ? v[2] : -v[1]);
+        if (c == 1) return rr == 0 ? -v[2] : (rr == 1 ? (T)0 : v[0]);
+        return rr == 0 ? v[1] : (rr == 1 ? -v[0] : (T)0);
+    };
+    if (r < 3 && k < 3) return sk(p, 0, r) * sk(q, 0, k) + sk(p, 1, r) * sk(q, 1, k) + sk(p, 2, r) * sk(q, 2, k);
+    if (r < 3) return sk(p, k - 3, r);
+    if (k < 3) return sk(q, r - 3, k);
+    return r == k ? (T)1 : (T)0;
 }
+
+constexpr int kGroupLanes = 8;
+constexpr int kDiagStride = 23;  // u[3][6], lambda^2, rb[3], channel count
 
 // Diagonal descriptor of term t for node n: D += lambda^2 sum_c u_c u_c^T,
 // b += sum_c u_c rb_c.
@@ -652,72 +590,118 @@ __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mv
 }
 
 // --------------------------------------------------- off-diagonal blocks --
-// 8 lanes per unordered pair (i < j): A_ij(r, k) = sum_t sum_c u_c[r] v_c[k],
-// written to row i and, transposed, to row j (the reference computes both
-// orderings separately, JtJMaterializer.cu:270-365)
+// One thread per unordered pair (i < j), accumulating in registers. Every
+// term type but smooth contributes w_i w_j lambda^2 sum_c g_c g_c^T (dense and
+// foreground: one channel g = J; feature and cross: three Huber-weighted twist
+// rows), a symmetric product, so the thread keeps the 21 upper-triangle sums
+// only. A pair has at most two smooth terms (its graph edges i->j and j->i);
+// their asymmetric contribution -lambda_s^2 sum_c f_c(p_i) f_c(p_j)^T is added
+// when the block is written. computeJtJNonDiagonalBlockKernel and
+// computeSmoothJtJBlock (JtJMaterializer.cu:20-528, jtj_block_jacobian.cuh:8-65)
+// compute the same sums; only the upper block (i, j) is stored, (j, i) is read
+// as its transpose.
+__device__ constexpr int sym_idx(int r, int k) { return r * 6 - (r * (r - 1)) / 2 + (k - r); }  // r <= k
+
+template <class Acc>
+__device__ inline void add_sym_outer(Acc S[21], const Acc sg[6], const Acc g[6]) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int k = r; k < 6; ++k) S[sym_idx(r, k)] += sg[r] * g[k];
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
-    constexpr int kWarps = 4;
-    __shared__ Acc stage[kWarps][32][kPairStride];
-    __shared__ int nchs[kWarps][32];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2) return;
     TermOffsets off;
     off.load(C);
     const uint32_t P = C->half_pairs;
-    const uint32_t w = threadIdx.x >> 5, lane = lane_id();
-    const uint32_t g = lane / kGroupLanes, l8 = lane % kGroupLanes;
-    // lane-owned elements e = l8 + 8 m (m < 5, e < 36)
-    int er[5], ek[5];
+    const Acc l2_fg = (Acc)(lam.foreground * lam.foreground);
+    const Acc l2_feat = (Acc)(lam.feature * lam.feature), l2_cross = (Acc)(lam.cross_view * lam.cross_view);
+    // pairs grouped by entry count, so the lanes of a warp loop equally long
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        const uint32_t h = I.pair_order[i];
+        const uint32_t key = I.half_key[h];
+        const uint32_t ni = key / I.enc, nj = key % I.enc;
+        const uint2 rg = I.half_range[h];
+        Acc S[21];
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-        const int e = (int)l8 + 8 * m;
-        er[m] = e < 36 ? e / 6 : -1;
-        ek[m] = e < 36 ? e % 6 : 0;
-    }
-    const uint32_t groups = gridDim.x * kWarps * 4;
-    const uint32_t first = (blockIdx.x * kWarps + w) * 4;
-    for (uint32_t hbase = first; hbase < P; hbase += groups) {
-        const uint32_t h = hbase + g;
-        const bool active = h < P;
-        uint32_t ni = 0, nj = 0;
-        uint2 rg = make_uint2(0, 0);
-        if (active) {
-            const uint32_t key = I.half_key[h];
-            ni = key / I.enc;
-            nj = key % I.enc;
-            rg = I.half_range[h];
-        }
-        uint32_t nchunks = (rg.y - rg.x + kGroupLanes - 1) / kGroupLanes;
-        for (int o = 8; o <= 16; o <<= 1) nchunks = max(nchunks, __shfl_xor_sync(0xffffffffu, nchunks, o));
-        Acc acc[5] = {0, 0, 0, 0, 0};
-        for (uint32_t ch = 0; ch < nchunks; ++ch) {
-            const uint32_t p = rg.x + ch * kGroupLanes + l8;
-            nchs[w][lane] = p < rg.y ? stage_pair<Acc>(I, off, lam, I.np_index[p], ni, nj, stage[w][lane]) : 0;
-            __syncwarp();
-#pragma unroll 2
-            for (int q = 0; q < kGroupLanes; ++q) {
-                const Acc* d = stage[w][g * kGroupLanes + q];
-                const int nch = nchs[w][g * kGroupLanes + q];
-                for (int c = 0; c < nch; ++c) {
-                    const Acc* u = d + 6 * c;
-                    const Acc* v = d + 18 + 6 * c;
+        for (int q = 0; q < 21; ++q) S[q] = 0;
+        uint32_t smooth_k[2] = {kInvalid, kInvalid};
+        for (uint32_t p = rg.x; p < rg.y; ++p) {
+            uint32_t k;
+            const TermType ty = off.typed(I.np_index[p], k);
+            if (ty == kDense || ty == kForeground) {
+                const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+                const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+                if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0
+                const ushort4 kn = term_nodes(I, ty, k);
+                const float4 w4 = term_weights(I, ty, k);
+                Acc s = (Acc)weight_of(kn, w4, ni) * (Acc)weight_of(kn, w4, nj);
+                if (ty == kForeground) s *= l2_fg;
+                const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
+                Acc sg[6];
 #pragma unroll
-                    for (int m = 0; m < 5; ++m)
-                        if (er[m] >= 0) acc[m] += u[er[m]] * v[ek[m]];
+                for (int q = 0; q < 6; ++q) sg[q] = s * g[q];
+                add_sym_outer(S, sg, g);
+            } else if (ty == kSmooth) {
+                if (smooth_k[0] == kInvalid) smooth_k[0] = k;
+                else smooth_k[1] = k;
+            } else if (ty == kFeature || ty == kCross) {
+                const bool f = ty == kFeature;
+                const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
+                const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
+                const ushort4 kn = term_nodes(I, ty, k);
+                const float4 w4 = term_weights(I, ty, k);
+                const Acc s = (Acc)weight_of(kn, w4, ni) * (Acc)weight_of(kn, w4, nj) * (f ? l2_feat : l2_cross);
+                const float hw[3] = {huber_weight(rw.x), huber_weight(rw.y), huber_weight(rw.z)};
+                Acc fr[3][6];
+                twist_rows<Acc>((Acc)wv.x, (Acc)wv.y, (Acc)wv.z, fr);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    Acc g[6], sg[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) {
+                        g[q] = (Acc)hw[c] * fr[c][q];
+                        sg[q] = s * g[q];
+                    }
+                    add_sym_outer(S, sg, g);
                 }
             }
-            __syncwarp();
         }
-        if (active) {
-            // the upper block (i, j); (j, i) is read as its transpose
-            const size_t up = 36 * (size_t)(h + ni + 1);
+        // smooth terms: J_i,c = +-f_c(p_i), J_j,c = -+f_c(p_j), so their
+        // product carries a minus (geometry_icp_jacobian.cuh:323-343); the
+        // elements of sum_c f_c(p_i) f_c(p_j)^T come from the two points
+        Acc pi[2][3], pj[2][3];
+        bool has[2] = {false, false};
 #pragma unroll
-            for (int m = 0; m < 5; ++m)
-                if (er[m] >= 0) BlockStore<MIXED>::ptr(I)[up + blk_idx(er[m], ek[m])] = acc[m];
+        for (int m = 0; m < 2; ++m) {
+            if (smooth_k[m] == kInvalid) continue;
+            const uint32_t k = smooth_k[m];
+            const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
+            if (b.z == 0.f) continue;
+            const bool is_i = ni == I.graph[k].x;
+            const float4 qi = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
+            const float4 qj = is_i ? make_float4(a.w, b.x, b.y, 0.f) : a;
+            pi[m][0] = (Acc)qi.x; pi[m][1] = (Acc)qi.y; pi[m][2] = (Acc)qi.z;
+            pj[m][0] = (Acc)qj.x; pj[m][1] = (Acc)qj.y; pj[m][2] = (Acc)qj.z;
+            has[m] = true;
         }
+        const Acc l2_smooth = -(Acc)(lam.smooth * lam.smooth);
+        typename BlockStore<MIXED>::V* out = BlockStore<MIXED>::ptr(I) + 36 * (size_t)(h + ni + 1);
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                Acc v = S[r <= k ? sym_idx(r, k) : sym_idx(k, r)];
+#pragma unroll
+                for (int m = 0; m < 2; ++m)
+                    if (has[m]) v += l2_smooth * twist_rows_product<Acc>(pi[m], pj[m], r, k);
+                out[blk_idx(r, k)] = v;
+            }
     }
 }
 
@@ -1279,7 +1263,7 @@ cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty
     if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 128, 0, st, d, lam);
     else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
     if (materialize) {
-        const uint32_t gp = min((lc.cap_pairs + 15) / 16, (uint32_t)lc.sm_count * 16);
+        const uint32_t gp = min((lc.cap_pairs + 127) / 128, (uint32_t)lc.sm_count * 8);
         if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, st, d, lam);
         else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, st, d, lam);
     }
@@ -1330,7 +1314,7 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
             break;
         case MVDR_STAGE_OFFDIAG: {
-            const uint32_t gp = min((lc.cap_pairs + 15) / 16, (uint32_t)lc.sm_count * 16);
+            const uint32_t gp = min((lc.cap_pairs + 127) / 128, (uint32_t)lc.sm_count * 8);
             if (mixed) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, st, d, lam);
             else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, st, d, lam);
             break;

@@ -19,6 +19,12 @@ namespace mvdr {
 constexpr int kWarp = 32;
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kTransposedBlock = 0x80000000u;
+// entry-count buckets of the half pairs (bucket 0 = longest; counts of
+// kLenBuckets - 1 or more share bucket 0)
+constexpr uint32_t kLenBuckets = 256;
+__host__ __device__ constexpr uint32_t len_bucket_of(uint32_t len) {
+    return kLenBuckets - 1 - (len < kLenBuckets - 1 ? len : kLenBuckets - 1);
+}
 
 // Element (r, k) of a stored 6x6 JtJ block. The layout keeps row r as three
 // pairs (k = 0-1, 2-3, 4-5) at pair slots r, 6 + r, 12 + r, so six threads that
@@ -244,6 +250,8 @@ struct InstDesc {
     uint32_t* tmp_start;    // [K2 cap]
     uint32_t* half_key;     // [P cap]
     uint2* half_range;      // [P cap]
+    uint32_t* pair_order;   // [P cap] half pairs grouped by entry count, longest first
+    uint32_t* len_bucket;   // [2 * kLenBuckets] pairs per entry-count bucket, then scatter cursors
     uint32_t* lower_count;  // [N+1]
     uint32_t* lower_cursor; // [N]
     uint32_t* blkrow_offset;// [N+1]

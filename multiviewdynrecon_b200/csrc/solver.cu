@@ -160,6 +160,8 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.tmp_start = a.take<uint32_t>(lc.cap_k2);
     I.half_key = a.take<uint32_t>(lc.cap_pairs);
     I.half_range = a.take<uint2>(lc.cap_pairs);
+    I.pair_order = a.take<uint32_t>(lc.cap_pairs);
+    I.len_bucket = a.take<uint32_t>(2 * kLenBuckets);
     I.lower_count = a.take<uint32_t>(N + 1);
     I.lower_cursor = a.take<uint32_t>(N + 1);
     I.blkrow_offset = a.take<uint32_t>(N + 1);
