@@ -611,7 +611,7 @@ __device__ inline void add_sym_outer(Acc S[21], const Acc sg[6], const Acc g[6])
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
+__global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
@@ -631,15 +631,36 @@ __global__ void __launch_bounds__(128) offdiag_kernel(const InstDesc* insts, mvd
 #pragma unroll
         for (int q = 0; q < 21; ++q) S[q] = 0;
         uint32_t smooth_k[2] = {kInvalid, kInvalid};
-        for (uint32_t p = rg.x; p < rg.y; ++p) {
+        // software pipeline over the pair's entries: the term id two entries
+        // ahead and the pixel-term record one entry ahead are in flight while
+        // the current entry is summed
+        uint32_t t_next = rg.x < rg.y ? I.np_index[rg.x] : 0u;
+        uint32_t t_next2 = rg.x + 1 < rg.y ? I.np_index[rg.x + 1] : 0u;
+        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa, pw = pa;
+        ushort4 pk = make_ushort4(0, 0, 0, 0);
+        auto fetch_pixel_term = [&](uint32_t t) {
             uint32_t k;
-            const TermType ty = off.typed(I.np_index[p], k);
+            const TermType ty = off.typed(t, k);
             if (ty == kDense || ty == kForeground) {
                 const uint32_t idx = ty == kDense ? k : off.o[0] + k;
-                const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+                pa = I.term_jr[2 * (size_t)idx];
+                pb = I.term_jr[2 * (size_t)idx + 1];
+                pk = term_nodes(I, ty, k);
+                pw = term_weights(I, ty, k);
+            }
+        };
+        if (rg.x < rg.y) fetch_pixel_term(t_next);
+        for (uint32_t p = rg.x; p < rg.y; ++p) {
+            const uint32_t t = t_next;
+            const float4 a = pa, b = pb, w4 = pw;
+            const ushort4 kn = pk;
+            t_next = t_next2;
+            if (p + 2 < rg.y) t_next2 = I.np_index[p + 2];
+            if (p + 1 < rg.y) fetch_pixel_term(t_next);
+            uint32_t k;
+            const TermType ty = off.typed(t, k);
+            if (ty == kDense || ty == kForeground) {
                 if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0
-                const ushort4 kn = term_nodes(I, ty, k);
-                const float4 w4 = term_weights(I, ty, k);
                 Acc s = (Acc)weight_of(kn, w4, ni) * (Acc)weight_of(kn, w4, nj);
                 if (ty == kForeground) s *= l2_fg;
                 const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
