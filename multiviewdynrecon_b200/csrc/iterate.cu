@@ -333,13 +333,17 @@ __device__ inline void gauss_jordan6(const float* Din, float* out) {
 // the RECIPROCALS of the diagonal stored on the diagonal so that the solves
 // applied every PCG iteration only multiply
 template <class T> __device__ inline void cholesky6(const T* A, double* L) {
+#pragma unroll
     for (int j = 0; j < 6; ++j) {
         double s = A[6 * j + j];
+#pragma unroll
         for (int k = 0; k < j; ++k) s -= L[j * (j + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
         const double inv = 1.0 / sqrt(s);
         L[j * (j + 1) / 2 + j] = inv;
+#pragma unroll
         for (int i = j + 1; i < 6; ++i) {
             double t = A[6 * i + j];
+#pragma unroll
             for (int k = 0; k < j; ++k) t -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
             L[i * (i + 1) / 2 + j] = t * inv;
         }
@@ -382,15 +386,7 @@ template <> struct BlockStore<false> {
     __device__ static V* ptr(const InstDesc& I) { return I.bsr; }
 };
 
-// ------------------------------- element-parallel block accumulation -----
-// Diagonal blocks: a group of 8 lanes owns one node; a warp holds 4 groups.
-// The group stages 8 of its terms
-// at a time in shared memory, each as weighted twist-Jacobian rows already in
-// the accumulation precision, then every lane accumulates the 4-5 block
-// elements it owns over the staged terms. The inner loop is shared loads and
-// fused multiply-adds only: no type conversions, no cross-lane reduction, and
-// all 8 lanes of a group busy.
-//
+// ------------------------------------------------- JtJ block helpers -----
 // Twist Jacobian row of a point-to-point or smooth residual at point p
 // (geometry_icp_jacobian.cuh:91-120, 323-343): f_c(p) = [row c of [p]x^T ; e_c].
 template <class T> __device__ inline void twist_rows(T px, T py, T pz, T f[3][6]) {
@@ -414,178 +410,169 @@ template <class T> __device__ inline T twist_rows_product(const T p[3], const T 
     return r == k ? (T)1 : (T)0;
 }
 
-constexpr int kGroupLanes = 8;
-constexpr int kDiagStride = 23;  // u[3][6], lambda^2, rb[3], channel count
+// upper-triangle index of a symmetric 6x6 block (r <= k)
+__device__ constexpr int sym_idx(int r, int k) { return r * 6 - (r * (r - 1)) / 2 + (k - r); }
 
-// Diagonal descriptor of term t for node n: D += lambda^2 sum_c u_c u_c^T,
-// b += sum_c u_c rb_c.
-template <class T>
-__device__ inline int stage_diag(const InstDesc& I, const TermOffsets& off, const mvdr_penalty& lam, uint32_t t,
-                                  uint32_t n, T* o) {
-    uint32_t k;
-    const TermType ty = off.typed(t, k);
-    int nch = 0;
-    switch (ty) {
-        case kDense:
-        case kForeground: {
-            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
-            const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
-            const T l2 = ty == kDense ? (T)1 : cvt<T>(lam.foreground * lam.foreground);
-            const T w = cvt<T>(weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n));
-            const T J[6] = {cvt<T>(a.x), cvt<T>(a.y), cvt<T>(a.z), cvt<T>(a.w), cvt<T>(b.x), cvt<T>(b.y)};
+// S += sg g^T on the upper triangle (sg is a multiple of g, so the product is
+// symmetric)
+template <class Acc>
+__device__ inline void add_sym_outer(Acc S[21], const Acc sg[6], const Acc g[6]) {
 #pragma unroll
-            for (int q = 0; q < 6; ++q) o[q] = w * J[q];
-            o[18] = l2;
-            o[19] = -l2 * cvt<T>(b.z);
-            nch = 1;
-            break;
-        }
-        case kSmooth: {
-            const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
-            if (b.z == 0.f) break;
-            const float4 rr = I.smooth[3 * (size_t)k + 2];
-            const bool is_i = n == I.graph[k].x;
-            const float4 p = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
-            T fr[3][6];
-            twist_rows<T>(cvt<T>(p.x), cvt<T>(p.y), cvt<T>(p.z), fr);
-            const T l2 = cvt<T>(lam.smooth * lam.smooth);
-            const T sg = is_i ? (T)1 : (T)-1;
-            const T rc[3] = {cvt<T>(rr.x), cvt<T>(rr.y), cvt<T>(rr.z)};
+    for (int r = 0; r < 6; ++r)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-#pragma unroll
-                for (int q = 0; q < 6; ++q) o[6 * c + q] = fr[c][q];
-                o[19 + c] = -l2 * sg * rc[c];
-            }
-            o[18] = l2;
-            nch = 3;
-            break;
-        }
-        case kFeature:
-        case kCross: {
-            const bool f = ty == kFeature;
-            const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
-            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
-            const T l2 = f ? cvt<T>(lam.feature * lam.feature) : cvt<T>(lam.cross_view * lam.cross_view);
-            const T w = cvt<T>(weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), n));
-            const float raw[3] = {rw.x, rw.y, rw.z};
-            T fr[3][6];
-            twist_rows<T>(cvt<T>(wv.x), cvt<T>(wv.y), cvt<T>(wv.z), fr);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const T hw = cvt<T>(huber_weight(raw[c]));
-#pragma unroll
-                for (int q = 0; q < 6; ++q) o[6 * c + q] = w * hw * fr[c][q];
-                o[19 + c] = -l2 * hw * cvt<T>(raw[c]);
-            }
-            o[18] = l2;
-            nch = 3;
-            break;
-        }
-        default: break;
-    }
-    return nch;
+        for (int k = r; k < 6; ++k) S[sym_idx(r, k)] += sg[r] * g[k];
 }
+
+// ---------------------------------------------------- diagonal blocks ----
+// One warp per node. The lanes take the node's terms round-robin and keep
+// D_i = sum_t lambda_t^2 w_ti^2 sum_c g_c g_c^T (21 upper-triangle sums) and
+// b_i = -sum_t lambda_t^2 w_ti sum_c g_c r_c (6 sums) in registers; one fixed
+// butterfly then reduces the 27 sums across the warp, so the result does not
+// depend on scheduling. computeBlockDiagonalPreconditionerKernel and
+// computeJtResidualWithIndexKernel (PreconditionerBlocked.cu:18-399,
+// JtDotResidualIndexed.cu:18-382) compute the same sums. A CTA takes
+// kDiagNodes nodes; their damped blocks wait in shared memory and one warp
+// then factors them, a node per lane (Cholesky in double for mixed precision,
+// the Gauss-Jordan inverse of BlockDiagonalPreconditionerInverse.cu:7-60 in
+// float).
+constexpr uint32_t kDiagNodes = 32;
 
 template <bool MIXED>
 __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
-    constexpr int kWarps = 4;
-    __shared__ Acc stage[kWarps][32][kDiagStride];
-    __shared__ int nchs[kWarps][32];
-    __shared__ Acc vals[kWarps][4][28];
+    __shared__ Acc s_blocks[kDiagNodes][21];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->half_pairs > I.cap_pairs) return;
     TermOffsets off;
     off.load(C);
-    const uint32_t w = threadIdx.x >> 5, lane = lane_id();
-    const uint32_t g = lane / kGroupLanes, l8 = lane % kGroupLanes;
-    // lane-owned elements e = l8 + 8 m: 0..20 the upper triangle of D, 21..26 b
-    int er[4], ek[4];
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const Acc l2_fg = (Acc)(lam.foreground * lam.foreground), l2_smooth = (Acc)(lam.smooth * lam.smooth);
+    const Acc l2_feat = (Acc)(lam.feature * lam.feature), l2_cross = (Acc)(lam.cross_view * lam.cross_view);
+    for (uint32_t base = blockIdx.x * kDiagNodes; base < I.N; base += gridDim.x * kDiagNodes) {
+        for (uint32_t j = warp; j < kDiagNodes && base + j < I.N; j += nwarps) {
+            const uint32_t node = base + j;
+            const uint32_t b0 = I.n2t_offset[node], b1 = I.n2t_offset[node + 1];
+            Acc S[21], R[6];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const int e = (int)l8 + 8 * m;
-        er[m] = 0;
-        ek[m] = 0;
-        int c = 0;
-        for (int r = 0; r < 6; ++r)
-            for (int k2 = r; k2 < 6; ++k2, ++c)
-                if (c == e) { er[m] = r; ek[m] = k2; }
-        if (e >= 21) { er[m] = e - 21; ek[m] = -1; }
-        if (e >= 27) { er[m] = 0; ek[m] = -2; }
-    }
-    const uint32_t groups = gridDim.x * kWarps * 4;
-    const uint32_t first = (blockIdx.x * kWarps + w) * 4;
-    for (uint32_t gbase = first; gbase < I.N + 0u; gbase += groups) {
-        const uint32_t node = gbase + g;
-        const bool active = node < I.N;
-        const uint32_t b = active ? I.n2t_offset[node] : 0, e = active ? I.n2t_offset[node + 1] : 0;
-        // chunks of this warp: the longest group decides
-        uint32_t nchunks = (e - b + kGroupLanes - 1) / kGroupLanes;
-        for (int o = 8; o <= 16; o <<= 1) nchunks = max(nchunks, __shfl_xor_sync(0xffffffffu, nchunks, o));
-        Acc acc[4] = {0, 0, 0, 0};
-        for (uint32_t ch = 0; ch < nchunks; ++ch) {
-            const uint32_t p = b + ch * kGroupLanes + l8;
-            nchs[w][lane] = p < e ? stage_diag<Acc>(I, off, lam, I.n2t_index[p], node, stage[w][lane]) : 0;
-            __syncwarp();
-#pragma unroll 2
-            for (int q = 0; q < kGroupLanes; ++q) {
-                const Acc* d = stage[w][g * kGroupLanes + q];
-                const int nch = nchs[w][g * kGroupLanes + q];
-                for (int c = 0; c < nch; ++c) {
-                    const Acc* u = d + 6 * c;
+            for (int q = 0; q < 21; ++q) S[q] = 0;
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        if (ek[m] >= 0) acc[m] += d[18] * u[er[m]] * u[ek[m]];
-                        else if (ek[m] == -1) acc[m] += u[er[m]] * d[19 + c];
+            for (int q = 0; q < 6; ++q) R[q] = 0;
+            for (uint32_t p = b0 + lane; p < b1; p += 32) {
+                uint32_t k;
+                const TermType ty = off.typed(I.n2t_index[p], k);
+                if (ty == kDense || ty == kForeground) {
+                    const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+                    const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+                    if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0, r = 0
+                    const Acc l2 = ty == kDense ? (Acc)1 : l2_fg;
+                    const Acc w = (Acc)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+                    const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
+                    const Acc sw = l2 * w * w, rw = -l2 * w * (Acc)b.z;
+                    Acc sg[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) {
+                        sg[q] = sw * g[q];
+                        R[q] += rw * g[q];
+                    }
+                    add_sym_outer(S, sg, g);
+                } else if (ty == kSmooth) {
+                    // computeSmoothTermJacobian (geometry_icp_jacobian.cuh:323-343):
+                    // J_i,c = f_c(T_i x_j), J_j,c = -f_c(T_j x_j)
+                    const float4 a = I.smooth[3 * (size_t)k], b = I.smooth[3 * (size_t)k + 1];
+                    if (b.z == 0.f) continue;
+                    const float4 rr = I.smooth[3 * (size_t)k + 2];
+                    const bool is_i = node == I.graph[k].x;
+                    const float4 pt = is_i ? a : make_float4(a.w, b.x, b.y, 0.f);
+                    Acc fr[3][6];
+                    twist_rows<Acc>((Acc)pt.x, (Acc)pt.y, (Acc)pt.z, fr);
+                    const Acc rc[3] = {(Acc)rr.x, (Acc)rr.y, (Acc)rr.z};
+                    const Acc sgn = is_i ? (Acc)1 : (Acc)-1;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        Acc sg[6];
+                        const Acc rw = -l2_smooth * sgn * rc[c];
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) {
+                            sg[q] = l2_smooth * fr[c][q];
+                            R[q] += rw * fr[c][q];
+                        }
+                        add_sym_outer(S, sg, fr[c]);
+                    }
+                } else if (ty == kFeature || ty == kCross) {
+                    const bool f = ty == kFeature;
+                    const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
+                    const float4 raw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
+                    const Acc l2 = f ? l2_feat : l2_cross;
+                    const Acc w = (Acc)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+                    Acc fr[3][6];
+                    twist_rows<Acc>((Acc)wv.x, (Acc)wv.y, (Acc)wv.z, fr);
+                    const float rv[3] = {raw.x, raw.y, raw.z};
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const Acc hw = (Acc)huber_weight(rv[c]);
+                        const Acc rw = -l2 * hw * (Acc)rv[c];
+                        Acc g[6], sg[6];
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) {
+                            g[q] = w * hw * fr[c][q];
+                            sg[q] = l2 * g[q];
+                            R[q] += rw * g[q];
+                        }
+                        add_sym_outer(S, sg, g);
                     }
                 }
             }
-            __syncwarp();
-        }
-        // gather the 27 values of each group, damping on the diagonal
+            // fixed-order butterfly: every lane ends with the warp totals
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const int el = (int)l8 + 8 * m;
-            if (el < 27) vals[w][g][el] = acc[m] + ((ek[m] >= 0 && er[m] == ek[m]) ? (Acc)1e-2f : (Acc)0);
-        }
-        __syncwarp();
-        if (active) {
+            for (int q = 0; q < 21; ++q) S[q] = warp_sum(S[q]);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) R[q] = warp_sum(R[q]);
+#pragma unroll
+            for (int r = 0; r < 6; ++r) S[sym_idx(r, r)] += (Acc)1e-2f;  // damping
             const size_t blk = 36 * (size_t)(I.half_offset[node] + node);
-            for (uint32_t i = l8; i < 36; i += kGroupLanes) {
-                const int r = i / 6, k2 = i % 6;
-                const int lo = min(r, k2), hi = max(r, k2);
-                const Acc v = vals[w][g][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
-                I.diag[36 * (size_t)node + i] = (float)v;
-                BlockStore<MIXED>::ptr(I)[blk + blk_idx(r, k2)] = v;
-            }
-            if (l8 < 6) I.jtr[6 * (size_t)node + l8] = (float)vals[w][g][21 + l8];
-            if (l8 == 0) {
-                Acc D[36];
+            typename BlockStore<MIXED>::V* store = BlockStore<MIXED>::ptr(I);
+            // lanes 0..35 of the block (lanes 0..3 write two elements)
 #pragma unroll
-                for (int r = 0; r < 6; ++r)
+            for (int r = 0; r < 6; ++r)
 #pragma unroll
-                    for (int k2 = 0; k2 < 6; ++k2) {
-                        const int lo = r < k2 ? r : k2, hi = r < k2 ? k2 : r;
-                        D[6 * r + k2] = vals[w][g][lo * 6 - (lo * (lo - 1)) / 2 + (hi - lo)];
-                    }
-                if (MIXED) {
-                    double L[21];
-                    cholesky6(D, L);
-#pragma unroll
-                    for (int i = 0; i < 21; ++i) I.chol[21 * (size_t)node + i] = L[i];
-                } else {
-                    float Df[36], Mi[36];
-#pragma unroll
-                    for (int i = 0; i < 36; ++i) Df[i] = (float)D[i];
-                    gauss_jordan6(Df, Mi);
-#pragma unroll
-                    for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
+                for (int k2 = 0; k2 < 6; ++k2) {
+                    const uint32_t i = 6 * r + k2;
+                    if (i % 32 != lane) continue;
+                    const Acc v = S[r <= k2 ? sym_idx(r, k2) : sym_idx(k2, r)];
+                    I.diag[36 * (size_t)node + i] = (float)v;
+                    store[blk + blk_idx(r, k2)] = v;
                 }
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (lane == (uint32_t)(q + 8)) I.jtr[6 * (size_t)node + q] = (float)R[q];
+#pragma unroll
+            for (int q = 0; q < 21; ++q)
+                if (lane == (uint32_t)q) s_blocks[j][q] = S[q];
+        }
+        __syncthreads();
+        if (warp == 0 && base + lane < I.N) {
+            const uint32_t node = base + lane;
+            Acc D[36];
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+#pragma unroll
+                for (int k2 = 0; k2 < 6; ++k2) D[6 * r + k2] = s_blocks[lane][r <= k2 ? sym_idx(r, k2) : sym_idx(k2, r)];
+            if constexpr (MIXED) {
+                double L[21];
+                cholesky6(D, L);
+#pragma unroll
+                for (int i = 0; i < 21; ++i) I.chol[21 * (size_t)node + i] = L[i];
+            } else {
+                float Df[36], Mi[36];
+#pragma unroll
+                for (int i = 0; i < 36; ++i) Df[i] = (float)D[i];
+                gauss_jordan6(Df, Mi);
+#pragma unroll
+                for (int i = 0; i < 36; ++i) I.minv[36 * (size_t)node + i] = Mi[i];
             }
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
@@ -600,16 +587,6 @@ __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mv
 // computeSmoothJtJBlock (JtJMaterializer.cu:20-528, jtj_block_jacobian.cuh:8-65)
 // compute the same sums; only the upper block (i, j) is stored, (j, i) is read
 // as its transpose.
-__device__ constexpr int sym_idx(int r, int k) { return r * 6 - (r * (r - 1)) / 2 + (k - r); }  // r <= k
-
-template <class Acc>
-__device__ inline void add_sym_outer(Acc S[21], const Acc sg[6], const Acc g[6]) {
-#pragma unroll
-    for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int k = r; k < 6; ++k) S[sym_idx(r, k)] += sg[r] * g[k];
-}
-
 template <bool MIXED>
 __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
@@ -1280,7 +1257,7 @@ cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, cudaStream_t st)
 
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, bool materialize,
                             cudaStream_t st) {
-    const uint32_t gn = (lc.max_nodes + 15) / 16;
+    const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 128, 0, st, d, lam);
     else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
     if (materialize) {
@@ -1327,7 +1304,7 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
-    const uint32_t gn = (lc.max_nodes + 15) / 16;
+    const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     switch (stage) {
         case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
         case MVDR_STAGE_DIAG:
