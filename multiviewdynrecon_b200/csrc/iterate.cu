@@ -811,96 +811,93 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
     return (float)acc;
 }
 
+// ----------------------------------------------------- PCG direction ----
+// d = s + beta d_prev (BlockPCG.cuh:167-181), formed once per iteration for
+// the whole vector, so that the SpMV reads its operand directly; mixed
+// precision also keeps it in double, the SpMV's accumulation type.
+template <bool MIXED>
+__global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* insts, int parity) {
+    const InstDesc& I = insts[blockIdx.y];
+    const float* dprev = parity ? I.d0 : I.d1;
+    float* dcur = parity ? I.d1 : I.d0;
+    const float beta = (float)I.scalars[2];
+    const uint32_t n = 6 * I.N;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const float dv = I.s[e] + beta * dprev[e];
+        dcur[e] = dv;
+        if (MIXED) I.dd[e] = (double)dv;
+    }
+}
+
 // ------------------------------------------------------- tiled SpMV -----
-// A CTA owns kTileRows consecutive block rows. It first gathers x = s + beta
-// d_prev, in the storage precision, for every entry of those rows (bsr_col
-// gives the block column) into shared memory; the entries of consecutive rows
-// are contiguous, so this is one coalesced sweep of bsr_col. After that no
-// block address depends on a load, and the row loop streams the blocks from
-// HBM with many loads in flight (the block positions are staged in shared
-// memory with x, so a block load waits on no global load). Six threads per
-// block row: thread r reads row r of each stored block (three pair loads; the
-// six threads together sweep the block contiguously, see blk_idx). For an
-// upper or diagonal block that row
-// gives y_r directly; for a lower block, stored as its transpose, it is column
-// r of the needed block and adds x_r times it to all six rows, which the row's
-// threads sum through shared memory at the end. The stored transpose of a
-// lower block belongs to a row of this or an earlier tile, so it is usually
-// still in L2. Tiles with more than kTileMaxBlocks entries go in pieces.
+// A CTA owns kTileRows consecutive block rows; kTileSplit threads per scalar
+// row take alternate blocks of the row. Thread r of a row reads row r of each
+// stored block (three pair loads; the six threads together sweep the block
+// contiguously, see blk_idx) and the column's direction from the L2-resident
+// d. For an upper or diagonal block that row gives y_r directly; for a lower
+// block, stored as its transpose, it is column r of the needed block and adds
+// x_r times it to all six rows, which the row's threads sum through shared
+// memory at the end. Block and direction addresses depend only on the
+// sequential bsr_pos / bsr_col entries, so many loads stay in flight. The
+// stored transpose of a lower block belongs to a row of this or an earlier
+// tile, so it is usually still in L2.
 constexpr uint32_t kTileRows = 16;
 constexpr uint32_t kTileSplit = 2;  // threads per scalar row, taking alternate blocks
 constexpr uint32_t kTileThreads = 6 * kTileSplit * kTileRows;
-constexpr uint32_t kTileMaxBlocks = 384;
 
 template <class V> struct Pair;
 template <> struct Pair<double> { using type = double2; };
 template <> struct Pair<float> { using type = float2; };
 
-// q = A d with d = s + beta d_prev formed on the fly (BlockPCG.cuh:167-181 fused
-// into the SpMV of the next iteration); d.q partial; alpha = delta / d.q.
+// the SpMV operand: the direction in the storage precision
+template <bool MIXED> __device__ inline const typename BlockStore<MIXED>::V* direction(const InstDesc& I, int parity);
+template <> __device__ inline const double* direction<true>(const InstDesc& I, int) { return I.dd; }
+template <> __device__ inline const float* direction<false>(const InstDesc& I, int parity) {
+    return parity ? I.d1 : I.d0;
+}
+
+// q = A d, d.q partial; alpha = delta / d.q
 template <bool MIXED>
 __global__ void __launch_bounds__(kTileThreads) pcg_spmv_kernel(const InstDesc* insts, int parity) {
     using V = typename BlockStore<MIXED>::V;
     using V2 = typename Pair<V>::type;
-    __shared__ __align__(16) V s_x[kTileMaxBlocks * 6];
-    __shared__ uint32_t s_pos[kTileMaxBlocks];
     __shared__ V s_cols[kTileRows][kTileSplit * 6][7];
     const InstDesc& I = insts[blockIdx.y];
     using T = typename std::conditional<MIXED, double, float>::type;
     const V* store = BlockStore<MIXED>::ptr(I);
-    const float* dprev = parity ? I.d0 : I.d1;
-    float* dcur = parity ? I.d1 : I.d0;
-    const float beta = (float)I.scalars[2];
+    const V* xvec = direction<MIXED>(I, parity);
     const uint32_t t = threadIdx.x;
     T part = 0;
     const uint32_t r0 = blockIdx.x * kTileRows;
     if (r0 < I.N) {
         const uint32_t r1 = min(r0 + kTileRows, I.N);
-        const uint32_t b_begin = I.blkrow_offset[r0] + r0, b_end = I.blkrow_offset[r1] + r1;
         const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
         const bool computes = row < r1;
-        uint32_t rb = 0, re = 0;
-        if (computes) {
-            rb = I.blkrow_offset[row] + row;
-            re = I.blkrow_offset[row + 1] + row + 1;
-        }
         V acc = 0;
         V col_acc[6] = {0, 0, 0, 0, 0, 0};
-        for (uint32_t pb = b_begin; pb < b_end; pb += kTileMaxBlocks) {
-            const uint32_t pe = min(pb + kTileMaxBlocks, b_end), nb = pe - pb;
-            for (uint32_t i = t; i < nb; i += kTileThreads) s_pos[i] = I.bsr_pos[pb + i];
-#pragma unroll 4
-            for (uint32_t i = t; i < nb * 6; i += kTileThreads) {
-                const size_t e = 6 * (size_t)I.bsr_col[pb + i / 6] + i % 6;
-                s_x[i] = (V)(I.s[e] + beta * dprev[e]);
-            }
-            __syncthreads();
-            if (computes) {
-                // blocks rb + half, rb + half + kTileSplit, ... that lie in this piece
-                uint32_t mb = max(rb, pb);
-                mb += (rb + half + kTileSplit - mb % kTileSplit) % kTileSplit;
-                const uint32_t me = min(re, pe);
-#pragma unroll 4
-                for (uint32_t b = mb; b < me; b += kTileSplit) {
-                    const uint32_t pos = s_pos[b - pb];
-                    const V2* blk = reinterpret_cast<const V2*>(store + 36 * (size_t)(pos & ~kTransposedBlock));
-                    const V2 a01 = blk[rr], a23 = blk[6 + rr], a45 = blk[12 + rr];
-                    const V av[6] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y};
-                    const V* xv = s_x + 6 * (b - pb);
-                    if (pos & kTransposedBlock) {
-                        const V xr = xv[rr];
+        if (computes) {
+            const uint32_t rb = I.blkrow_offset[row] + row, re = I.blkrow_offset[row + 1] + row + 1;
+#pragma unroll 2
+            for (uint32_t b = rb + half; b < re; b += kTileSplit) {
+                const uint32_t pos = I.bsr_pos[b];
+                const uint32_t col = I.bsr_col[b];
+                const V2* blk = reinterpret_cast<const V2*>(store + 36 * (size_t)(pos & ~kTransposedBlock));
+                const V2 a01 = blk[rr], a23 = blk[6 + rr], a45 = blk[12 + rr];
+                const V av[6] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y};
+                const V* xc = xvec + 6 * (size_t)col;
+                if (pos & kTransposedBlock) {
+                    const V xr = xc[rr];
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) col_acc[k] += av[k] * xr;
-                    } else {
+                    for (int k = 0; k < 6; ++k) col_acc[k] += av[k] * xr;
+                } else {
+                    const V2* x2 = reinterpret_cast<const V2*>(xc);
+                    const V2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
+                    const V xv[6] = {x01.x, x01.y, x23.x, x23.y, x45.x, x45.y};
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
-                    }
+                    for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
                 }
             }
-            __syncthreads();  // the next piece overwrites s_x
-        }
-        // slot 6 of a thread's row-sum entry holds its direct (row) sum
-        if (computes) {
+            // slot 6 of a thread's row-sum entry holds its direct (row) sum
 #pragma unroll
             for (int k = 0; k < 6; ++k) s_cols[lr][6 * half + rr][k] = col_acc[k];
             s_cols[lr][6 * half + rr][6] = acc;
@@ -916,10 +913,8 @@ __global__ void __launch_bounds__(kTileThreads) pcg_spmv_kernel(const InstDesc* 
             }
             const float qv = (float)acc;
             const size_t e = 6 * (size_t)row + rr;
-            const float dv = I.s[e] + beta * dprev[e];
-            dcur[e] = dv;
             I.q[e] = qv;
-            part += (T)dv * (T)qv;
+            part += (T)xvec[e] * (T)qv;
         }
     }
     T tot;
@@ -1278,6 +1273,7 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
+    const uint32_t gvec = min((6 * lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gwarp = (lc.max_nodes + 7) / 8;
     const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
     if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d);
@@ -1291,8 +1287,13 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
             if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
         } else {
-            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
-            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
+            if (mixed) {
+                MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity);
+                MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
+            } else {
+                MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity);
+                MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
+            }
         }
         if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity);
         else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity);
@@ -1304,6 +1305,7 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
+    const uint32_t gvec = min((6 * lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     switch (stage) {
         case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
@@ -1318,8 +1320,13 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             break;
         }
         case MVDR_STAGE_SPMV:
-            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
-            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
+            if (mixed) {
+                MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0);
+                MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
+            } else {
+                MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0);
+                MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
+            }
             break;
         case MVDR_STAGE_PCG_UPDATE:
             if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0);

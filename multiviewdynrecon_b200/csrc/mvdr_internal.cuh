@@ -289,6 +289,7 @@ struct InstDesc {
     float* q;
     float* d0;
     float* d1;
+    double* dd;             // mixed precision: the PCG direction in double (the SpMV operand)
     float* jp;              // matrix-free scratch: J.p per scalar term
     double* scalars;        // PCG scalars: [0] delta, [1] alpha, [2] beta, [3] dq
     double* partials;       // per-CTA partial sums

@@ -191,6 +191,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.q = a.take<float>(6 * N);
     I.d0 = a.take<float>(6 * N);
     I.d1 = a.take<float>(6 * N);
+    I.dd = mixed ? a.take<double>(6 * N) : nullptr;
     // J.p per scalar term of the matrix-free operator (double in mixed precision)
     I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
     I.scalars = a.take<double>(8);
