@@ -4,7 +4,8 @@ Workload (one step): a batch of independent multi-view solves, each 3 views at
 640x480 around a torso-like ellipsoid, 4096 nodes, 8-NN graph, 4-NN skinning,
 all terms (dense depth, foreground mask, 1000 sparse feature pairs per view,
 2000 cross-view pairs per adjacent view pair), 5 Gauss-Newton x 15 PCG
-iterations, mixed precision (float bulk, double reductions and block Cholesky).
+iterations, mixed precision (float Jacobians and PCG vectors; double residual
+chain, JtJ blocks, reductions and block Cholesky).
 Each instance shares the synthetic geometry and has its own random initial
 warp field. Every step re-binds the inputs (which resets each warp field) and
 runs the index build plus all Gauss-Newton iterations of every instance as one
@@ -126,6 +127,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+def measured_traffic(args):
+    """DRAM bytes (read + write) per launch of pcg_spmv_kernel from the ncu
+    capture summarised in profiles/ for the default workload; None for other
+    workloads or when the summary is absent."""
+    default = (args.batch == 16 and args.nodes == 4096 and args.width == 640 and args.height == 480
+               and args.precision == "mixed" and args.mode == "materialized")
+    path = os.path.join(ROOT, "profiles", "pcg_spmv_torso_3view_4096nodes_16inst.md")
+    if not default or not os.path.exists(path):
+        return None, None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("| DRAM read + write |"):
+                parts = line.split("|")[2].replace("MB", "").split("+")
+                return int(sum(float(p) for p in parts) * 1e6), "profiles/pcg_spmv_torso_3view_4096nodes_16inst.md"
+    return None, None
+
+
 def algorithmic_bytes(counts, N, mixed=True):
     """Compulsory HBM bytes per stage and instance (each array read or written
     once). JtJ is kept as half storage: N diagonal + P upper 6x6 blocks, in
@@ -143,7 +161,8 @@ def algorithmic_bytes(counts, N, mixed=True):
         "terms": 122 * Td + 86 * Tf + 29 * Ts + 72 * (Tp + Tc) + 32 * N,
         "diag": term_data + 4 * counts.node2term_entries + 144 * N + 36 * elem * N + 24 * N + precond,
         "offdiag": term_data + 4 * counts.nodepair_entries + 12 * P + 36 * elem * P,
-        "spmv": blocks + entries + 4 * (N + 1) + 4 * 24 * N,
+        "spmv": blocks + entries + 4 * (N + 1) + 24 * N * elem // 4 + 24 * N,
+        "direction": 3 * 24 * N + (48 * N if mixed else 0),
         "pcg_update": 24 * N * 6 + precond,
         "update": 24 * N + 64 * N,
     }
@@ -217,7 +236,8 @@ def run_ours(args, rank, world, dist):
         stream.synchronize()
         for name, sid in (("index", abi.STAGE_INDEX), ("terms", abi.STAGE_TERMS), ("diag", abi.STAGE_DIAG),
                           ("offdiag", abi.STAGE_OFFDIAG), ("spmv", abi.STAGE_SPMV),
-                          ("pcg_update", abi.STAGE_PCG_UPDATE), ("update", abi.STAGE_UPDATE)):
+                          ("direction", abi.STAGE_DIRECTION), ("pcg_update", abi.STAGE_PCG_UPDATE),
+                          ("update", abi.STAGE_UPDATE)):
             if name == "offdiag" and mode != abi.MODE_MATERIALIZED:
                 continue
             for _ in range(2):
@@ -238,9 +258,10 @@ def run_ours(args, rank, world, dist):
     peak, peak_kind = load_peaks()
     spmv = stages["spmv"]
     spmv_bytes = B * abytes["spmv"]
+    traffic, traffic_src = measured_traffic(args)
     roofline = {"kernel": "pcg_spmv_kernel", "bound": "hbm", "achieved": spmv["GBps"], "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s", "frac": round(spmv["GBps"] / peak, 4),
-                "traffic": None, "algorithmic_bytes_per_launch": spmv_bytes,
+                "traffic": traffic, "traffic_source": traffic_src, "algorithmic_bytes_per_launch": spmv_bytes,
                 "launch_ms": spmv["ms"]}
 
     # e2e: host buffers -> device copies -> solve -> warp fields back to host

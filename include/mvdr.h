@@ -70,10 +70,10 @@ typedef enum mvdr_status {
  * MIXED: Jacobians, stored residuals and PCG vectors in float. Double is used
  *        where float rounding would move the increment by more than 1e-4:
  *        the warped-point / residual chain of each term (positions of about
- *        1 m give residuals of about 1 mm), the accumulation of the JtJ blocks
- *        and Jt r (stored as float plus a 16-bit correction), the SpMV row
- *        sums, the PCG dot products and norms, and the 6x6 block Cholesky of
- *        the preconditioner. */
+ *        1 m give residuals of about 1 mm), the accumulation and storage of the
+ *        JtJ blocks, the accumulation of Jt r, the SpMV row sums, the PCG dot
+ *        products and norms, and the 6x6 block Cholesky of the
+ *        preconditioner. */
 typedef enum mvdr_precision {
     MVDR_PRECISION_FP32 = 0,
     MVDR_PRECISION_MIXED = 1
@@ -364,9 +364,10 @@ enum {
     MVDR_STAGE_TERMS = 1,      /* term evaluation                                */
     MVDR_STAGE_DIAG = 2,       /* diagonal blocks, Jt r and the preconditioner   */
     MVDR_STAGE_OFFDIAG = 3,    /* off-diagonal JtJ blocks (materialised mode)    */
-    MVDR_STAGE_SPMV = 4,       /* one PCG operator application (SpMV + d.q)      */
+    MVDR_STAGE_SPMV = 4,       /* one PCG SpMV (q = A d, d.q) on the current d   */
     MVDR_STAGE_PCG_UPDATE = 5, /* one PCG vector update (x, r, s, r.s)           */
-    MVDR_STAGE_UPDATE = 6      /* warp-field update                              */
+    MVDR_STAGE_UPDATE = 6,     /* warp-field update                              */
+    MVDR_STAGE_DIRECTION = 7   /* one PCG direction update d = s + beta d_prev   */
 };
 /* Enqueue the kernels of one stage for every instance of the batch, with the
  * lambdas of Gauss-Newton iteration 0. The stage reads the state left by the

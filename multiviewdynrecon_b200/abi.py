@@ -19,7 +19,8 @@ STATUS_NAMES = {0: "MVDR_OK", 1: "MVDR_EINVAL", 2: "MVDR_ECAPACITY", 3: "MVDR_EC
 PRECISION_FP32, PRECISION_MIXED = 0, 1
 MODE_MATERIALIZED, MODE_MATRIX_FREE = 0, 1
 COMPAT_REF_VIEW_LOOKUP = 1
-(STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE) = range(7)
+(STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE,
+ STAGE_DIRECTION) = range(8)
 
 (ARRAY_DENSE_PIXELS, ARRAY_DENSE_KNN, ARRAY_DENSE_KNN_WEIGHT, ARRAY_FOREGROUND_PIXELS, ARRAY_NODE2TERM_OFFSET,
  ARRAY_NODE2TERM_INDEX, ARRAY_HALF_NODEPAIR_KEY, ARRAY_NODEPAIR_TERM_INDEX, ARRAY_NODEPAIR_KEY,

@@ -455,8 +455,15 @@ __global__ void __launch_bounds__(256) np_row_count_kernel(const InstDesc* insts
 }
 
 // CTA per node: gather (j, t) keys of the row, sort them, write the term
-// values of the row and the row's unique pairs (to a temporary per-row area)
-__global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts) {
+// values of the row and the row's unique pairs (to a temporary per-row area).
+// Launched twice: once with a small shared-memory footprint for the rows of
+// at most `max_len` entries (nearly all), so that many CTAs share an SM, and
+// once, on a small grid, with the capacity-sized footprint for the rows above
+// `min_len`; each launch leaves the other's rows alone.
+constexpr uint32_t kRowSmall = 2048;
+
+__global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts, uint32_t min_len,
+                                                           uint32_t max_len) {
     extern __shared__ unsigned long long s64[];
     __shared__ uint32_t fill;
     __shared__ uint32_t wtot[8];
@@ -468,6 +475,7 @@ __global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts
     for (uint32_t node = blockIdx.x; node < I.N; node += gridDim.x) {
         const uint32_t len = I.row_count[node];
         const uint32_t out = I.row_offset[node];
+        if (len < min_len || len > max_len) continue;
         if (len == 0) {
             if (threadIdx.x == 0) I.upper_count[node] = 0;
             continue;
@@ -716,7 +724,13 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     // node pair -> term
     MVDR_LAUNCH(np_row_count_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanRows);
-    MVDR_LAUNCH(np_row_build_kernel, grid2(lc.max_nodes, B), 256, (size_t)lc.cap_row * 8, st, d);
+    // without a second launch the first one also takes (and flags) the rows
+    // above the capacity
+    MVDR_LAUNCH(np_row_build_kernel, grid2(lc.max_nodes, B), 256, (size_t)min(lc.cap_row, kRowSmall) * 8, st, d, 0u,
+                lc.cap_row > kRowSmall ? kRowSmall : 0xFFFFFFFFu);
+    if (lc.cap_row > kRowSmall)
+        MVDR_LAUNCH(np_row_build_kernel, grid2(min(lc.max_nodes, (uint32_t)lc.sm_count), B), 256,
+                    (size_t)lc.cap_row * 8, st, d, kRowSmall + 1, 0xFFFFFFFFu);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanUpper);
     MVDR_LAUNCH(np_half_compact_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanBlkRows);

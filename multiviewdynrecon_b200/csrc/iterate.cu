@@ -1320,13 +1320,12 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             break;
         }
         case MVDR_STAGE_SPMV:
-            if (mixed) {
-                MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0);
-                MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
-            } else {
-                MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0);
-                MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
-            }
+            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
+            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
+            break;
+        case MVDR_STAGE_DIRECTION:
+            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0);
+            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0);
             break;
         case MVDR_STAGE_PCG_UPDATE:
             if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0);

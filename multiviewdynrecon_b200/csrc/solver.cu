@@ -855,7 +855,7 @@ int mvdr_batch_enqueue_stage(mvdr_batch* b, int stage, void* stream) {
     int rc = all_bound(bb);
     if (rc != MVDR_OK) return rc;
     if (stage == MVDR_STAGE_INDEX) return enqueue_index(bb, (cudaStream_t)stream);
-    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_UPDATE) return fail(MVDR_EINVAL, "unknown stage");
+    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_DIRECTION) return fail(MVDR_EINVAL, "unknown stage");
     CU(launch_stage(bb.lc, bb.d_inst, penalty_for(bb.cfg, 0), stage, (cudaStream_t)stream));
     return MVDR_OK;
 }
