@@ -263,6 +263,13 @@ MVDR_API int mvdr_solve(mvdr_solver* solver, uint32_t gn_iterations, uint32_t pc
 /* SolvedNodeSE3 (NonRigidSolver.h:214): copies the current node SE(3) array
  * (num_nodes dual quaternions) to `dst`, which may be host or device memory. */
 MVDR_API int mvdr_get_node_se3(mvdr_solver* solver, mvdr_dual_quaternion* dst, void* stream);
+/* Enqueue a copy of the current warp field (num_nodes dual quaternions) into
+ * dst (device or pinned host memory) on `stream` and return at once: the
+ * counterpart of the reference's SolvedNodeSE3() device view, for callers
+ * that overlap solves. Unlike mvdr_get_node_se3 it does not read the device
+ * error record; read error_flags with mvdr_get_counts once the stream is
+ * done. */
+MVDR_API int mvdr_copy_node_se3_async(mvdr_solver* solver, mvdr_dual_quaternion* dst, void* stream);
 
 /* Synchronises `stream` and returns the sizes of the current index. */
 MVDR_API int mvdr_get_counts(mvdr_solver* solver, mvdr_counts* out, void* stream);
@@ -353,6 +360,8 @@ MVDR_API int mvdr_batch_set_inputs_host(mvdr_batch* batch, uint32_t instance, co
 MVDR_API int mvdr_batch_solve(mvdr_batch* batch, uint32_t gn_iterations, uint32_t pcg_iterations,
                      int use_graph, void* stream);
 MVDR_API int mvdr_batch_get_node_se3(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst, void* stream);
+MVDR_API int mvdr_batch_copy_node_se3_async(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst,
+                                            void* stream);
 /* The single-instance view of one batch member (not owned; do not destroy). */
 MVDR_API int mvdr_batch_instance(mvdr_batch* batch, uint32_t instance, mvdr_solver** out);
 

@@ -45,6 +45,8 @@ def _declare(L):
         "mvdr_gn_iteration": (i32, [vp, u32, vp]),
         "mvdr_solve": (i32, [vp, u32, u32, vp]),
         "mvdr_get_node_se3": (i32, [vp, vp, vp]),
+        "mvdr_copy_node_se3_async": (i32, [vp, vp, vp]),
+        "mvdr_batch_copy_node_se3_async": (i32, [vp, u32, vp, vp]),
         "mvdr_get_counts": (i32, [vp, P(abi.Counts), vp]),
         "mvdr_get_energy": (i32, [vp, P(C.c_double), vp]),
         "mvdr_get_array": (i32, [vp, i32, vp, C.c_size_t, P(C.c_size_t), vp]),

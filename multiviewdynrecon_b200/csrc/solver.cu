@@ -78,6 +78,10 @@ struct Batch {
     size_t per_inst_bytes = 0;
     std::vector<OwnedInputs> owned;
     std::vector<uint8_t> has_inputs;
+    // the descriptor last copied to d_inst per instance: a rebind with the
+    // same buffers and sizes skips the (pageable, possibly blocking) upload
+    std::vector<InstDesc> uploaded;
+    std::vector<uint8_t> uploaded_valid;
     uint32_t gn_iter = 0;
     // graph cache: (gn, pcg) -> exec
     std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;
@@ -302,6 +306,8 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     }
     b->owned.resize(B);
     b->has_inputs.assign(B, 0);
+    b->uploaded.resize(B);
+    b->uploaded_valid.assign(B, 0);
     e = cudaMemcpy(b->d_inst, b->host.data(), sizeof(InstDesc) * B, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         delete b;
@@ -428,7 +434,11 @@ static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStrea
     // SolverIterationData::SetWarpFieldInitialValue (SolverIterationData.cpp:37-50)
     CU(cudaMemcpyAsync(I.se3, in->node_se3, sizeof(DQ) * I.N, cudaMemcpyDefault, st));
     CU(cudaMemsetAsync(I.counts, 0, sizeof(DeviceCounts), st));
-    CU(cudaMemcpyAsync(b.d_inst + inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice, st));
+    if (!b.uploaded_valid[inst] || std::memcmp(&b.uploaded[inst], &I, sizeof(InstDesc)) != 0) {
+        CU(cudaMemcpyAsync(b.d_inst + inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice, st));
+        b.uploaded[inst] = I;
+        b.uploaded_valid[inst] = 1;
+    }
     b.has_inputs[inst] = 1;
     b.gn_iter = 0;
     return MVDR_OK;
@@ -482,14 +492,40 @@ static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cuda
         o.bytes = total;
     }
     std::vector<void*> dst(items.size(), nullptr);
+    // Arrays that follow each other on the host at the same offsets as their
+    // device copies (gaps below 256 bytes, as a packing allocator leaves) are
+    // sent as one copy: a few large transfers instead of one per array keep
+    // the stream's queue short, so the caller's thread does not stall when it
+    // overlaps uploads with solves.
+    const char* run_src = nullptr;
+    char* run_dst = nullptr;
+    size_t run_len = 0;
+    auto flush = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        if (run_len) e = cudaMemcpyAsync(run_dst, run_src, run_len, cudaMemcpyHostToDevice, st);
+        run_len = 0;
+        return e;
+    };
     size_t off = 0;
     for (size_t i = 0; i < items.size(); ++i) {
         if (items[i].bytes && items[i].src) {
-            dst[i] = static_cast<char*>(o.mem) + off;
-            CU(cudaMemcpyAsync(dst[i], items[i].src, items[i].bytes, cudaMemcpyHostToDevice, st));
+            char* d = static_cast<char*>(o.mem) + off;
+            const char* src = static_cast<const char*>(items[i].src);
+            dst[i] = d;
+            const bool joins = run_len && src >= run_src + run_len && (size_t)(src - (run_src + run_len)) < 256 &&
+                               (size_t)(src - run_src) == (size_t)(d - run_dst);
+            if (joins) {
+                run_len = (size_t)(src - run_src) + items[i].bytes;
+            } else {
+                CU(flush());
+                run_src = src;
+                run_dst = d;
+                run_len = items[i].bytes;
+            }
         }
         off += (items[i].bytes + 255) & ~(size_t)255;
     }
+    CU(flush());
     size_t k = 0;
     for (uint32_t v = 0; v < in->num_views; ++v) {
         mvdr_view_inputs& V = dev.views[v];
@@ -772,6 +808,14 @@ int mvdr_get_node_se3(mvdr_solver* s, mvdr_dual_quaternion* dst, void* stream) {
     return MVDR_OK;
 }
 
+int mvdr_copy_node_se3_async(mvdr_solver* s, mvdr_dual_quaternion* dst, void* stream) {
+    if (!s || !dst) return fail(MVDR_EINVAL, "null argument");
+    Batch& b = *s->batch;
+    CU(cudaMemcpyAsync(dst, b.host[s->inst].se3, sizeof(DQ) * b.host[s->inst].N, cudaMemcpyDefault,
+                       (cudaStream_t)stream));
+    return MVDR_OK;
+}
+
 int mvdr_get_counts(mvdr_solver* s, mvdr_counts* out, void* stream) {
     if (!s || !out) return fail(MVDR_EINVAL, "null argument");
     DeviceCounts c;
@@ -841,6 +885,11 @@ int mvdr_batch_solve(mvdr_batch* b, uint32_t gn, uint32_t pcg, int use_graph, vo
 int mvdr_batch_get_node_se3(mvdr_batch* b, uint32_t i, mvdr_dual_quaternion* dst, void* stream) {
     if (!b || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
     return mvdr_get_node_se3(&b->batch->views[i]->s, dst, stream);
+}
+
+int mvdr_batch_copy_node_se3_async(mvdr_batch* b, uint32_t i, mvdr_dual_quaternion* dst, void* stream) {
+    if (!b || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
+    return mvdr_copy_node_se3_async(&b->batch->views[i]->s, dst, stream);
 }
 
 int mvdr_batch_instance(mvdr_batch* b, uint32_t i, mvdr_solver** out) {

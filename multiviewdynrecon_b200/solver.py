@@ -49,18 +49,36 @@ class DeviceScene:
         self.tensors = {}
         self.device = device
         self.pin = pin
+        arrays = []
+
+        def collect(name, arr):
+            a = np.ascontiguousarray(arr)
+            if a.size:
+                arrays.append((name, a.view(np.uint8).reshape(-1)))
+            return None
+
+        abi.fill_inputs(scene, collect)
+        if pin:
+            # one pinned arena, arrays at 256-byte offsets in input order: the
+            # library's owned device copy has the same layout, so the upload
+            # of an instance is a single transfer
+            offs, total = {}, 0
+            for name, a in arrays:
+                offs[name] = total
+                total += (a.size + 255) & ~255
+            arena = torch.empty(total, dtype=torch.uint8).pin_memory()
+            view = arena.numpy()
+            for name, a in arrays:
+                view[offs[name]:offs[name] + a.size] = a
+                self.tensors[name] = arena[offs[name]:offs[name] + a.size]
+            self._arena = arena
+        else:
+            for name, a in arrays:
+                self.tensors[name] = torch.from_numpy(a.copy()).to(device)
 
         def ptr(name, arr):
-            a = np.ascontiguousarray(arr)
-            if a.size == 0:
-                return None
-            t = torch.from_numpy(a.view(np.uint8).reshape(-1).copy())
-            if pin:
-                t = t.pin_memory()
-            else:
-                t = t.to(device)
-            self.tensors[name] = t
-            return t.data_ptr()
+            t = self.tensors.get(name)
+            return None if t is None else t.data_ptr()
 
         self.inputs = abi.fill_inputs(scene, ptr)
 
@@ -117,6 +135,13 @@ class NonRigidSolver:
     def solved_node_se3(self, stream=None):
         out = torch.empty((self.num_nodes, 8), dtype=torch.float32, device="cuda")
         check(lib().mvdr_get_node_se3(self.h, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
+        return out
+
+    def solved_node_se3_async(self, out, stream=None):
+        """Enqueue the warp-field copy into `out` (device or pinned host) and
+        return without synchronising; device-side errors are read later with
+        counts()."""
+        check(lib().mvdr_copy_node_se3_async(self.h, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
         return out
 
     def counts(self, stream=None):
@@ -192,6 +217,12 @@ class BatchSolver:
         if out is None:
             out = torch.empty((n, 8), dtype=torch.float32, device="cuda")
         check(lib().mvdr_batch_get_node_se3(self.h, i, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
+        return out
+
+    def node_se3_async(self, i, out, stream=None):
+        """Enqueue instance i's warp-field copy into `out`; no synchronisation
+        and no error check (see NonRigidSolver.solved_node_se3_async)."""
+        check(lib().mvdr_batch_copy_node_se3_async(self.h, i, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
         return out
 
     def instance(self, i):

@@ -291,3 +291,19 @@ def test_capacity_overflow_is_reported():
     ok, _ = make_gpu(scene)
     ok.solve_non_rigid_alignment(1, 2)
     ok.solved_node_se3()
+
+
+def test_async_warp_field_copy_matches_checked_copy():
+    """mvdr_copy_node_se3_async enqueues the same warp field that the checked
+    mvdr_get_node_se3 returns, into pinned host memory on a side stream."""
+    scene = small_scene("torso")
+    g, _ = make_gpu(scene)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        g.solve_non_rigid_alignment(scene.gn_iterations, scene.pcg_iterations, stream=stream)
+        out = torch.empty((scene.num_nodes, 8), dtype=torch.float32, pin_memory=True)
+        g.solved_node_se3_async(out, stream=stream)
+    stream.synchronize()
+    assert g.counts(stream=stream).error_flags == 0
+    ref = g.solved_node_se3(stream=stream).cpu()
+    assert torch.equal(out, ref)
