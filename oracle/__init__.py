@@ -58,6 +58,7 @@ def lib():
         L.orc_dq_to_mat34.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_mat34_to_dq.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_apply_twist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_set_node_se3_f64.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_gauss_jordan_inverse.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
         _lib = L
@@ -153,7 +154,12 @@ class Oracle:
         lib().orc_set_increment(self.h, _p(x))
 
     def set_node_se3(self, dq):
-        """Continue from another run's warp field (N x 8 float)."""
+        """Continue from another run's warp field (N x 8; float32 is taken as
+        is, float64 keeps its full precision)."""
+        if np.asarray(dq).dtype == np.float64:
+            dq = np.ascontiguousarray(dq, np.float64)
+            lib().orc_set_node_se3_f64(self.h, _p(dq))
+            return
         dq = np.ascontiguousarray(dq, np.float32)
         lib().orc_set_node_se3(self.h, _p(dq))
 

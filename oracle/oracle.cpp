@@ -1165,6 +1165,16 @@ void orc_set_node_se3(void* h, const float* dq) {
     }
 }
 
+/* Replace the current warp field with double-precision dual quaternions
+ * (finite-difference checks perturb the field below float resolution). */
+void orc_set_node_se3_f64(void* h, const double* dq) {
+    Oracle* o = (Oracle*)h;
+    for (uint32_t i = 0; i < o->N; ++i) {
+        const double* d = dq + 8 * (size_t)i;
+        o->se3d[i] = {{d[0], d[1], d[2], d[3]}, {d[4], d[5], d[6], d[7]}};
+    }
+}
+
 /* One full Gauss-Newton iteration. */
 void orc_gn_iteration(void* h, uint32_t pcg) {
     Oracle* o = (Oracle*)h;

@@ -355,3 +355,31 @@ def test_golden_fixtures(oracle_mod, name):
     o.update()
     assert max_relative_error(o.get(abi.ARRAY_NODE_SE3), g["ARRAY_NODE_SE3"], 1e-7) < 1e-5
     assert math.isclose(o.energy(), float(g["energy"]), rel_tol=1e-6)
+
+
+@pytest.mark.parametrize("kind,uniform,tol", [("torso", True, 1e-5), ("body", True, 1e-5),
+                                              ("torso", False, 1e-3)])
+def test_adjoint_products_match_finite_differences(oracle_mod, kind, uniform, tol):
+    """The oracle's own J^T r and J^T J p (FP64) equal central finite
+    differences of its weighted residuals on 64 random twist coordinates: to
+    rounding on a uniform warp field, where the skinning Jacobian model is
+    exact, and to its first-order accuracy on a per-node perturbed field."""
+    from fd_adjoint import DAMPING, fd_adjoint_reference, fd_config, random_coords, uniform_field
+    scene = small_scene(kind)
+    if uniform:
+        scene = uniform_field(scene)
+    cfg = fd_config(scene)
+    rng = np.random.default_rng(21)
+    coords = random_coords(rng, scene.num_nodes)
+    p = rng.normal(size=len(coords))
+    b_fd, jtjp_fd, o = fd_adjoint_reference(oracle_mod, scene, cfg, coords, p)
+    o.assemble()
+    b = o.get(abi.ARRAY_JTR, as_double=True).reshape(-1, 6)
+    b_or = np.array([b[n, c] for n, c in coords])
+    assert rel_norm_error(b_or, b_fd) < tol
+    x = np.zeros(6 * scene.num_nodes)
+    for (n, c), v in zip(coords, p):
+        x[6 * n + c] += v
+    y = o.apply_jtj(x)
+    y_or = np.array([y[6 * n + c] - DAMPING * x[6 * n + c] for n, c in coords])
+    assert rel_norm_error(y_or, jtjp_fd) < tol
