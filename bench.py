@@ -60,10 +60,32 @@ def parse():
     return p.parse_args()
 
 
+def instance_seeds(rank, batch):
+    """Seeds of the initial warp fields of one rank's instances: every rank
+    solves its own, disjoint set of instances (weak scaling, no collective in
+    the solve)."""
+    return [1000 * rank + i for i in range(batch)]
+
+
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time; every rank must call it (one all-reduce)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, batch, ms):
+    """Whole-job solves/s: all ranks' instances over the slowest rank's time."""
+    return world * batch / (ms / 1e3)
+
+
 def make_scenes(args, rank):
     from multiviewdynrecon_b200 import synth
     base = synth.torso_multi_view(seed=2, num_nodes=args.nodes, width=args.width, height=args.height)
-    scenes = [synth.perturb_warp_field(base, seed=1000 * rank + i) for i in range(args.batch)]
+    scenes = [synth.perturb_warp_field(base, seed=sd) for sd in instance_seeds(rank, args.batch)]
     return base, scenes
 
 
@@ -214,13 +236,10 @@ def run_ours(args, rank, world, dist):
         e1.record(stream)
         e1.synchronize()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, "cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * B / (ms / 1e3)
+    value = job_value(world, B, ms)
 
     # accuracy of instance 0 and counts
     inst0 = batch.instance(0)
@@ -305,12 +324,8 @@ def run_ours(args, rank, world, dist):
         e2e_step(k)
     b2.record(solve_stream)
     b2.synchronize()
-    e2e_ms = a.elapsed_time(b2) / args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": round(world * B / (e2e_ms / 1e3), 3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+    e2e_ms = max_over_ranks(a.elapsed_time(b2) / args.steps, dist, "cuda")
+    e2e = {"value": round(job_value(world, B, e2e_ms), 3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
            "pipeline": "uploads in order on a copy stream, overlapping the previous step's solve"}
     for bt in e2e_batches:  # device-side error record of every e2e solve
