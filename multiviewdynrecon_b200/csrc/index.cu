@@ -387,7 +387,65 @@ __global__ void __launch_bounds__(256) n2t_scatter_kernel(const InstDesc* insts)
     }
 }
 
-// sort each node's term segment ascending (one CTA per node)
+// Sort each node's term segment ascending, one warp per node, in registers:
+// element i = 32 s + lane sits in slot s of a lane; a bitonic network over
+// kWarpSortSlots * 32 keys exchanges across lanes with shuffles (partner
+// distance < 32) and inside a lane between slots otherwise. Segments longer
+// than that are left to n2t_sort_kernel.
+constexpr int kWarpSortSlots = 8;
+constexpr uint32_t kWarpSortMax = 32u * kWarpSortSlots;
+
+__global__ void __launch_bounds__(256) n2t_warp_sort_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (I.counts->node2term_entries > I.cap_k1) return;
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
+        const uint32_t len = e - b;
+        if (len <= 1 || len > kWarpSortMax) continue;
+        uint32_t v[kWarpSortSlots];
+#pragma unroll
+        for (int sl = 0; sl < kWarpSortSlots; ++sl) {
+            const uint32_t i = 32u * sl + lane;
+            v[sl] = i < len ? I.n2t_index[b + i] : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (uint32_t k = 2; k <= kWarpSortMax; k <<= 1) {
+#pragma unroll
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                if (j >= 32) {
+                    const int sj = (int)(j >> 5);
+#pragma unroll
+                    for (int sl = 0; sl < kWarpSortSlots; ++sl) {
+                        if (sl & sj) continue;
+                        const uint32_t i = 32u * sl + lane;
+                        const bool up = (i & k) == 0;
+                        const uint32_t a = v[sl], c = v[sl | sj];
+                        v[sl] = up ? min(a, c) : max(a, c);
+                        v[sl | sj] = up ? max(a, c) : min(a, c);
+                    }
+                } else {
+#pragma unroll
+                    for (int sl = 0; sl < kWarpSortSlots; ++sl) {
+                        const uint32_t i = 32u * sl + lane;
+                        const uint32_t o = __shfl_xor_sync(0xffffffffu, v[sl], j);
+                        const bool up = (i & k) == 0, lower = (i & j) == 0;
+                        v[sl] = (up == lower) ? min(v[sl], o) : max(v[sl], o);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int sl = 0; sl < kWarpSortSlots; ++sl) {
+            const uint32_t i = 32u * sl + lane;
+            if (i < len) I.n2t_index[b + i] = v[sl];
+        }
+    }
+}
+
+// sort each node's term segment ascending (one CTA per node) for the
+// segments longer than kWarpSortMax
 __global__ void __launch_bounds__(256) n2t_sort_kernel(const InstDesc* insts) {
     extern __shared__ uint32_t s32[];
     const InstDesc& I = insts[blockIdx.y];
@@ -395,7 +453,7 @@ __global__ void __launch_bounds__(256) n2t_sort_kernel(const InstDesc* insts) {
     for (uint32_t node = blockIdx.x; node < I.N; node += gridDim.x) {
         const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
         const uint32_t len = e - b;
-        if (len <= 1) continue;
+        if (len <= kWarpSortMax) continue;
         if (len > I.cap_seg) {
             if (threadIdx.x == 0) set_error(I, kErrSegmentTooLong);
             continue;
@@ -720,7 +778,9 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     MVDR_LAUNCH(n2t_count_kernel, grid2(spread, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanN2T);
     MVDR_LAUNCH(n2t_scatter_kernel, grid2(spread, B), 256, 0, st, d);
-    MVDR_LAUNCH(n2t_sort_kernel, grid2(lc.max_nodes, B), 256, (size_t)lc.cap_seg * 4, st, d);
+    MVDR_LAUNCH(n2t_warp_sort_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
+    MVDR_LAUNCH(n2t_sort_kernel, grid2(min(lc.max_nodes, (uint32_t)lc.sm_count), B), 256, (size_t)lc.cap_seg * 4, st,
+                d);
     // node pair -> term
     MVDR_LAUNCH(np_row_count_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanRows);
