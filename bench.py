@@ -214,6 +214,11 @@ def run_ours(args, rank, world, dist):
         bind_all()
         batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
 
+    # SpMV tile shape for this workload (one timed sweep of the candidates)
+    with torch.cuda.stream(stream):
+        bind_all()
+        spmv_shape, spmv_shape_ms = batch.autotune(stream=stream)
+
     # kernels per solve: one direct (non-graph) solve counted through the ABI
     with torch.cuda.stream(stream):
         bind_all()
@@ -291,6 +296,9 @@ def run_ours(args, rank, world, dist):
     # its warp fields inside the timed region.
     host_scenes = [DeviceScene(s, pin=True) for s in scenes]
     e2e_batches = [batch, BatchSolver(cfg, B)]
+    for i, ds in enumerate(dev_scenes):
+        e2e_batches[1].set_input(i, ds, stream=stream)
+    e2e_batches[1].autotune(stream=stream)
     copy_stream, solve_stream = torch.cuda.Stream(), stream
     uploaded = [torch.cuda.Event(), torch.cuda.Event()]
     solved = [torch.cuda.Event(), torch.cuda.Event()]
@@ -358,6 +366,9 @@ def run_ours(args, rank, world, dist):
         single.close()
 
     return dict(value=value, ms=ms, kernels_per_step=kernels_per_step, clocks=clocks.summary(), stages=stages,
+                spmv_tile={"rows_per_cta": spmv_shape[0], "threads_per_row": 6 * spmv_shape[1],
+                           "candidates_ms": {f"{r}x{6 * sp}": round(t, 5)
+                                             for (r, sp), t in zip(abi.SPMV_SHAPES, spmv_shape_ms)}},
                 roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base)
 
 
@@ -452,7 +463,8 @@ def main():
                        "parallelism": f"independent instances, {world} GPU(s), no collective in the solve"},
             "gpu_launches": int(r["kernels_per_step"] * args.steps),
             "kernels_per_step": int(r["kernels_per_step"]),
-            "clocks": r["clocks"], "roofline": r["roofline"], "stages": r["stages"], "e2e": r["e2e"],
+            "clocks": r["clocks"], "roofline": r["roofline"], "stages": r["stages"], "spmv_tile": r["spmv_tile"],
+            "e2e": r["e2e"],
             "plain_fp32": r["plain"],
             "speedup_vs_plain_fp32": (round(r["value"] / r["plain"]["value"], 3) if r["plain"] else None),
             "cpu_baseline": cpu,

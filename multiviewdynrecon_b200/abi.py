@@ -21,6 +21,10 @@ MODE_MATERIALIZED, MODE_MATRIX_FREE = 0, 1
 COMPAT_REF_VIEW_LOOKUP = 1
 (STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE,
  STAGE_DIRECTION) = range(8)
+# candidate SpMV tile shapes (block rows per CTA, threads per scalar row), in
+# the order mvdr_batch_autotune reports their times
+SPMV_SHAPES = [(16, 2), (8, 2), (16, 1), (32, 1), (16, 3), (8, 4), (32, 2)]
+NUM_SPMV_SHAPES = len(SPMV_SHAPES)
 
 (ARRAY_DENSE_PIXELS, ARRAY_DENSE_KNN, ARRAY_DENSE_KNN_WEIGHT, ARRAY_FOREGROUND_PIXELS, ARRAY_NODE2TERM_OFFSET,
  ARRAY_NODE2TERM_INDEX, ARRAY_HALF_NODEPAIR_KEY, ARRAY_NODEPAIR_TERM_INDEX, ARRAY_NODEPAIR_KEY,

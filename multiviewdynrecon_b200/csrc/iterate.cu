@@ -830,8 +830,8 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
 }
 
 // ------------------------------------------------------- tiled SpMV -----
-// A CTA owns kTileRows consecutive block rows; kTileSplit threads per scalar
-// row take alternate blocks of the row. Thread r of a row reads row r of each
+// A CTA owns ROWS consecutive block rows; SPLIT threads per scalar row take
+// every SPLIT-th block of the row (the autotuner picks ROWS and SPLIT). Thread r of a row reads row r of each
 // stored block (three pair loads; the six threads together sweep the block
 // contiguously, see blk_idx) and the column's direction from the L2-resident
 // d. For an upper or diagonal block that row gives y_r directly; for a lower
@@ -841,9 +841,7 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
 // sequential bsr_pos / bsr_col entries, so many loads stay in flight. The
 // stored transpose of a lower block belongs to a row of this or an earlier
 // tile, so it is usually still in L2.
-constexpr uint32_t kTileRows = 16;
-constexpr uint32_t kTileSplit = 2;  // threads per scalar row, taking alternate blocks
-constexpr uint32_t kTileThreads = 6 * kTileSplit * kTileRows;
+const SpmvShape kSpmvShapes[kNumSpmvShapes] = {{16, 2}, {8, 2}, {16, 1}, {32, 1}, {16, 3}, {8, 4}, {32, 2}};
 
 template <class V> struct Pair;
 template <> struct Pair<double> { using type = double2; };
@@ -857,8 +855,8 @@ template <> __device__ inline const float* direction<false>(const InstDesc& I, i
 }
 
 // q = A d, d.q partial; alpha = delta / d.q
-template <bool MIXED>
-__global__ void __launch_bounds__(kTileThreads) pcg_spmv_kernel(const InstDesc* insts, int parity) {
+template <bool MIXED, uint32_t kTileRows, uint32_t kTileSplit>
+__global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(const InstDesc* insts, int parity) {
     using V = typename BlockStore<MIXED>::V;
     using V2 = typename Pair<V>::type;
     __shared__ V s_cols[kTileRows][kTileSplit * 6][7];
@@ -1272,7 +1270,6 @@ cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& 
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
-    const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
     const uint32_t gvec = min((6 * lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gwarp = (lc.max_nodes + 7) / 8;
     const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
@@ -1287,13 +1284,10 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
             if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
         } else {
-            if (mixed) {
-                MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity);
-                MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
-            } else {
-                MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity);
-                MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, parity);
-            }
+            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity);
+            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity);
+            const cudaError_t e = launch_spmv(lc, d, parity, st);
+            if (e != cudaSuccess) return e;
         }
         if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity);
         else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity);
@@ -1301,10 +1295,34 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     return cudaGetLastError();
 }
 
+template <bool MIXED, uint32_t R, uint32_t S>
+static void spmv_shape_launch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
+    auto* kernel = &pcg_spmv_kernel<MIXED, R, S>;
+    MVDR_LAUNCH(kernel, grid2((lc.max_nodes + R - 1) / R, lc.B), 6 * S * R, 0, st, d, parity);
+}
+
+template <bool MIXED>
+static void spmv_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
+    switch (lc.spmv_shape) {
+        case 1: spmv_shape_launch<MIXED, 8, 2>(lc, d, parity, st); break;
+        case 2: spmv_shape_launch<MIXED, 16, 1>(lc, d, parity, st); break;
+        case 3: spmv_shape_launch<MIXED, 32, 1>(lc, d, parity, st); break;
+        case 4: spmv_shape_launch<MIXED, 16, 3>(lc, d, parity, st); break;
+        case 5: spmv_shape_launch<MIXED, 8, 4>(lc, d, parity, st); break;
+        case 6: spmv_shape_launch<MIXED, 32, 2>(lc, d, parity, st); break;
+        default: spmv_shape_launch<MIXED, 16, 2>(lc, d, parity, st); break;
+    }
+}
+
+cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
+    if (lc.precision == MVDR_PRECISION_MIXED) spmv_dispatch<true>(lc, d, parity, st);
+    else spmv_dispatch<false>(lc, d, parity, st);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, int stage, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
-    const uint32_t gtile = (lc.max_nodes + kTileRows - 1) / kTileRows;
     const uint32_t gvec = min((6 * lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     switch (stage) {
@@ -1320,9 +1338,7 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             break;
         }
         case MVDR_STAGE_SPMV:
-            if (mixed) MVDR_LAUNCH(pcg_spmv_kernel<true>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
-            else MVDR_LAUNCH(pcg_spmv_kernel<false>, grid2(gtile, lc.B), kTileThreads, 0, st, d, 0);
-            break;
+            return launch_spmv(lc, d, 0, st);
         case MVDR_STAGE_DIRECTION:
             if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0);
             else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0);

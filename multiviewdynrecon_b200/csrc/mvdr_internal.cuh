@@ -308,6 +308,7 @@ struct LaunchCfg {
     uint32_t chunks_per_view;
     int precision, mode;
     int sm_count;
+    int spmv_shape;  // index into the SpMV tile shapes (chosen by the autotuner)
 };
 
 // ----------------------------------------------------------- launchers --
@@ -317,6 +318,16 @@ void count_launch();
 
 // raise the dynamic shared-memory limit of the segment-sort kernels
 cudaError_t set_index_smem_limits(size_t seg_bytes, size_t row_bytes);
+
+// SpMV tile shapes the autotuner chooses from: block rows per CTA and threads
+// per scalar row (each taking every `split`-th block of the row)
+struct SpmvShape {
+    uint32_t rows, split;
+};
+constexpr int kNumSpmvShapes = 7;
+extern const SpmvShape kSpmvShapes[kNumSpmvShapes];
+// one PCG SpMV (q = A d, d.q) with the shape lc.spmv_shape
+cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st);
 
 cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
 cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);

@@ -892,6 +892,54 @@ int mvdr_batch_copy_node_se3_async(mvdr_batch* b, uint32_t i, mvdr_dual_quaterni
     return mvdr_copy_node_se3_async(&b->batch->views[i]->s, dst, stream);
 }
 
+int mvdr_batch_autotune(mvdr_batch* bh, void* stream, double* times_ms, uint32_t capacity, uint32_t* rows,
+                        uint32_t* split) {
+    if (!bh) return fail(MVDR_EINVAL, "batch is null");
+    Batch& b = *bh->batch;
+    const cudaStream_t st = (cudaStream_t)stream;
+    if (b.cfg.mode == MVDR_MODE_MATERIALIZED) {
+        int rc = all_bound(b);
+        if (rc != MVDR_OK) return rc;
+        rc = enqueue_index(b, st);
+        if (rc == MVDR_OK) rc = enqueue_iteration(b, 0, 1, st);
+        if (rc != MVDR_OK) return rc;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CU(cudaEventCreate(&e0));
+        CU(cudaEventCreate(&e1));
+        constexpr int kReps = 20;
+        int best = 0;
+        float best_ms = 0.f;
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < kNumSpmvShapes && e == cudaSuccess; ++i) {
+            LaunchCfg lc = b.lc;
+            lc.spmv_shape = i;
+            for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = launch_spmv(lc, b.d_inst, 0, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+            for (int r = 0; r < kReps && e == cudaSuccess; ++r) e = launch_spmv(lc, b.d_inst, 0, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            ms /= kReps;
+            if (times_ms && (uint32_t)i < capacity) times_ms[i] = ms;
+            if (i == 0 || ms < best_ms) {
+                best = i;
+                best_ms = ms;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (e != cudaSuccess) return fail(MVDR_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
+        b.lc.spmv_shape = best;
+        for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
+        b.graphs.clear();
+        b.gn_iter = 0;
+    }
+    if (rows) *rows = kSpmvShapes[b.lc.spmv_shape].rows;
+    if (split) *split = kSpmvShapes[b.lc.spmv_shape].split;
+    return MVDR_OK;
+}
+
 int mvdr_batch_instance(mvdr_batch* b, uint32_t i, mvdr_solver** out) {
     if (!b || !out || i >= b->batch->B) return fail(MVDR_EINVAL, "bad batch or instance");
     *out = &b->batch->views[i]->s;

@@ -225,6 +225,15 @@ class BatchSolver:
         check(lib().mvdr_batch_copy_node_se3_async(self.h, i, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
         return out
 
+    def autotune(self, stream=None):
+        """Pick the SpMV tile shape for this batch (see mvdr_batch_autotune);
+        the inputs must be bound again before the next solve. Returns
+        ((rows, threads_per_row), per-candidate ms)."""
+        times = (C.c_double * 16)()
+        rows, split = C.c_uint32(), C.c_uint32()
+        check(lib().mvdr_batch_autotune(self.h, _stream_handle(stream), times, 16, C.byref(rows), C.byref(split)))
+        return (rows.value, split.value), [t for t in times[:abi.NUM_SPMV_SHAPES]]
+
     def instance(self, i):
         """NonRigidSolver-like view of one member (for checks); not owned."""
         h = C.c_void_p()

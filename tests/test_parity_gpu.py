@@ -338,3 +338,27 @@ def test_adjoint_products_vs_finite_differences(oracle_mod, mode):
     y = g.apply_jtj(torch.from_numpy(x).cuda()).cpu().numpy().astype(np.float64)
     y_g = np.array([y[6 * n + c] - DAMPING * x[6 * n + c] for n, c in coords])
     assert rel_norm_error(y_g, jtjp_fd) < 1e-4
+
+
+def test_autotuned_spmv_shape_solves_the_same_system():
+    """mvdr_batch_autotune picks one of the SpMV tile shapes; solves with the
+    chosen shape agree with the default shape's (only the order of the row
+    sums differs)."""
+    scene = small_scene("torso")
+    cfg = abi.make_config(scene, precision=abi.PRECISION_MIXED)
+    ref = BatchSolver(cfg, 2)
+    tuned = BatchSolver(cfg, 2)
+    for b in (ref, tuned):
+        for i in range(2):
+            b.set_input(i, scene)
+    shape, times = tuned.autotune()
+    assert shape in abi.SPMV_SHAPES and len(times) == abi.NUM_SPMV_SHAPES and min(times) > 0
+    for i in range(2):
+        tuned.set_input(i, scene)  # the autotuner ran one iteration
+    for b in (ref, tuned):
+        b.solve(scene.gn_iterations, scene.pcg_iterations)
+    torch.cuda.synchronize()
+    for i in range(2):
+        xa = ref.instance(i).get_array(abi.ARRAY_INCREMENT)
+        xb = tuned.instance(i).get_array(abi.ARRAY_INCREMENT)
+        assert rel_norm_error(xb, xa) < 1e-5
