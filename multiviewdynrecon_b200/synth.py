@@ -303,35 +303,23 @@ def _poisson_disk(points, n, rng, r_hint):
     pts = np.asarray(points, np.float64)
     order = rng.permutation(len(pts))
 
+    ordered = pts[order]
+    tree = cKDTree(ordered)
+
     def throw(r):
-        cell = r / math.sqrt(3.0)
-        keys = np.floor(pts[order] / cell).astype(np.int64)
-        grid = {}
+        # greedy pass in `order`: a candidate is accepted when no accepted
+        # point lies within r (strictly); the neighbour lists come from one
+        # vectorised KD-tree query
+        nbrs = tree.query_ball_point(ordered, r * (1.0 - 1e-12))
+        blocked = np.zeros(len(order), bool)
         acc = []
-        rr = r * r
-        reach = 2
         for k in range(len(order)):
-            key = (int(keys[k, 0]), int(keys[k, 1]), int(keys[k, 2]))
-            p = pts[order[k]]
-            ok = True
-            for dx in range(-reach, reach + 1):
-                for dy in range(-reach, reach + 1):
-                    for dz in range(-reach, reach + 1):
-                        j = grid.get((key[0] + dx, key[1] + dy, key[2] + dz))
-                        if j is not None:
-                            q = pts[j]
-                            if (p[0] - q[0]) ** 2 + (p[1] - q[1]) ** 2 + (p[2] - q[2]) ** 2 < rr:
-                                ok = False
-                                break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if ok:
-                grid[key] = order[k]
-                acc.append(order[k])
-                if len(acc) >= n:
-                    break
+            if blocked[k]:
+                continue
+            acc.append(order[k])
+            if len(acc) >= n:
+                break
+            blocked[nbrs[k]] = True
         return acc
 
     # thin the candidate set first so the sequential pass stays short
@@ -369,7 +357,7 @@ def _knn_weights(d2, r):
     return w.astype(np.float32)
 
 
-def _build(name, shapes, cams, W, H, fx, fy, cx, cy, num_nodes, seed, *, node_radius=0.025,
+def _build(name, shapes, cams, W, H, fx, fy, cx, cy, num_nodes, seed, *, auto_radius=False, node_radius=0.025,
            depth_noise=0.002, rot_sigma_deg=2.0, trans_sigma=0.005, features_per_view=0,
            cross_per_pair=0, rigid_offset=False, terms=None, gn=3, pcg=10, outlier_fraction=0.05):
     rng = np.random.default_rng(seed)
@@ -402,10 +390,16 @@ def _build(name, shapes, cams, W, H, fx, fy, cx, cy, num_nodes, seed, *, node_ra
 
     # nodes
     cand = _candidate_thin(surfels, 3 * num_nodes, rng)
-    area_guess = len(cand)
-    nodes_idx = _poisson_disk(surfels[cand], num_nodes, rng, r_hint=0.08)
+    r_hint = 0.08
+    if auto_radius:
+        # start the dart throwing near its final radius: the surface area from
+        # the candidates' spacing, then sqrt(area / n) with a margin (a few
+        # passes instead of tens for large node counts)
+        d_nn = cKDTree(surfels[cand]).query(surfels[cand], k=2)[0][:, 1]
+        area = len(cand) * float(np.mean(d_nn)) ** 2
+        r_hint = 1.3 * math.sqrt(area / num_nodes)
+    nodes_idx = _poisson_disk(surfels[cand], num_nodes, rng, r_hint=r_hint)
     node_pos = surfels[cand][nodes_idx]
-    del area_guess
     tree = cKDTree(node_pos)
     dgraph, igraph = tree.query(node_pos, k=9)
     graph = np.zeros((num_nodes * 8, 2), np.uint16)
@@ -545,7 +539,7 @@ def sphere_single_view(seed=1, num_nodes=2048, width=640, height=480, rigid_offs
 
 
 def torso_multi_view(seed=2, num_nodes=4096, num_views=3, width=640, height=480, features_per_view=1000,
-                     cross_per_pair=2000, rigid_offset=False, distance=1.3):
+                     cross_per_pair=2000, rigid_offset=False, distance=1.3, auto_radius=False):
     """Multi-view: `num_views` cameras spaced evenly (120 deg for 3) around a
     torso-like ellipsoid (semi-axes 0.25/0.15/0.6 m), all terms, 5 GN x 15 PCG."""
     sx = width / 640.0
@@ -562,13 +556,13 @@ def torso_multi_view(seed=2, num_nodes=4096, num_views=3, width=640, height=480,
             R, o = np.eye(3), np.zeros(3)
         cams.append((R, o))
     return _build(f"torso_{num_views}view", shapes, cams, width, height, 570.0 * sx, 570.0 * sy, 320.0 * sx,
-                  240.0 * sy, num_nodes, seed, features_per_view=features_per_view,
+                  240.0 * sy, num_nodes, seed, auto_radius=auto_radius, features_per_view=features_per_view,
                   cross_per_pair=cross_per_pair, rigid_offset=rigid_offset,
                   terms=dict(foreground=True, feature=True, cross_view=True), gn=5, pcg=15)
 
 
 def articulated_body(seed=5, num_nodes=32768, num_views=5, width=1280, height=720, cross_total=20000,
-                     distance=2.2):
+                     distance=2.2, auto_radius=False):
     """Large single solve: ellipsoid torso + 4 capsule limbs with random joint
     bends <= 30 deg, `num_views` views, 8 GN x 20 PCG."""
     rng = np.random.default_rng(seed + 1000)
@@ -596,7 +590,7 @@ def articulated_body(seed=5, num_nodes=32768, num_views=5, width=1280, height=72
     fx = 570.0 * width / 640.0
     per_pair = cross_total // max(1, num_views)
     return _build("articulated_5view", shapes, cams, width, height, fx, fx, width / 2.0, height / 2.0, num_nodes,
-                  seed, features_per_view=0, cross_per_pair=per_pair,
+                  seed, auto_radius=auto_radius, features_per_view=0, cross_per_pair=per_pair,
                   terms=dict(foreground=False, feature=False, cross_view=True), gn=8, pcg=20)
 
 
@@ -608,7 +602,8 @@ def batch_instances(seed=4, count=16, min_nodes=1024, max_nodes=16384, width=640
     for k in range(count):
         n = int(round(math.exp(rng.uniform(math.log(min_nodes), math.log(max_nodes)))))
         v = int(rng.integers(1, 5))
-        out.append(torso_multi_view(seed=seed * 100 + k, num_nodes=n, num_views=v, width=width, height=height))
+        out.append(torso_multi_view(seed=seed * 100 + k, num_nodes=n, num_views=v, width=width, height=height,
+                                    auto_radius=True))
     return out
 
 
