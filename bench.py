@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison leg")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--workload", default="torso", choices=["torso", "uneven", "body"],
+                   help="torso: the headline batch (default); uneven: 16 instances with 1024-16384 nodes and "
+                        "1-4 views; body: one 32768-node, 5-view 1280x720 solve")
     return p.parse_args()
 
 
@@ -177,7 +180,8 @@ def algorithmic_bytes(counts, N, mixed=True):
     """Compulsory HBM bytes per stage and instance (each array read or written
     once). JtJ is kept as half storage: N diagonal + P upper 6x6 blocks, in
     double (mixed precision) or float; the full block-row layout has N + 2P
-    entries of (column, position)."""
+    entries of (column, position). The PCG vectors are double in mixed
+    precision."""
     Td, Ts, Tf, Tp, Tc = (counts.dense_terms, counts.smooth_terms, counts.foreground_terms, counts.feature_terms,
                           counts.cross_terms)
     P = counts.half_pairs
@@ -190,9 +194,10 @@ def algorithmic_bytes(counts, N, mixed=True):
         "terms": 122 * Td + 86 * Tf + 29 * Ts + 72 * (Tp + Tc) + 32 * N,
         "diag": term_data + 4 * counts.node2term_entries + 144 * N + 36 * elem * N + 24 * N + precond,
         "offdiag": term_data + 4 * counts.nodepair_entries + 12 * P + 36 * elem * P,
-        "spmv": blocks + entries + 4 * (N + 1) + 24 * N * elem // 4 + 24 * N,
-        "direction": 3 * 24 * N + (48 * N if mixed else 0),
-        "pcg_update": 24 * N * 6 + precond,
+        # direction read, q written (6 values per node in the solve's precision)
+        "spmv": blocks + entries + 4 * (N + 1) + 2 * 6 * elem * N,
+        "direction": 3 * 6 * elem * N,  # s and d_prev read, d written
+        "pcg_update": 7 * 6 * elem * N + precond,  # x rw, r rw, d, q read, s written
         "update": 24 * N + 64 * N,
     }
 
@@ -379,6 +384,148 @@ def run_ours(args, rank, world, dist):
                 roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base)
 
 
+def first_increment_errors(scenes, cfg_for, gpu_increments, pcg, threads):
+    """Relative 2-norm error of the first Gauss-Newton increment of each
+    instance against the FP64 oracle, with the GPU's pixel and validity
+    decisions (host threads; the oracle's ctypes calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    import oracle
+    from multiviewdynrecon_b200 import abi
+
+    def one(k):
+        sc, (jr, sm, x) = scenes[k], gpu_increments[k]
+        o = oracle.Oracle(sc, cfg_for(sc), fp64=True)
+        o.build_index()
+        o.freeze(jr, sm)
+        o.eval_terms()
+        o.assemble()
+        o.pcg(pcg)
+        x64 = o.get(abi.ARRAY_INCREMENT, as_double=True).reshape(-1)
+        return float(np.linalg.norm(x.reshape(-1) - x64) / max(np.linalg.norm(x64), 1e-300))
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(one, range(len(scenes))))
+
+
+def time_solves(solve, steps, warmup, stream):
+    import torch
+    for _ in range(warmup):
+        solve()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        solve()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def spmv_stage(lib, abi, batch, stream, reps=20):
+    import torch
+    for _ in range(2):
+        lib().mvdr_batch_enqueue_stage(batch.h, abi.STAGE_SPMV, stream.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        lib().mvdr_batch_enqueue_stage(batch.h, abi.STAGE_SPMV, stream.cuda_stream)
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def run_extra_workload(args):
+    """The uneven batch and the large single solve: one JSON line each,
+    documenting configurations beside the headline."""
+    import torch
+    from multiviewdynrecon_b200 import abi, lib, synth
+    from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    t0 = time.perf_counter()
+    if args.workload == "uneven":
+        scenes = synth.batch_instances()
+        gn, pcg = 5, 15
+        caps = dict(max_nodes=max(s.num_nodes for s in scenes), max_views=max(s.num_views for s in scenes),
+                    width=640, height=480, use_foreground=True, use_feature=True, use_cross_view=True,
+                    max_surfels=max(s.num_surfels for s in scenes),
+                    max_feature_terms=max(s.feature.count for s in scenes),
+                    max_cross_terms=max(s.cross_view.count for s in scenes))
+        cfg_for = lambda sc: abi.make_config(sc)  # noqa: E731 - the oracle sizes each instance itself
+        modes = [("materialized", abi.MODE_MATERIALIZED)]
+    else:
+        scenes = [synth.articulated_body(auto_radius=True)]
+        gn, pcg = 8, 20
+        caps = None
+        cfg_for = lambda sc: abi.make_config(sc)  # noqa: E731
+        modes = [("materialized", abi.MODE_MATERIALIZED), ("matrix_free", abi.MODE_MATRIX_FREE)]
+    gen_s = time.perf_counter() - t0
+    dev = [DeviceScene(sc) for sc in scenes]
+    B = len(scenes)
+    line = {"workload": args.workload, "instances": B, "nodes": [sc.num_nodes for sc in scenes],
+            "views": [sc.num_views for sc in scenes], "image": [scenes[0].width, scenes[0].height],
+            "gn": gn, "pcg": pcg, "generation_s": round(gen_s, 1), "modes": {}}
+    incs = None
+    for name, mode in modes:
+        cfg = (abi.make_config(None, precision=abi.PRECISION_MIXED, mode=mode, **caps) if caps
+               else abi.make_config(scenes[0], precision=abi.PRECISION_MIXED, mode=mode))
+        batch = BatchSolver(cfg, B)
+
+        def bind():
+            for i, ds in enumerate(dev):
+                batch.set_input(i, ds, stream=stream)
+
+        with torch.cuda.stream(stream):
+            bind()
+            shape = batch.autotune(stream=stream)[0] if mode == abi.MODE_MATERIALIZED else None
+            ms = time_solves(lambda: (bind(), batch.solve(gn, pcg, use_graph=True, stream=stream)), args.steps,
+                             max(3, args.warmup), stream)
+            entry = {"solves_per_s": round(B / (ms / 1e3), 3), "ms_per_step": round(ms, 3)}
+            if mode == abi.MODE_MATERIALIZED:
+                bind()
+                batch.solve(gn, pcg, use_graph=False, stream=stream)
+                sp = spmv_stage(lib, abi, batch, stream)
+                counts = [batch.instance(i).counts() for i in range(B)]
+                nbytes = sum(algorithmic_bytes(c, sc.num_nodes, True)["spmv"] for c, sc in zip(counts, scenes))
+                peak, _ = load_peaks()
+                entry["spmv"] = {"ms": round(sp, 5), "GBps": round(nbytes / 1e9 / (sp / 1e3), 1),
+                                 "frac_of_measured_hbm": round(nbytes / 1e9 / (sp / 1e3) / peak, 4),
+                                 "tile": {"rows_per_cta": shape[0], "threads_per_row": 6 * shape[1]}}
+                entry["dense_terms"] = [c.dense_terms for c in counts]
+                # first increments for the FP64 comparison
+                bind()
+                batch.solve(1, pcg, use_graph=False, stream=stream)
+                torch.cuda.synchronize()
+                incs = []
+                for i in range(B):
+                    v = batch.instance(i)
+                    v.num_nodes = scenes[i].num_nodes
+                    incs.append((v.get_array(abi.ARRAY_TERM_JACOBIAN), v.get_array(abi.ARRAY_SMOOTH_TERMS),
+                                 v.get_array(abi.ARRAY_INCREMENT)))
+        line["modes"][name] = entry
+        batch.close()
+    # plain FP32 form of the uneven batch: one instance per solve, no graph
+    if args.workload == "uneven":
+        from multiviewdynrecon_b200.solver import NonRigidSolver
+        tot = 0.0
+        for sc, ds in zip(scenes, dev):
+            single = NonRigidSolver(abi.make_config(sc, precision=abi.PRECISION_FP32))
+            with torch.cuda.stream(stream):
+                ms = time_solves(lambda: (single.set_solver_input(ds, stream=stream),
+                                          single.solve_non_rigid_alignment(gn, pcg, stream=stream)), 2, 1, stream)
+            tot += ms
+            single.close()
+        line["plain_fp32"] = {"solves_per_s": round(B / (tot / 1e3), 3), "form": "one instance per solve, no graph"}
+        line["speedup_vs_plain_fp32"] = round(line["modes"]["materialized"]["solves_per_s"] /
+                                              line["plain_fp32"]["solves_per_s"], 3)
+    t1 = time.perf_counter()
+    errs = first_increment_errors(scenes, cfg_for, incs, pcg, os.cpu_count() or 1)
+    line["first_increment_rel_err_vs_fp64"] = [float("%.3g" % e) for e in errs]
+    line["fp64_check_s"] = round(time.perf_counter() - t1, 1)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def cpu_solve_instance(scene, gn, pcg):
     import oracle
     from multiviewdynrecon_b200 import abi
@@ -441,6 +588,9 @@ def main():
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
+
+    if args.workload != "torso":
+        return run_extra_workload(args) if rank == 0 else 0
 
     if world > 1:
         import torch

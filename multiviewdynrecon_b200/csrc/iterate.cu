@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(128) diag_rhs_kernel(const InstDesc* insts, mv
                 }
 #pragma unroll
             for (int q = 0; q < 6; ++q)
-                if (lane == (uint32_t)(q + 8)) I.jtr[6 * (size_t)node + q] = (float)R[q];
+                if (lane == (uint32_t)(q + 8)) PcgVec<MIXED>::jtr(I)[6 * (size_t)node + q] = R[q];
 #pragma unroll
             for (int q = 0; q < 21; ++q)
                 if (lane == (uint32_t)q) s_blocks[j][q] = S[q];
@@ -753,19 +753,14 @@ template <bool MIXED>
 __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     using T = typename std::conditional<MIXED, double, float>::type;
+    using PV = PcgVec<MIXED>;
     T part = 0;
     for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
-        float bv[6];
+        T bv[6], sv[6];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) bv[i] = I.jtr[6 * (size_t)node + i];
-        float sv[6];
-        if (MIXED) {
-            double bd[6], xd[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) bd[i] = bv[i];
-            cholesky6_solve(I.chol + 21 * (size_t)node, bd, xd);
-#pragma unroll
-            for (int i = 0; i < 6; ++i) sv[i] = (float)xd[i];
+        for (int i = 0; i < 6; ++i) bv[i] = PV::jtr(I)[6 * (size_t)node + i];
+        if constexpr (MIXED) {
+            cholesky6_solve(I.chol + 21 * (size_t)node, bv, sv);
         } else {
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
@@ -778,11 +773,11 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             const size_t e = 6 * (size_t)node + i;
-            I.r[e] = bv[i];
-            I.s[e] = sv[i];
-            I.d1[e] = 0.f;
-            I.x[e] = 0.f;
-            part += (T)bv[i] * (T)sv[i];
+            PV::r(I)[e] = bv[i];
+            PV::s(I)[e] = sv[i];
+            PV::d(I, 1)[e] = 0;
+            PV::x(I)[e] = 0;
+            part += bv[i] * sv[i];
         }
     }
     T tot;
@@ -813,20 +808,19 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
 
 // ----------------------------------------------------- PCG direction ----
 // d = s + beta d_prev (BlockPCG.cuh:167-181), formed once per iteration for
-// the whole vector, so that the SpMV reads its operand directly; mixed
-// precision also keeps it in double, the SpMV's accumulation type.
+// the whole vector, so that the SpMV reads its operand directly
 template <bool MIXED>
 __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* insts, int parity) {
     const InstDesc& I = insts[blockIdx.y];
-    const float* dprev = parity ? I.d0 : I.d1;
-    float* dcur = parity ? I.d1 : I.d0;
-    const float beta = (float)I.scalars[2];
+    using PV = PcgVec<MIXED>;
+    using T = typename PV::T;
+    const T* dprev = PV::d(I, !parity);
+    T* dcur = PV::d(I, parity);
+    const T* sv = PV::s(I);
+    const T beta = (T)I.scalars[2];
     const uint32_t n = 6 * I.N;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const float dv = I.s[e] + beta * dprev[e];
-        dcur[e] = dv;
-        if (MIXED) I.dd[e] = (double)dv;
-    }
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        dcur[e] = sv[e] + beta * dprev[e];
 }
 
 // ------------------------------------------------------- tiled SpMV -----
@@ -847,11 +841,9 @@ template <class V> struct Pair;
 template <> struct Pair<double> { using type = double2; };
 template <> struct Pair<float> { using type = float2; };
 
-// the SpMV operand: the direction in the storage precision
-template <bool MIXED> __device__ inline const typename BlockStore<MIXED>::V* direction(const InstDesc& I, int parity);
-template <> __device__ inline const double* direction<true>(const InstDesc& I, int) { return I.dd; }
-template <> __device__ inline const float* direction<false>(const InstDesc& I, int parity) {
-    return parity ? I.d1 : I.d0;
+// the SpMV operand: this iteration's direction
+template <bool MIXED> __device__ inline const typename BlockStore<MIXED>::V* direction(const InstDesc& I, int parity) {
+    return PcgVec<MIXED>::d(I, parity);
 }
 
 // q = A d, d.q partial; alpha = delta / d.q
@@ -909,10 +901,9 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
 #pragma unroll
                 for (int c = 0; c < 6; ++c) acc += s_cols[lr][6 * h + c][rr];
             }
-            const float qv = (float)acc;
             const size_t e = 6 * (size_t)row + rr;
-            I.q[e] = qv;
-            part += (T)xvec[e] * (T)qv;
+            PcgVec<MIXED>::q(I)[e] = acc;
+            part += (T)xvec[e] * (T)acc;
         }
     }
     T tot;
@@ -928,27 +919,22 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
 template <bool MIXED>
 __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity) {
     const InstDesc& I = insts[blockIdx.y];
-    using T = typename std::conditional<MIXED, double, float>::type;
-    const float* d = parity ? I.d1 : I.d0;
-    const float alpha = (float)I.scalars[1];
+    using PV = PcgVec<MIXED>;
+    using T = typename PV::T;
+    const T* d = PV::d(I, parity);
+    const T alpha = (T)I.scalars[1];
     T part = 0;
     for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
-        float rv[6];
+        T rv[6], sv[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             const size_t e = 6 * (size_t)node + i;
-            I.x[e] += alpha * d[e];
-            rv[i] = I.r[e] - alpha * I.q[e];
-            I.r[e] = rv[i];
+            PV::x(I)[e] += alpha * d[e];
+            rv[i] = PV::r(I)[e] - alpha * PV::q(I)[e];
+            PV::r(I)[e] = rv[i];
         }
-        float sv[6];
-        if (MIXED) {
-            double bd[6], xd[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) bd[i] = rv[i];
-            cholesky6_solve(I.chol + 21 * (size_t)node, bd, xd);
-#pragma unroll
-            for (int i = 0; i < 6; ++i) sv[i] = (float)xd[i];
+        if constexpr (MIXED) {
+            cholesky6_solve(I.chol + 21 * (size_t)node, rv, sv);
         } else {
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
@@ -960,8 +946,8 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
         }
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
-            I.s[6 * (size_t)node + i] = sv[i];
-            part += (T)rv[i] * (T)sv[i];
+            PV::s(I)[6 * (size_t)node + i] = sv[i];
+            part += rv[i] * sv[i];
         }
     }
     T tot;
@@ -987,9 +973,10 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
     TermOffsets off;
     off.load(I.counts);
     const uint32_t T = off.o[4];
-    const float beta = fused ? (float)I.scalars[2] : 0.f;
-    const float* s = fused ? I.s : xin;
-    const float* dp = parity ? I.d0 : I.d1;
+    using PV = PcgVec<MIXED>;
+    const typename PV::T beta = fused ? (typename PV::T)I.scalars[2] : 0;
+    const typename PV::T* sv = PV::s(I);
+    const typename PV::T* dp = PV::d(I, !parity);
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         uint32_t k;
         const TermType ty = off.typed(t, k);
@@ -1002,16 +989,16 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
             if (node >= I.N) continue;
             TermRows tr;
             const int ch = term_rows(I, off, lam, t, node, tr);
-            float p[6];
+            Acc p[6];
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
                 const size_t e = 6 * (size_t)node + i;
-                p[i] = fused ? s[e] + beta * dp[e] : s[e];
+                p[i] = fused ? (Acc)(sv[e] + beta * dp[e]) : (Acc)xin[e];
             }
             for (int c = 0; c < ch; ++c) {
                 Acc a = 0;
 #pragma unroll
-                for (int i = 0; i < 6; ++i) a += (Acc)tr.J[c][i] * (Acc)p[i];
+                for (int i = 0; i < 6; ++i) a += (Acc)tr.J[c][i] * p[i];
                 out[c] += (Acc)tr.w * a;
             }
         }
@@ -1039,9 +1026,10 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
     using T = typename std::conditional<MIXED, double, float>::type;
     TermOffsets off;
     off.load(I.counts);
-    const float* dprev = parity ? I.d0 : I.d1;
-    float* dcur = parity ? I.d1 : I.d0;
-    const float beta = pcg ? (float)I.scalars[2] : 0.f;
+    using PV = PcgVec<MIXED>;
+    const T* dprev = PV::d(I, !parity);
+    T* dcur = PV::d(I, parity);
+    const T beta = pcg ? (T)I.scalars[2] : (T)0;
     T part = 0;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
@@ -1067,16 +1055,14 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
 #pragma unroll
             for (int q = 0; q < 6; ++q) a = (q == (int)lane) ? acc[q] : a;
             const size_t el = 6 * (size_t)node + lane;
-            float dv;
-            if (pcg) dv = I.s[el] + beta * dprev[el];
-            else dv = xin[el];
-            const float qv = (float)(a + (T)1e-2f * (T)dv);
+            const T dv = pcg ? PV::s(I)[el] + beta * dprev[el] : (T)xin[el];
+            const T qv = a + (T)1e-2f * dv;
             if (pcg) {
                 dcur[el] = dv;
-                I.q[el] = qv;
-                part += (T)dv * (T)qv;
+                PV::q(I)[el] = qv;
+                part += dv * qv;
             } else {
-                yout[el] = qv;
+                yout[el] = (float)qv;
             }
         }
     }
@@ -1105,12 +1091,13 @@ __global__ void __launch_bounds__(192) bsr_apply_kernel(const InstDesc* insts, c
 
 // ----------------------------------------------------------- update -------
 // applyWarpFieldUpdateKernel (SolverIterationData.cu:9-57)
+template <bool MIXED>
 __global__ void __launch_bounds__(128) update_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
         float tw[6];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) tw[i] = I.x[6 * (size_t)node + i];
+        for (int i = 0; i < 6; ++i) tw[i] = (float)PcgVec<MIXED>::x(I)[6 * (size_t)node + i];
         M34 se3;
         const float3 w = mk3(tw[0], tw[1], tw[2]);
         if (fabsf(w.x) + fabsf(w.y) + fabsf(w.z) < 1e-4f) {
@@ -1355,7 +1342,8 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
 
 cudaError_t launch_update(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
     const uint32_t g = (lc.max_nodes + 127) / 128;
-    MVDR_LAUNCH(update_kernel, grid2(g, lc.B), 128, 0, st, d);
+    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(update_kernel<true>, grid2(g, lc.B), 128, 0, st, d);
+    else MVDR_LAUNCH(update_kernel<false>, grid2(g, lc.B), 128, 0, st, d);
     return cudaGetLastError();
 }
 

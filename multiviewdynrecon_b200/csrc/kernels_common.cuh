@@ -175,6 +175,30 @@ __device__ inline float weight_of(ushort4 knn, float4 w, uint32_t node) {
 
 __device__ inline void set_error(const InstDesc& I, uint32_t bit) { atomicOr(&I.counts->error_flags, bit); }
 
+// Jt r and the PCG vectors in the arithmetic of the linear solve: float for
+// FP32, double for mixed precision (where float rounding of the right-hand
+// side or the vectors alone moves the increment of a 15k-node system by
+// ~2e-4)
+template <bool MIXED> struct PcgVec;
+template <> struct PcgVec<true> {
+    using T = double;
+    __device__ static T* jtr(const InstDesc& I) { return I.jtr_d; }
+    __device__ static T* x(const InstDesc& I) { return I.x_d; }
+    __device__ static T* r(const InstDesc& I) { return I.r_d; }
+    __device__ static T* s(const InstDesc& I) { return I.s_d; }
+    __device__ static T* q(const InstDesc& I) { return I.q_d; }
+    __device__ static T* d(const InstDesc& I, int odd) { return odd ? I.d1_d : I.d0_d; }
+};
+template <> struct PcgVec<false> {
+    using T = float;
+    __device__ static T* jtr(const InstDesc& I) { return I.jtr; }
+    __device__ static T* x(const InstDesc& I) { return I.x; }
+    __device__ static T* r(const InstDesc& I) { return I.r; }
+    __device__ static T* s(const InstDesc& I) { return I.s; }
+    __device__ static T* q(const InstDesc& I) { return I.q; }
+    __device__ static T* d(const InstDesc& I, int odd) { return odd ? I.d1 : I.d0; }
+};
+
 // A(r, k) of entry e of the full block-row layout, read from the half storage
 __device__ inline float stored_block_element(const InstDesc& I, uint32_t e, uint32_t r, uint32_t k) {
     const uint32_t pos = I.bsr_pos[e];

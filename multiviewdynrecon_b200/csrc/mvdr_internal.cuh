@@ -271,7 +271,8 @@ struct InstDesc {
     float* diag;            // [36N] JtJ diagonal blocks incl. damping
     float* minv;            // [36N] preconditioner (inverse diagonal), float
     double* chol;           // [21N] Cholesky factors (mixed precision)
-    float* jtr;             // [6N]
+    float* jtr;                // [6N]
+    double* jtr_d;          // mixed precision: Jt r in double
     // JtJ in half storage: per block row i its diagonal block at
     // half_offset[i] + i, then the upper blocks of its half pairs h at h + i + 1
     // (element order blk_idx). A lower block (i, j), j < i, is the transpose
@@ -283,13 +284,20 @@ struct InstDesc {
     uint32_t* bsr_col;      // block column
     uint32_t* bsr_pos;      // half-storage block | kTransposedBlock when read transposed
     // pcg vectors [6N each]
+    // PCG vectors [6N] (d double-buffered by iteration parity): float for
+    // FP32, double for mixed precision (PcgVec selects)
     float* x;
     float* r;
     float* s;
     float* q;
     float* d0;
     float* d1;
-    double* dd;             // mixed precision: the PCG direction in double (the SpMV operand)
+    double* x_d;
+    double* r_d;
+    double* s_d;
+    double* q_d;
+    double* d0_d;
+    double* d1_d;
     float* jp;              // matrix-free scratch: J.p per scalar term
     double* scalars;        // PCG scalars: [0] delta, [1] alpha, [2] beta, [3] dq
     double* partials;       // per-CTA partial sums

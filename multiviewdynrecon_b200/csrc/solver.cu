@@ -183,19 +183,28 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.diag = a.take<float>(36 * N);
     I.minv = a.take<float>(36 * N);
     I.chol = a.take<double>(21 * N);
-    I.jtr = a.take<float>(6 * N);
+    I.jtr = a.take<float>(6 * N);  // also the float export in mixed precision
+    I.jtr_d = lc.precision == MVDR_PRECISION_MIXED ? a.take<double>(6 * N) : nullptr;
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     I.bsr = mixed ? nullptr : a.take<float>(36 * (N + (size_t)lc.cap_pairs));
     I.bsr_d = mixed ? a.take<double>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
     I.bsr_col = a.take<uint32_t>(N + 2 * (size_t)lc.cap_pairs);
     I.bsr_pos = a.take<uint32_t>(N + 2 * (size_t)lc.cap_pairs);
-    I.x = a.take<float>(6 * N);
-    I.r = a.take<float>(6 * N);
-    I.s = a.take<float>(6 * N);
-    I.q = a.take<float>(6 * N);
-    I.d0 = a.take<float>(6 * N);
-    I.d1 = a.take<float>(6 * N);
-    I.dd = mixed ? a.take<double>(6 * N) : nullptr;
+    if (mixed) {
+        I.x_d = a.take<double>(6 * N);
+        I.r_d = a.take<double>(6 * N);
+        I.s_d = a.take<double>(6 * N);
+        I.q_d = a.take<double>(6 * N);
+        I.d0_d = a.take<double>(6 * N);
+        I.d1_d = a.take<double>(6 * N);
+    } else {
+        I.x = a.take<float>(6 * N);
+        I.r = a.take<float>(6 * N);
+        I.s = a.take<float>(6 * N);
+        I.q = a.take<float>(6 * N);
+        I.d0 = a.take<float>(6 * N);
+        I.d1 = a.take<float>(6 * N);
+    }
     // J.p per scalar term of the matrix-free operator (double in mixed precision)
     I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
     I.scalars = a.take<double>(8);
@@ -646,6 +655,17 @@ static int check_flags(const DeviceCounts& c) {
     return MVDR_OK;
 }
 
+// a double vector exported as float (the export format of JTR / INCREMENT)
+static int copy_out_as_float(void* dst, const double* src, size_t count, size_t cap, size_t* written) {
+    if (written) *written = 4 * count;
+    if (4 * count > cap) return fail(MVDR_ECAPACITY, "destination buffer too small");
+    std::vector<double> h(count);
+    if (count) CU(cudaMemcpy(h.data(), src, 8 * count, cudaMemcpyDeviceToHost));
+    std::vector<float> f(h.begin(), h.end());
+    if (count) CU(cudaMemcpy(dst, f.data(), 4 * count, cudaMemcpyDefault));
+    return MVDR_OK;
+}
+
 static int copy_out(void* dst, const void* src, size_t bytes, size_t cap, size_t* written) {
     if (written) *written = bytes;
     if (bytes > cap) return fail(MVDR_ECAPACITY, "destination buffer too small");
@@ -680,8 +700,12 @@ static int get_array(Batch& b, uint32_t inst, int which, void* dst, size_t cap, 
         case MVDR_ARRAY_WARPED_CORRESPONDENCE:
             return copy_out(dst, I.warped, 32 * ((size_t)I.Tp + I.Tc), cap, written);
         case MVDR_ARRAY_DIAG_BLOCKS: return copy_out(dst, I.diag, 4 * 36 * N, cap, written);
-        case MVDR_ARRAY_JTR: return copy_out(dst, I.jtr, 4 * 6 * N, cap, written);
-        case MVDR_ARRAY_INCREMENT: return copy_out(dst, I.x, 4 * 6 * N, cap, written);
+        case MVDR_ARRAY_JTR:
+            return I.jtr_d ? copy_out_as_float(dst, I.jtr_d, 6 * N, cap, written)
+                           : copy_out(dst, I.jtr, 4 * 6 * N, cap, written);
+        case MVDR_ARRAY_INCREMENT:
+            return I.x_d ? copy_out_as_float(dst, I.x_d, 6 * N, cap, written)
+                         : copy_out(dst, I.x, 4 * 6 * N, cap, written);
         case MVDR_ARRAY_NODE_SE3: return copy_out(dst, I.se3, 32 * N, cap, written);
         case MVDR_ARRAY_PRECONDITIONER:
         case MVDR_ARRAY_OFFDIAG_BLOCKS:
