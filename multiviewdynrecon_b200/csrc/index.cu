@@ -512,84 +512,124 @@ __global__ void __launch_bounds__(256) np_row_count_kernel(const InstDesc* insts
     }
 }
 
-// CTA per node: gather (j, t) keys of the row, sort them, write the term
-// values of the row and the row's unique pairs (to a temporary per-row area).
-// Launched twice: once with a small shared-memory footprint for the rows of
-// at most `max_len` entries (nearly all), so that many CTAs share an SM, and
-// once, on a small grid, with the capacity-sized footprint for the rows above
-// `min_len`; each launch leaves the other's rows alone.
-constexpr uint32_t kRowSmall = 2048;
+// Warp per node: the row's (j, t) entries, j > node, in ascending (j, t) order
+// without sorting. The node's term list is already ascending in t, so for
+// each distinct partner j (ascending, found by a warp minimum) one sweep of
+// the list emits the terms that contain j, in t order, and finds the next
+// partner. The first kRowCache * 32 terms stay in registers (the term id and
+// its partners, packed 16-bit); longer lists re-read the rest each sweep. A
+// term that lists a partner twice contributes two adjacent entries, like the
+// duplicate keys of a sort. Writes np_index, the per-pair (key, start) of the
+// row and upper_count.
+constexpr int kRowCache = 8;
 
-__global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts, uint32_t min_len,
-                                                           uint32_t max_len) {
-    extern __shared__ unsigned long long s64[];
-    __shared__ uint32_t fill;
-    __shared__ uint32_t wtot[8];
+__device__ inline void unpack_partners(uint2 pk, uint32_t j[4]) {
+    j[0] = pk.x & 0xFFFFu; j[1] = pk.x >> 16; j[2] = pk.y & 0xFFFFu; j[3] = pk.y >> 16;
+}
+
+// the term's partners above `node` packed as four 16-bit ids (0xFFFF = none)
+__device__ inline uint2 packed_partners(const InstDesc& I, const TermOffsets& off, uint32_t node, uint32_t t) {
+    uint32_t js[4];
+    const uint32_t c = upper_entries_of(I, off, node, t, js);
+    uint32_t v[4] = {0xFFFFu, 0xFFFFu, 0xFFFFu, 0xFFFFu};
+    for (uint32_t q = 0; q < c; ++q) v[q] = js[q];
+    return make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
+}
+
+__global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->nodepair_entries > I.cap_k2) return;
     TermOffsets off;
     off.load(I.counts);
-    for (uint32_t node = blockIdx.x; node < I.N; node += gridDim.x) {
-        const uint32_t len = I.row_count[node];
-        const uint32_t out = I.row_offset[node];
-        if (len < min_len || len > max_len) continue;
-        if (len == 0) {
-            if (threadIdx.x == 0) I.upper_count[node] = 0;
-            continue;
+    const uint32_t lane = lane_id();
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        const uint32_t b0 = I.n2t_offset[node], b1 = I.n2t_offset[node + 1];
+        const uint32_t out = I.row_offset[node], len = I.row_count[node];
+        uint32_t ct[kRowCache];
+        uint2 cj[kRowCache];
+#pragma unroll
+        for (int m = 0; m < kRowCache; ++m) {
+            const uint32_t p = b0 + lane + 32u * m;
+            ct[m] = p < b1 ? I.n2t_index[p] : kInvalid;
+            cj[m] = p < b1 ? packed_partners(I, off, node, ct[m]) : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         }
-        if (len > I.cap_row) {
-            if (threadIdx.x == 0) { set_error(I, kErrRowTooLong); I.upper_count[node] = 0; }
-            continue;
-        }
-        if (threadIdx.x == 0) fill = 0;
-        __syncthreads();
-        const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
-        for (uint32_t p = b + threadIdx.x; p < e; p += blockDim.x) {
-            const uint32_t t = I.n2t_index[p];
+        // emit the slice's entries for partner j at out + pos; returns the
+        // smallest partner above j seen in the slice
+        auto slice = [&](uint32_t t, uint2 pk, uint32_t j, uint32_t& pos) -> uint32_t {
             uint32_t js[4];
-            const uint32_t c = upper_entries_of(I, off, node, t, js);
-            if (c) {
-                const uint32_t base = atomicAdd(&fill, c);
-                for (uint32_t q = 0; q < c; ++q) s64[base + q] = ((unsigned long long)js[q] << 32) | t;
+            unpack_partners(pk, js);
+            uint32_t mult = 0, nxt = 0xFFFFFFFFu;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                mult += js[q] == j ? 1u : 0u;
+                if (js[q] != 0xFFFFu && js[q] > j) nxt = min(nxt, js[q]);
             }
+            uint32_t pre, total;
+            if (__any_sync(0xffffffffu, mult > 1)) {
+                pre = mult;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, pre, o);
+                    if (lane >= (uint32_t)o) pre += v;
+                }
+                total = __shfl_sync(0xffffffffu, pre, 31);
+                pre -= mult;
+            } else {
+                const uint32_t bal = __ballot_sync(0xffffffffu, mult != 0);
+                pre = __popc(bal & lt_mask);
+                total = __popc(bal);
+            }
+            for (uint32_t c = 0; c < mult; ++c)
+                if (pos + pre + c < len) I.np_index[out + pos + pre + c] = t;
+            pos += total;
+            return nxt;
+        };
+        // first partner: the smallest id above node
+        uint32_t j;
+        {
+            uint32_t mn = 0xFFFFFFFFu;
+#pragma unroll
+            for (int m = 0; m < kRowCache; ++m) {
+                uint32_t js[4];
+                unpack_partners(cj[m], js);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (js[q] != 0xFFFFu) mn = min(mn, js[q]);
+            }
+            for (uint32_t p = b0 + 32u * kRowCache + lane; p < b1; p += 32) {
+                uint32_t js[4];
+                unpack_partners(packed_partners(I, off, node, I.n2t_index[p]), js);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (js[q] != 0xFFFFu) mn = min(mn, js[q]);
+            }
+            j = warp_min_u32(mn);
         }
-        __syncthreads();
-        const uint32_t n2 = next_pow2(len);
-        for (uint32_t i = len + threadIdx.x; i < n2; i += blockDim.x) s64[i] = ~0ull;
-        __syncthreads();
-        block_bitonic_sort(s64, n2);
-        // values, and unique-j run starts (block scan over the row)
-        uint32_t carry = 0;
-        for (uint32_t base = 0; base < len; base += blockDim.x) {
-            const uint32_t i = base + threadIdx.x;
-            bool start = false;
-            uint32_t j = 0;
-            if (i < len) {
-                const unsigned long long key = s64[i];
-                I.np_index[out + i] = (uint32_t)key;
-                j = (uint32_t)(key >> 32);
-                start = (i == 0) || ((uint32_t)(s64[i - 1] >> 32) != j);
+        uint32_t pos = 0, runs = 0;
+        while (j != 0xFFFFFFFFu) {
+            if (lane == 0 && pos < len) {
+                I.tmp_key[out + runs] = node * I.enc + j;
+                I.tmp_start[out + runs] = out + pos;
             }
-            const uint32_t bal = __ballot_sync(0xffffffffu, start);
-            const uint32_t lp = __popc(bal & ((1u << lane_id()) - 1u));
-            if (lane_id() == 0) wtot[threadIdx.x >> 5] = __popc(bal);
-            __syncthreads();
-            uint32_t wb = 0, slice = 0;
-            for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
-                if (w < (threadIdx.x >> 5)) wb += wtot[w];
-                slice += wtot[w];
+            uint32_t nxt = 0xFFFFFFFFu;
+#pragma unroll
+            for (int m = 0; m < kRowCache; ++m) {
+                if (b0 + 32u * m >= b1) break;  // warp-uniform
+                nxt = min(nxt, slice(ct[m], cj[m], j, pos));
             }
-            if (start) {
-                const uint32_t u = carry + wb + lp;
-                I.tmp_key[out + u] = node * I.enc + j;
-                I.tmp_start[out + u] = out + i;
+            for (uint32_t base = b0 + 32u * kRowCache; base < b1; base += 32) {
+                const uint32_t p = base + lane;
+                const uint32_t t = p < b1 ? I.n2t_index[p] : kInvalid;
+                const uint2 pk = p < b1 ? packed_partners(I, off, node, t) : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+                nxt = min(nxt, slice(t, pk, j, pos));
             }
-            carry += slice;
-            __syncthreads();
+            ++runs;
+            j = warp_min_u32(nxt);
         }
-        if (threadIdx.x == 0) I.upper_count[node] = carry;
-        __syncthreads();
+        if (lane == 0) I.upper_count[node] = runs;
     }
 }
 
@@ -753,10 +793,8 @@ __global__ void __launch_bounds__(256) bin_colptr_kernel(const InstDesc* insts) 
 
 static inline dim3 grid2(uint32_t x, uint32_t B) { return dim3(x ? x : 1, B); }
 
-cudaError_t set_index_smem_limits(size_t seg_bytes, size_t row_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(n2t_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_bytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(np_row_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_bytes);
+cudaError_t set_index_smem_limits(size_t seg_bytes) {
+    return cudaFuncSetAttribute(n2t_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_bytes);
 }
 
 cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
@@ -784,13 +822,7 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     // node pair -> term
     MVDR_LAUNCH(np_row_count_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanRows);
-    // without a second launch the first one also takes (and flags) the rows
-    // above the capacity
-    MVDR_LAUNCH(np_row_build_kernel, grid2(lc.max_nodes, B), 256, (size_t)min(lc.cap_row, kRowSmall) * 8, st, d, 0u,
-                lc.cap_row > kRowSmall ? kRowSmall : 0xFFFFFFFFu);
-    if (lc.cap_row > kRowSmall)
-        MVDR_LAUNCH(np_row_build_kernel, grid2(min(lc.max_nodes, (uint32_t)lc.sm_count), B), 256,
-                    (size_t)lc.cap_row * 8, st, d, kRowSmall + 1, 0xFFFFFFFFu);
+    MVDR_LAUNCH(np_row_build_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanUpper);
     MVDR_LAUNCH(np_half_compact_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanBlkRows);

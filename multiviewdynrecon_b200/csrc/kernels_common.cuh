@@ -26,6 +26,12 @@ __device__ inline uint32_t warp_max_u32(uint32_t v) {
     return v;
 }
 
+__device__ inline uint32_t warp_min_u32(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 // inclusive warp scan
 __device__ inline uint32_t warp_inclusive_scan(uint32_t v) {
     const uint32_t lane = lane_id();

@@ -304,14 +304,14 @@ struct InstDesc {
     double* energy;         // [max GN iterations + 1]
 
     // capacities
-    uint32_t cap_dense, cap_fg, cap_k1, cap_k2, cap_pairs, cap_seg, cap_row, cap_bb;
+    uint32_t cap_dense, cap_fg, cap_k1, cap_k2, cap_pairs, cap_seg, cap_bb;
     uint32_t chunks_per_view;
 };
 
 struct LaunchCfg {
     uint32_t B;            // instances
     uint32_t max_nodes, max_views, width, height;
-    uint32_t cap_dense, cap_fg, cap_terms, cap_k1, cap_k2, cap_pairs, cap_seg, cap_row, cap_bb;
+    uint32_t cap_dense, cap_fg, cap_terms, cap_k1, cap_k2, cap_pairs, cap_seg, cap_bb;
     uint32_t max_edges, max_tp, max_tc;
     uint32_t chunks_per_view;
     int precision, mode;
@@ -325,7 +325,7 @@ struct LaunchCfg {
 void count_launch();
 
 // raise the dynamic shared-memory limit of the segment-sort kernels
-cudaError_t set_index_smem_limits(size_t seg_bytes, size_t row_bytes);
+cudaError_t set_index_smem_limits(size_t seg_bytes);
 
 // SpMV tile shapes the autotuner chooses from: block rows per CTA and threads
 // per scalar row (each taking every `split`-th block of the row)

@@ -216,7 +216,6 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.cap_k2 = lc.cap_k2;
     I.cap_pairs = lc.cap_pairs;
     I.cap_seg = lc.cap_seg;
-    I.cap_row = lc.cap_row;
     I.cap_bb = lc.cap_bb;
     I.chunks_per_view = lc.chunks_per_view;
     return a.off;
@@ -269,19 +268,18 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     // a segment up to the next power of two
     auto pow2 = [](uint32_t v) { uint32_t p = 1; while (p < v) p <<= 1; return p; };
     lc.cap_seg = std::min<uint32_t>(pow2(cfg->max_terms_per_node ? cfg->max_terms_per_node : 4096), 16384);
-    lc.cap_row = std::min<uint32_t>(pow2(2 * lc.cap_seg), 16384);
     lc.cap_bb = 36 * (cfg->max_nodes + 2 * lc.cap_pairs);
     lc.chunks_per_view = (cfg->image_width * cfg->image_height + 2047) / 2048;
     lc.precision = cfg->precision;
     lc.mode = cfg->mode;
     lc.sm_count = prop.multiProcessorCount;
 
-    const size_t smem_seg = (size_t)lc.cap_seg * 4, smem_row = (size_t)lc.cap_row * 8;
-    if (smem_seg > (size_t)prop.sharedMemPerBlockOptin || smem_row > (size_t)prop.sharedMemPerBlockOptin) {
+    const size_t smem_seg = (size_t)lc.cap_seg * 4;
+    if (smem_seg > (size_t)prop.sharedMemPerBlockOptin) {
         delete b;
         return fail(MVDR_EINVAL, "max_terms_per_node too large for shared memory");
     }
-    if (set_index_smem_limits(smem_seg, smem_row) != cudaSuccess) {
+    if (set_index_smem_limits(smem_seg) != cudaSuccess) {
         delete b;
         return fail(MVDR_ECUDA, "cudaFuncSetAttribute failed");
     }
