@@ -11,9 +11,10 @@
 // SolverIterationData.cu:9-57, ResidualEvaluator.cu:71-142.
 //
 // Accumulation: every per-node and per-pair sum is a warp-shuffle reduction
-// of lane partials; global reductions (dot products, energy) use per-CTA
-// partials summed in fixed order by the last CTA. No floating-point atomics,
-// so every result is reproducible run to run.
+// of lane partials; global reductions use per-CTA partials summed in a fixed
+// order, by the kernel that consumes them (PCG dots) or by the last CTA
+// (energy). No floating-point atomics, so every result is reproducible run to
+// run.
 #include <type_traits>
 
 #include "kernels_common.cuh"
@@ -743,9 +744,53 @@ __device__ inline bool block_partial_and_last(const InstDesc& I, T v, int ticket
     return true;
 }
 
+// Split reduction for the PCG dots. Every CTA of the producing launch stores
+// its block sum in a region of the partials; a kernel launched after it on
+// the same stream sums the stored partials with one warp in a fixed order.
+// Each consuming CTA computes the same value, and no producing CTA waits for
+// the others (no ticket, fence or atomic on the SpMV's critical path).
+// Regions: kRegDelta + parity holds delta = r.s of the iteration with that
+// parity (pcg_init writes iteration 0's, pcg_update the next one's), kRegDq
+// holds d.q of the current iteration.
+constexpr uint32_t kRegDelta = 1, kRegDq = 3;
+
+template <class T> __device__ inline void store_block_partial(const InstDesc& I, uint32_t region, T v) {
+    __shared__ T ws[32];
+    v = warp_sum(v);
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T s = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += ws[w];
+        I.partials[(size_t)region * I.part_stride + blockIdx.x] = (double)s;
+    }
+}
+
+// the sum of the `count` partials of `region`, in every thread
+template <class T> __device__ inline T sum_block_partials(const InstDesc& I, uint32_t region, uint32_t count) {
+    __shared__ T total;
+    __syncthreads();  // every thread has read the previous call's total
+    if (threadIdx.x < 32) {
+        const double* p = I.partials + (size_t)region * I.part_stride;
+        T s = 0;
+        for (uint32_t c = lane_id(); c < count; c += 32) s += (T)__ldcg(p + c);
+        s = warp_sum(s);
+        if (threadIdx.x == 0) total = s;
+    }
+    __syncthreads();
+    return total;
+}
+
+// beta = delta_k / delta_(k-1) of iteration k (0 for the first), from the
+// `nd` partials of the init / update launches
+template <class T>
+__device__ inline T pcg_beta(const InstDesc& I, int parity, int first, uint32_t nd) {
+    const T dk = sum_block_partials<T>(I, kRegDelta + parity, nd);
+    const T dkm1 = sum_block_partials<T>(I, kRegDelta + (parity ^ 1), nd);
+    return first ? (T)0 : dk / dkm1;
+}
+
 // ---------------------------------------------------------------- PCG -----
-// Scalars per instance (double storage): [0] delta = r.s, [1] alpha,
-// [2] beta, [3] d.q. In FP32 mode they are computed in float.
 
 // blockPCGZeroInitKernel (BlockPCG.cuh:65-111): r = b, s = M^-1 b, x = 0,
 // delta = r.s; the first direction is d = s (beta = 0)
@@ -780,11 +825,7 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
             part += bv[i] * sv[i];
         }
     }
-    T tot;
-    if (block_partial_and_last<T>(I, part, 0, &tot) && threadIdx.x == 0) {
-        I.scalars[0] = (double)tot;
-        I.scalars[2] = 0.0;
-    }
+    store_block_partial<T>(I, kRegDelta, part);
 }
 
 // One scalar row r of y = A x for block row br, walking the full block-row
@@ -810,14 +851,15 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
 // d = s + beta d_prev (BlockPCG.cuh:167-181), formed once per iteration for
 // the whole vector, so that the SpMV reads its operand directly
 template <bool MIXED>
-__global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* insts, int parity) {
+__global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* insts, int parity, int first,
+                                                            uint32_t nd) {
     const InstDesc& I = insts[blockIdx.y];
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
     const T* dprev = PV::d(I, !parity);
     T* dcur = PV::d(I, parity);
     const T* sv = PV::s(I);
-    const T beta = (T)I.scalars[2];
+    const T beta = pcg_beta<T>(I, parity, first, nd);
     const uint32_t n = 6 * I.N;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
         dcur[e] = sv[e] + beta * dprev[e];
@@ -906,23 +948,22 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
             part += (T)xvec[e] * (T)acc;
         }
     }
-    T tot;
-    if (block_partial_and_last<T>(I, part, 1, &tot) && threadIdx.x == 0) {
-        I.scalars[3] = (double)tot;
-        if (MIXED) I.scalars[1] = I.scalars[0] / (double)tot;
-        else I.scalars[1] = (double)((float)I.scalars[0] / (float)tot);
-    }
+    store_block_partial<T>(I, kRegDq, part);
 }
 
-// blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): x += alpha d, r -= alpha q,
-// s = M^-1 r, delta_new = r.s, beta = delta_new / delta
+// blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): alpha = delta / d.q,
+// x += alpha d, r -= alpha q, s = M^-1 r, delta_new = r.s (beta follows in
+// the next direction). `nd` and `nq`: CTAs of the launches that stored the
+// delta and d.q partials.
 template <bool MIXED>
-__global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity) {
+__global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity, uint32_t nd,
+                                                         uint32_t nq) {
     const InstDesc& I = insts[blockIdx.y];
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
     const T* d = PV::d(I, parity);
-    const T alpha = (T)I.scalars[1];
+    const T delta = sum_block_partials<T>(I, kRegDelta + parity, nd);
+    const T alpha = delta / sum_block_partials<T>(I, kRegDq, nq);
     T part = 0;
     for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
         T rv[6], sv[6];
@@ -950,15 +991,7 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
             part += rv[i] * sv[i];
         }
     }
-    T tot;
-    if (block_partial_and_last<T>(I, part, 2, &tot) && threadIdx.x == 0) {
-        if (MIXED) {
-            I.scalars[2] = (double)tot / I.scalars[0];
-        } else {
-            I.scalars[2] = (double)((float)tot / (float)I.scalars[0]);
-        }
-        I.scalars[0] = (double)tot;
-    }
+    store_block_partial<T>(I, kRegDelta + (parity ^ 1), part);
 }
 
 // ------------------------------------------------------ matrix-free JtJ ---
@@ -966,7 +999,7 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
 // with p = s + beta * d_prev formed on the fly when `fused` is set
 template <bool MIXED>
 __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
-                                                      mvdr_penalty lam) {
+                                                      int first, uint32_t nd, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
     if (bad_inputs(I)) return;
@@ -974,7 +1007,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
     off.load(I.counts);
     const uint32_t T = off.o[4];
     using PV = PcgVec<MIXED>;
-    const typename PV::T beta = fused ? (typename PV::T)I.scalars[2] : 0;
+    const typename PV::T beta = fused ? pcg_beta<typename PV::T>(I, parity, first, nd) : 0;
     const typename PV::T* sv = PV::s(I);
     const typename PV::T* dp = PV::d(I, !parity);
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
@@ -1021,7 +1054,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
 // q and the d.q partial, like pcg_spmv_kernel.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
-                                                       int parity, mvdr_penalty lam) {
+                                                       int parity, int first, uint32_t nd, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
     using T = typename std::conditional<MIXED, double, float>::type;
     TermOffsets off;
@@ -1029,7 +1062,7 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
     using PV = PcgVec<MIXED>;
     const T* dprev = PV::d(I, !parity);
     T* dcur = PV::d(I, parity);
-    const T beta = pcg ? (T)I.scalars[2] : (T)0;
+    const T beta = pcg ? pcg_beta<T>(I, parity, first, nd) : (T)0;
     T part = 0;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
@@ -1066,14 +1099,7 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
             }
         }
     }
-    if (pcg) {
-        T tot;
-        if (block_partial_and_last<T>(I, part, 1, &tot) && threadIdx.x == 0) {
-            I.scalars[3] = (double)tot;
-            if (MIXED) I.scalars[1] = I.scalars[0] / (double)tot;
-            else I.scalars[1] = (double)((float)I.scalars[0] / (float)tot);
-        }
-    }
+    if (pcg) store_block_partial<T>(I, kRegDq, part);
 }
 
 // y = A x with the materialised operator (no PCG side effects)
@@ -1254,6 +1280,12 @@ cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& 
     return cudaGetLastError();
 }
 
+// CTAs per instance of the SpMV launch with the current shape
+static uint32_t spmv_grid(const LaunchCfg& lc) {
+    const uint32_t R = kSpmvShapes[lc.spmv_shape].rows;
+    return (lc.max_nodes + R - 1) / R;
+}
+
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
@@ -1263,21 +1295,24 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d);
     else MVDR_LAUNCH(pcg_init_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d);
     for (uint32_t it = 0; it < iters; ++it) {
-        const int parity = (int)(it & 1u);
+        const int parity = (int)(it & 1u), first = it == 0;
+        uint32_t nq;  // CTAs that store the d.q partials
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
             // J.(s + beta d_prev) per term, then Jt per node (+ damping, d, q, d.q)
-            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
-            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
-            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
-            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
+            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, first, gnode, lam);
+            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, first, gnode, lam);
+            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, first, gnode, lam);
+            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, first, gnode, lam);
+            nq = gwarp;
         } else {
-            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity);
-            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity);
+            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
             const cudaError_t e = launch_spmv(lc, d, parity, st);
             if (e != cudaSuccess) return e;
+            nq = spmv_grid(lc);
         }
-        if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity);
-        else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity);
+        if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity, gnode, nq);
+        else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity, gnode, nq);
     }
     return cudaGetLastError();
 }
@@ -1327,12 +1362,12 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
         case MVDR_STAGE_SPMV:
             return launch_spmv(lc, d, 0, st);
         case MVDR_STAGE_DIRECTION:
-            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0);
-            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0);
+            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
+            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
             break;
         case MVDR_STAGE_PCG_UPDATE:
-            if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0);
-            else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, 0);
+            if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0, gnode, spmv_grid(lc));
+            else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, 0, gnode, spmv_grid(lc));
             break;
         case MVDR_STAGE_UPDATE: return launch_update(lc, d, st);
         default: return cudaErrorInvalidValue;
@@ -1353,11 +1388,11 @@ cudaError_t launch_apply_jtj(const LaunchCfg& lc, InstDesc* d, const mvdr_penalt
     if (lc.mode == MVDR_MODE_MATRIX_FREE) {
         const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
         if (lc.precision == MVDR_PRECISION_MIXED) {
-            MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
-            MVDR_LAUNCH(apply_jt_kernel<true>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
+            MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, 1, 0u, lam);
+            MVDR_LAUNCH(apply_jt_kernel<true>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, 1, 0u, lam);
         } else {
-            MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
-            MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
+            MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, 1, 0u, lam);
+            MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, 1, 0u, lam);
         }
     } else {
         if (lc.precision == MVDR_PRECISION_MIXED)

@@ -299,8 +299,8 @@ struct InstDesc {
     double* d0_d;
     double* d1_d;
     float* jp;              // matrix-free scratch: J.p per scalar term
-    double* scalars;        // PCG scalars: [0] delta, [1] alpha, [2] beta, [3] dq
-    double* partials;       // per-CTA partial sums
+    double* partials;       // per-CTA partial sums: 4 regions of part_stride
+    uint32_t part_stride;   // >= the CTAs per instance of any launch
     double* energy;         // [max GN iterations + 1]
 
     // capacities

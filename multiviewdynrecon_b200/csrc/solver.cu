@@ -207,8 +207,9 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     }
     // J.p per scalar term of the matrix-free operator (double in mixed precision)
     I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
-    I.scalars = a.take<double>(8);
-    I.partials = a.take<double>(partial_slots);
+    // region 0: last-CTA reductions; 1, 2: PCG delta by iteration parity; 3: d.q
+    I.partials = a.take<double>(4 * (size_t)partial_slots);
+    I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
     I.cap_dense = lc.cap_dense;
     I.cap_fg = lc.cap_fg;
