@@ -176,6 +176,18 @@ def measured_traffic(args):
     return None, None
 
 
+def spmv_tile_desc(shape):
+    """The SpMV tile shape (rows, split, form) in words."""
+    rows, split, form = shape
+    return {"rows_per_cta": rows, "threads_per_row": 6 * split,
+            "lower_blocks": "row reads, shared-memory exchange" if form == 0 else "column reads"}
+
+
+def spmv_tile_label(shape):
+    rows, split, form = shape
+    return f"{'row' if form == 0 else 'col'}{rows}x{6 * split}"
+
+
 def algorithmic_bytes(counts, N, mixed=True):
     """Compulsory HBM bytes per stage and instance (each array read or written
     once). JtJ is kept as half storage: N diagonal + P upper 6x6 blocks, in
@@ -378,9 +390,9 @@ def run_ours(args, rank, world, dist):
         single.close()
 
     return dict(value=value, ms=ms, kernels_per_step=kernels_per_step, clocks=clocks.summary(), stages=stages,
-                spmv_tile={"rows_per_cta": spmv_shape[0], "threads_per_row": 6 * spmv_shape[1],
-                           "candidates_ms": {f"{r}x{6 * sp}": round(t, 5)
-                                             for (r, sp), t in zip(abi.SPMV_SHAPES, spmv_shape_ms)}},
+                spmv_tile=dict(spmv_tile_desc(spmv_shape),
+                               candidates_ms={spmv_tile_label(sh): round(t, 5)
+                                              for sh, t in zip(abi.SPMV_SHAPES, spmv_shape_ms)}),
                 roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base)
 
 
@@ -490,7 +502,7 @@ def run_extra_workload(args):
                 peak, _ = load_peaks()
                 entry["spmv"] = {"ms": round(sp, 5), "GBps": round(nbytes / 1e9 / (sp / 1e3), 1),
                                  "frac_of_measured_hbm": round(nbytes / 1e9 / (sp / 1e3) / peak, 4),
-                                 "tile": {"rows_per_cta": shape[0], "threads_per_row": 6 * shape[1]}}
+                                 "tile": spmv_tile_desc(shape)}
                 entry["dense_terms"] = [c.dense_terms for c in counts]
                 # first increments for the FP64 comparison
                 bind()

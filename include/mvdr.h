@@ -359,17 +359,25 @@ MVDR_API int mvdr_batch_set_inputs_host(mvdr_batch* batch, uint32_t instance, co
  * Gauss-Newton iterations are captured once as a CUDA graph and replayed. */
 MVDR_API int mvdr_batch_solve(mvdr_batch* batch, uint32_t gn_iterations, uint32_t pcg_iterations,
                      int use_graph, void* stream);
-/* Choose the PCG SpMV tile shape (block rows per CTA and threads per scalar
- * row) for this batch's matrices. It builds the index and runs one
+/* Choose the PCG SpMV tile shape (block rows per CTA, threads per scalar row
+ * / 6, and the form: 0 reads a lower block's rows and exchanges the column
+ * sums through shared memory, 1 reads its columns) for this batch's
+ * matrices. It builds the index and runs one
  * Gauss-Newton iteration on the bound inputs, which moves the warp fields
  * (bind the inputs again before solving), then times every candidate shape
  * on the assembled operator, keeps the fastest for later solves and drops the
- * captured graphs. Writes the chosen shape to *rows / *split and, when
+ * captured graphs. Writes the chosen shape to *rows / *split / *form (each
+ * may be NULL) and, when
  * times_ms is not NULL, the mean time of each candidate (up to `capacity`
  * entries, in candidate order). Synchronises `stream`. A matrix-free batch
  * keeps its shape. */
 MVDR_API int mvdr_batch_autotune(mvdr_batch* batch, void* stream, double* times_ms, uint32_t capacity,
-                                 uint32_t* rows, uint32_t* split);
+                                 uint32_t* rows, uint32_t* split, uint32_t* form);
+/* Use SpMV tile shape `shape` (0 .. MVDR_NUM_SPMV_SHAPES - 1, the
+ * autotuner's candidate order) for later solves of this batch, in place of
+ * the autotuner's choice; drops the captured graphs. */
+#define MVDR_NUM_SPMV_SHAPES 12u
+MVDR_API int mvdr_batch_set_spmv_shape(mvdr_batch* batch, uint32_t shape);
 MVDR_API int mvdr_batch_get_node_se3(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst, void* stream);
 MVDR_API int mvdr_batch_copy_node_se3_async(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst,
                                             void* stream);

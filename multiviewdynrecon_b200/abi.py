@@ -23,7 +23,11 @@ COMPAT_REF_VIEW_LOOKUP = 1
  STAGE_DIRECTION) = range(8)
 # candidate SpMV tile shapes (block rows per CTA, threads per scalar row), in
 # the order mvdr_batch_autotune reports their times
-SPMV_SHAPES = [(16, 2), (8, 2), (16, 1), (32, 1), (16, 3), (8, 4), (32, 2)]
+# SpMV tile shapes (block rows per CTA, threads per scalar row / 6, form) in
+# the autotuner's order. Form 0 reads a lower block's row and exchanges the
+# column sums through shared memory; form 1 reads its column.
+SPMV_SHAPES = [(16, 2, 0), (8, 2, 0), (16, 1, 0), (32, 1, 0), (16, 3, 0), (8, 4, 0), (32, 2, 0),
+               (16, 1, 1), (32, 1, 1), (8, 2, 1), (16, 2, 1), (4, 4, 1)]
 NUM_SPMV_SHAPES = len(SPMV_SHAPES)
 
 (ARRAY_DENSE_PIXELS, ARRAY_DENSE_KNN, ARRAY_DENSE_KNN_WEIGHT, ARRAY_FOREGROUND_PIXELS, ARRAY_NODE2TERM_OFFSET,

@@ -732,8 +732,7 @@ __global__ void __launch_bounds__(128) np_lower_sort_kernel(const InstDesc* inst
                 pos = I.sym_half[b + i - 1] + min(node, col) + 1;
                 if (col < node) pos |= kTransposedBlock;
             }
-            I.bsr_col[b + node + i] = col;
-            I.bsr_pos[b + node + i] = pos;
+            I.bsr_ent[b + node + i] = make_uint2(pos, col);
         }
         __syncwarp();
     }

@@ -837,10 +837,11 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
     const uint32_t e0 = I.blkrow_offset[br] + br, e1 = I.blkrow_offset[br + 1] + br + 1;
     V acc = 0;
     for (uint32_t e = e0; e < e1; ++e) {
-        const uint32_t pos = I.bsr_pos[e];
+        const uint2 ent = I.bsr_ent[e];
+        const uint32_t pos = ent.x;
         const V* blk = store + 36 * (size_t)(pos & ~kTransposedBlock);
         const bool tr = (pos & kTransposedBlock) != 0;
-        const float* xc = x + 6 * (size_t)I.bsr_col[e];
+        const float* xc = x + 6 * (size_t)ent.y;
 #pragma unroll
         for (int k = 0; k < 6; ++k) acc += blk[tr ? blk_idx(k, r) : blk_idx(r, k)] * (V)xc[k];
     }
@@ -874,10 +875,11 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
 // block, stored as its transpose, it is column r of the needed block and adds
 // x_r times it to all six rows, which the row's threads sum through shared
 // memory at the end. Block and direction addresses depend only on the
-// sequential bsr_pos / bsr_col entries, so many loads stay in flight. The
+// sequential (position, column) entries, so many loads stay in flight. The
 // stored transpose of a lower block belongs to a row of this or an earlier
 // tile, so it is usually still in L2.
-const SpmvShape kSpmvShapes[kNumSpmvShapes] = {{16, 2}, {8, 2}, {16, 1}, {32, 1}, {16, 3}, {8, 4}, {32, 2}};
+const SpmvShape kSpmvShapes[kNumSpmvShapes] = {{16, 2, 0}, {8, 2, 0},  {16, 1, 0}, {32, 1, 0}, {16, 3, 0}, {8, 4, 0},
+                                                {32, 2, 0}, {16, 1, 1}, {32, 1, 1}, {8, 2, 1},  {16, 2, 1}, {4, 4, 1}};
 
 template <class V> struct Pair;
 template <> struct Pair<double> { using type = double2; };
@@ -901,7 +903,7 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
     const uint32_t t = threadIdx.x;
     T part = 0;
     const uint32_t r0 = blockIdx.x * kTileRows;
-    if (r0 < I.N) {
+    if (r0 < I.N && index_complete(I)) {
         const uint32_t r1 = min(r0 + kTileRows, I.N);
         const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
         const bool computes = row < r1;
@@ -911,8 +913,8 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
             const uint32_t rb = I.blkrow_offset[row] + row, re = I.blkrow_offset[row + 1] + row + 1;
 #pragma unroll 2
             for (uint32_t b = rb + half; b < re; b += kTileSplit) {
-                const uint32_t pos = I.bsr_pos[b];
-                const uint32_t col = I.bsr_col[b];
+                const uint2 ent = I.bsr_ent[b];
+                const uint32_t pos = ent.x, col = ent.y;
                 const V2* blk = reinterpret_cast<const V2*>(store + 36 * (size_t)(pos & ~kTransposedBlock));
                 const V2 a01 = blk[rr], a23 = blk[6 + rr], a45 = blk[12 + rr];
                 const V av[6] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y};
@@ -943,6 +945,69 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
 #pragma unroll
                 for (int c = 0; c < 6; ++c) acc += s_cols[lr][6 * h + c][rr];
             }
+            const size_t e = 6 * (size_t)row + rr;
+            PcgVec<MIXED>::q(I)[e] = acc;
+            part += (T)xvec[e] * (T)acc;
+        }
+    }
+    store_block_partial<T>(I, kRegDq, part);
+}
+
+// Column form: thread r of a row reads, for a lower entry, column r of the
+// stored block (six scalar loads from the three 96-byte pair columns), so
+// every entry adds to the thread's own q_r and no shared-memory exchange is
+// needed; SPLIT > 1 sums the split threads' q_r in shared memory.
+template <bool MIXED, uint32_t kTileRows, uint32_t kTileSplit>
+__global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_col_kernel(const InstDesc* insts, int parity) {
+    using V = typename BlockStore<MIXED>::V;
+    using V2 = typename Pair<V>::type;
+    using T = typename std::conditional<MIXED, double, float>::type;
+    static_assert((6 * kTileSplit * kTileRows) % 32 == 0, "whole warps");
+    __shared__ V s_part[kTileSplit > 1 ? kTileRows * 6 * kTileSplit : 1];
+    const InstDesc& I = insts[blockIdx.y];
+    const V* store = BlockStore<MIXED>::ptr(I);
+    const V* xvec = direction<MIXED>(I, parity);
+    const uint32_t t = threadIdx.x;
+    T part = 0;
+    const uint32_t r0 = blockIdx.x * kTileRows;
+    if (r0 < I.N && index_complete(I)) {
+        const uint32_t r1 = min(r0 + kTileRows, I.N);
+        const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
+        const bool computes = row < r1;
+        V acc = 0;
+        if (computes) {
+            const uint32_t rb = I.blkrow_offset[row] + row, re = I.blkrow_offset[row + 1] + row + 1;
+            const uint32_t cfirst = blk_idx(0, rr);  // column rr: cfirst + 2k, k = 0..5
+#pragma unroll 2
+            for (uint32_t b = rb + half; b < re; b += kTileSplit) {
+                const uint2 ent = I.bsr_ent[b];
+                const V* blk = store + 36 * (size_t)(ent.x & ~kTransposedBlock);
+                const V2* x2 = reinterpret_cast<const V2*>(xvec + 6 * (size_t)ent.y);
+                const V2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
+                const V xv[6] = {x01.x, x01.y, x23.x, x23.y, x45.x, x45.y};
+                V av[6];
+                if (ent.x & kTransposedBlock) {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) av[k] = blk[cfirst + 2 * k];
+                } else {
+                    const V2* b2 = reinterpret_cast<const V2*>(blk);
+                    const V2 a01 = b2[rr], a23 = b2[6 + rr], a45 = b2[12 + rr];
+                    av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y; av[4] = a45.x; av[5] = a45.y;
+                }
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
+            }
+        }
+        if constexpr (kTileSplit > 1) {
+            if (computes) s_part[(lr * kTileSplit + half) * 6 + rr] = acc;
+            __syncthreads();
+            if (computes && half == 0) {
+                acc = 0;
+#pragma unroll
+                for (uint32_t h = 0; h < kTileSplit; ++h) acc += s_part[(lr * kTileSplit + h) * 6 + rr];
+            }
+        }
+        if (computes && half == 0) {
             const size_t e = 6 * (size_t)row + rr;
             PcgVec<MIXED>::q(I)[e] = acc;
             part += (T)xvec[e] * (T)acc;
@@ -1111,7 +1176,7 @@ __global__ void __launch_bounds__(192) bsr_apply_kernel(const InstDesc* insts, c
         const uint32_t br = base + threadIdx.x / 6;
         const uint32_t r = threadIdx.x % 6;
         if (threadIdx.x >= rows_per_cta * 6 || br >= I.N) continue;
-        yout[6 * (size_t)br + r] = bsr_row<MIXED>(I, br, r, xin);
+        yout[6 * (size_t)br + r] = index_complete(I) ? bsr_row<MIXED>(I, br, r, xin) : 0.f;
     }
 }
 
@@ -1323,6 +1388,12 @@ static void spmv_shape_launch(const LaunchCfg& lc, InstDesc* d, int parity, cuda
     MVDR_LAUNCH(kernel, grid2((lc.max_nodes + R - 1) / R, lc.B), 6 * S * R, 0, st, d, parity);
 }
 
+template <bool MIXED, uint32_t R, uint32_t S>
+static void spmv_col_launch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
+    auto* kernel = &pcg_spmv_col_kernel<MIXED, R, S>;
+    MVDR_LAUNCH(kernel, grid2((lc.max_nodes + R - 1) / R, lc.B), 6 * S * R, 0, st, d, parity);
+}
+
 template <bool MIXED>
 static void spmv_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
     switch (lc.spmv_shape) {
@@ -1332,6 +1403,11 @@ static void spmv_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStre
         case 4: spmv_shape_launch<MIXED, 16, 3>(lc, d, parity, st); break;
         case 5: spmv_shape_launch<MIXED, 8, 4>(lc, d, parity, st); break;
         case 6: spmv_shape_launch<MIXED, 32, 2>(lc, d, parity, st); break;
+        case 7: spmv_col_launch<MIXED, 16, 1>(lc, d, parity, st); break;
+        case 8: spmv_col_launch<MIXED, 32, 1>(lc, d, parity, st); break;
+        case 9: spmv_col_launch<MIXED, 8, 2>(lc, d, parity, st); break;
+        case 10: spmv_col_launch<MIXED, 16, 2>(lc, d, parity, st); break;
+        case 11: spmv_col_launch<MIXED, 4, 4>(lc, d, parity, st); break;
         default: spmv_shape_launch<MIXED, 16, 2>(lc, d, parity, st); break;
     }
 }

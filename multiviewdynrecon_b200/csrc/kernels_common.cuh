@@ -207,10 +207,22 @@ template <> struct PcgVec<false> {
 
 // A(r, k) of entry e of the full block-row layout, read from the half storage
 __device__ inline float stored_block_element(const InstDesc& I, uint32_t e, uint32_t r, uint32_t k) {
-    const uint32_t pos = I.bsr_pos[e];
+    const uint32_t pos = I.bsr_ent[e].x;
     const size_t blk = 36 * (size_t)(pos & ~kTransposedBlock);
     const uint32_t idx = (pos & kTransposedBlock) ? blk_idx(k, r) : blk_idx(r, k);
     return I.bsr_d ? (float)I.bsr_d[blk + idx] : I.bsr[blk + idx];
+}
+
+// true when this instance's index is complete: every count within its
+// capacity and no segment or row skipped. Kernels that walk the block-row
+// structure skip an instance whose index is not (its host call then reports
+// the capacity error).
+__device__ inline bool index_complete(const InstDesc& I) {
+    const DeviceCounts* C = I.counts;
+    constexpr uint32_t kIndexErrors = kErrNode2TermCapacity | kErrNodePairEntryCapacity | kErrHalfPairCapacity |
+                                      kErrSegmentTooLong | kErrRowTooLong;
+    return C->node2term_entries <= I.cap_k1 && C->nodepair_entries <= I.cap_k2 && C->half_pairs <= I.cap_pairs &&
+           (*(volatile const uint32_t*)&C->error_flags & kIndexErrors) == 0;
 }
 
 // true when the input check found an out-of-range node or surfel id

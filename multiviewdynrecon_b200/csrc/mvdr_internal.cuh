@@ -281,8 +281,8 @@ struct InstDesc {
     double* bsr_d;          // mixed precision: the same blocks in double
     // per entry of the full (symmetric) block-row layout, row i: the diagonal,
     // then its symmetric keys in order [N + 2P cap]
-    uint32_t* bsr_col;      // block column
-    uint32_t* bsr_pos;      // half-storage block | kTransposedBlock when read transposed
+    // (half-storage block | kTransposedBlock when read transposed, block column)
+    uint2* bsr_ent;
     // pcg vectors [6N each]
     // PCG vectors [6N] (d double-buffered by iteration parity): float for
     // FP32, double for mixed precision (PcgVec selects)
@@ -330,9 +330,9 @@ cudaError_t set_index_smem_limits(size_t seg_bytes);
 // SpMV tile shapes the autotuner chooses from: block rows per CTA and threads
 // per scalar row (each taking every `split`-th block of the row)
 struct SpmvShape {
-    uint32_t rows, split;
+    uint32_t rows, split, form;
 };
-constexpr int kNumSpmvShapes = 7;
+constexpr int kNumSpmvShapes = 12;
 extern const SpmvShape kSpmvShapes[kNumSpmvShapes];
 // one PCG SpMV (q = A d, d.q) with the shape lc.spmv_shape
 cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st);

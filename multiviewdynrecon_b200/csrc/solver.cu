@@ -188,8 +188,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     I.bsr = mixed ? nullptr : a.take<float>(36 * (N + (size_t)lc.cap_pairs));
     I.bsr_d = mixed ? a.take<double>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
-    I.bsr_col = a.take<uint32_t>(N + 2 * (size_t)lc.cap_pairs);
-    I.bsr_pos = a.take<uint32_t>(N + 2 * (size_t)lc.cap_pairs);
+    I.bsr_ent = a.take<uint2>(N + 2 * (size_t)lc.cap_pairs);
     if (mixed) {
         I.x_d = a.take<double>(6 * N);
         I.r_d = a.take<double>(6 * N);
@@ -916,7 +915,7 @@ int mvdr_batch_copy_node_se3_async(mvdr_batch* b, uint32_t i, mvdr_dual_quaterni
 }
 
 int mvdr_batch_autotune(mvdr_batch* bh, void* stream, double* times_ms, uint32_t capacity, uint32_t* rows,
-                        uint32_t* split) {
+                        uint32_t* split, uint32_t* form) {
     if (!bh) return fail(MVDR_EINVAL, "batch is null");
     Batch& b = *bh->batch;
     const cudaStream_t st = (cudaStream_t)stream;
@@ -960,6 +959,18 @@ int mvdr_batch_autotune(mvdr_batch* bh, void* stream, double* times_ms, uint32_t
     }
     if (rows) *rows = kSpmvShapes[b.lc.spmv_shape].rows;
     if (split) *split = kSpmvShapes[b.lc.spmv_shape].split;
+    if (form) *form = kSpmvShapes[b.lc.spmv_shape].form;
+    return MVDR_OK;
+}
+
+static_assert(kNumSpmvShapes == (int)MVDR_NUM_SPMV_SHAPES, "public shape count");
+
+int mvdr_batch_set_spmv_shape(mvdr_batch* bh, uint32_t shape) {
+    if (!bh || shape >= (uint32_t)kNumSpmvShapes) return fail(MVDR_EINVAL, "bad batch or SpMV shape");
+    Batch& b = *bh->batch;
+    b.lc.spmv_shape = (int)shape;
+    for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
+    b.graphs.clear();
     return MVDR_OK;
 }
 

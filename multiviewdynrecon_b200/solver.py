@@ -228,11 +228,17 @@ class BatchSolver:
     def autotune(self, stream=None):
         """Pick the SpMV tile shape for this batch (see mvdr_batch_autotune);
         the inputs must be bound again before the next solve. Returns
-        ((rows, threads_per_row), per-candidate ms)."""
-        times = (C.c_double * 16)()
-        rows, split = C.c_uint32(), C.c_uint32()
-        check(lib().mvdr_batch_autotune(self.h, _stream_handle(stream), times, 16, C.byref(rows), C.byref(split)))
-        return (rows.value, split.value), [t for t in times[:abi.NUM_SPMV_SHAPES]]
+        ((rows, split, form), per-candidate ms), the shape as in
+        abi.SPMV_SHAPES."""
+        times = (C.c_double * 32)()
+        rows, split, form = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().mvdr_batch_autotune(self.h, _stream_handle(stream), times, 32, C.byref(rows), C.byref(split),
+                                        C.byref(form)))
+        return (rows.value, split.value, form.value), [t for t in times[:abi.NUM_SPMV_SHAPES]]
+
+    def set_spmv_shape(self, index):
+        """Use SpMV tile shape `index` of abi.SPMV_SHAPES for later solves."""
+        check(lib().mvdr_batch_set_spmv_shape(self.h, index))
 
     def instance(self, i):
         """NonRigidSolver-like view of one member (for checks); not owned."""

@@ -55,3 +55,10 @@ def test_config_default_and_errors_without_gpu(L):
     assert L.mvdr_create(C.byref(bad), C.byref(h)) == abi.MVDR_EINVAL
     assert L.mvdr_destroy(None) == abi.MVDR_OK
     assert L.mvdr_set_inputs(None, None, None) == abi.MVDR_EINVAL
+
+
+def test_spmv_shape_count_matches_header(L):
+    text = open(HEADER).read()
+    n = int(re.search(r"#define MVDR_NUM_SPMV_SHAPES (\d+)u", text).group(1))
+    assert n == abi.NUM_SPMV_SHAPES
+    assert L.mvdr_batch_set_spmv_shape(None, 0) == abi.MVDR_EINVAL

@@ -340,6 +340,30 @@ def test_adjoint_products_vs_finite_differences(oracle_mod, mode):
     assert rel_norm_error(y_g, jtjp_fd) < 1e-4
 
 
+# FP32: 5 GN x 15 PCG iterations in float amplify a reordered sum to about
+# 1e-2 of the increment (measured between two tile shapes)
+@pytest.mark.parametrize("precision,tol", [(abi.PRECISION_MIXED, 1e-5), (abi.PRECISION_FP32, 3e-2)])
+def test_every_spmv_shape_solves_the_same_system(precision, tol):
+    """Every SpMV tile shape gives the first shape's increments up to the
+    order of its sums, and reruns of one shape are bit-identical."""
+    scene = small_scene("torso")
+    cfg = abi.make_config(scene, precision=precision)
+    b = BatchSolver(cfg, 2)
+    results = []
+    for k in list(range(abi.NUM_SPMV_SHAPES)) + [abi.NUM_SPMV_SHAPES - 1]:
+        b.set_spmv_shape(k)
+        for i in range(2):
+            b.set_input(i, scene)
+        b.solve(scene.gn_iterations, scene.pcg_iterations)
+        torch.cuda.synchronize()
+        results.append([b.instance(i).get_array(abi.ARRAY_INCREMENT) for i in range(2)])
+    for k, res in enumerate(results[:-1]):
+        for i in range(2):
+            assert rel_norm_error(res[i], results[0][i]) < tol, (abi.SPMV_SHAPES[k], i)
+    for i in range(2):
+        assert np.array_equal(results[-1][i], results[-2][i])
+
+
 def test_autotuned_spmv_shape_solves_the_same_system():
     """mvdr_batch_autotune picks one of the SpMV tile shapes; solves with the
     chosen shape agree with the default shape's (only the order of the row
