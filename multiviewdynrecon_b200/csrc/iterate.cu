@@ -766,27 +766,32 @@ template <class T> __device__ inline void store_block_partial(const InstDesc& I,
     }
 }
 
-// the sum of the `count` partials of `region`, in every thread
-template <class T> __device__ inline T sum_block_partials(const InstDesc& I, uint32_t region, uint32_t count) {
-    __shared__ T total;
-    __syncthreads();  // every thread has read the previous call's total
-    if (threadIdx.x < 32) {
-        const double* p = I.partials + (size_t)region * I.part_stride;
+// The sums of the partials of two regions (warp 0 sums region a, warp 1
+// region b, each in a fixed order), in every thread. blockDim.x >= 64.
+template <class T>
+__device__ inline void sum_two_block_partials(const InstDesc& I, uint32_t ra, uint32_t na, uint32_t rb, uint32_t nb,
+                                              T* a, T* b) {
+    __shared__ T total[2];
+    const uint32_t w = threadIdx.x >> 5;
+    if (w < 2) {
+        const double* p = I.partials + (size_t)(w == 0 ? ra : rb) * I.part_stride;
+        const uint32_t n = w == 0 ? na : nb;
         T s = 0;
-        for (uint32_t c = lane_id(); c < count; c += 32) s += (T)__ldcg(p + c);
+        for (uint32_t c = lane_id(); c < n; c += 32) s += (T)__ldcg(p + c);
         s = warp_sum(s);
-        if (threadIdx.x == 0) total = s;
+        if (lane_id() == 0) total[w] = s;
     }
     __syncthreads();
-    return total;
+    *a = total[0];
+    *b = total[1];
 }
 
 // beta = delta_k / delta_(k-1) of iteration k (0 for the first), from the
 // `nd` partials of the init / update launches
 template <class T>
 __device__ inline T pcg_beta(const InstDesc& I, int parity, int first, uint32_t nd) {
-    const T dk = sum_block_partials<T>(I, kRegDelta + parity, nd);
-    const T dkm1 = sum_block_partials<T>(I, kRegDelta + (parity ^ 1), nd);
+    T dk, dkm1;
+    sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDelta + (parity ^ 1), nd, &dk, &dkm1);
     return first ? (T)0 : dk / dkm1;
 }
 
@@ -857,13 +862,12 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
     const InstDesc& I = insts[blockIdx.y];
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
-    const T* dprev = PV::d(I, !parity);
-    T* dcur = PV::d(I, parity);
-    const T* sv = PV::s(I);
+    // one element per thread (the grid covers 6N), loaded before beta's sums
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool has = e < 6 * I.N;
+    const T sv = has ? PV::s(I)[e] : (T)0, dp = has ? PV::d(I, !parity)[e] : (T)0;
     const T beta = pcg_beta<T>(I, parity, first, nd);
-    const uint32_t n = 6 * I.N;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
-        dcur[e] = sv[e] + beta * dprev[e];
+    if (has) PV::d(I, parity)[e] = sv + beta * dp;
 }
 
 // ------------------------------------------------------- tiled SpMV -----
@@ -1018,43 +1022,79 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_col_kerne
 
 // blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): alpha = delta / d.q,
 // x += alpha d, r -= alpha q, s = M^-1 r, delta_new = r.s (beta follows in
-// the next direction). `nd` and `nq`: CTAs of the launches that stored the
-// delta and d.q partials.
+// the next direction). A thread per node; the grid covers every node. The
+// node's vectors and preconditioner are loaded before the partial sums, so
+// their latency overlaps the sums. `nd` and `nq`: CTAs of the launches that
+// stored the delta and d.q partials.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity, uint32_t nd,
                                                          uint32_t nq) {
     const InstDesc& I = insts[blockIdx.y];
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
-    const T* d = PV::d(I, parity);
-    const T delta = sum_block_partials<T>(I, kRegDelta + parity, nd);
-    const T alpha = delta / sum_block_partials<T>(I, kRegDq, nq);
+    using T2 = typename Pair<T>::type;
+    constexpr int kPre = MIXED ? 21 : 36;  // Cholesky factor / inverse entries
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool has = node < I.N;
+    T xv[6], dv[6], rv[6], qv[6];
+    T pre[kPre];
+    if (has) {
+        auto load6 = [&](const T* v, T out[6]) {
+            const T2* p = reinterpret_cast<const T2*>(v + 6 * (size_t)node);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const T2 w = p[i];
+                out[2 * i] = w.x;
+                out[2 * i + 1] = w.y;
+            }
+        };
+        load6(PV::x(I), xv);
+        load6(PV::d(I, parity), dv);
+        load6(PV::r(I), rv);
+        load6(PV::q(I), qv);
+#pragma unroll
+        for (int i = 0; i < kPre; ++i) {
+            if constexpr (MIXED) pre[i] = I.chol[21 * (size_t)node + i];
+            else pre[i] = I.minv[36 * (size_t)node + i];
+        }
+    }
+    T delta, dq;
+    sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDq, nq, &delta, &dq);
+    const T alpha = delta / dq;
     T part = 0;
-    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
-        T rv[6], sv[6];
+    if (has) {
+        T sv[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
-            const size_t e = 6 * (size_t)node + i;
-            PV::x(I)[e] += alpha * d[e];
-            rv[i] = PV::r(I)[e] - alpha * PV::q(I)[e];
-            PV::r(I)[e] = rv[i];
+            xv[i] += alpha * dv[i];
+            rv[i] -= alpha * qv[i];
         }
         if constexpr (MIXED) {
-            cholesky6_solve(I.chol + 21 * (size_t)node, rv, sv);
+            cholesky6_solve(pre, rv, sv);
         } else {
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
                 float a = 0.f;
 #pragma unroll
-                for (int i = 0; i < 6; ++i) a += I.minv[36 * (size_t)node + 6 * j + i] * rv[i];
+                for (int i = 0; i < 6; ++i) a += pre[6 * j + i] * rv[i];
                 sv[j] = a;
             }
         }
+        auto store6 = [&](T* v, const T in[6]) {
+            T2* p = reinterpret_cast<T2*>(v + 6 * (size_t)node);
 #pragma unroll
-        for (int i = 0; i < 6; ++i) {
-            PV::s(I)[6 * (size_t)node + i] = sv[i];
-            part += rv[i] * sv[i];
-        }
+            for (int i = 0; i < 3; ++i) {
+                T2 w;
+                w.x = in[2 * i];
+                w.y = in[2 * i + 1];
+                p[i] = w;
+            }
+        };
+        store6(PV::x(I), xv);
+        store6(PV::r(I), rv);
+        store6(PV::s(I), sv);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) part += rv[i] * sv[i];
     }
     store_block_partial<T>(I, kRegDelta + (parity ^ 1), part);
 }
@@ -1353,8 +1393,9 @@ static uint32_t spmv_grid(const LaunchCfg& lc) {
 
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
-    const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
-    const uint32_t gvec = min((6 * lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
+    // the update's and direction's grids cover every node / element
+    const uint32_t gnode = (lc.max_nodes + 255) / 256;
+    const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gwarp = (lc.max_nodes + 7) / 8;
     const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
     if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d);
@@ -1420,8 +1461,8 @@ cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream
 
 cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, int stage, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
-    const uint32_t gnode = min((lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
-    const uint32_t gvec = min((6 * lc.max_nodes + 255) / 256, (uint32_t)lc.sm_count * 4);
+    const uint32_t gnode = (lc.max_nodes + 255) / 256;
+    const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     switch (stage) {
         case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
