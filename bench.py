@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     p.add_argument("--mode", default="materialized", choices=["materialized", "matrix_free"])
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison leg")
+    p.add_argument("--spmv-shape", type=int, default=-1,
+                   help="use this SpMV tile shape (index into abi.SPMV_SHAPES) instead of the autotuner's")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--workload", default="torso", choices=["torso", "uneven", "body"],
@@ -238,10 +240,15 @@ def run_ours(args, rank, world, dist):
         bind_all()
         batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
 
-    # SpMV tile shape for this workload (one timed sweep of the candidates)
+    # SpMV tile shape for this workload (one timed sweep of the candidates,
+    # or the shape given on the command line)
     with torch.cuda.stream(stream):
         bind_all()
-        spmv_shape, spmv_shape_ms = batch.autotune(stream=stream)
+        if args.spmv_shape >= 0:
+            batch.set_spmv_shape(args.spmv_shape)
+            spmv_shape, spmv_shape_ms = abi.SPMV_SHAPES[args.spmv_shape], []
+        else:
+            spmv_shape, spmv_shape_ms = batch.autotune(stream=stream)
 
     # kernels per solve: one direct (non-graph) solve counted through the ABI
     with torch.cuda.stream(stream):
@@ -307,7 +314,7 @@ def run_ours(args, rank, world, dist):
     spmv = stages["spmv"]
     spmv_bytes = B * abytes["spmv"]
     traffic, traffic_src = measured_traffic(args)
-    roofline = {"kernel": "pcg_spmv_kernel", "bound": "hbm", "achieved": spmv["GBps"], "peak": peak,
+    roofline = {"kernel": "pcg_spmv_col_kernel" if spmv_shape[2] == 1 else "pcg_spmv_kernel", "bound": "hbm", "achieved": spmv["GBps"], "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s", "frac": round(spmv["GBps"] / peak, 4),
                 "traffic": traffic, "traffic_source": traffic_src, "algorithmic_bytes_per_launch": spmv_bytes,
                 "launch_ms": spmv["ms"]}
@@ -322,7 +329,10 @@ def run_ours(args, rank, world, dist):
     e2e_batches = [batch, BatchSolver(cfg, B)]
     for i, ds in enumerate(dev_scenes):
         e2e_batches[1].set_input(i, ds, stream=stream)
-    e2e_batches[1].autotune(stream=stream)
+    if args.spmv_shape >= 0:
+        e2e_batches[1].set_spmv_shape(args.spmv_shape)
+    else:
+        e2e_batches[1].autotune(stream=stream)
     copy_stream, solve_stream = torch.cuda.Stream(), stream
     uploaded = [torch.cuda.Event(), torch.cuda.Event()]
     solved = [torch.cuda.Event(), torch.cuda.Event()]
