@@ -788,6 +788,60 @@ __global__ void __launch_bounds__(256) bin_colptr_kernel(const InstDesc* insts) 
     }
 }
 
+// ------------------------------------------------- per-entry weights -----
+// The skinning weight of each index entry's node(s) in its term, recorded once
+// per solve (the weights are inputs), so that the assembly kernels read one
+// coalesced value per entry instead of the term's node and weight records.
+// The values are those of weight_of (PreconditionerBlocked.cu:23-29).
+
+// warp per node: n2t_w[p] for the node's terms
+__global__ void __launch_bounds__(256) n2t_weight_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (I.counts->node2term_entries > I.cap_k1) return;
+    TermOffsets off;
+    off.load(I.counts);
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+        const uint32_t b0 = I.n2t_offset[node], b1 = I.n2t_offset[node + 1];
+        for (uint32_t p = b0 + lane_id(); p < b1; p += 32) {
+            uint32_t k;
+            const TermType ty = off.typed(I.n2t_index[p], k);
+            I.n2t_w[p] = ty == kSmooth || ty == kInvalidTerm
+                             ? 0.f
+                             : weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+        }
+    }
+}
+
+// warp per node i: np_w[p] = (w_i, w_j) for the terms of each pair (i, j),
+// pair by pair, the lanes over the pair's entries
+__global__ void __launch_bounds__(256) np_weight_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    const DeviceCounts* C = I.counts;
+    if (C->half_pairs > I.cap_pairs || C->nodepair_entries > I.cap_k2 || C->node2term_entries > I.cap_k1) return;
+    TermOffsets off;
+    off.load(C);
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t ni = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); ni < I.N; ni += warps) {
+        const uint32_t h0 = I.half_offset[ni], nu = I.upper_count[ni];
+        for (uint32_t h = h0; h < h0 + nu; ++h) {
+            const uint32_t nj = I.half_key[h] % I.enc;
+            const uint2 rg = I.half_range[h];
+            for (uint32_t p = rg.x + lane_id(); p < rg.y; p += 32) {
+                uint32_t k;
+                const TermType ty = off.typed(I.np_index[p], k);
+                float2 w = make_float2(0.f, 0.f);
+                if (ty != kSmooth && ty != kInvalidTerm) {
+                    const ushort4 kn = term_nodes(I, ty, k);
+                    const float4 w4 = term_weights(I, ty, k);
+                    w = make_float2(weight_of(kn, w4, ni), weight_of(kn, w4, nj));
+                }
+                I.np_w[p] = w;
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------ launch -----
 
 static inline dim3 grid2(uint32_t x, uint32_t B) { return dim3(x ? x : 1, B); }
@@ -827,6 +881,8 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanBlkRows);
     MVDR_LAUNCH(np_sym_scatter_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     MVDR_LAUNCH(np_lower_sort_kernel, grid2((lc.max_nodes + 3) / 4, B), 128, 0, st, d);
+    MVDR_LAUNCH(n2t_weight_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
+    MVDR_LAUNCH(np_weight_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
     // bin-block CSR structure
     MVDR_LAUNCH(bin_length_kernel, grid2((6 * lc.max_nodes / 32 + 256) / 256, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanBins);

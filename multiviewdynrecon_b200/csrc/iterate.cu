@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(128, 5) diag_rhs_kernel(const InstDesc* insts,
                     const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
                     if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0, r = 0
                     const Acc l2 = ty == kDense ? (Acc)1 : l2_fg;
-                    const Acc w = (Acc)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+                    const Acc w = (Acc)I.n2t_w[p];
                     const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
                     const Acc sw = l2 * w * w, rw = -l2 * w * (Acc)b.z;
 #pragma unroll
@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(128, 5) diag_rhs_kernel(const InstDesc* insts,
                     const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
                     const float4 raw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
                     const Acc l2 = f ? l2_feat : l2_cross;
-                    const Acc w = (Acc)weight_of(term_nodes(I, ty, k), term_weights(I, ty, k), node);
+                    const Acc w = (Acc)I.n2t_w[p];
                     Acc fr[3][6];
                     twist_rows<Acc>((Acc)wv.x, (Acc)wv.y, (Acc)wv.z, fr);
                     const float rv[3] = {raw.x, raw.y, raw.z};
@@ -606,8 +606,7 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
     // pairs grouped by entry count, so the lanes of a warp loop equally long
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
         const uint32_t h = I.pair_order[i];
-        const uint32_t key = I.half_key[h];
-        const uint32_t ni = key / I.enc, nj = key % I.enc;
+        const uint32_t ni = I.half_key[h] / I.enc;
         const uint2 rg = I.half_range[h];
         Acc S[21];
 #pragma unroll
@@ -618,32 +617,31 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
         // the current entry is summed
         uint32_t t_next = rg.x < rg.y ? I.np_index[rg.x] : 0u;
         uint32_t t_next2 = rg.x + 1 < rg.y ? I.np_index[rg.x + 1] : 0u;
-        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa, pw = pa;
-        ushort4 pk = make_ushort4(0, 0, 0, 0);
-        auto fetch_pixel_term = [&](uint32_t t) {
+        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+        float2 pw = make_float2(0.f, 0.f);
+        auto fetch_pixel_term = [&](uint32_t t, uint32_t p) {
             uint32_t k;
             const TermType ty = off.typed(t, k);
             if (ty == kDense || ty == kForeground) {
                 const uint32_t idx = ty == kDense ? k : off.o[0] + k;
                 pa = I.term_jr[2 * (size_t)idx];
                 pb = I.term_jr[2 * (size_t)idx + 1];
-                pk = term_nodes(I, ty, k);
-                pw = term_weights(I, ty, k);
+                pw = I.np_w[p];
             }
         };
-        if (rg.x < rg.y) fetch_pixel_term(t_next);
+        if (rg.x < rg.y) fetch_pixel_term(t_next, rg.x);
         for (uint32_t p = rg.x; p < rg.y; ++p) {
             const uint32_t t = t_next;
-            const float4 a = pa, b = pb, w4 = pw;
-            const ushort4 kn = pk;
+            const float4 a = pa, b = pb;
+            const float2 wij = pw;
             t_next = t_next2;
             if (p + 2 < rg.y) t_next2 = I.np_index[p + 2];
-            if (p + 1 < rg.y) fetch_pixel_term(t_next);
+            if (p + 1 < rg.y) fetch_pixel_term(t_next, p + 1);
             uint32_t k;
             const TermType ty = off.typed(t, k);
             if (ty == kDense || ty == kForeground) {
                 if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0
-                Acc s = (Acc)weight_of(kn, w4, ni) * (Acc)weight_of(kn, w4, nj);
+                Acc s = (Acc)wij.x * (Acc)wij.y;
                 if (ty == kForeground) s *= l2_fg;
                 const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
                 add_scaled_outer(S, s, g);
@@ -654,9 +652,8 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
                 const bool f = ty == kFeature;
                 const float4 wv = I.warped[2 * (size_t)(f ? k : I.Tp + k)];
                 const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
-                const ushort4 kn = term_nodes(I, ty, k);
-                const float4 w4 = term_weights(I, ty, k);
-                const Acc s = (Acc)weight_of(kn, w4, ni) * (Acc)weight_of(kn, w4, nj) * (f ? l2_feat : l2_cross);
+                const float2 wp = I.np_w[p];
+                const Acc s = (Acc)wp.x * (Acc)wp.y * (f ? l2_feat : l2_cross);
                 const float hw[3] = {huber_weight(rw.x), huber_weight(rw.y), huber_weight(rw.z)};
                 Acc fr[3][6];
                 twist_rows<Acc>((Acc)wv.x, (Acc)wv.y, (Acc)wv.z, fr);

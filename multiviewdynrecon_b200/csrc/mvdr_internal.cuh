@@ -240,10 +240,12 @@ struct InstDesc {
     uint32_t* n2t_offset;   // [N+1]
     uint32_t* n2t_cursor;   // [N]
     uint32_t* n2t_index;    // [K1 cap]
+    float* n2t_w;           // [K1 cap] skinning weight of the entry's node in its term (0 for smooth)
     // node pair -> term
     uint32_t* row_count;    // [N+1] entries (j, t) with j > i per row
     uint32_t* row_offset;   // [N+1]
     uint32_t* np_index;     // [K2 cap]
+    float2* np_w;           // [K2 cap] skinning weights of the pair's (i, j) nodes in the entry's term
     uint32_t* upper_count;  // [N+1]
     uint32_t* half_offset;  // [N+1]
     uint32_t* tmp_key;      // [K2 cap] per-row unique pairs before compaction

@@ -155,9 +155,11 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.n2t_offset = a.take<uint32_t>(N + 1);
     I.n2t_cursor = a.take<uint32_t>(N + 1);
     I.n2t_index = a.take<uint32_t>(lc.cap_k1);
+    I.n2t_w = a.take<float>(lc.cap_k1);
     I.row_count = a.take<uint32_t>(N + 1);
     I.row_offset = a.take<uint32_t>(N + 1);
     I.np_index = a.take<uint32_t>(lc.cap_k2);
+    I.np_w = a.take<float2>(lc.cap_k2);
     I.upper_count = a.take<uint32_t>(N + 1);
     I.half_offset = a.take<uint32_t>(N + 1);
     I.tmp_key = a.take<uint32_t>(lc.cap_k2);
