@@ -268,25 +268,39 @@ __global__ void term_offsets_kernel(const InstDesc* insts) {
 
 // ------------------------------------------------------ node -> term -----
 
+// Neighbouring pixels share their KNN nodes, so the lanes of a warp that
+// hold the same node are merged (match_any) and one lane adds the group's
+// count: one atomic per distinct node and slot in the warp.
 __global__ void __launch_bounds__(256) n2t_count_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     if (bad_inputs(I)) return;
     TermOffsets off;
     off.load(I.counts);
-    const uint32_t T = off.o[4];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        uint32_t k;
-        const TermType ty = off.typed(t, k);
-        const ushort4 n = term_nodes(I, ty, k);
-        const uint32_t m = ty == kSmooth ? 2 : 4;
-        const unsigned short a[4] = {n.x, n.y, n.z, n.w};
-        for (uint32_t j = 0; j < m; ++j) {
-            if (a[j] < I.N) atomicAdd(&I.n2t_count[a[j]], 1u);
-            else set_error(I, kErrBadNodeIndex);
+    const uint32_t T = off.o[4], lane = lane_id();
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // the warp's 32 terms per step, so that every lane takes part in the match
+    for (uint32_t tw = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); tw < T; tw += stride) {
+        const uint32_t t = tw + lane;
+        uint32_t a[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+        if (t < T) {
+            uint32_t k;
+            const TermType ty = off.typed(t, k);
+            const ushort4 n = term_nodes(I, ty, k);
+            const uint32_t m = ty == kSmooth ? 2 : 4;
+            const unsigned short v[4] = {n.x, n.y, n.z, n.w};
+            for (uint32_t j = 0; j < m; ++j) {
+                if (v[j] < I.N) a[j] = v[j];
+                else set_error(I, kErrBadNodeIndex);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t grp = __match_any_sync(0xffffffffu, a[j]);
+            if (a[j] != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(grp) - 1))
+                atomicAdd(&I.n2t_count[a[j]], (uint32_t)__popc(grp));
         }
     }
 }
-
 // single-CTA exclusive scans over per-node arrays
 enum ScanWhat : int { kScanN2T = 0, kScanRows = 1, kScanUpper = 2, kScanBlkRows = 3, kScanBins = 4 };
 
@@ -366,23 +380,37 @@ __global__ void __launch_bounds__(1024) node_scan_kernel(const InstDesc* insts, 
     }
 }
 
+// The same grouping: the group's first lane reserves the group's slots and
+// every lane takes its rank in the group (the sort that follows orders them).
 __global__ void __launch_bounds__(256) n2t_scatter_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     TermOffsets off;
     off.load(I.counts);
-    const uint32_t T = off.o[4];
+    const uint32_t T = off.o[4], lane = lane_id();
     const uint32_t K1 = I.counts->node2term_entries;
     if (K1 > I.cap_k1) return;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        uint32_t k;
-        const TermType ty = off.typed(t, k);
-        const ushort4 n = term_nodes(I, ty, k);
-        const uint32_t m = ty == kSmooth ? 2 : 4;
-        const unsigned short a[4] = {n.x, n.y, n.z, n.w};
-        for (uint32_t j = 0; j < m; ++j) {
-            if (a[j] >= I.N) continue;
-            const uint32_t pos = I.n2t_offset[a[j]] + atomicAdd(&I.n2t_cursor[a[j]], 1u);
-            I.n2t_index[pos] = t;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t tw = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); tw < T; tw += stride) {
+        const uint32_t t = tw + lane;
+        uint32_t a[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+        if (t < T) {
+            uint32_t k;
+            const TermType ty = off.typed(t, k);
+            const ushort4 n = term_nodes(I, ty, k);
+            const uint32_t m = ty == kSmooth ? 2 : 4;
+            const unsigned short v[4] = {n.x, n.y, n.z, n.w};
+            for (uint32_t j = 0; j < m; ++j)
+                if (v[j] < I.N) a[j] = v[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t grp = __match_any_sync(0xffffffffu, a[j]);
+            const uint32_t leader = __ffs(grp) - 1;
+            uint32_t base = 0;
+            if (a[j] != 0xFFFFFFFFu && lane == leader) base = atomicAdd(&I.n2t_cursor[a[j]], (uint32_t)__popc(grp));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (a[j] != 0xFFFFFFFFu)
+                I.n2t_index[I.n2t_offset[a[j]] + base + __popc(grp & ((1u << lane) - 1u))] = t;
         }
     }
 }
