@@ -17,7 +17,7 @@
 
 namespace mvdr {
 
-constexpr uint32_t kChunk = 2048;  // pixels per compaction CTA (256 threads x 8)
+constexpr uint32_t kChunk = kChunkPixels;
 
 // ----------------------------------------------------- input checks -----
 // Node ids of the skinning, the node graph and the correspondences must be
@@ -101,7 +101,11 @@ __global__ void __launch_bounds__(256) compact_count_kernel(const InstDesc* inst
         const uint32_t npix = width * height;
         for (uint32_t k = 0; k < kChunk / 256; ++k) {
             const uint32_t p = c * kChunk + k * 256 + threadIdx.x;
-            if (p < npix) cnt += Pred::eval(I, view, p % width, p / width) ? 1u : 0u;
+            const bool ok = p < npix && Pred::eval(I, view, p % width, p / width);
+            // the write pass reads the predicate back from these bits
+            const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+            if (lane_id() == 0) I.pix_mask[(size_t)view * cpv * (kChunk / 32) + p / 32] = bal;
+            cnt += ok ? 1u : 0u;
         }
     }
     cnt = warp_sum(cnt);
@@ -151,15 +155,14 @@ __global__ void __launch_bounds__(256) compact_write_kernel(const InstDesc* inst
     const InstDesc& I = insts[blockIdx.y];
     const uint32_t view = blockIdx.x / cpv, c = blockIdx.x % cpv;
     if (view >= I.num_views) return;
-    const uint32_t npix = width * height;
     const uint32_t cap = foreground ? I.cap_fg : I.cap_dense;
     __shared__ uint32_t wtot[8];
     uint32_t carry = I.chunk_count[blockIdx.x];
     for (uint32_t k = 0; k < kChunk / 256; ++k) {
         const uint32_t p = c * kChunk + k * 256 + threadIdx.x;
         const uint32_t x = p % width, y = p / width;
-        const bool ok = p < npix && Pred::eval(I, view, x, y);
-        const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+        const uint32_t bal = I.pix_mask[(size_t)view * cpv * (kChunk / 32) + p / 32];
+        const bool ok = (bal >> lane_id()) & 1u;
         const uint32_t lane_prefix = __popc(bal & ((1u << lane_id()) - 1u));
         if (lane_id() == 0) wtot[threadIdx.x >> 5] = __popc(bal);
         __syncthreads();
@@ -417,13 +420,16 @@ __global__ void __launch_bounds__(256) n2t_scatter_kernel(const InstDesc* insts)
 
 // Sort each node's term segment ascending, one warp per node, in registers:
 // element i = 32 s + lane sits in slot s of a lane; a bitonic network over
-// kWarpSortSlots * 32 keys exchanges across lanes with shuffles (partner
-// distance < 32) and inside a lane between slots otherwise. Segments longer
-// than that are left to n2t_sort_kernel.
-constexpr int kWarpSortSlots = 8;
-constexpr uint32_t kWarpSortMax = 32u * kWarpSortSlots;
+// kSlots * 32 keys exchanges across lanes with shuffles (partner distance
+// < 32) and inside a lane between slots otherwise. A launch takes the
+// segments of (min_len, 32 kSlots] terms; three launches (8, 16, 32 slots)
+// cover up to kWarpSortMax, and n2t_sort_kernel the longer ones.
+constexpr uint32_t kWarpSortMax = 1024;
 
-__global__ void __launch_bounds__(256) n2t_warp_sort_kernel(const InstDesc* insts) {
+template <int kSlots>
+__global__ void __launch_bounds__(256) n2t_warp_sort_kernel(const InstDesc* insts, uint32_t min_len) {
+    constexpr int kWarpSortSlots = kSlots;
+    constexpr uint32_t kMax = 32u * kSlots;
     const InstDesc& I = insts[blockIdx.y];
     if (I.counts->node2term_entries > I.cap_k1) return;
     const uint32_t lane = lane_id();
@@ -431,7 +437,11 @@ __global__ void __launch_bounds__(256) n2t_warp_sort_kernel(const InstDesc* inst
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
         const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
         const uint32_t len = e - b;
-        if (len <= 1 || len > kWarpSortMax) continue;
+        if (len <= min_len || len <= 1 || len > kMax) continue;
+        if (len > I.cap_seg) {  // the segment exceeds max_terms_per_node
+            if (lane == 0) set_error(I, kErrSegmentTooLong);
+            continue;
+        }
         uint32_t v[kWarpSortSlots];
 #pragma unroll
         for (int sl = 0; sl < kWarpSortSlots; ++sl) {
@@ -439,7 +449,7 @@ __global__ void __launch_bounds__(256) n2t_warp_sort_kernel(const InstDesc* inst
             v[sl] = i < len ? I.n2t_index[b + i] : 0xFFFFFFFFu;
         }
 #pragma unroll
-        for (uint32_t k = 2; k <= kWarpSortMax; k <<= 1) {
+        for (uint32_t k = 2; k <= kMax; k <<= 1) {
 #pragma unroll
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
                 if (j >= 32) {
@@ -897,7 +907,9 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     MVDR_LAUNCH(n2t_count_kernel, grid2(spread, B), 256, 0, st, d);
     MVDR_LAUNCH(node_scan_kernel, grid2(1, B), 1024, 0, st, d, (int)kScanN2T);
     MVDR_LAUNCH(n2t_scatter_kernel, grid2(spread, B), 256, 0, st, d);
-    MVDR_LAUNCH(n2t_warp_sort_kernel, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d);
+    MVDR_LAUNCH(n2t_warp_sort_kernel<8>, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d, 0u);
+    MVDR_LAUNCH(n2t_warp_sort_kernel<16>, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d, 256u);
+    MVDR_LAUNCH(n2t_warp_sort_kernel<32>, grid2((lc.max_nodes + 7) / 8, B), 256, 0, st, d, 512u);
     MVDR_LAUNCH(n2t_sort_kernel, grid2(min(lc.max_nodes, (uint32_t)lc.sm_count), B), 256, (size_t)lc.cap_seg * 4, st,
                 d);
     // node pair -> term

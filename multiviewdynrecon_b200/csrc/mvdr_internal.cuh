@@ -33,6 +33,8 @@ __host__ __device__ constexpr uint32_t len_bucket_of(uint32_t len) {
 // another instruction's read).
 __host__ __device__ constexpr uint32_t blk_idx(uint32_t r, uint32_t k) { return 12 * (k >> 1) + 2 * r + (k & 1); }
 
+constexpr uint32_t kChunkPixels = 2048;  // pixels per compaction CTA (256 threads x 8)
+
 // error flag bits (DeviceCounts::error_flags)
 enum : uint32_t {
     kErrDenseCapacity = 1u << 0,
@@ -225,6 +227,7 @@ struct InstDesc {
     DQ* se3;                // current warp field
     // compaction: per dense/foreground term
     uint32_t* chunk_count;  // [num chunk slots]
+    uint32_t* pix_mask;     // predicate bit per pixel of the current compaction [views * chunks * 64]
     ushort4* dense_pix;     // (x, y, view, 0)
     ushort4* dense_knn;
     float4* dense_w;

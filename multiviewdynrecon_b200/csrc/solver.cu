@@ -141,6 +141,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.counts = a.take<DeviceCounts>(1);
     I.se3 = a.take<DQ>(N);
     I.chunk_count = a.take<uint32_t>((size_t)lc.chunks_per_view * lc.max_views + 1);
+    I.pix_mask = a.take<uint32_t>((size_t)lc.chunks_per_view * lc.max_views * (kChunkPixels / 32));
     I.dense_pix = a.take<ushort4>(lc.cap_dense);
     I.dense_knn = a.take<ushort4>(lc.cap_dense);
     I.dense_w = a.take<float4>(lc.cap_dense);
@@ -271,7 +272,7 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     auto pow2 = [](uint32_t v) { uint32_t p = 1; while (p < v) p <<= 1; return p; };
     lc.cap_seg = std::min<uint32_t>(pow2(cfg->max_terms_per_node ? cfg->max_terms_per_node : 4096), 16384);
     lc.cap_bb = 36 * (cfg->max_nodes + 2 * lc.cap_pairs);
-    lc.chunks_per_view = (cfg->image_width * cfg->image_height + 2047) / 2048;
+    lc.chunks_per_view = (cfg->image_width * cfg->image_height + kChunkPixels - 1) / kChunkPixels;
     lc.precision = cfg->precision;
     lc.mode = cfg->mode;
     lc.sm_count = prop.multiProcessorCount;
