@@ -624,8 +624,7 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
             const TermType ty = off.typed(t, k);
             if (ty == kDense || ty == kForeground) {
                 const uint32_t idx = ty == kDense ? k : off.o[0] + k;
-                pa = I.term_jr[2 * (size_t)idx];
-                pb = I.term_jr[2 * (size_t)idx + 1];
+                load_record32(I.term_jr + 2 * (size_t)idx, pa, pb);
                 pw = I.np_w[p];
             }
         };

@@ -225,6 +225,13 @@ __device__ inline bool index_complete(const InstDesc& I) {
            (*(volatile const uint32_t*)&C->error_flags & kIndexErrors) == 0;
 }
 
+// The 32-byte record (two float4) at p in one 256-bit load (p 32-byte aligned)
+__device__ inline void load_record32(const float4* p, float4& a, float4& b) {
+    asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p));
+}
+
 // true when the input check found an out-of-range node or surfel id
 __device__ inline bool bad_inputs(const InstDesc& I) {
     return (*(volatile const uint32_t*)&I.counts->error_flags & kErrBadNodeIndex) != 0;
