@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     p.add_argument("--mode", default="materialized", choices=["materialized", "matrix_free"])
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison leg")
+    p.add_argument("--pcg-persistent", action="store_true",
+                   help="run each PCG solve as one persistent cooperative launch")
     p.add_argument("--spmv-shape", type=int, default=-1,
                    help="use this SpMV tile shape (index into abi.SPMV_SHAPES) instead of the autotuner's")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -244,6 +246,8 @@ def run_ours(args, rank, world, dist):
     # or the shape given on the command line)
     with torch.cuda.stream(stream):
         bind_all()
+        if args.pcg_persistent:
+            batch.set_pcg_persistent(True)
         if args.spmv_shape >= 0:
             batch.set_spmv_shape(args.spmv_shape)
             spmv_shape, spmv_shape_ms = abi.SPMV_SHAPES[args.spmv_shape], []
@@ -329,6 +333,8 @@ def run_ours(args, rank, world, dist):
     e2e_batches = [batch, BatchSolver(cfg, B)]
     for i, ds in enumerate(dev_scenes):
         e2e_batches[1].set_input(i, ds, stream=stream)
+    if args.pcg_persistent:
+        e2e_batches[1].set_pcg_persistent(True)
     if args.spmv_shape >= 0:
         e2e_batches[1].set_spmv_shape(args.spmv_shape)
     else:
@@ -637,6 +643,7 @@ def main():
             "config": {"workload": WORKLOAD, "instances_per_gpu": args.batch, "views": 3,
                        "image": [args.width, args.height], "nodes": args.nodes, "gn": args.gn, "pcg": args.pcg,
                        "precision": args.precision, "mode": args.mode, "graph": True,
+                       "pcg": "persistent" if args.pcg_persistent else "launches",
                        "l2": "aggregate working set of the batch well above the 126 MB L2; no flush",
                        "dense_terms": c.dense_terms, "half_pairs": c.half_pairs,
                        "parallelism": f"independent instances, {world} GPU(s), no collective in the solve"},

@@ -748,7 +748,8 @@ __device__ inline bool block_partial_and_last(const InstDesc& I, T v, int ticket
 // holds d.q of the current iteration.
 constexpr uint32_t kRegDelta = 1, kRegDq = 3;
 
-template <class T> __device__ inline void store_block_partial(const InstDesc& I, uint32_t region, T v) {
+template <class T>
+__device__ inline void store_block_partial(const InstDesc& I, uint32_t region, T v, uint32_t slot = 0xFFFFFFFFu) {
     __shared__ T ws[32];
     v = warp_sum(v);
     if (lane_id() == 0) ws[threadIdx.x >> 5] = v;
@@ -756,7 +757,7 @@ template <class T> __device__ inline void store_block_partial(const InstDesc& I,
     if (threadIdx.x == 0) {
         T s = 0;
         for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += ws[w];
-        I.partials[(size_t)region * I.part_stride + blockIdx.x] = (double)s;
+        I.partials[(size_t)region * I.part_stride + (slot == 0xFFFFFFFFu ? blockIdx.x : slot)] = (double)s;
     }
 }
 
@@ -1093,6 +1094,202 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
     store_block_partial<T>(I, kRegDelta + (parity ^ 1), part);
 }
 
+// ------------------------------------------------------ persistent PCG ---
+// One cooperative launch runs every PCG iteration of every instance. The
+// CTAs are split among the instances (one each, the rest in proportion to
+// their node counts: the per-instance work queues); an instance's CTAs run
+// init, then per iteration the direction, the SpMV (column form, kPersistRows
+// block rows per tile) and the update, and meet at an instance barrier
+// between steps. Instances never wait for one another, so one instance's
+// barrier and reduction latency overlaps the others' loads. The dots are the
+// same split reductions as in the launched form, with one partial per CTA of
+// the instance.
+constexpr uint32_t kPersistThreads = 256, kPersistRows = 40;
+constexpr uint64_t kBarrierLimitNs = 500ull * 1000 * 1000;  // a step takes microseconds
+
+__device__ inline uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ inline uint32_t ld_acquire_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All CTAs of the instance arrive; returns false (and flags the instance)
+// when the wait exceeds kBarrierLimitNs.
+__device__ inline bool instance_barrier(const InstDesc& I, uint32_t* ctr, uint32_t target) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctr, 1u);
+        int ok = 1;
+        if (ld_acquire_u32(ctr) < target) {
+            const uint64_t t0 = global_ns();
+            while (ld_acquire_u32(ctr) < target) {
+                if (global_ns() - t0 > kBarrierLimitNs) {
+                    ok = 0;
+                    set_error(I, kErrWaitTimeout);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(const InstDesc* insts, uint32_t B,
+                                                                              uint32_t iters) {
+    using PV = PcgVec<MIXED>;
+    using T = typename PV::T;
+    using V = typename BlockStore<MIXED>::V;
+    using V2 = typename Pair<V>::type;
+    // this CTA's instance: instance i owns CTAs [i + (G - B) P_i / P, ...),
+    // P_i the nodes of the instances before it
+    const uint32_t G = gridDim.x;
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < B; ++i) total += insts[i].N;
+    uint32_t inst = 0, c0 = 0, c1 = 0;
+    uint64_t pre = 0;
+    for (uint32_t i = 0; i < B; ++i) {
+        const uint64_t nxt = pre + insts[i].N;
+        const uint32_t b0 = i + (uint32_t)((G - B) * pre / (total ? total : 1));
+        const uint32_t b1 = i + 1 + (uint32_t)((G - B) * nxt / (total ? total : 1));
+        if (blockIdx.x >= b0 && blockIdx.x < b1) { inst = i; c0 = b0; c1 = b1; }
+        pre = nxt;
+    }
+    const InstDesc& I = insts[inst];
+    const uint32_t c = blockIdx.x - c0, nc = c1 - c0;
+    uint32_t* bar = I.pcg_bar;
+    uint32_t passed = 0;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const bool index_ok = index_complete(I);
+    // init: r = b, s = M^-1 b, x = 0, d_prev = 0, delta_0
+    {
+        T part = 0;
+        for (uint32_t node = c * nt + tid; node < I.N; node += nc * nt) {
+            T bv[6], sv[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) bv[i] = PV::jtr(I)[6 * (size_t)node + i];
+            if constexpr (MIXED) {
+                cholesky6_solve(I.chol + 21 * (size_t)node, bv, sv);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    float a = 0.f;
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) a += I.minv[36 * (size_t)node + 6 * j + i] * bv[i];
+                    sv[j] = a;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const size_t e = 6 * (size_t)node + i;
+                PV::r(I)[e] = bv[i];
+                PV::s(I)[e] = sv[i];
+                PV::d(I, 1)[e] = 0;
+                PV::x(I)[e] = 0;
+                part += bv[i] * sv[i];
+            }
+        }
+        store_block_partial<T>(I, kRegDelta, part, c);
+    }
+    if (!instance_barrier(I, bar, ++passed * nc)) return;
+    for (uint32_t it = 0; it < iters; ++it) {
+        const int parity = (int)(it & 1u);
+        // direction
+        {
+            const T beta = pcg_beta<T>(I, parity, it == 0, nc);
+            const T* dprev = PV::d(I, !parity);
+            T* dcur = PV::d(I, parity);
+            for (uint32_t e = c * nt + tid; e < 6 * I.N; e += nc * nt) dcur[e] = PV::s(I)[e] + beta * dprev[e];
+        }
+        if (!instance_barrier(I, bar, ++passed * nc)) return;
+        // SpMV over tiles of kPersistRows block rows, column form
+        {
+            const V* store = BlockStore<MIXED>::ptr(I);
+            const V* xvec = PV::d(I, parity);
+            T part = 0;
+            const uint32_t lr = tid / 6, rr = tid % 6;
+            for (uint32_t r0 = c * kPersistRows; index_ok && r0 < I.N; r0 += nc * kPersistRows) {
+                const uint32_t row = r0 + lr;
+                if (lr >= kPersistRows || row >= I.N) continue;
+                const uint32_t rb = I.blkrow_offset[row] + row, re = I.blkrow_offset[row + 1] + row + 1;
+                const uint32_t cfirst = blk_idx(0, rr);
+                V acc = 0;
+#pragma unroll 2
+                for (uint32_t b = rb; b < re; ++b) {
+                    const uint2 ent = I.bsr_ent[b];
+                    const V* blk = store + 36 * (size_t)(ent.x & ~kTransposedBlock);
+                    const V2* x2 = reinterpret_cast<const V2*>(xvec + 6 * (size_t)ent.y);
+                    const V2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
+                    const V xv[6] = {x01.x, x01.y, x23.x, x23.y, x45.x, x45.y};
+                    V av[6];
+                    if (ent.x & kTransposedBlock) {
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) av[k] = blk[cfirst + 2 * k];
+                    } else {
+                        const V2* b2 = reinterpret_cast<const V2*>(blk);
+                        const V2 a01 = b2[rr], a23 = b2[6 + rr], a45 = b2[12 + rr];
+                        av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y; av[4] = a45.x; av[5] = a45.y;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) acc += av[k] * xv[k];
+                }
+                const size_t e = 6 * (size_t)row + rr;
+                PV::q(I)[e] = acc;
+                part += (T)xvec[e] * (T)acc;
+            }
+            store_block_partial<T>(I, kRegDq, part, c);
+        }
+        if (!instance_barrier(I, bar, ++passed * nc)) return;
+        // update: alpha = delta / d.q, x, r, s, delta_new
+        {
+            T delta, dq;
+            sum_two_block_partials<T>(I, kRegDelta + parity, nc, kRegDq, nc, &delta, &dq);
+            const T alpha = delta / dq;
+            const T* d = PV::d(I, parity);
+            T part = 0;
+            for (uint32_t node = c * nt + tid; node < I.N; node += nc * nt) {
+                T rv[6], sv[6];
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    const size_t e = 6 * (size_t)node + i;
+                    PV::x(I)[e] += alpha * d[e];
+                    rv[i] = PV::r(I)[e] - alpha * PV::q(I)[e];
+                    PV::r(I)[e] = rv[i];
+                }
+                if constexpr (MIXED) {
+                    cholesky6_solve(I.chol + 21 * (size_t)node, rv, sv);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) {
+                        float a = 0.f;
+#pragma unroll
+                        for (int i = 0; i < 6; ++i) a += I.minv[36 * (size_t)node + 6 * j + i] * rv[i];
+                        sv[j] = a;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    PV::s(I)[6 * (size_t)node + i] = sv[i];
+                    part += rv[i] * sv[i];
+                }
+            }
+            store_block_partial<T>(I, kRegDelta + (parity ^ 1), part, c);
+        }
+        if (!instance_barrier(I, bar, ++passed * nc)) return;
+    }
+}
+
 // ------------------------------------------------------ matrix-free JtJ ---
 // J.p per term (ApplyJacobianDot.cu:127-198): jp[3t + c] for each channel,
 // with p = s + beta * d_prev formed on the fly when `fused` is set
@@ -1385,7 +1582,39 @@ static uint32_t spmv_grid(const LaunchCfg& lc) {
     return (lc.max_nodes + R - 1) / R;
 }
 
+uint32_t persistent_pcg_grid(int mixed, int sm_count) {
+    int nb = 0;
+    const cudaError_t e =
+        mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pcg_persistent_kernel<true>, kPersistThreads, 0)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pcg_persistent_kernel<false>, kPersistThreads, 0);
+    return e == cudaSuccess && nb > 0 ? (uint32_t)nb * (uint32_t)sm_count : 0u;
+}
+
+// one cooperative launch: every CTA is resident, so the instance barriers
+// cannot wait on a CTA that has not started
+static cudaError_t launch_pcg_persistent(const LaunchCfg& lc, InstDesc* d, uint32_t iters, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(lc.pcg_bars, 0, sizeof(uint32_t) * 32 * lc.B, st);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(lc.pcg_grid);
+    cfg.blockDim = dim3(kPersistThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const uint32_t B = lc.B;
+    e = lc.precision == MVDR_PRECISION_MIXED
+            ? cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<true>, (const InstDesc*)d, B, iters)
+            : cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<false>, (const InstDesc*)d, B, iters);
+    count_launch();
+    return e;
+}
+
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
+    if (lc.pcg_persistent && lc.mode == MVDR_MODE_MATERIALIZED) return launch_pcg_persistent(lc, d, iters, st);
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     // the update's and direction's grids cover every node / element
     const uint32_t gnode = (lc.max_nodes + 255) / 256;

@@ -47,6 +47,7 @@ enum : uint32_t {
     kErrBinBlockCapacity = 1u << 7,
     kErrNonFinite = 1u << 8,
     kErrBadNodeIndex = 1u << 9,
+    kErrWaitTimeout = 1u << 10,  // a bounded device-side wait gave up
 };
 
 // ------------------------------------------------------------- math ----
@@ -306,6 +307,7 @@ struct InstDesc {
     float* jp;              // matrix-free scratch: J.p per scalar term
     double* partials;       // per-CTA partial sums: 4 regions of part_stride
     uint32_t part_stride;   // >= the CTAs per instance of any launch
+    uint32_t* pcg_bar;      // persistent PCG: this instance's barrier counter (batch-owned)
     double* energy;         // [max GN iterations + 1]
 
     // capacities
@@ -322,12 +324,19 @@ struct LaunchCfg {
     int precision, mode;
     int sm_count;
     int spmv_shape;  // index into the SpMV tile shapes (chosen by the autotuner)
+    // persistent PCG: one cooperative launch per PCG solve (materialised mode)
+    int pcg_persistent;
+    uint32_t pcg_grid;   // co-resident CTAs of pcg_persistent_kernel
+    uint32_t* pcg_bars;  // B barrier counters, 32 words apart
 };
 
 // ----------------------------------------------------------- launchers --
 // Each launcher enqueues kernels on `st` for all instances. They return
 // cudaGetLastError() of the last launch.
 void count_launch();
+
+// co-resident CTAs of the persistent PCG kernel on this device (0 on error)
+uint32_t persistent_pcg_grid(int mixed, int sm_count);
 
 // raise the dynamic shared-memory limit of the segment-sort kernels
 cudaError_t set_index_smem_limits(size_t seg_bytes);

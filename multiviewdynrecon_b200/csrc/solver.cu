@@ -73,6 +73,7 @@ struct Batch {
     uint32_t cap_edges = 0;
     std::vector<InstDesc> host;
     InstDesc* d_inst = nullptr;
+    uint32_t* d_bars = nullptr;  // persistent PCG barrier counters
     void* arena = nullptr;
     size_t arena_bytes = 0;
     size_t per_inst_bytes = 0;
@@ -112,6 +113,7 @@ Batch::~Batch() {
     for (auto& o : owned)
         if (o.mem) cudaFree(o.mem);
     if (d_inst) cudaFree(d_inst);
+    if (d_bars) cudaFree(d_bars);
     if (arena) cudaFree(arena);
     for (auto* v : views) delete v;
 }
@@ -302,6 +304,7 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     }
     e = cudaMemset(b->arena, 0, b->arena_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_inst, sizeof(InstDesc) * B);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_bars, sizeof(uint32_t) * 32 * B);
     if (e != cudaSuccess) {
         delete b;
         return fail(MVDR_ECUDA, std::string("workspace setup failed: ") + cudaGetErrorString(e));
@@ -313,7 +316,11 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
         InstDesc& I = b->host[i];
         std::memset(&I, 0, sizeof(I));
         layout_instance(a, I, lc, b->cap_edges, lc.max_tp, lc.max_tc, gmax);
+        I.pcg_bar = b->d_bars + 32 * i;
     }
+    b->lc.pcg_bars = b->d_bars;
+    b->lc.pcg_persistent = 0;
+    b->lc.pcg_grid = persistent_pcg_grid(lc.precision == MVDR_PRECISION_MIXED, lc.sm_count);
     b->owned.resize(B);
     b->has_inputs.assign(B, 0);
     b->uploaded.resize(B);
@@ -653,6 +660,7 @@ static int check_flags(const DeviceCounts& c) {
         return fail(MVDR_ECAPACITY, buf);
     }
     if (c.error_flags & kErrBadNodeIndex) return fail(MVDR_EINVAL, "node or surfel index out of range in inputs");
+    if (c.error_flags & kErrWaitTimeout) return fail(MVDR_ETIMEOUT, "a bounded device-side wait gave up");
     return MVDR_OK;
 }
 
@@ -972,6 +980,17 @@ int mvdr_batch_set_spmv_shape(mvdr_batch* bh, uint32_t shape) {
     if (!bh || shape >= (uint32_t)kNumSpmvShapes) return fail(MVDR_EINVAL, "bad batch or SpMV shape");
     Batch& b = *bh->batch;
     b.lc.spmv_shape = (int)shape;
+    for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
+    b.graphs.clear();
+    return MVDR_OK;
+}
+
+int mvdr_batch_set_pcg_persistent(mvdr_batch* bh, int on) {
+    if (!bh) return fail(MVDR_EINVAL, "batch is null");
+    Batch& b = *bh->batch;
+    if (on && b.cfg.mode != MVDR_MODE_MATERIALIZED) return fail(MVDR_EINVAL, "persistent PCG needs the materialised mode");
+    if (on && b.lc.pcg_grid < b.B) return fail(MVDR_EINVAL, "more instances than co-resident persistent CTAs");
+    b.lc.pcg_persistent = on ? 1 : 0;
     for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
     b.graphs.clear();
     return MVDR_OK;

@@ -236,6 +236,11 @@ class BatchSolver:
                                         C.byref(form)))
         return (rows.value, split.value, form.value), [t for t in times[:abi.NUM_SPMV_SHAPES]]
 
+    def set_pcg_persistent(self, on=True):
+        """One persistent cooperative launch per PCG solve (materialised
+        mode) instead of three launches per iteration."""
+        check(lib().mvdr_batch_set_pcg_persistent(self.h, 1 if on else 0))
+
     def set_spmv_shape(self, index):
         """Use SpMV tile shape `index` of abi.SPMV_SHAPES for later solves."""
         check(lib().mvdr_batch_set_spmv_shape(self.h, index))

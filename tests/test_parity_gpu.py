@@ -364,6 +364,33 @@ def test_every_spmv_shape_solves_the_same_system(precision, tol):
         assert np.array_equal(results[-1][i], results[-2][i])
 
 
+@pytest.mark.parametrize("precision,tol", [(abi.PRECISION_MIXED, 1e-5), (abi.PRECISION_FP32, 3e-2)])
+def test_persistent_pcg_solves_the_same_system(precision, tol):
+    """The persistent PCG (one cooperative launch per PCG solve, instances of
+    uneven size on their own CTAs and barriers) gives the launched PCG's
+    increments up to the grouping of its dot sums; reruns are bit-identical."""
+    scenes = [small_scene("torso"), small_scene("sphere")]  # both 160 x 120
+    caps = dict(max_nodes=max(s.num_nodes for s in scenes), max_views=3, width=160, height=120,
+                use_foreground=True, use_feature=True, use_cross_view=True,
+                max_surfels=max(s.num_surfels for s in scenes),
+                max_feature_terms=max(s.feature.count for s in scenes),
+                max_cross_terms=max(s.cross_view.count for s in scenes))
+    cfg = abi.make_config(None, precision=precision, **caps)
+    ref, per = BatchSolver(cfg, 2), BatchSolver(cfg, 2)
+    per.set_pcg_persistent(True)
+    out = {}
+    for name, b in (("ref", ref), ("per", per), ("per2", per)):
+        for i, s in enumerate(scenes):
+            b.set_input(i, s)
+        b.solve(3, 10)
+        torch.cuda.synchronize()
+        out[name] = [b.instance(i).get_array(abi.ARRAY_INCREMENT) for i in range(2)]
+        assert all(b.instance(i).counts().error_flags == 0 for i in range(2))
+    for i in range(2):
+        assert rel_norm_error(out["per"][i], out["ref"][i]) < tol
+        assert np.array_equal(out["per"][i], out["per2"][i])
+
+
 def test_autotuned_spmv_shape_solves_the_same_system():
     """mvdr_batch_autotune picks one of the SpMV tile shapes; solves with the
     chosen shape agree with the default shape's (only the order of the row
