@@ -1440,7 +1440,12 @@ __global__ void __launch_bounds__(128) update_kernel(const InstDesc* insts) {
             se3.r[8] = t * ax.z * ax.z + c;
         }
         se3.t[0] = tw[3]; se3.t[1] = tw[4]; se3.t[2] = tw[5];
-        const M34 p = dq_to_mat34(load_dq(I.se3, node));
+        // two 128-bit read-only loads: this kernel's loads of the field are
+        // coalesced (node per thread), the 256-bit form only helps gathers
+        DQ cur;
+        cur.q0 = __ldg(reinterpret_cast<const float4*>(I.se3 + node));
+        cur.q1 = __ldg(reinterpret_cast<const float4*>(I.se3 + node) + 1);
+        const M34 p = dq_to_mat34(cur);
         M34 n;
 #pragma unroll
         for (int r = 0; r < 3; ++r) {

@@ -83,11 +83,13 @@ struct DQ {
     float4 q0, q1;
 };
 
+// one 256-bit load: `field` is the solver's own 32-byte aligned warp field
 __device__ inline DQ load_dq(const DQ* field, uint32_t i) {
-    const float4* p = reinterpret_cast<const float4*>(field + i);
     DQ d;
-    d.q0 = __ldg(p);
-    d.q1 = __ldg(p + 1);
+    asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(d.q0.x), "=f"(d.q0.y), "=f"(d.q0.z), "=f"(d.q0.w), "=f"(d.q1.x), "=f"(d.q1.y), "=f"(d.q1.z),
+                   "=f"(d.q1.w)
+                 : "l"(field + i));
     return d;
 }
 
