@@ -92,7 +92,7 @@ struct ForegroundPred {
 };
 
 template <class Pred>
-__global__ void __launch_bounds__(256) compact_count_kernel(const InstDesc* insts, uint32_t width, uint32_t height,
+__global__ void __launch_bounds__(256, 6) compact_count_kernel(const InstDesc* insts, uint32_t width, uint32_t height,
                                                             uint32_t cpv) {
     const InstDesc& I = insts[blockIdx.y];
     const uint32_t view = blockIdx.x / cpv, c = blockIdx.x % cpv;
@@ -574,7 +574,7 @@ __device__ inline uint2 packed_partners(const InstDesc& I, const TermOffsets& of
     return make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
 }
 
-__global__ void __launch_bounds__(256) np_row_build_kernel(const InstDesc* insts) {
+__global__ void __launch_bounds__(256, 4) np_row_build_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->nodepair_entries > I.cap_k2) return;
