@@ -451,10 +451,10 @@ __device__ inline void add_sym_outer(Acc S[21], const Acc sg[6], const Acc g[6])
 // float).
 constexpr uint32_t kDiagNodes = 32;
 
-// 5 CTAs per SM: the register cap (102) costs a few spilled bytes but the
-// extra warps hide more of the term gathers' latency (-16 % measured)
+// 4 CTAs per SM (128 registers, no spills): with the term loads software-
+// pipelined, fewer but spill-free warps win (measured against 5 CTAs)
 template <bool MIXED>
-__global__ void __launch_bounds__(128, 5) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
+__global__ void __launch_bounds__(128, 4) diag_rhs_kernel(const InstDesc* insts, mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
     __shared__ Acc s_blocks[kDiagNodes][21];
     const InstDesc& I = insts[blockIdx.y];
@@ -474,15 +474,37 @@ __global__ void __launch_bounds__(128, 5) diag_rhs_kernel(const InstDesc* insts,
             for (int q = 0; q < 21; ++q) S[q] = 0;
 #pragma unroll
             for (int q = 0; q < 6; ++q) R[q] = 0;
-            for (uint32_t p = b0 + lane; p < b1; p += 32) {
+            // software pipeline over the lane's terms: the term id two steps
+            // ahead and the pixel-term record and weight one step ahead are in
+            // flight while the current term is summed
+            uint32_t t1 = b0 + lane < b1 ? I.n2t_index[b0 + lane] : kInvalid;
+            uint32_t t2 = b0 + lane + 32 < b1 ? I.n2t_index[b0 + lane + 32] : kInvalid;
+            float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+            float pw = 0.f;
+            auto fetch_pixel_term = [&](uint32_t t, uint32_t pp) {
                 uint32_t k;
-                const TermType ty = off.typed(I.n2t_index[p], k);
+                const TermType ty = off.typed(t, k);
                 if (ty == kDense || ty == kForeground) {
                     const uint32_t idx = ty == kDense ? k : off.o[0] + k;
-                    const float4 a = I.term_jr[2 * (size_t)idx], b = I.term_jr[2 * (size_t)idx + 1];
+                    pa = I.term_jr[2 * (size_t)idx];
+                    pb = I.term_jr[2 * (size_t)idx + 1];
+                    pw = I.n2t_w[pp];
+                }
+            };
+            if (b0 + lane < b1) fetch_pixel_term(t1, b0 + lane);
+            for (uint32_t p = b0 + lane; p < b1; p += 32) {
+                const uint32_t t = t1;
+                const float4 a = pa, b = pb;
+                const float wf = pw;
+                t1 = t2;
+                if (p + 64 < b1) t2 = I.n2t_index[p + 64];
+                if (p + 32 < b1) fetch_pixel_term(t1, p + 32);
+                uint32_t k;
+                const TermType ty = off.typed(t, k);
+                if (ty == kDense || ty == kForeground) {
                     if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0, r = 0
                     const Acc l2 = ty == kDense ? (Acc)1 : l2_fg;
-                    const Acc w = (Acc)I.n2t_w[p];
+                    const Acc w = (Acc)wf;
                     const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
                     const Acc sw = l2 * w * w, rw = -l2 * w * (Acc)b.z;
 #pragma unroll
