@@ -21,8 +21,6 @@ MODE_MATERIALIZED, MODE_MATRIX_FREE = 0, 1
 COMPAT_REF_VIEW_LOOKUP = 1
 (STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE,
  STAGE_DIRECTION) = range(8)
-# candidate SpMV tile shapes (block rows per CTA, threads per scalar row), in
-# the order mvdr_batch_autotune reports their times
 # SpMV tile shapes (block rows per CTA, threads per scalar row / 6, form) in
 # the autotuner's order. Form 0 reads a lower block's row and exchanges the
 # column sums through shared memory; form 1 reads its column.
