@@ -1600,10 +1600,15 @@ cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty
 }
 
 cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t slot, cudaStream_t st) {
-    const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 4);
+    // one CTA per SM and instance: few CTAs meet at the last-CTA reduction
+    const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count);
     MVDR_LAUNCH(energy_kernel, grid2(g, lc.B), 256, 0, st, d, lam, slot);
     return cudaGetLastError();
 }
+
+// PCG init and update: a thread per node in CTAs of 64, so that the small
+// grid spreads over every SM
+constexpr uint32_t kPcgNodeThreads = 64;
 
 // CTAs per instance of the SpMV launch with the current shape
 static uint32_t spmv_grid(const LaunchCfg& lc) {
@@ -1646,12 +1651,12 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     if (lc.pcg_persistent && lc.mode == MVDR_MODE_MATERIALIZED) return launch_pcg_persistent(lc, d, iters, st);
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     // the update's and direction's grids cover every node / element
-    const uint32_t gnode = (lc.max_nodes + 255) / 256;
+    const uint32_t gnode = (lc.max_nodes + kPcgNodeThreads - 1) / kPcgNodeThreads;
     const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gwarp = (lc.max_nodes + 7) / 8;
     const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-    if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d);
-    else MVDR_LAUNCH(pcg_init_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d);
+    if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
+    else MVDR_LAUNCH(pcg_init_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
     for (uint32_t it = 0; it < iters; ++it) {
         const int parity = (int)(it & 1u), first = it == 0;
         uint32_t nq;  // CTAs that store the d.q partials
@@ -1669,8 +1674,8 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
             if (e != cudaSuccess) return e;
             nq = spmv_grid(lc);
         }
-        if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, parity, gnode, nq);
-        else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, parity, gnode, nq);
+        if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
+        else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
     }
     return cudaGetLastError();
 }
@@ -1713,7 +1718,7 @@ cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream
 
 cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, int stage, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
-    const uint32_t gnode = (lc.max_nodes + 255) / 256;
+    const uint32_t gnode = (lc.max_nodes + kPcgNodeThreads - 1) / kPcgNodeThreads;
     const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     switch (stage) {
@@ -1735,8 +1740,8 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
             break;
         case MVDR_STAGE_PCG_UPDATE:
-            if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), 256, 0, st, d, 0, gnode, spmv_grid(lc));
-            else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), 256, 0, st, d, 0, gnode, spmv_grid(lc));
+            if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
+            else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
             break;
         case MVDR_STAGE_UPDATE: return launch_update(lc, d, st);
         default: return cudaErrorInvalidValue;
