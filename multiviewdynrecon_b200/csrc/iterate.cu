@@ -12,9 +12,8 @@
 //
 // Accumulation: every per-node and per-pair sum is a warp-shuffle reduction
 // of lane partials; global reductions use per-CTA partials summed in a fixed
-// order, by the kernel that consumes them (PCG dots) or by the last CTA
-// (energy). No floating-point atomics, so every result is reproducible run to
-// run.
+// order by the kernel that consumes them (PCG dots, energy). No floating-point
+// atomics, so every result is reproducible run to run.
 #include <type_traits>
 
 #include "kernels_common.cuh"
@@ -113,13 +112,15 @@ __device__ inline R34T<T> blended_se3(const DQ* field, const unsigned short* nod
 // 4 CTAs per SM (64 registers, a few spilled) hide the gathers of the warp
 // field and the maps better than 2 (-32 % measured)
 template <class T>
-__global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* insts) {
+__global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* insts, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
-    if (bad_inputs(I)) return;
     TermOffsets off;
     off.load(I.counts);
     const uint32_t Td = off.o[0];
-    const uint32_t T_all = off.o[4];
+    const uint32_t T_all = bad_inputs(I) ? 0u : off.o[4];
+    // the lambda-weighted squared residuals of this CTA's terms
+    // (ResidualEvaluator.cu:71-226): the energy of the linearisation point
+    double energy = 0;
     const float clip = 64.f * I.node_radius * I.node_radius;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T_all; t += gridDim.x * blockDim.x) {
         uint32_t k;
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             }
             I.term_jr[2 * (size_t)k] = o0;
             I.term_jr[2 * (size_t)k + 1] = o1;
+            energy += (double)o1.z * o1.z;
         } else if (ty == kSmooth) {
             // forwardWarpSmootherNodeKernel (NodeGraphSmoothHandler.cu:10-43)
             const ushort2 e = I.graph[k];
@@ -180,7 +182,12 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             const float valid = dot3(dd, dd) > clip ? 0.f : 1.f;
             I.smooth[3 * (size_t)k] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)b.x);
             I.smooth[3 * (size_t)k + 1] = make_float4((float)b.y, (float)b.z, valid, 0.f);
-            I.smooth[3 * (size_t)k + 2] = make_float4((float)(a.x - b.x), (float)(a.y - b.y), (float)(a.z - b.z), 0.f);
+            const float4 rr = make_float4((float)(a.x - b.x), (float)(a.y - b.y), (float)(a.z - b.z), 0.f);
+            I.smooth[3 * (size_t)k + 2] = rr;
+            if (valid != 0.f) {
+                const float r0 = lam.smooth * rr.x, r1 = lam.smooth * rr.y, r2 = lam.smooth * rr.z;
+                energy += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+            }
         } else if (ty == kForeground) {
             // computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual;
             // the canonical vertex is taken to frame 0 first, as the dense term does
@@ -214,6 +221,10 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             }
             I.term_jr[2 * (size_t)(Td + k)] = o0;
             I.term_jr[2 * (size_t)(Td + k) + 1] = o1;
+            {
+                const float v = lam.foreground * o1.z;
+                energy += (double)v * v;
+            }
         } else if (ty == kFeature || ty == kCross) {
             // forwardWarpFeatureVertexKernel (SparseCorrespondenceHandler.cu:202-220)
             const bool f = ty == kFeature;
@@ -229,7 +240,24 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             const size_t o = 2 * (size_t)(f ? k : I.Tp + k);
             I.warped[o] = make_float4((float)wv.x, (float)wv.y, (float)wv.z, 1.0f);
             I.warped[o + 1] = make_float4((float)raw.x, (float)raw.y, (float)raw.z, 0.0f);
+            const float l = f ? lam.feature : lam.cross_view;
+            const float rv[3] = {(float)raw.x, (float)raw.y, (float)raw.z};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float v = l * (huber_weight(rv[c]) * rv[c]);
+                energy += (double)v * v;
+            }
         }
+    }
+    // one partial per CTA (reduction region 0), summed by energy_sum_kernel
+    __shared__ double ws[8];
+    energy = warp_sum(energy);
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = energy;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double e = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) e += ws[w];
+        I.partials[blockIdx.x] = e;
     }
 }
 
@@ -723,45 +751,6 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
 }
 
 // ----------------------------------------------------------- reductions ---
-// Last-CTA reduction: every CTA of instance blockIdx.y stores a partial; the
-// last CTA to arrive sums them with all its threads in a fixed order (thread t
-// takes partials t, t + blockDim.x, ..., then a fixed tree), so the result is
-// reproducible. Returns true in every thread of that CTA; *total is valid in
-// thread 0. blockDim.x must be a multiple of 32.
-template <class T>
-__device__ inline bool block_partial_and_last(const InstDesc& I, T v, int ticket, T* total) {
-    __shared__ T ws[32];
-    __shared__ bool last;
-    const uint32_t nw = blockDim.x >> 5;
-    v = warp_sum(v);
-    if (lane_id() == 0) ws[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        T s = 0;
-        for (uint32_t w = 0; w < nw; ++w) s += ws[w];
-        I.partials[blockIdx.x] = (double)s;
-        __threadfence();
-        const uint32_t prev = atomicAdd(&I.counts->reduce_ticket[ticket], 1u);
-        last = prev == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    T s = 0;
-    for (uint32_t c = threadIdx.x; c < gridDim.x; c += blockDim.x) s += (T)__ldcg(I.partials + c);
-    s = warp_sum(s);
-    __syncthreads();  // every thread has read ws above
-    if (lane_id() == 0) ws[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        T tsum = 0;
-        for (uint32_t w = 0; w < nw; ++w) tsum += ws[w];
-        *total = tsum;
-        I.counts->reduce_ticket[ticket] = 0;
-    }
-    return true;
-}
-
 // Split reduction for the PCG dots. Every CTA of the producing launch stores
 // its block sum in a region of the partials; a kernel launched after it on
 // the same stream sums the stored partials with one warp in a fixed order.
@@ -1509,40 +1498,21 @@ __global__ void __launch_bounds__(128) update_kernel(const InstDesc* insts) {
 
 // ------------------------------------------------------------- energy -----
 // computeTermResidualKernel (ResidualEvaluator.cu:71-142): sum (lambda r)^2
-__global__ void __launch_bounds__(256) energy_kernel(const InstDesc* insts, mvdr_penalty lam, uint32_t slot) {
+// The energy of the linearisation point: the term evaluation's `count`
+// per-CTA partials summed in a fixed order (one CTA per instance)
+__global__ void __launch_bounds__(256) energy_sum_kernel(const InstDesc* insts, uint32_t count, uint32_t slot) {
     const InstDesc& I = insts[blockIdx.y];
-    TermOffsets off;
-    off.load(I.counts);
-    const uint32_t T = off.o[4];
-    double part = 0;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-        uint32_t k;
-        const TermType ty = off.typed(t, k);
-        if (ty == kDense || ty == kForeground) {
-            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
-            const float l = ty == kDense ? 1.0f : lam.foreground;
-            const float v = l * I.term_jr[2 * (size_t)idx + 1].z;
-            part += (double)v * v;
-        } else if (ty == kSmooth) {
-            const float4 b = I.smooth[3 * (size_t)k + 1], rr = I.smooth[3 * (size_t)k + 2];
-            if (b.z != 0.f) {
-                const float r0 = lam.smooth * rr.x, r1 = lam.smooth * rr.y, r2 = lam.smooth * rr.z;
-                part += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
-            }
-        } else if (ty == kFeature || ty == kCross) {
-            const bool f = ty == kFeature;
-            const float4 rw = I.warped[2 * (size_t)(f ? k : I.Tp + k) + 1];
-            const float l = f ? lam.feature : lam.cross_view;
-            const float raw[3] = {rw.x, rw.y, rw.z};
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float v = l * (huber_weight(raw[c]) * raw[c]);
-                part += (double)v * v;
-            }
-        }
+    __shared__ double ws[8];
+    double e = 0;
+    for (uint32_t c = threadIdx.x; c < count; c += blockDim.x) e += I.partials[c];
+    e = warp_sum(e);
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) tot += ws[w];
+        I.energy[slot] = tot;
     }
-    double tot;
-    if (block_partial_and_last<double>(I, part, 3, &tot) && threadIdx.x == 0) I.energy[slot] = tot;
 }
 
 // --------------------------------------------------------- exports -------
@@ -1579,10 +1549,14 @@ __global__ void export_preconditioner_kernel(const InstDesc* insts, uint32_t ins
 
 static inline dim3 grid2(uint32_t x, uint32_t B) { return dim3(x ? x : 1, B); }
 
-cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, cudaStream_t st) {
-    const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(eval_terms_kernel<double>, grid2(g, lc.B), 256, 0, st, d);
-    else MVDR_LAUNCH(eval_terms_kernel<float>, grid2(g, lc.B), 256, 0, st, d);
+static uint32_t eval_terms_grid(const LaunchCfg& lc) {
+    return min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
+}
+
+cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, cudaStream_t st) {
+    const uint32_t g = eval_terms_grid(lc);
+    if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(eval_terms_kernel<double>, grid2(g, lc.B), 256, 0, st, d, lam);
+    else MVDR_LAUNCH(eval_terms_kernel<float>, grid2(g, lc.B), 256, 0, st, d, lam);
     return cudaGetLastError();
 }
 
@@ -1599,10 +1573,8 @@ cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty
     return cudaGetLastError();
 }
 
-cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t slot, cudaStream_t st) {
-    // one CTA per SM and instance: few CTAs meet at the last-CTA reduction
-    const uint32_t g = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count);
-    MVDR_LAUNCH(energy_kernel, grid2(g, lc.B), 256, 0, st, d, lam, slot);
+cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, uint32_t slot, cudaStream_t st) {
+    MVDR_LAUNCH(energy_sum_kernel, grid2(1, lc.B), 256, 0, st, d, eval_terms_grid(lc), slot);
     return cudaGetLastError();
 }
 
@@ -1722,7 +1694,7 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
     const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
     switch (stage) {
-        case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, st);
+        case MVDR_STAGE_TERMS: return launch_eval_terms(lc, d, lam, st);
         case MVDR_STAGE_DIAG:
             if (mixed) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 128, 0, st, d, lam);
             else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);

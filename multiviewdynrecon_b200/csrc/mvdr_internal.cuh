@@ -200,7 +200,7 @@ struct DeviceCounts {
     uint32_t term_offset[5];  // prefix ends of Dense, Smooth, Foreground, Feature, Cross
     uint32_t dense_view_count[MVDR_MAX_VIEWS];
     uint32_t fg_view_count[MVDR_MAX_VIEWS];
-    uint32_t reduce_ticket[4];  // last-block reduction counters
+    uint32_t reduce_ticket[4];  // unused (keeps the record's layout)
 };
 
 struct InstDesc {
@@ -354,11 +354,11 @@ extern const SpmvShape kSpmvShapes[kNumSpmvShapes];
 cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st);
 
 cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
-cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
+// term evaluation; also stores the energy partials that launch_energy sums
+cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, cudaStream_t st);
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, bool materialize,
                             cudaStream_t st);
-cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t slot,
-                          cudaStream_t st);
+cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d_inst, uint32_t slot, cudaStream_t st);
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t iters,
                        cudaStream_t st);
 cudaError_t launch_update(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);

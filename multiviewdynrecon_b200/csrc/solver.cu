@@ -211,7 +211,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     }
     // J.p per scalar term of the matrix-free operator (double in mixed precision)
     I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
-    // region 0: last-CTA reductions; 1, 2: PCG delta by iteration parity; 3: d.q
+    // region 0: energy; 1, 2: PCG delta by iteration parity; 3: d.q
     I.partials = a.take<double>(4 * (size_t)partial_slots);
     I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
@@ -589,8 +589,8 @@ static int enqueue_index(Batch& b, cudaStream_t st) {
 
 static int enqueue_iteration(Batch& b, uint32_t iter, uint32_t pcg, cudaStream_t st) {
     const mvdr_penalty lam = penalty_for(b.cfg, iter);
-    CU(launch_eval_terms(b.lc, b.d_inst, st));
-    CU(launch_energy(b.lc, b.d_inst, lam, std::min<uint32_t>(iter, 63), st));
+    CU(launch_eval_terms(b.lc, b.d_inst, lam, st));
+    CU(launch_energy(b.lc, b.d_inst, std::min<uint32_t>(iter, 63), st));
     CU(launch_assemble(b.lc, b.d_inst, lam, b.cfg.mode == MVDR_MODE_MATERIALIZED, st));
     CU(launch_pcg(b.lc, b.d_inst, lam, pcg, st));
     CU(launch_update(b.lc, b.d_inst, st));
