@@ -643,7 +643,7 @@ def main():
             "config": {"workload": WORKLOAD, "instances_per_gpu": args.batch, "views": 3,
                        "image": [args.width, args.height], "nodes": args.nodes, "gn": args.gn, "pcg": args.pcg,
                        "precision": args.precision, "mode": args.mode, "graph": True,
-                       "pcg": "persistent" if args.pcg_persistent else "launches",
+                       "pcg_form": "persistent" if args.pcg_persistent else "launches",
                        "l2": "aggregate working set of the batch well above the 126 MB L2; no flush",
                        "dense_terms": c.dense_terms, "half_pairs": c.half_pairs,
                        "parallelism": f"independent instances, {world} GPU(s), no collective in the solve"},
