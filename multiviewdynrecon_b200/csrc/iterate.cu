@@ -468,9 +468,9 @@ __device__ inline void add_sym_outer(Acc S[21], const Acc sg[6], const Acc g[6])
 // ---------------------------------------------------- diagonal blocks ----
 // One warp per node. The lanes take the node's terms round-robin and keep
 // D_i = sum_t lambda_t^2 w_ti^2 sum_c g_c g_c^T (21 upper-triangle sums) and
-// b_i = -sum_t lambda_t^2 w_ti sum_c g_c r_c (6 sums) in registers; one fixed
-// butterfly then reduces the 27 sums across the warp, so the result does not
-// depend on scheduling. computeBlockDiagonalPreconditionerKernel and
+// b_i = -sum_t lambda_t^2 w_ti sum_c g_c r_c (6 sums) in registers; a fixed
+// reduce-scatter (five halving exchanges) then leaves each of 27 lanes with
+// one warp total, so the result does not depend on scheduling. computeBlockDiagonalPreconditionerKernel and
 // computeJtResidualWithIndexKernel (PreconditionerBlocked.cu:18-399,
 // JtDotResidualIndexed.cu:18-382) compute the same sums. A CTA takes
 // kDiagNodes nodes; their damped blocks wait in shared memory and one warp
@@ -493,6 +493,11 @@ __global__ void __launch_bounds__(128, 4) diag_rhs_kernel(const InstDesc* insts,
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const Acc l2_fg = (Acc)(lam.foreground * lam.foreground), l2_smooth = (Acc)(lam.smooth * lam.smooth);
     const Acc l2_feat = (Acc)(lam.feature * lam.feature), l2_cross = (Acc)(lam.cross_view * lam.cross_view);
+    // the upper-triangle entry (orr, okk) of D whose total this lane receives
+    uint32_t orr = 0, okk = 0;
+    for (uint32_t r = 0, q = 0; r < 6; ++r)
+        for (uint32_t k = r; k < 6; ++k, ++q)
+            if (q == lane) { orr = r; okk = k; }
     for (uint32_t base = blockIdx.x * kDiagNodes; base < I.N; base += gridDim.x * kDiagNodes) {
         for (uint32_t j = warp; j < kDiagNodes && base + j < I.N; j += nwarps) {
             const uint32_t node = base + j;
@@ -580,32 +585,38 @@ __global__ void __launch_bounds__(128, 4) diag_rhs_kernel(const InstDesc* insts,
                     }
                 }
             }
-            // fixed-order butterfly: every lane ends with the warp totals
+            // fixed-order reduce-scatter: five halving steps leave lane q with
+            // the warp total of value q (q < 21: D entry q, 21 + k: b_k)
+            Acc v[32];
 #pragma unroll
-            for (int q = 0; q < 21; ++q) S[q] = warp_sum(S[q]);
+            for (int q = 0; q < 21; ++q) v[q] = S[q];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) R[q] = warp_sum(R[q]);
+            for (int q = 0; q < 6; ++q) v[21 + q] = R[q];
 #pragma unroll
-            for (int r = 0; r < 6; ++r) S[sym_idx(r, r)] += (Acc)1e-2f;  // damping
+            for (int q = 27; q < 32; ++q) v[q] = 0;
+#pragma unroll
+            for (int dist = 16; dist > 0; dist >>= 1) {
+                const bool upper = (lane & (uint32_t)dist) != 0;
+#pragma unroll
+                for (int i = 0; i < dist; ++i) {
+                    const Acc keep = upper ? v[i + dist] : v[i];
+                    const Acc send = upper ? v[i] : v[i + dist];
+                    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, dist);
+                }
+            }
+            const Acc tot = v[0];
             const size_t blk = 36 * (size_t)(I.half_offset[node] + node);
             typename BlockStore<MIXED>::V* store = BlockStore<MIXED>::ptr(I);
-            // lanes 0..35 of the block (lanes 0..3 write two elements)
-#pragma unroll
-            for (int r = 0; r < 6; ++r)
-#pragma unroll
-                for (int k2 = 0; k2 < 6; ++k2) {
-                    const uint32_t i = 6 * r + k2;
-                    if (i % 32 != lane) continue;
-                    const Acc v = S[r <= k2 ? sym_idx(r, k2) : sym_idx(k2, r)];
-                    I.diag[36 * (size_t)node + i] = (float)v;
-                    store[blk + blk_idx(r, k2)] = v;
-                }
-#pragma unroll
-            for (int q = 0; q < 6; ++q)
-                if (lane == (uint32_t)(q + 8)) PcgVec<MIXED>::jtr(I)[6 * (size_t)node + q] = R[q];
-#pragma unroll
-            for (int q = 0; q < 21; ++q)
-                if (lane == (uint32_t)q) s_blocks[j][q] = S[q];
+            if (lane < 21) {
+                const Acc d = tot + (orr == okk ? (Acc)1e-2f : (Acc)0);  // damping
+                I.diag[36 * (size_t)node + 6 * orr + okk] = (float)d;
+                I.diag[36 * (size_t)node + 6 * okk + orr] = (float)d;
+                store[blk + blk_idx(orr, okk)] = d;
+                store[blk + blk_idx(okk, orr)] = d;
+                s_blocks[j][lane] = d;
+            } else if (lane < 27) {
+                PcgVec<MIXED>::jtr(I)[6 * (size_t)node + lane - 21] = tot;
+            }
         }
         __syncthreads();
         if (warp == 0 && base + lane < I.N) {
