@@ -1400,14 +1400,27 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
                 for (int i = 0; i < 6; ++i) acc[i] += sc * (T)tr.J[c][i] * y;
             }
         }
-#pragma unroll
-        for (int i = 0; i < 6; ++i) acc[i] = warp_sum(acc[i]);
+        // fixed-order reduce-scatter of the 6 sums (padded to 8): three
+        // halving exchanges leave value q with lanes 4q .. 4q + 3, two
+        // butterfly steps finish it
         const uint32_t lane = lane_id();
-        if (lane < 6) {
-            T a = 0;
+        T v[8] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], (T)0, (T)0};
 #pragma unroll
-            for (int q = 0; q < 6; ++q) a = (q == (int)lane) ? acc[q] : a;
-            const size_t el = 6 * (size_t)node + lane;
+        for (int dist = 16, n = 4; dist >= 4; dist >>= 1, n >>= 1) {
+            const bool upper = (lane & (uint32_t)dist) != 0;
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                const T keep = upper ? v[i + n] : v[i];
+                const T send = upper ? v[i] : v[i + n];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, dist);
+            }
+        }
+        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+        const uint32_t qi = lane >> 2;
+        if ((lane & 3u) == 0 && qi < 6) {
+            const T a = v[0];
+            const size_t el = 6 * (size_t)node + qi;
             const T dv = pcg ? PV::s(I)[el] + beta * dprev[el] : (T)xin[el];
             const T qv = a + (T)1e-2f * dv;
             if (pcg) {
