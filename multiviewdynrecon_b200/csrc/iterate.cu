@@ -1315,26 +1315,52 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
 }
 
 // ------------------------------------------------------ matrix-free JtJ ---
-// J.p per term (ApplyJacobianDot.cu:127-198): jp[3t + c] for each channel,
-// with p = s + beta * d_prev formed on the fly when `fused` is set
+// J.p per term (ApplyJacobianDot.cu:127-198), stored channel-major:
+// jp[c * T + t], T the solve's term count. A pixel term's rows for its nodes
+// are one Jacobian row scaled by each node's skinning weight, so its J.p is
+// that row times the weight-blended p (one record load per term). With
+// `fused` set p is the PCG direction d of this iteration, else xin.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
-                                                      int first, uint32_t nd, mvdr_penalty lam) {
+                                                      mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
     if (bad_inputs(I)) return;
     TermOffsets off;
     off.load(I.counts);
     const uint32_t T = off.o[4];
-    using PV = PcgVec<MIXED>;
-    const typename PV::T beta = fused ? pcg_beta<typename PV::T>(I, parity, first, nd) : 0;
-    const typename PV::T* sv = PV::s(I);
-    const typename PV::T* dp = PV::d(I, !parity);
+    const typename PcgVec<MIXED>::T* dv = PcgVec<MIXED>::d(I, parity);
+    // mixed precision keeps J.p in double (jp holds 3 doubles per term)
+    Acc* jp = reinterpret_cast<Acc*>(I.jp);
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         uint32_t k;
         const TermType ty = off.typed(t, k);
         const ushort4 nn = term_nodes(I, ty, k);
         const unsigned short nodes[4] = {nn.x, nn.y, nn.z, nn.w};
+        if (ty == kDense || ty == kForeground) {
+            const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+            float4 ra, rb;
+            load_record32(I.term_jr + 2 * (size_t)idx, ra, rb);
+            const float4 w4 = term_weights(I, ty, k);
+            Acc pb[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t node = nodes[q];
+                if (node >= I.N) continue;
+                const Acc w = (Acc)weight_of(nn, w4, node);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    const size_t e = 6 * (size_t)node + i;
+                    pb[i] += w * (fused ? (Acc)dv[e] : (Acc)xin[e]);
+                }
+            }
+            const Acc g[6] = {(Acc)ra.x, (Acc)ra.y, (Acc)ra.z, (Acc)ra.w, (Acc)rb.x, (Acc)rb.y};
+            Acc o = 0;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) o += g[i] * pb[i];
+            jp[t] = o;
+            continue;
+        }
         const int m = ty == kSmooth ? 2 : 4;
         Acc out[3] = {0, 0, 0};
         for (int q = 0; q < m; ++q) {
@@ -1346,7 +1372,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
                 const size_t e = 6 * (size_t)node + i;
-                p[i] = fused ? (Acc)(sv[e] + beta * dp[e]) : (Acc)xin[e];
+                p[i] = fused ? (Acc)dv[e] : (Acc)xin[e];
             }
             for (int c = 0; c < ch; ++c) {
                 Acc a = 0;
@@ -1355,47 +1381,54 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
                 out[c] += (Acc)tr.w * a;
             }
         }
-        // mixed precision keeps J.p in double (jp holds 3 doubles per term)
-        if (MIXED) {
-            double* jp = reinterpret_cast<double*>(I.jp);
-            jp[3 * (size_t)t] = out[0];
-            jp[3 * (size_t)t + 1] = out[1];
-            jp[3 * (size_t)t + 2] = out[2];
-        } else {
-            I.jp[3 * (size_t)t] = (float)out[0];
-            I.jp[3 * (size_t)t + 1] = (float)out[1];
-            I.jp[3 * (size_t)t + 2] = (float)out[2];
-        }
+        jp[t] = out[0];
+        jp[(size_t)T + t] = out[1];
+        jp[2 * (size_t)T + t] = out[2];
     }
 }
 
 // Jt.y per node (ApplyJacobianTransposeDot.cu:29-155) plus the 1e-2 damping;
-// warp per node. With `pcg` set it also forms this node's direction d, stores
-// q and the d.q partial, like pcg_spmv_kernel.
+// warp per node, the lanes over its terms. A pixel term's row is its record
+// scaled by the entry's recorded skinning weight. With `pcg` set the operand
+// is this iteration's direction d; the kernel stores q and the d.q partial,
+// like pcg_spmv_kernel.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
-                                                       int parity, int first, uint32_t nd, mvdr_penalty lam) {
+                                                       int parity, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
     using T = typename std::conditional<MIXED, double, float>::type;
     TermOffsets off;
     off.load(I.counts);
+    const uint32_t Tn = off.o[4];
     using PV = PcgVec<MIXED>;
-    const T* dprev = PV::d(I, !parity);
-    T* dcur = PV::d(I, parity);
-    const T beta = pcg ? pcg_beta<T>(I, parity, first, nd) : (T)0;
+    const T* dcur = PV::d(I, parity);
+    const T* jp = reinterpret_cast<const T*>(I.jp);
+    const T l2_fg = (T)(lam.foreground * lam.foreground);
     T part = 0;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
         T acc[6] = {0, 0, 0, 0, 0, 0};
         const uint32_t b = I.n2t_offset[node], e = I.n2t_offset[node + 1];
-        const double* jpd = reinterpret_cast<const double*>(I.jp);
         for (uint32_t p = b + lane_id(); p < e; p += 32) {
             const uint32_t t = I.n2t_index[p];
+            uint32_t k;
+            const TermType ty = off.typed(t, k);
+            if (ty == kDense || ty == kForeground) {
+                const uint32_t idx = ty == kDense ? k : off.o[0] + k;
+                float4 ra, rb;
+                load_record32(I.term_jr + 2 * (size_t)idx, ra, rb);
+                const T sc = (ty == kDense ? (T)1 : l2_fg) * (T)I.n2t_w[p];
+                const T y = jp[t];
+                const float g[6] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y};
+#pragma unroll
+                for (int i = 0; i < 6; ++i) acc[i] += sc * (T)g[i] * y;
+                continue;
+            }
             TermRows tr;
             const int ch = term_rows(I, off, lam, t, node, tr);
             const T sc = (T)tr.lam2 * (T)tr.w;
             for (int c = 0; c < ch; ++c) {
-                const T y = MIXED ? (T)jpd[3 * (size_t)t + c] : (T)I.jp[3 * (size_t)t + c];
+                const T y = jp[(size_t)c * Tn + t];
 #pragma unroll
                 for (int i = 0; i < 6; ++i) acc[i] += sc * (T)tr.J[c][i] * y;
             }
@@ -1419,12 +1452,10 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
         v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
         const uint32_t qi = lane >> 2;
         if ((lane & 3u) == 0 && qi < 6) {
-            const T a = v[0];
             const size_t el = 6 * (size_t)node + qi;
-            const T dv = pcg ? PV::s(I)[el] + beta * dprev[el] : (T)xin[el];
-            const T qv = a + (T)1e-2f * dv;
+            const T dv = pcg ? dcur[el] : (T)xin[el];
+            const T qv = v[0] + (T)1e-2f * dv;
             if (pcg) {
-                dcur[el] = dv;
                 PV::q(I)[el] = qv;
                 part += dv * qv;
             } else {
@@ -1657,11 +1688,13 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
         const int parity = (int)(it & 1u), first = it == 0;
         uint32_t nq;  // CTAs that store the d.q partials
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
-            // J.(s + beta d_prev) per term, then Jt per node (+ damping, d, q, d.q)
-            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, first, gnode, lam);
-            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, first, gnode, lam);
-            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, first, gnode, lam);
-            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, first, gnode, lam);
+            // d = s + beta d_prev, J.d per term, then Jt per node (+ damping, q, d.q)
+            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
+            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
+            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
+            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             nq = gwarp;
         } else {
             if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
@@ -1758,11 +1791,11 @@ cudaError_t launch_apply_jtj(const LaunchCfg& lc, InstDesc* d, const mvdr_penalt
     if (lc.mode == MVDR_MODE_MATRIX_FREE) {
         const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
         if (lc.precision == MVDR_PRECISION_MIXED) {
-            MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, 1, 0u, lam);
-            MVDR_LAUNCH(apply_jt_kernel<true>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, 1, 0u, lam);
+            MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
+            MVDR_LAUNCH(apply_jt_kernel<true>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
         } else {
-            MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, 1, 0u, lam);
-            MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, 1, 0u, lam);
+            MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
+            MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
         }
     } else {
         if (lc.precision == MVDR_PRECISION_MIXED)
