@@ -1687,18 +1687,17 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     for (uint32_t it = 0; it < iters; ++it) {
         const int parity = (int)(it & 1u), first = it == 0;
         uint32_t nq;  // CTAs that store the d.q partials
+        // d = s + beta d_prev, then q = A d with its d.q partials
+        if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+        else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
-            // d = s + beta d_prev, J.d per term, then Jt per node (+ damping, q, d.q)
-            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
-            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+            // J.d per term, then Jt per node (+ damping, q, d.q)
             if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
             else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
             if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
             nq = gwarp;
         } else {
-            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
-            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
             const cudaError_t e = launch_spmv(lc, d, parity, st);
             if (e != cudaSuccess) return e;
             nq = spmv_grid(lc);
