@@ -402,7 +402,10 @@ enum {
     MVDR_STAGE_SPMV = 4,       /* one PCG SpMV (q = A d, d.q) on the current d   */
     MVDR_STAGE_PCG_UPDATE = 5, /* one PCG vector update (x, r, s, r.s)           */
     MVDR_STAGE_UPDATE = 6,     /* warp-field update                              */
-    MVDR_STAGE_DIRECTION = 7   /* one PCG direction update d = s + beta d_prev   */
+    MVDR_STAGE_DIRECTION = 7,  /* one PCG direction update d = s + beta d_prev   */
+    MVDR_STAGE_MATRIX_FREE = 8 /* one matrix-free product q = (JtJ + 1e-2 I) d
+                                  and d.q, as J.d per term then Jt per node
+                                  (matrix-free mode only; EINVAL otherwise)      */
 };
 /* Enqueue the kernels of one stage for every instance of the batch, with the
  * lambdas of Gauss-Newton iteration 0. The stage reads the state left by the

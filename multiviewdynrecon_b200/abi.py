@@ -20,7 +20,7 @@ PRECISION_FP32, PRECISION_MIXED = 0, 1
 MODE_MATERIALIZED, MODE_MATRIX_FREE = 0, 1
 COMPAT_REF_VIEW_LOOKUP = 1
 (STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE,
- STAGE_DIRECTION) = range(8)
+ STAGE_DIRECTION, STAGE_MATRIX_FREE) = range(9)
 # SpMV tile shapes (block rows per CTA, threads per scalar row / 6, form) in
 # the autotuner's order. Form 0 reads a lower block's row and exchanges the
 # column sums through shared memory; form 1 reads its column.

@@ -1772,6 +1772,16 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
             break;
         case MVDR_STAGE_UPDATE: return launch_update(lc, d, st);
+        case MVDR_STAGE_MATRIX_FREE: {
+            // the launches of one matrix-free PCG iteration after its direction
+            const uint32_t gwarp = (lc.max_nodes + 7) / 8;
+            const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
+            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, 0, 1, lam);
+            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, 0, 1, lam);
+            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, 0, lam);
+            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, 0, lam);
+            break;
+        }
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -1008,7 +1008,10 @@ int mvdr_batch_enqueue_stage(mvdr_batch* b, int stage, void* stream) {
     int rc = all_bound(bb);
     if (rc != MVDR_OK) return rc;
     if (stage == MVDR_STAGE_INDEX) return enqueue_index(bb, (cudaStream_t)stream);
-    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_DIRECTION) return fail(MVDR_EINVAL, "unknown stage");
+    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_MATRIX_FREE) return fail(MVDR_EINVAL, "unknown stage");
+    // the J.d scratch exists only in the matrix-free mode
+    if (stage == MVDR_STAGE_MATRIX_FREE && bb.cfg.mode != MVDR_MODE_MATRIX_FREE)
+        return fail(MVDR_EINVAL, "the matrix-free stage needs the matrix-free mode");
     CU(launch_stage(bb.lc, bb.d_inst, penalty_for(bb.cfg, 0), stage, (cudaStream_t)stream));
     return MVDR_OK;
 }

@@ -413,3 +413,26 @@ def test_autotuned_spmv_shape_solves_the_same_system():
         xa = ref.instance(i).get_array(abi.ARRAY_INCREMENT)
         xb = tuned.instance(i).get_array(abi.ARRAY_INCREMENT)
         assert rel_norm_error(xb, xa) < 1e-5
+
+
+def test_matrix_free_stage_only_in_matrix_free_mode():
+    """mvdr_batch_enqueue_stage(MVDR_STAGE_MATRIX_FREE) runs one matrix-free
+    PCG product on the state of the last solve; its J.d scratch exists only in
+    the matrix-free mode, so the materialised mode rejects it with
+    MVDR_EINVAL and launches nothing."""
+    import ctypes as C
+    from multiviewdynrecon_b200 import lib
+    scene = small_scene("torso")
+    for mode, want in ((abi.MODE_MATRIX_FREE, abi.MVDR_OK), (abi.MODE_MATERIALIZED, abi.MVDR_EINVAL)):
+        b = BatchSolver(abi.make_config(scene, mode=mode), 1)
+        b.set_input(0, scene)
+        b.solve(1, 5)
+        torch.cuda.synchronize()
+        k0 = lib().mvdr_kernel_launch_count()
+        st = lib().mvdr_batch_enqueue_stage(b.h, abi.STAGE_MATRIX_FREE,
+                                            C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        assert st == want
+        assert lib().mvdr_kernel_launch_count() - k0 == (2 if want == abi.MVDR_OK else 0)
+        assert b.instance(0).counts().error_flags == 0
+        b.close()
