@@ -62,3 +62,24 @@ def test_spmv_shape_count_matches_header(L):
     n = int(re.search(r"#define MVDR_NUM_SPMV_SHAPES (\d+)u", text).group(1))
     assert n == abi.NUM_SPMV_SHAPES
     assert L.mvdr_batch_set_spmv_shape(None, 0) == abi.MVDR_EINVAL
+
+
+def test_enum_constants_match_header():
+    """Every MVDR_* enumerator of the header (status codes, precision, mode,
+    stage and array ids) has the value the ctypes mirror uses."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    found = dict((k, int(v)) for k, v in re.findall(r"\b(MVDR_[A-Z0-9_]+)\s*=\s*(\d+)\b", text))
+    mirror = {"MVDR_OK": abi.MVDR_OK, "MVDR_EINVAL": abi.MVDR_EINVAL, "MVDR_ECAPACITY": abi.MVDR_ECAPACITY,
+              "MVDR_ECUDA": abi.MVDR_ECUDA, "MVDR_ETIMEOUT": abi.MVDR_ETIMEOUT,
+              "MVDR_ENONFINITE": abi.MVDR_ENONFINITE, "MVDR_ESTATE": abi.MVDR_ESTATE,
+              "MVDR_PRECISION_FP32": abi.PRECISION_FP32, "MVDR_PRECISION_MIXED": abi.PRECISION_MIXED,
+              "MVDR_MODE_MATERIALIZED": abi.MODE_MATERIALIZED, "MVDR_MODE_MATRIX_FREE": abi.MODE_MATRIX_FREE}
+    for name in dir(abi):
+        if name.startswith(("STAGE_", "ARRAY_")):
+            mirror["MVDR_" + name] = getattr(abi, name)
+    stages = sorted(k for k in found if k.startswith("MVDR_STAGE_"))
+    arrays = sorted(k for k in found if k.startswith("MVDR_ARRAY_"))
+    assert stages == sorted(k for k in mirror if k.startswith("MVDR_STAGE_"))
+    assert arrays == sorted(k for k in mirror if k.startswith("MVDR_ARRAY_"))
+    for k, v in mirror.items():
+        assert found.get(k) == v, k
