@@ -98,7 +98,15 @@ enum {
     /* Sample each compacted pixel's maps by the cumulative per-view lookup of
      * CalculateDensityMapCameraViewDpt (DenseDepthJacobianResidual.cu:14-22)
      * instead of the pixel's own view tag. Only differs when num_views > 1. */
-    MVDR_COMPAT_REF_VIEW_LOOKUP = 1u << 0
+    MVDR_COMPAT_REF_VIEW_LOOKUP = 1u << 0,
+    /* Warp the foreground (and density) term's reference vertex as it is
+     * stored in its camera's frame, as computeImageDensityJacobainAndResidual
+     * does (density_map_jacobian.cuh:32-36), instead of first moving it to
+     * frame 0 with InitialCameraSE3 like the dense-depth term
+     * (DenseDepthJacobianResidual.cu:43-50) and the foreground pixel
+     * selection (DensityForegroundMapHandler.cu:60-72). Only differs for
+     * views whose InitialCameraSE3 is not the identity. */
+    MVDR_COMPAT_REF_FOREGROUND_FRAME = 1u << 1
 };
 
 typedef struct mvdr_float4 { float x, y, z, w; } mvdr_float4;
@@ -337,7 +345,9 @@ MVDR_API int mvdr_apply_jtj(mvdr_solver* solver, const float* x, float* y, void*
  * static device array that each GPU loading the library holds until the
  * process exits. The first call on a device looks up that array's address
  * (cudaGetSymbolAddress), so make the first call on each device before any
- * stream capture. All calls share the array: calls whose work overlaps on the
+ * stream capture. Every later call on a stream that is not capturing looks the
+ * address up again, so a cudaDeviceReset between calls leaves no stale
+ * address behind. All calls share the array: calls whose work overlaps on the
  * GPU (on different streams, or from several host threads) race and give wrong
  * results; serialise them. num_block_rows above MVDR_NOALLOC_MAX_BLOCK_ROWS is
  * rejected with MVDR_ECAPACITY. A column index outside [0, num_block_rows)
@@ -385,6 +395,15 @@ MVDR_API int mvdr_batch_set_spmv_shape(mvdr_batch* batch, uint32_t shape);
  * captured graphs. MVDR_EINVAL for a matrix-free batch or a batch with more
  * instances than the device holds co-resident CTAs of the kernel. */
 MVDR_API int mvdr_batch_set_pcg_persistent(mvdr_batch* batch, int on);
+/* Bounded waits of the persistent PCG. Each instance barrier gives up after
+ * `limit_ns` nanoseconds (default 0.5 s, at most 10 s): the kernel's CTAs
+ * return, the instance is flagged and the next checked read reports
+ * MVDR_ETIMEOUT; the context stays usable. `extra_arrivals` > 0 makes every
+ * barrier wait for that many arrivals beyond the instance's own CTAs, which
+ * never come: it exists to exercise the timeout path and is 0 otherwise.
+ * The reference has no bounded waits (its PCG is launched kernel by kernel,
+ * BlockPCG.cuh:383-458). Drops the captured graphs. */
+MVDR_API int mvdr_batch_set_wait_limit(mvdr_batch* batch, uint64_t limit_ns, uint32_t extra_arrivals);
 MVDR_API int mvdr_batch_get_node_se3(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst, void* stream);
 MVDR_API int mvdr_batch_copy_node_se3_async(mvdr_batch* batch, uint32_t instance, mvdr_dual_quaternion* dst,
                                             void* stream);

@@ -62,6 +62,7 @@ def _declare(L):
         "mvdr_batch_autotune": (i32, [vp, vp, P(C.c_double), u32, P(u32), P(u32), P(u32)]),
         "mvdr_batch_set_spmv_shape": (i32, [vp, u32]),
         "mvdr_batch_set_pcg_persistent": (i32, [vp, i32]),
+        "mvdr_batch_set_wait_limit": (i32, [vp, C.c_uint64, u32]),
         "mvdr_batch_enqueue_stage": (i32, [vp, i32, vp]),
         "mvdr_last_error_string": (C.c_char_p, []),
         "mvdr_kernel_launch_count": (C.c_uint64, []),

@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "MVDR_OK", 1: "MVDR_EINVAL", 2: "MVDR_ECAPACITY", 3: "MVDR_EC
 PRECISION_FP32, PRECISION_MIXED = 0, 1
 MODE_MATERIALIZED, MODE_MATRIX_FREE = 0, 1
 COMPAT_REF_VIEW_LOOKUP = 1
+COMPAT_REF_FOREGROUND_FRAME = 2
 (STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE,
  STAGE_DIRECTION, STAGE_MATRIX_FREE) = range(9)
 # SpMV tile shapes (block rows per CTA, threads per scalar row / 6, form) in

@@ -223,7 +223,10 @@ __global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* ins
         const ViewDesc& V = I.views[v];
         const size_t p = (size_t)pix.y * V.pitch + pix.x;
         const float4 cv = V.ref_v[p];
-        float3 a = apply3(V.init, mk3(cv.x, cv.y, cv.z));
+        // the foreground term's vertex stays in its camera's frame in the
+        // reference's form (density_map_jacobian.cuh:32-36)
+        const bool raw_frame = fg && (I.compat & MVDR_COMPAT_REF_FOREGROUND_FRAME);
+        float3 a = raw_frame ? mk3(cv.x, cv.y, cv.z) : apply3(V.init, mk3(cv.x, cv.y, cv.z));
         if (!fg && mixed) {
             // The point-to-plane residual subtracts two ~1 m positions, and
             // near convergence Jt r cancels by orders of magnitude more, so

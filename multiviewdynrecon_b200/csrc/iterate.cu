@@ -121,6 +121,9 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
     // the lambda-weighted squared residuals of this CTA's terms
     // (ResidualEvaluator.cu:71-226): the energy of the linearisation point
     double energy = 0;
+    // a NaN or Inf in a warped point or a residual (from the inputs or the
+    // warp field) flags the instance, MVDR_ENONFINITE on the host
+    bool nonfinite = false;
     const float clip = 64.f * I.node_radius * I.node_radius;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T_all; t += gridDim.x * blockDim.x) {
         uint32_t k;
@@ -147,6 +150,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             const V3T<T> nc = rotv(iinv, rotv(w2c, wn));
             const int u = project_coord((float)vc.x, (float)vc.z, V.fx, V.cx);
             const int w = project_coord((float)vc.y, (float)vc.z, V.fy, V.cy);
+            nonfinite |= !isfinite((float)vc.x) || !isfinite((float)vc.y) || !isfinite((float)vc.z);
             float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
             if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height) {
                 const size_t p = (size_t)w * V.pitch + u;
@@ -160,6 +164,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
                 if (dotv(df, df) > (T)(0.075f * 0.075f)) valid = false;
                 if (valid) {
                     const float r = (float)dotv(dn, sub(vc, dv));
+                    nonfinite |= !isfinite(r);
                     const float3 dnf = mk3(dn4.x, dn4.y, dn4.z);
                     const float3 tr = rotT3(V.w2c, rot3(V.init, dnf));
                     const float3 ro = cross3(mk3((float)wv.x, (float)wv.y, (float)wv.z), tr);
@@ -183,6 +188,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             I.smooth[3 * (size_t)k] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)b.x);
             I.smooth[3 * (size_t)k + 1] = make_float4((float)b.y, (float)b.z, valid, 0.f);
             const float4 rr = make_float4((float)(a.x - b.x), (float)(a.y - b.y), (float)(a.z - b.z), 0.f);
+            nonfinite |= !isfinite(rr.x) || !isfinite(rr.y) || !isfinite(rr.z);
             I.smooth[3 * (size_t)k + 2] = rr;
             if (valid != 0.f) {
                 const float r0 = lam.smooth * rr.x, r1 = lam.smooth * rr.y, r2 = lam.smooth * rr.z;
@@ -190,7 +196,9 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             }
         } else if (ty == kForeground) {
             // computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual;
-            // the canonical vertex is taken to frame 0 first, as the dense term does
+            // fg_cv holds the canonical vertex in frame 0, as the dense term
+            // uses it, or with MVDR_COMPAT_REF_FOREGROUND_FRAME in its own
+            // camera's frame, as density_map_jacobian.cuh:32-36 warps it
             const float4 cv = I.fg_cv[k];
             const uint32_t v = __float_as_uint(cv.w);
             const ViewDesc& V = I.views[v];
@@ -206,6 +214,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             const float3 vc = mk3((float)vct.x, (float)vct.y, (float)vct.z);
             const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
             const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
+            nonfinite |= !isfinite(vc.x) || !isfinite(vc.y) || !isfinite(vc.z);
             float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
             if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height && V.fg != nullptr) {
                 const size_t p = (size_t)w * V.pitch + u;
@@ -218,6 +227,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
                 g = rotT3(V.w2c, rot3(V.init, g));
                 o0 = make_float4(-g.y * wv.z + g.z * wv.y, g.x * wv.z - g.z * wv.x, -g.x * wv.y + g.y * wv.x, g.x);
                 o1 = make_float4(g.y, g.z, img - 0.0f, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+                nonfinite |= !isfinite(o1.z) || !isfinite(g.x) || !isfinite(g.y) || !isfinite(g.z);
             }
             I.term_jr[2 * (size_t)(Td + k)] = o0;
             I.term_jr[2 * (size_t)(Td + k) + 1] = o1;
@@ -237,6 +247,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
             const V3T<T> wv = appv(se3, v3t(cvt<T>(ref.x), cvt<T>(ref.y), cvt<T>(ref.z)));
             const V3T<T> raw = sub(wv, v3t(cvt<T>(tg.x), cvt<T>(tg.y), cvt<T>(tg.z)));
+            nonfinite |= !isfinite((float)raw.x) || !isfinite((float)raw.y) || !isfinite((float)raw.z);
             const size_t o = 2 * (size_t)(f ? k : I.Tp + k);
             I.warped[o] = make_float4((float)wv.x, (float)wv.y, (float)wv.z, 1.0f);
             I.warped[o + 1] = make_float4((float)raw.x, (float)raw.y, (float)raw.z, 0.0f);
@@ -249,6 +260,7 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             }
         }
     }
+    if (__any_sync(0xffffffffu, nonfinite) && lane_id() == 0) set_error(I, kErrNonFinite);
     // one partial per CTA (reduction region 0), summed by energy_sum_kernel
     __shared__ double ws[8];
     energy = warp_sum(energy);
@@ -811,7 +823,18 @@ template <class T>
 __device__ inline T pcg_beta(const InstDesc& I, int parity, int first, uint32_t nd) {
     T dk, dkm1;
     sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDelta + (parity ^ 1), nd, &dk, &dkm1);
-    return first ? (T)0 : dk / dkm1;
+    // a zero delta_(k-1) (the residual vanished) restarts with d = s
+    return first || dkm1 == (T)0 ? (T)0 : dk / dkm1;
+}
+
+// alpha = delta / d.q; a zero d.q (an exactly zero right-hand side) gives a
+// zero step where the reference (BlockPCG.cuh:120-161) divides 0 by 0. A
+// non-finite alpha (NaN or Inf reached the system) flags the instance, from
+// the instance's `leader` CTA only.
+template <class T> __device__ inline T pcg_alpha(const InstDesc& I, T delta, T dq, bool leader) {
+    const T alpha = dq != (T)0 ? delta / dq : (T)0;
+    if (leader && threadIdx.x == 0 && !isfinite(alpha)) set_error(I, kErrNonFinite);
+    return alpha;
 }
 
 // ---------------------------------------------------------------- PCG -----
@@ -1079,7 +1102,7 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
     }
     T delta, dq;
     sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDq, nq, &delta, &dq);
-    const T alpha = delta / dq;
+    const T alpha = pcg_alpha<T>(I, delta, dq, blockIdx.x == 0);
     T part = 0;
     if (has) {
         T sv[6];
@@ -1129,7 +1152,6 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
 // same split reductions as in the launched form, with one partial per CTA of
 // the instance.
 constexpr uint32_t kPersistThreads = 256, kPersistRows = 40;
-constexpr uint64_t kBarrierLimitNs = 500ull * 1000 * 1000;  // a step takes microseconds
 
 __device__ inline uint64_t global_ns() {
     uint64_t t;
@@ -1143,8 +1165,8 @@ __device__ inline uint32_t ld_acquire_u32(const uint32_t* p) {
 }
 
 // All CTAs of the instance arrive; returns false (and flags the instance)
-// when the wait exceeds kBarrierLimitNs.
-__device__ inline bool instance_barrier(const InstDesc& I, uint32_t* ctr, uint32_t target) {
+// when the wait exceeds limit_ns.
+__device__ inline bool instance_barrier(const InstDesc& I, uint32_t* ctr, uint32_t target, uint64_t limit_ns) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1154,7 +1176,7 @@ __device__ inline bool instance_barrier(const InstDesc& I, uint32_t* ctr, uint32
         if (ld_acquire_u32(ctr) < target) {
             const uint64_t t0 = global_ns();
             while (ld_acquire_u32(ctr) < target) {
-                if (global_ns() - t0 > kBarrierLimitNs) {
+                if (global_ns() - t0 > limit_ns) {
                     ok = 0;
                     set_error(I, kErrWaitTimeout);
                     break;
@@ -1171,7 +1193,8 @@ __device__ inline bool instance_barrier(const InstDesc& I, uint32_t* ctr, uint32
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(const InstDesc* insts, uint32_t B,
-                                                                              uint32_t iters) {
+                                                                              uint32_t iters, uint64_t limit_ns,
+                                                                              uint32_t extra) {
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
     using V = typename BlockStore<MIXED>::V;
@@ -1226,7 +1249,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
         }
         store_block_partial<T>(I, kRegDelta, part, c);
     }
-    if (!instance_barrier(I, bar, ++passed * nc)) return;
+    if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
     for (uint32_t it = 0; it < iters; ++it) {
         const int parity = (int)(it & 1u);
         // direction
@@ -1236,7 +1259,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
             T* dcur = PV::d(I, parity);
             for (uint32_t e = c * nt + tid; e < 6 * I.N; e += nc * nt) dcur[e] = PV::s(I)[e] + beta * dprev[e];
         }
-        if (!instance_barrier(I, bar, ++passed * nc)) return;
+        if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
         // SpMV over tiles of kPersistRows block rows, column form
         {
             const V* store = BlockStore<MIXED>::ptr(I);
@@ -1274,12 +1297,12 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
             }
             store_block_partial<T>(I, kRegDq, part, c);
         }
-        if (!instance_barrier(I, bar, ++passed * nc)) return;
+        if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
         // update: alpha = delta / d.q, x, r, s, delta_new
         {
             T delta, dq;
             sum_two_block_partials<T>(I, kRegDelta + parity, nc, kRegDq, nc, &delta, &dq);
-            const T alpha = delta / dq;
+            const T alpha = pcg_alpha<T>(I, delta, dq, c == 0);
             const T* d = PV::d(I, parity);
             T part = 0;
             for (uint32_t node = c * nt + tid; node < I.N; node += nc * nt) {
@@ -1310,7 +1333,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
             }
             store_block_partial<T>(I, kRegDelta + (parity ^ 1), part, c);
         }
-        if (!instance_barrier(I, bar, ++passed * nc)) return;
+        if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
     }
 }
 
@@ -1545,6 +1568,9 @@ __global__ void __launch_bounds__(128) update_kernel(const InstDesc* insts) {
         q1.x = tq.w * q.x + tq.x * q.w + tq.y * q.z - tq.z * q.y;
         q1.y = tq.w * q.y - tq.x * q.z + tq.y * q.w + tq.z * q.x;
         q1.z = tq.w * q.z + tq.x * q.y - tq.y * q.x + tq.z * q.w;
+        if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z) || !isfinite(q.w) || !isfinite(q1.x) ||
+            !isfinite(q1.y) || !isfinite(q1.z) || !isfinite(q1.w))
+            set_error(I, kErrNonFinite);
         float4* out = reinterpret_cast<float4*>(I.se3 + node);
         out[0] = q;
         out[1] = q1;
@@ -1668,8 +1694,10 @@ static cudaError_t launch_pcg_persistent(const LaunchCfg& lc, InstDesc* d, uint3
     cfg.numAttrs = 1;
     const uint32_t B = lc.B;
     e = lc.precision == MVDR_PRECISION_MIXED
-            ? cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<true>, (const InstDesc*)d, B, iters)
-            : cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<false>, (const InstDesc*)d, B, iters);
+            ? cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<true>, (const InstDesc*)d, B, iters, lc.wait_limit_ns,
+                                 lc.wait_extra_arrivals)
+            : cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<false>, (const InstDesc*)d, B, iters, lc.wait_limit_ns,
+                                 lc.wait_extra_arrivals);
     count_launch();
     return e;
 }

@@ -330,7 +330,15 @@ struct LaunchCfg {
     int pcg_persistent;
     uint32_t pcg_grid;   // co-resident CTAs of pcg_persistent_kernel
     uint32_t* pcg_bars;  // B barrier counters, 32 words apart
+    // bounded waits of the persistent PCG's instance barriers: the limit of
+    // each wait, and arrivals each barrier waits for beyond the instance's
+    // CTAs (non-zero only to exercise the timeout path)
+    uint64_t wait_limit_ns;
+    uint32_t wait_extra_arrivals;
 };
+
+constexpr uint64_t kDefaultWaitLimitNs = 500ull * 1000 * 1000;  // a barrier step takes microseconds
+constexpr uint64_t kMaxWaitLimitNs = 10ull * 1000 * 1000 * 1000;
 
 // ----------------------------------------------------------- launchers --
 // Each launcher enqueues kernels on `st` for all instances. They return

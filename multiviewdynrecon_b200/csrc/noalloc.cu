@@ -13,8 +13,8 @@
 // per-CTA partial sums of x.y, a completion ticket and an error flag. They live
 // in the file-scope array g_noalloc_scratch below, which every GPU that loads
 // the library holds until the process exits. Host code cannot use that name as
-// a device address, so the entry point looks the address up once per device
-// with cudaGetSymbolAddress and passes it to the kernel.
+// a device address, so the entry point looks the address up with
+// cudaGetSymbolAddress on the current device and passes it to the kernel.
 #include "kernels_common.cuh"
 
 #include <mutex>
@@ -42,19 +42,28 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 double* g_scratch_ptr[kMaxDevices] = {};
 
-// The device address of g_noalloc_scratch on the current device, looked up on
-// the first call that runs on that device.
-cudaError_t scratch_for_current_device(double** out) {
+// The device address of g_noalloc_scratch on the current device. A call on a
+// stream that is not being captured looks the address up again (a
+// cudaDeviceReset since the last call reloads the module, and the old address
+// would belong to the destroyed context) and keeps it for the device; a call
+// on a capturing stream uses the kept address, because the lookup may load
+// the module, which a capture does not allow.
+cudaError_t scratch_for_current_device(cudaStream_t st, double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_scratch_ptr[dev] = static_cast<double*>(p);
+    } else if (!g_scratch_ptr[dev]) {
+        return cudaErrorStreamCaptureUnsupported;  // no call on this device before the capture
     }
     *out = g_scratch_ptr[dev];
     return cudaSuccess;
@@ -138,9 +147,9 @@ extern "C" MVDR_API int mvdr_bsr6_spmv_dot_noalloc(uint32_t num_block_rows, uint
                                                   std::to_string(MVDR_NOALLOC_MAX_BLOCK_ROWS));
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     double* scratch = nullptr;
-    cudaError_t e = scratch_for_current_device(&scratch);
+    cudaError_t e = scratch_for_current_device(st, &scratch);
     if (e != cudaSuccess)
-        return record_failure(MVDR_ECUDA, std::string("mvdr_bsr6_spmv_dot_noalloc: cudaGetSymbolAddress: ") +
+        return record_failure(MVDR_ECUDA, std::string("mvdr_bsr6_spmv_dot_noalloc: scratch address lookup: ") +
                                               cudaGetErrorString(e));
     if (num_block_rows == 0) {
         e = cudaMemsetAsync(x_dot_y, 0, sizeof(double), st);

@@ -320,6 +320,8 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     }
     b->lc.pcg_bars = b->d_bars;
     b->lc.pcg_persistent = 0;
+    b->lc.wait_limit_ns = kDefaultWaitLimitNs;
+    b->lc.wait_extra_arrivals = 0;
     b->lc.pcg_grid = persistent_pcg_grid(lc.precision == MVDR_PRECISION_MIXED, lc.sm_count);
     b->owned.resize(B);
     b->has_inputs.assign(B, 0);
@@ -661,6 +663,8 @@ static int check_flags(const DeviceCounts& c) {
     }
     if (c.error_flags & kErrBadNodeIndex) return fail(MVDR_EINVAL, "node or surfel index out of range in inputs");
     if (c.error_flags & kErrWaitTimeout) return fail(MVDR_ETIMEOUT, "a bounded device-side wait gave up");
+    if (c.error_flags & kErrNonFinite)
+        return fail(MVDR_ENONFINITE, "NaN or Inf in a residual, the PCG step or the warp field");
     return MVDR_OK;
 }
 
@@ -991,6 +995,17 @@ int mvdr_batch_set_pcg_persistent(mvdr_batch* bh, int on) {
     if (on && b.cfg.mode != MVDR_MODE_MATERIALIZED) return fail(MVDR_EINVAL, "persistent PCG needs the materialised mode");
     if (on && b.lc.pcg_grid < b.B) return fail(MVDR_EINVAL, "more instances than co-resident persistent CTAs");
     b.lc.pcg_persistent = on ? 1 : 0;
+    for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
+    b.graphs.clear();
+    return MVDR_OK;
+}
+
+int mvdr_batch_set_wait_limit(mvdr_batch* bh, uint64_t limit_ns, uint32_t extra_arrivals) {
+    if (!bh) return fail(MVDR_EINVAL, "batch is null");
+    if (limit_ns == 0 || limit_ns > kMaxWaitLimitNs) return fail(MVDR_EINVAL, "wait limit must be in (0, 10 s]");
+    Batch& b = *bh->batch;
+    b.lc.wait_limit_ns = limit_ns;
+    b.lc.wait_extra_arrivals = extra_arrivals;
     for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
     b.graphs.clear();
     return MVDR_OK;

@@ -241,6 +241,12 @@ class BatchSolver:
         mode) instead of three launches per iteration."""
         check(lib().mvdr_batch_set_pcg_persistent(self.h, 1 if on else 0))
 
+    def set_wait_limit(self, limit_ns, extra_arrivals=0):
+        """Limit of each bounded barrier wait of the persistent PCG;
+        extra_arrivals > 0 makes every barrier wait for arrivals that never
+        come (exercises the MVDR_ETIMEOUT path)."""
+        check(lib().mvdr_batch_set_wait_limit(self.h, int(limit_ns), int(extra_arrivals)))
+
     def set_spmv_shape(self, index):
         """Use SpMV tile shape `index` of abi.SPMV_SHAPES for later solves."""
         check(lib().mvdr_batch_set_spmv_shape(self.h, index))

@@ -754,13 +754,17 @@ struct Oracle {
         }
         // foreground: computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual
         // (DensityForegroundJacobianResidual.cu:93-142, density_map_jacobian.cuh:12-79).
-        // The reference vertex is taken to frame 0 first, as the dense term does.
+        // The reference vertex is taken to frame 0 first, as the dense term
+        // does; MVDR_COMPAT_REF_FOREGROUND_FRAME warps it in its own camera's
+        // frame, as density_map_jacobian.cuh:32-36 does.
+        const bool raw_frame = (cfg.compat_flags & MVDR_COMPAT_REF_FOREGROUND_FRAME) != 0;
         for (u32 idx = 0; idx < Tf; ++idx) {
             const u16* px = &fg_pix[4 * (size_t)idx];
             const u32 v = view_of(idx, fg_pix.data(), fg_view_count);
             const ViewData& d = views[v];
             const size_t p = (size_t)px[1] * W + px[0];
-            const V3<R> cv0 = init[v].apply(V3<R>{(R)d.ref_v[p].x, (R)d.ref_v[p].y, (R)d.ref_v[p].z});
+            const V3<R> cv = {(R)d.ref_v[p].x, (R)d.ref_v[p].y, (R)d.ref_v[p].z};
+            const V3<R> cv0 = raw_frame ? cv : init[v].apply(cv);
             const M34<R> se3 = se3_matrix(blend(f, &fg_knn[4 * (size_t)idx], &fg_w[idx].x));
             const V3<R> wv = se3.apply(cv0);
             V3<R> vc = w2c[v].apply(wv);
@@ -1036,12 +1040,14 @@ struct Oracle {
         for (u32 it = 0; it < iters; ++it) {
             spmv<R>(d, q);
             const R dq = vdot(d, q);
-            const R alpha = delta / dq;
+            // a zero d.q (a right-hand side that is exactly zero) gives a zero
+            // step where the reference would divide 0 by 0
+            const R alpha = dq != (R)0 ? delta / dq : (R)0;
             for (size_t i = 0; i < n; ++i) { xx[i] += alpha * d[i]; t[i] = r[i] - alpha * q[i]; }
             precond(t, s);
             const R delta_old = delta;
             delta = vdot(t, s);
-            const R beta = delta / delta_old;
+            const R beta = delta_old != (R)0 ? delta / delta_old : (R)0;
             for (size_t i = 0; i < n; ++i) d[i] = s[i] + beta * d[i];
             std::swap(r, t);
         }

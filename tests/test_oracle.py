@@ -333,6 +333,51 @@ def test_compat_view_lookup_only_changes_multiview(oracle_mod):
                           o.get(abi.ARRAY_TERM_JACOBIAN).view(np.uint32))
 
 
+@pytest.mark.parametrize("compat", [False, True])
+def test_foreground_terms_match_the_reference_formula(oracle_mod, compat):
+    """The oracle's foreground terms against an independent restatement of
+    computeImageDensityJacobainAndResidual (density_map_jacobian.cuh:12-79):
+    by default with the reference vertex moved to frame 0 first, and under
+    MVDR_COMPAT_REF_FOREGROUND_FRAME warped in its own camera's frame as the
+    reference does. Views 1 and 2 of the torso have InitialCameraSE3 != I,
+    so the two forms differ there and agree on view 0."""
+    from image_terms import foreground_terms
+    scene = small_scene("torso")
+    flags = abi.COMPAT_REF_FOREGROUND_FRAME if compat else 0
+    o = oracle_mod.Oracle(scene, abi.make_config(scene, compat_flags=flags), fp64=True)
+    o.build_index()
+    o.eval_terms()
+    Td = o.counts().dense_terms
+    pix = o.get(abi.ARRAY_FOREGROUND_PIXELS)
+    jr = o.get(abi.ARRAY_TERM_JACOBIAN)[Td:]
+    got = jr.astype(np.float64)
+    want = foreground_terms(scene, pix, frame0=not compat)
+    got_pix = np.ascontiguousarray(jr[:, 7]).view(np.uint32).astype(np.int64)
+    got_pix = np.where(got_pix == abi.MVDR_INVALID_INDEX, -1, got_pix)
+    same = got_pix == want[:, 7].astype(np.int64)
+    assert same.mean() > 0.999
+    assert max_relative_error(got[same, :7], want[same, :7], 1e-6 * np.abs(want[:, :7]).max()) < 1e-5
+    # the other form really differs on the views with a camera offset
+    other = foreground_terms(scene, pix, frame0=compat)
+    on_v0 = pix[:, 2] == 0
+    assert np.allclose(other[on_v0, :7], want[on_v0, :7], rtol=1e-9, atol=1e-12)
+    assert np.abs(other[~on_v0, :7] - want[~on_v0, :7]).max() > 1e-3 * np.abs(want[:, :7]).max()
+
+
+def test_compat_foreground_frame_changes_only_foreground_terms(oracle_mod):
+    scene = small_scene("torso")
+    a = _run_oracle(oracle_mod, scene)
+    o = oracle_mod.Oracle(scene, abi.make_config(scene, compat_flags=abi.COMPAT_REF_FOREGROUND_FRAME))
+    o.build_index()
+    o.eval_terms()
+    Td = a.counts().dense_terms
+    ja, jb = a.get(abi.ARRAY_TERM_JACOBIAN), o.get(abi.ARRAY_TERM_JACOBIAN)
+    assert np.array_equal(ja[:Td].view(np.uint32), jb[:Td].view(np.uint32))
+    assert not np.array_equal(ja[Td:].view(np.uint32), jb[Td:].view(np.uint32))
+    for which in (abi.ARRAY_FOREGROUND_PIXELS, abi.ARRAY_NODE2TERM_INDEX, abi.ARRAY_NODEPAIR_KEY):
+        assert np.array_equal(a.get(which), o.get(which))
+
+
 @pytest.mark.parametrize("name", ["sphere_small", "torso_small"])
 def test_golden_fixtures(oracle_mod, name):
     path = os.path.join(GOLDEN, f"{name}.npz")

@@ -95,6 +95,40 @@ def test_term_evaluation(oracle_mod, kind):
     assert max_relative_error(gw, ow, 1e-6) < 1e-4
 
 
+@pytest.mark.parametrize("flags", [abi.COMPAT_REF_FOREGROUND_FRAME,
+                                   abi.COMPAT_REF_FOREGROUND_FRAME | abi.COMPAT_REF_VIEW_LOOKUP])
+@pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_FP32])
+def test_term_evaluation_reference_compat_forms(oracle_mod, flags, precision):
+    """The reference's own forms of the foreground term (vertex warped in its
+    camera's frame) and of the pixel-to-view lookup: the kernel's terms equal
+    the oracle's, and its foreground terms equal an independent restatement of
+    density_map_jacobian.cuh:12-79 (with the pixel's own view)."""
+    from image_terms import foreground_terms
+    scene = small_scene("torso")
+    g, cfg = make_gpu(scene, precision=precision, compat_flags=flags)
+    g.build_index()
+    g.gn_iteration(scene.pcg_iterations)
+    torch.cuda.synchronize()
+    o = oracle_mod.Oracle(scene, cfg)
+    o.build_index()
+    o.eval_terms()
+    gj, oj = g.get_array(abi.ARRAY_TERM_JACOBIAN), o.get(abi.ARRAY_TERM_JACOBIAN)
+    assert gj.shape == oj.shape
+    same = gj[:, 7].view(np.uint32) == oj[:, 7].view(np.uint32)
+    assert (~same).sum() <= max(2, int(1e-3 * len(same)))
+    scale = np.abs(oj[same, :7]).max()
+    assert max_relative_error(gj[same, :7], oj[same, :7], 1e-6 * scale) < 1e-4
+    if not flags & abi.COMPAT_REF_VIEW_LOOKUP:
+        Td = g.counts().dense_terms
+        want = foreground_terms(scene, g.get_array(abi.ARRAY_FOREGROUND_PIXELS), frame0=False)
+        got = gj[Td:].astype(np.float64)
+        gp = np.ascontiguousarray(gj[Td:, 7]).view(np.uint32).astype(np.int64)
+        gp = np.where(gp == abi.MVDR_INVALID_INDEX, -1, gp)
+        ok = gp == want[:, 7].astype(np.int64)
+        assert ok.mean() > 0.999
+        assert max_relative_error(got[ok, :7], want[ok, :7], 1e-6 * np.abs(want[:, :7]).max()) < 1e-4
+
+
 @pytest.mark.parametrize("kind", KINDS)
 @pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_FP32])
 def test_assembly_and_pcg(oracle_mod, kind, precision):
