@@ -61,9 +61,13 @@ def parse():
                    help="use this SpMV tile shape (index into abi.SPMV_SHAPES) instead of the autotuner's")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="torso", choices=["torso", "uneven", "body"],
-                   help="torso: the headline batch (default); uneven: 16 instances with 1024-16384 nodes and "
-                        "1-4 views; body: one 32768-node, 5-view 1280x720 solve")
+    p.add_argument("--workload", default="torso", choices=["torso", "sphere", "uneven", "body"],
+                   help="torso: the headline batch (default); sphere: the 1-view 2048-node plain-method "
+                        "configuration; uneven: 16 instances with 1024-16384 nodes and 1-4 views; body: one "
+                        "32768-node, 5-view 1280x720 solve")
+    p.add_argument("--no-accuracy", action="store_true", help="skip the FP64 check of the timed configuration")
+    p.add_argument("--no-e2e", action="store_true",
+                   help="skip the end-to-end leg (for profiler captures only; the bench line then has no e2e)")
     return p.parse_args()
 
 
@@ -163,20 +167,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+PROFILE_SPMV = "profiles/pcg_spmv_scaled_torso_3view_4096nodes_16inst.md"
+
+
 def measured_traffic(args):
-    """DRAM bytes (read + write) per launch of pcg_spmv_kernel from the ncu
-    capture summarised in profiles/ for the default workload; None for other
-    workloads or when the summary is absent."""
+    """DRAM bytes (read + write) per launch of the headline SpMV kernel
+    (pcg_spmv_scaled_kernel) from the ncu capture of this workload summarised
+    in PROFILE_SPMV; None for other workloads or when no summary exists."""
     default = (args.batch == 16 and args.nodes == 4096 and args.width == 640 and args.height == 480
                and args.precision == "mixed" and args.mode == "materialized")
-    path = os.path.join(ROOT, "profiles", "pcg_spmv_torso_3view_4096nodes_16inst.md")
+    path = os.path.join(ROOT, PROFILE_SPMV)
     if not default or not os.path.exists(path):
         return None, None
     with open(path) as f:
         for line in f:
             if line.startswith("| DRAM read + write |"):
                 parts = line.split("|")[2].replace("MB", "").split("+")
-                return int(sum(float(p) for p in parts) * 1e6), "profiles/pcg_spmv_torso_3view_4096nodes_16inst.md"
+                return int(sum(float(p) for p in parts) * 1e6), PROFILE_SPMV
     return None, None
 
 
@@ -192,28 +199,42 @@ def spmv_tile_label(shape):
     return f"{'row' if form == 0 else 'col'}{rows}x{6 * split}"
 
 
-def algorithmic_bytes(counts, N, mixed=True):
+def algorithmic_bytes(counts, N, mixed=True, materialized=True):
     """Compulsory HBM bytes per stage and instance (each array read or written
-    once). JtJ is kept as half storage: N diagonal + P upper 6x6 blocks, in
-    double (mixed precision) or float; the full block-row layout has N + 2P
-    entries of (column, position). The PCG vectors are double in mixed
-    precision."""
+    once). JtJ is kept as half storage (N diagonal + P upper 6x6 blocks) with
+    N + 2P entries of (position, column) in the full block-row layout.
+    Mixed precision, materialised: the assembly writes the blocks in double,
+    the scaling turns the P upper blocks into float blocks of the
+    block-Jacobi scaled operator, whose identity diagonal the SpMV does not
+    read; the SpMV reads the float copy of the direction (24 B per node) and
+    the double direction (48 B), and writes the double product (48 B); the PCG
+    update needs no preconditioner. Plain FP32: float blocks with the
+    diagonal, float vectors, the 6x6 inverse per node."""
     Td, Ts, Tf, Tp, Tc = (counts.dense_terms, counts.smooth_terms, counts.foreground_terms, counts.feature_terms,
                           counts.cross_terms)
     P = counts.half_pairs
     elem = 8 if mixed else 4
-    blocks = 36 * elem * (N + P)
-    entries = 8 * (N + 2 * P)
+    scaled = mixed and materialized
     term_data = 52 * (Td + Tf) + 29 * Ts + 88 * (Tp + Tc)
     precond = 168 * N if mixed else 144 * N
+    if scaled:
+        spmv = 144 * P + 8 * 2 * P + 4 * (N + 1) + 24 * N + 48 * N + 48 * N
+        direction = 3 * 48 * N + 24 * N      # r and d_prev read, d and its float copy written
+        pcg_update = 6 * 48 * N               # x rw, r rw, d, q read
+    else:
+        spmv = 36 * elem * (N + P) + 8 * (N + 2 * P) + 4 * (N + 1) + 2 * 6 * elem * N
+        direction = 3 * 6 * elem * N          # s and d_prev read, d written
+        pcg_update = 7 * 6 * elem * N + precond  # x rw, r rw, d, q read, s written
     return {
         "terms": 122 * Td + 86 * Tf + 29 * Ts + 72 * (Tp + Tc) + 32 * N,
         "diag": term_data + 4 * counts.node2term_entries + 144 * N + 36 * elem * N + 24 * N + precond,
         "offdiag": term_data + 4 * counts.nodepair_entries + 12 * P + 36 * elem * P,
-        # direction read, q written (6 values per node in the solve's precision)
-        "spmv": blocks + entries + 4 * (N + 1) + 2 * 6 * elem * N,
-        "direction": 3 * 6 * elem * N,  # s and d_prev read, d written
-        "pcg_update": 7 * 6 * elem * N + precond,  # x rw, r rw, d, q read, s written
+        # the double upper blocks and their pair keys read, the float scaled blocks
+        # written, each node's Cholesky factor read once
+        "scale": 288 * P + 4 * P + 144 * P + 168 * N,
+        "spmv": spmv,
+        "direction": direction,
+        "pcg_update": pcg_update,
         "update": 24 * N + 64 * N,
         # matrix-free product: J.d reads each term's record, nodes and weights
         # (pixel 56 B, smooth 52 B, point-to-point 56 B) and d, and writes J.d
@@ -296,7 +317,8 @@ def run_ours(args, rank, world, dist):
 
     # per-stage timing on the same stream (CUDA events), all instances
     stages = {}
-    abytes = algorithmic_bytes(counts, base.num_nodes, mixed=args.precision == "mixed")
+    abytes = algorithmic_bytes(counts, base.num_nodes, mixed=args.precision == "mixed",
+                               materialized=mode == abi.MODE_MATERIALIZED)
     reps = 20
     with torch.cuda.stream(stream):
         bind_all()
@@ -306,10 +328,12 @@ def run_ours(args, rank, world, dist):
         # matrix-free pair (J.d per term, then Jt per node)
         op = ("spmv", abi.STAGE_SPMV) if mode == abi.MODE_MATERIALIZED else ("matrix_free", abi.STAGE_MATRIX_FREE)
         for name, sid in (("index", abi.STAGE_INDEX), ("terms", abi.STAGE_TERMS), ("diag", abi.STAGE_DIAG),
-                          ("offdiag", abi.STAGE_OFFDIAG), op,
+                          ("offdiag", abi.STAGE_OFFDIAG), ("scale", abi.STAGE_SCALE), op,
                           ("direction", abi.STAGE_DIRECTION), ("pcg_update", abi.STAGE_PCG_UPDATE),
                           ("update", abi.STAGE_UPDATE)):
-            if name == "offdiag" and mode != abi.MODE_MATERIALIZED:
+            if name in ("offdiag", "scale") and mode != abi.MODE_MATERIALIZED:
+                continue
+            if name == "scale" and args.precision != "mixed":
                 continue
             for _ in range(2):
                 lib().mvdr_batch_enqueue_stage(batch.h, sid, stream.cuda_stream)
@@ -330,7 +354,10 @@ def run_ours(args, rank, world, dist):
     if mode == abi.MODE_MATERIALIZED:
         spmv = stages["spmv"]
         spmv_bytes = B * abytes["spmv"]
-        kernel = "pcg_spmv_col_kernel" if spmv_shape[2] == 1 else "pcg_spmv_kernel"
+        if args.precision == "mixed":
+            kernel = "pcg_spmv_scaled_kernel"
+        else:
+            kernel = "pcg_spmv_col_kernel" if spmv_shape[2] == 1 else "pcg_spmv_kernel"
         traffic, traffic_src = measured_traffic(args)
     else:
         # no ncu capture of the matrix-free pair is committed
@@ -349,58 +376,63 @@ def run_ours(args, rank, world, dist):
     # the compute stream; a batch's upload waits for that batch's previous
     # solve. Every step still uploads all of its inputs and reads back all of
     # its warp fields inside the timed region.
-    host_scenes = [DeviceScene(s, pin=True) for s in scenes]
-    e2e_batches = [batch, BatchSolver(cfg, B)]
-    for i, ds in enumerate(dev_scenes):
-        e2e_batches[1].set_input(i, ds, stream=stream)
-    if args.pcg_persistent:
-        e2e_batches[1].set_pcg_persistent(True)
-    if args.spmv_shape >= 0:
-        e2e_batches[1].set_spmv_shape(args.spmv_shape)
+    e2e = None
+    if args.no_e2e:
+        host_scenes = []
     else:
-        e2e_batches[1].autotune(stream=stream)
-    copy_stream, solve_stream = torch.cuda.Stream(), stream
-    uploaded = [torch.cuda.Event(), torch.cuda.Event()]
-    solved = [torch.cuda.Event(), torch.cuda.Event()]
-    out_host = [[torch.empty((s.num_nodes, 8), dtype=torch.float32, pin_memory=True) for s in scenes]
-                for _ in range(2)]
-    h2d = sum(hs.nbytes for hs in host_scenes)
-    d2h = sum(o.numel() * 4 for o in out_host[0])
+        host_scenes = [DeviceScene(s, pin=True) for s in scenes]
+    if not args.no_e2e:
+        e2e_batches = [batch, BatchSolver(cfg, B)]
+        for i, ds in enumerate(dev_scenes):
+            e2e_batches[1].set_input(i, ds, stream=stream)
+        if args.pcg_persistent:
+            e2e_batches[1].set_pcg_persistent(True)
+        if args.spmv_shape >= 0:
+            e2e_batches[1].set_spmv_shape(args.spmv_shape)
+        else:
+            e2e_batches[1].autotune(stream=stream)
+        copy_stream, solve_stream = torch.cuda.Stream(), stream
+        uploaded = [torch.cuda.Event(), torch.cuda.Event()]
+        solved = [torch.cuda.Event(), torch.cuda.Event()]
+        out_host = [[torch.empty((s.num_nodes, 8), dtype=torch.float32, pin_memory=True) for s in scenes]
+                    for _ in range(2)]
+        h2d = sum(hs.nbytes for hs in host_scenes)
+        d2h = sum(o.numel() * 4 for o in out_host[0])
 
-    def e2e_step(k):
-        j = k % 2
-        bt = e2e_batches[j]
-        copy_stream.wait_event(solved[j])  # this batch's previous solve and readback are done
-        for i, hs in enumerate(host_scenes):
-            bt.set_input_host(i, hs, stream=copy_stream)
-        uploaded[j].record(copy_stream)
-        solve_stream.wait_event(uploaded[j])
-        bt.solve(args.gn, args.pcg, use_graph=True, stream=solve_stream)
-        for i in range(B):
-            bt.node_se3_async(i, out_host[j][i], stream=solve_stream)
-        solved[j].record(solve_stream)
+        def e2e_step(k):
+            j = k % 2
+            bt = e2e_batches[j]
+            copy_stream.wait_event(solved[j])  # this batch's previous solve and readback are done
+            for i, hs in enumerate(host_scenes):
+                bt.set_input_host(i, hs, stream=copy_stream)
+            uploaded[j].record(copy_stream)
+            solve_stream.wait_event(uploaded[j])
+            bt.solve(args.gn, args.pcg, use_graph=True, stream=solve_stream)
+            for i in range(B):
+                bt.node_se3_async(i, out_host[j][i], stream=solve_stream)
+            solved[j].record(solve_stream)
 
-    for k in range(max(2, args.warmup)):
-        e2e_step(k)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(copy_stream)
-    solve_stream.wait_event(a)
-    for k in range(args.steps):
-        e2e_step(k)
-    b2.record(solve_stream)
-    b2.synchronize()
-    e2e_ms = max_over_ranks(a.elapsed_time(b2) / args.steps, dist, "cuda")
-    e2e = {"value": round(job_value(world, B, e2e_ms), 3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
-           "pipeline": "uploads in order on a copy stream, overlapping the previous step's solve"}
-    for bt in e2e_batches:  # device-side error record of every e2e solve
-        for i in range(B):
-            if bt.instance(i).counts().error_flags:
-                raise RuntimeError(f"e2e solve of instance {i} flagged errors")
-    e2e_batches[1].close()
+        for k in range(max(2, args.warmup)):
+            e2e_step(k)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(copy_stream)
+        solve_stream.wait_event(a)
+        for k in range(args.steps):
+            e2e_step(k)
+        b2.record(solve_stream)
+        b2.synchronize()
+        e2e_ms = max_over_ranks(a.elapsed_time(b2) / args.steps, dist, "cuda")
+        e2e = {"value": round(job_value(world, B, e2e_ms), 3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
+               "pipeline": "uploads in order on a copy stream, overlapping the previous step's solve"}
+        for bt in e2e_batches:  # device-side error record of every e2e solve
+            for i in range(B):
+                if bt.instance(i).counts().error_flags:
+                    raise RuntimeError(f"e2e solve of instance {i} flagged errors")
+        e2e_batches[1].close()
 
     # plain FP32 form: one instance at a time, per-kernel launches, float dots
     plain = None
@@ -424,12 +456,44 @@ def run_ours(args, rank, world, dist):
         plain = {"value": round(1e3 / p_ms, 3), "unit": "solves/s", "ms_per_solve": round(p_ms, 4),
                  "form": "plain FP32, one instance per solve, no graph"}
         single.close()
+        # the same FP32 arithmetic batched and graph-replayed like the headline,
+        # to separate the gain of the precision scheme from that of batching
+        pb = BatchSolver(pcfg, B)
+        with torch.cuda.stream(stream):
+            def pstep():
+                for i, ds in enumerate(dev_scenes):
+                    pb.set_input(i, ds, stream=stream)
+                pb.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+            pstep()
+            if args.spmv_shape >= 0:
+                pb.set_spmv_shape(args.spmv_shape)
+            else:
+                pb.autotune(stream=stream)
+            pb_ms = time_solves(pstep, max(3, args.steps // 4), max(3, args.warmup), stream)
+        plain["batched_graph"] = {"value": round(B * 1e3 / pb_ms, 3), "unit": "solves/s",
+                                  "ms_per_step": round(pb_ms, 4),
+                                  "form": f"plain FP32, {B} instances per launch, CUDA graph (as the headline)"}
+        pb.close()
+
+    # accuracy of the timed configuration: instance 0's solve, every
+    # Gauss-Newton increment against the FP64 oracle (after the timed region)
+    accuracy = None
+    if not args.no_accuracy:
+        with torch.cuda.stream(stream):
+            errs, eerrs = increment_errors_vs_fp64(scenes[0], cfg, args.gn, args.pcg, batch=batch, bind=bind_all,
+                                                   stream=stream)
+        accuracy = {"dx_rel_err_vs_fp64": [float("%.3g" % e) for e in errs],
+                    "dx_rel_err_max": float("%.3g" % max(errs)),
+                    "energy_rel_err_vs_fp64_max": float("%.3g" % max(eerrs)),
+                    "instance": "0 of the timed batch", "bar": 1e-4,
+                    "method": "each GN increment vs the FP64 oracle linearised at the GPU's warp field of that "
+                              "iteration, with the GPU's projected pixels and validity decisions"}
 
     return dict(value=value, ms=ms, kernels_per_step=kernels_per_step, clocks=clocks.summary(), stages=stages,
                 spmv_tile=dict(spmv_tile_desc(spmv_shape),
                                candidates_ms={spmv_tile_label(sh): round(t, 5)
                                               for sh, t in zip(abi.SPMV_SHAPES, spmv_shape_ms)}),
-                roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base)
+                roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base, accuracy=accuracy)
 
 
 def first_increment_errors(scenes, cfg_for, gpu_increments, pcg, threads):
@@ -453,6 +517,54 @@ def first_increment_errors(scenes, cfg_for, gpu_increments, pcg, threads):
 
     with ThreadPoolExecutor(max_workers=threads) as ex:
         return list(ex.map(one, range(len(scenes))))
+
+
+def increment_errors_vs_fp64(scene, cfg, gn, pcg, batch=None, bind=None, stream=None):
+    """Every Gauss-Newton increment of one instance's solve against the FP64
+    oracle linearised at the GPU's warp field of that iteration, with the
+    GPU's projected pixels and validity decisions (relative 2-norm), and each
+    iteration's energy against the oracle's. With `batch` (and `bind`, which
+    rebinds every instance) the instance is instance 0 of that batch, solved
+    with 1, 2, ..., gn iterations; otherwise a single solver steps through the
+    iterations. Returns (errors, energy errors)."""
+    import torch
+    import oracle
+    from multiviewdynrecon_b200 import abi
+    from multiviewdynrecon_b200.solver import NonRigidSolver
+    o64 = oracle.Oracle(scene, cfg, fp64=True)
+    o64.build_index()
+    errs, eerrs = [], []
+    g = None
+    if batch is None:
+        g = NonRigidSolver(cfg)
+        g.set_solver_input(scene)
+        g.build_index()
+    field = np.ascontiguousarray(scene.node_se3, np.float32)
+    for k in range(gn):
+        o64.set_node_se3(field)
+        if g is not None:
+            g.gn_iteration(pcg)
+            torch.cuda.synchronize()
+            inst = g
+        else:
+            bind()
+            batch.solve(k + 1, pcg, use_graph=False, stream=stream)
+            torch.cuda.synchronize()
+            inst = batch.instance(0)
+        o64.freeze(inst.get_array(abi.ARRAY_TERM_JACOBIAN), inst.get_array(abi.ARRAY_SMOOTH_TERMS))
+        o64.eval_terms()
+        o64.assemble()
+        eg, eo = inst.energy(), o64.energy()
+        o64.pcg(pcg)
+        o64.update()
+        x64 = o64.get(abi.ARRAY_INCREMENT, as_double=True).reshape(-1)
+        x = inst.get_array(abi.ARRAY_INCREMENT).reshape(-1).astype(np.float64)
+        errs.append(float(np.linalg.norm(x - x64) / max(np.linalg.norm(x64), 1e-300)))
+        eerrs.append(abs(eg - eo) / max(abs(eo), 1e-300))
+        field = inst.get_array(abi.ARRAY_NODE_SE3)
+    if g is not None:
+        g.close()
+    return errs, eerrs
 
 
 def time_solves(solve, steps, warmup, stream):
@@ -500,13 +612,24 @@ def run_extra_workload(args):
                     max_feature_terms=max(s.feature.count for s in scenes),
                     max_cross_terms=max(s.cross_view.count for s in scenes))
         cfg_for = lambda sc: abi.make_config(sc)  # noqa: E731 - the oracle sizes each instance itself
-        modes = [("materialized", abi.MODE_MATERIALIZED)]
+        modes = [("materialized", abi.MODE_MATERIALIZED, abi.PRECISION_MIXED)]
+    elif args.workload == "sphere":
+        base = synth.sphere_single_view(seed=1, num_nodes=2048, width=640, height=480)
+        scenes = [synth.perturb_warp_field(base, seed=sd) for sd in instance_seeds(0, args.batch)]
+        gn, pcg = 3, 10
+        caps = None
+        cfg_for = lambda sc: abi.make_config(sc)  # noqa: E731
+        modes = [("materialized", abi.MODE_MATERIALIZED, abi.PRECISION_MIXED),
+                 ("materialized_fp32", abi.MODE_MATERIALIZED, abi.PRECISION_FP32)]
     else:
-        scenes = [synth.articulated_body(auto_radius=True)]
+        # framed tightly (5x the focal length of the other workloads) so that
+        # the body fills about 87 % of each 1280x720 view: ~4M dense terms
+        scenes = [synth.articulated_body(auto_radius=True, focal_scale=5.0)]
         gn, pcg = 8, 20
         caps = None
         cfg_for = lambda sc: abi.make_config(sc)  # noqa: E731
-        modes = [("materialized", abi.MODE_MATERIALIZED), ("matrix_free", abi.MODE_MATRIX_FREE)]
+        modes = [("materialized", abi.MODE_MATERIALIZED, abi.PRECISION_MIXED),
+                 ("matrix_free", abi.MODE_MATRIX_FREE, abi.PRECISION_MIXED)]
     gen_s = time.perf_counter() - t0
     dev = [DeviceScene(sc) for sc in scenes]
     B = len(scenes)
@@ -514,9 +637,9 @@ def run_extra_workload(args):
             "views": [sc.num_views for sc in scenes], "image": [scenes[0].width, scenes[0].height],
             "gn": gn, "pcg": pcg, "generation_s": round(gen_s, 1), "modes": {}}
     incs = None
-    for name, mode in modes:
-        cfg = (abi.make_config(None, precision=abi.PRECISION_MIXED, mode=mode, **caps) if caps
-               else abi.make_config(scenes[0], precision=abi.PRECISION_MIXED, mode=mode))
+    for name, mode, prec in modes:
+        cfg = (abi.make_config(None, precision=prec, mode=mode, **caps) if caps
+               else abi.make_config(scenes[0], precision=prec, mode=mode))
         batch = BatchSolver(cfg, B)
 
         def bind():
@@ -534,12 +657,22 @@ def run_extra_workload(args):
                 batch.solve(gn, pcg, use_graph=False, stream=stream)
                 sp = spmv_stage(lib, abi, batch, stream)
                 counts = [batch.instance(i).counts() for i in range(B)]
-                nbytes = sum(algorithmic_bytes(c, sc.num_nodes, True)["spmv"] for c, sc in zip(counts, scenes))
+                nbytes = sum(algorithmic_bytes(c, sc.num_nodes, prec == abi.PRECISION_MIXED)["spmv"]
+                             for c, sc in zip(counts, scenes))  # the materialised mode
                 peak, _ = load_peaks()
                 entry["spmv"] = {"ms": round(sp, 5), "GBps": round(nbytes / 1e9 / (sp / 1e3), 1),
                                  "frac_of_measured_hbm": round(nbytes / 1e9 / (sp / 1e3) / peak, 4),
                                  "tile": spmv_tile_desc(shape)}
                 entry["dense_terms"] = [c.dense_terms for c in counts]
+                if args.workload == "sphere":
+                    with torch.cuda.stream(stream):
+                        errs, eerrs = increment_errors_vs_fp64(scenes[0], cfg, gn, pcg, batch=batch, bind=bind,
+                                                               stream=stream)
+                    entry["dx_rel_err_vs_fp64"] = [float("%.3g" % e) for e in errs]
+                    entry["energy_rel_err_vs_fp64_max"] = float("%.3g" % max(eerrs))
+                    batch.close()
+                    line["modes"][name] = entry
+                    continue
                 # first increments for the FP64 comparison
                 bind()
                 batch.solve(1, pcg, use_graph=False, stream=stream)
@@ -552,8 +685,8 @@ def run_extra_workload(args):
                                  v.get_array(abi.ARRAY_INCREMENT)))
         line["modes"][name] = entry
         batch.close()
-    # plain FP32 form of the uneven batch: one instance per solve, no graph
-    if args.workload == "uneven":
+    # plain FP32 form: one instance per solve, no graph
+    if args.workload in ("uneven", "sphere"):
         from multiviewdynrecon_b200.solver import NonRigidSolver
         tot = 0.0
         for sc, ds in zip(scenes, dev):
@@ -566,10 +699,16 @@ def run_extra_workload(args):
         line["plain_fp32"] = {"solves_per_s": round(B / (tot / 1e3), 3), "form": "one instance per solve, no graph"}
         line["speedup_vs_plain_fp32"] = round(line["modes"]["materialized"]["solves_per_s"] /
                                               line["plain_fp32"]["solves_per_s"], 3)
-    t1 = time.perf_counter()
-    errs = first_increment_errors(scenes, cfg_for, incs, pcg, os.cpu_count() or 1)
-    line["first_increment_rel_err_vs_fp64"] = [float("%.3g" % e) for e in errs]
-    line["fp64_check_s"] = round(time.perf_counter() - t1, 1)
+    if args.workload == "sphere":
+        # the plain method on the host cores: the oracle's FP32 solve, 1 thread
+        v, n, dt = run_cpu_baseline(argparse.Namespace(gn=gn, pcg=pcg), scenes, 1, min(args.cpu_seconds, 10.0))
+        line["cpu_baseline"] = {"value": round(v, 4), "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": f"{n} whole solves on 1 thread in {dt:.1f} s"}
+    if incs is not None:
+        t1 = time.perf_counter()
+        errs = first_increment_errors(scenes, cfg_for, incs, pcg, os.cpu_count() or 1)
+        line["first_increment_rel_err_vs_fp64"] = [float("%.3g" % e) for e in errs]
+        line["fp64_check_s"] = round(time.perf_counter() - t1, 1)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -673,6 +812,9 @@ def main():
             "e2e": r["e2e"],
             "plain_fp32": r["plain"],
             "speedup_vs_plain_fp32": (round(r["value"] / r["plain"]["value"], 3) if r["plain"] else None),
+            "speedup_vs_plain_fp32_batched": (round(r["value"] / r["plain"]["batched_graph"]["value"], 3)
+                                              if r["plain"] else None),
+            "accuracy": r["accuracy"],
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

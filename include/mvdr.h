@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define MVDR_ABI_VERSION 1u
+#define MVDR_ABI_VERSION 2u
 #define MVDR_MAX_VIEWS 8u
 #define MVDR_INVALID_INDEX 0xFFFFFFFFu
 
@@ -160,6 +160,15 @@ typedef struct mvdr_config {
     /* penalties used when use_elastic_penalty == 0; with the schedule on, the
      * values of PenaltyConstants.cpp:25-51 are used instead. */
     mvdr_penalty penalty;
+    /* density (colour) term: a second scalar residual on every dense-depth
+     * pixel, observed grey level minus the rendered one, as the reference
+     * adds it under USE_DENSE_IMAGE_DENSITY_TERM (PreconditionerBlocked.cu:
+     * 216-219, JtDotResidualIndexed.cu:162-165, JtJMaterializer.cu:312-315,
+     * ResidualEvaluator.cu:94-99). Its weight is 1e-2 in the local phase of
+     * the schedule and 0 in the global phase (PenaltyConstants.cpp:25-45),
+     * penalty.density without the schedule. Needs the three density maps of
+     * every view. */
+    int32_t use_density;
 } mvdr_config;
 
 /* Per-view inputs: the rendered solver maps (Renderer::SolverMaps,
@@ -179,6 +188,10 @@ typedef struct mvdr_view_inputs {
     mvdr_intrinsic intrinsic;                  /* ClipColorIntrinsic[v]                */
     mvdr_mat34 world2camera;                   /* world2Camera[v] (canonical2Live)     */
     mvdr_mat34 initial_camera_se3;             /* InitialCameraSE3[v]: camera v -> 0   */
+    /* density term only (may be NULL otherwise): */
+    const mvdr_float4* normalized_rgb_map;     /* SolverMaps::normalized_rgb_map       */
+    const float* density_map;                  /* CameraObservation::grayScaleMap      */
+    const float* density_gradient_map;         /* grayScaleGradientMap, float2 per pixel */
 } mvdr_view_inputs;
 
 /* Correspondence terms after selection and compaction, as held by
@@ -250,6 +263,62 @@ MVDR_API int mvdr_set_inputs(mvdr_solver* solver, const mvdr_inputs* inputs, voi
  * with larger inputs than before, allocates those device buffers. */
 MVDR_API int mvdr_set_inputs_host(mvdr_solver* solver, const mvdr_inputs* inputs, void* stream);
 
+/* The per-view maps as the reference hands them over: texture objects
+ * (cudaTextureObject_t, passed as uint64_t) of Renderer::SolverMaps
+ * (render/Renderer.h:381-388) and CameraObservation
+ * (base/CameraObservation.h:16-63), which the reference samples with
+ * tex2D at integer pixel coordinates (DenseDepthJacobianResidual.cu:40-41,
+ * 68-69). 0 marks a map that is not used (the foreground maps when the
+ * foreground term is off, the density maps when the density term is off). */
+typedef struct mvdr_view_textures {
+    uint64_t reference_vertex_map;      /* SolverMaps::reference_vertex_map, float4  */
+    uint64_t reference_normal_map;      /* SolverMaps::reference_normal_map, float4  */
+    uint64_t index_map;                 /* SolverMaps::index_map, unsigned int       */
+    uint64_t normalized_rgb_map;        /* SolverMaps::normalized_rgb_map, float4    */
+    uint64_t vertex_confidence_map;     /* CameraObservation::vertexConfidenceMap    */
+    uint64_t normal_radius_map;         /* CameraObservation::normalRadiusMap        */
+    uint64_t filtered_foreground_mask;  /* filteredForegroundMask, float             */
+    uint64_t foreground_mask_gradient;  /* foregroundMaskGradientMap, float2         */
+    uint64_t density_map;               /* grayScaleMap, float                       */
+    uint64_t density_gradient_map;      /* grayScaleGradientMap, float2              */
+} mvdr_view_textures;
+
+/* SetSolverInput with the maps as texture objects (NonRigidSolver.h:133-140
+ * takes Renderer::SolverMaps and CameraObservation, whose maps are texture
+ * objects). textures[v] gives view v's maps; the map pointers and pitch of
+ * inputs->views[v] are ignored, every other field of *inputs is used as by
+ * mvdr_set_inputs (device pointers). Each map's resource (a cudaArray, as
+ * the reference's GL interop and texture helpers create, or pitched / linear
+ * device memory) is copied on `stream` into solver-owned buffers of
+ * image_width x image_height elements; a map of another size or channel
+ * format is rejected with MVDR_EINVAL, a mipmapped array too. The first call
+ * allocates those buffers. The solve then reads the copies, so the textures'
+ * memory may change after the copy has run on the stream. */
+MVDR_API int mvdr_set_inputs_textures(mvdr_solver* solver, const mvdr_inputs* inputs,
+                                      const mvdr_view_textures* textures, void* stream);
+
+/* The solver's warp field in device memory (num_nodes dual quaternions): the
+ * counterpart of the reference's SolvedNodeSE3() device view
+ * (NonRigidSolver.h:214). The pointer stays valid until the solver (or its
+ * batch) is destroyed; its contents are those of the last solve enqueued, so
+ * read it on that stream (or after synchronising it). Device-side errors are
+ * not checked here: read error_flags with mvdr_get_counts. */
+MVDR_API int mvdr_node_se3_device(mvdr_solver* solver, const mvdr_dual_quaternion** device_ptr);
+
+/* ---- input bundles (replay of one solve's inputs) -----------------------
+ * mvdr_save_input_bundle writes the configuration and every input array
+ * bound to the solver (device or owned copies) to a file; it synchronises
+ * `stream`. mvdr_load_input_bundle reads such a file into host memory: the
+ * bundle's config and inputs (HOST pointers into the bundle) can be given to
+ * mvdr_create and mvdr_set_inputs_host to replay the solve, e.g. to reproduce
+ * a parity failure on real inputs. The reference has no counterpart. */
+typedef struct mvdr_input_bundle mvdr_input_bundle;
+MVDR_API int mvdr_save_input_bundle(mvdr_solver* solver, const char* path, void* stream);
+MVDR_API int mvdr_load_input_bundle(const char* path, mvdr_input_bundle** out);
+MVDR_API const mvdr_config* mvdr_input_bundle_config(const mvdr_input_bundle* bundle);
+MVDR_API const mvdr_inputs* mvdr_input_bundle_inputs(const mvdr_input_bundle* bundle);
+MVDR_API void mvdr_free_input_bundle(mvdr_input_bundle* bundle);
+
 /* buildSolverIndexStreamed (NonRigidSolver.h:257, body not in the reference):
  * pixel selection and compaction (ImageTermKNNFetcher.cu:19-137,
  * DensityForegroundMapHandler.cu:34-146), node->term index
@@ -315,7 +384,9 @@ enum {
     MVDR_ARRAY_OFFDIAG_BLOCKS = 19,     /* float [2P][36] in symmetric-key order, blk[6k+r] = A(r,k) */
     MVDR_ARRAY_BINBLOCK_DATA = 20,      /* float [binblock_nnz] bin-block CSR values        */
     MVDR_ARRAY_INCREMENT = 21,          /* float [6N] PCG solution of the last iteration     */
-    MVDR_ARRAY_NODE_SE3 = 22            /* dual quaternion [N] current warp field            */
+    MVDR_ARRAY_NODE_SE3 = 22,           /* dual quaternion [N] current warp field            */
+    MVDR_ARRAY_DENSITY_JACOBIAN = 23    /* float [T_d][8]: density twist gradient (6), residual,
+                                           projected pixel (use_density only)                */
 };
 MVDR_API int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t capacity_bytes,
                    size_t* written_bytes, void* stream);
@@ -422,9 +493,12 @@ enum {
     MVDR_STAGE_PCG_UPDATE = 5, /* one PCG vector update (x, r, s, r.s)           */
     MVDR_STAGE_UPDATE = 6,     /* warp-field update                              */
     MVDR_STAGE_DIRECTION = 7,  /* one PCG direction update d = s + beta d_prev   */
-    MVDR_STAGE_MATRIX_FREE = 8 /* one matrix-free product q = (JtJ + 1e-2 I) d
+    MVDR_STAGE_MATRIX_FREE = 8, /* one matrix-free product q = (JtJ + 1e-2 I) d
                                   and d.q, as J.d per term then Jt per node
                                   (matrix-free mode only; EINVAL otherwise)      */
+    MVDR_STAGE_SCALE = 9       /* the block-Jacobi scaling of the off-diagonal
+                                  blocks into float (mixed precision,
+                                  materialised mode only; EINVAL otherwise)      */
 };
 /* Enqueue the kernels of one stage for every instance of the batch, with the
  * lambdas of Gauss-Newton iteration 0. The stage reads the state left by the

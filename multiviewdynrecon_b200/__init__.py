@@ -41,6 +41,13 @@ def _declare(L):
         "mvdr_destroy": (i32, [vp]),
         "mvdr_set_inputs": (i32, [vp, P(abi.Inputs), vp]),
         "mvdr_set_inputs_host": (i32, [vp, P(abi.Inputs), vp]),
+        "mvdr_set_inputs_textures": (i32, [vp, P(abi.Inputs), vp, vp]),
+        "mvdr_node_se3_device": (i32, [vp, P(vp)]),
+        "mvdr_save_input_bundle": (i32, [vp, C.c_char_p, vp]),
+        "mvdr_load_input_bundle": (i32, [C.c_char_p, P(vp)]),
+        "mvdr_input_bundle_config": (P(abi.Config), [vp]),
+        "mvdr_input_bundle_inputs": (P(abi.Inputs), [vp]),
+        "mvdr_free_input_bundle": (None, [vp]),
         "mvdr_build_index": (i32, [vp, vp]),
         "mvdr_gn_iteration": (i32, [vp, u32, vp]),
         "mvdr_solve": (i32, [vp, u32, u32, vp]),

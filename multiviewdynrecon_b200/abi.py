@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-MVDR_ABI_VERSION = 1
+MVDR_ABI_VERSION = 2
 MVDR_MAX_VIEWS = 8
 MVDR_INVALID_INDEX = 0xFFFFFFFF
 
@@ -21,7 +21,7 @@ MODE_MATERIALIZED, MODE_MATRIX_FREE = 0, 1
 COMPAT_REF_VIEW_LOOKUP = 1
 COMPAT_REF_FOREGROUND_FRAME = 2
 (STAGE_INDEX, STAGE_TERMS, STAGE_DIAG, STAGE_OFFDIAG, STAGE_SPMV, STAGE_PCG_UPDATE, STAGE_UPDATE,
- STAGE_DIRECTION, STAGE_MATRIX_FREE) = range(9)
+ STAGE_DIRECTION, STAGE_MATRIX_FREE, STAGE_SCALE) = range(10)
 # SpMV tile shapes (block rows per CTA, threads per scalar row / 6, form) in
 # the autotuner's order. Form 0 reads a lower block's row and exchanges the
 # column sums through shared memory; form 1 reads its column.
@@ -33,7 +33,8 @@ NUM_SPMV_SHAPES = len(SPMV_SHAPES)
  ARRAY_NODE2TERM_INDEX, ARRAY_HALF_NODEPAIR_KEY, ARRAY_NODEPAIR_TERM_INDEX, ARRAY_NODEPAIR_KEY,
  ARRAY_NODEPAIR_TERM_RANGE, ARRAY_BLKROW_OFFSET, ARRAY_BINBLOCK_ROWPTR, ARRAY_BINBLOCK_COLPTR,
  ARRAY_TERM_JACOBIAN, ARRAY_SMOOTH_TERMS, ARRAY_WARPED_CORRESPONDENCE, ARRAY_DIAG_BLOCKS, ARRAY_JTR,
- ARRAY_PRECONDITIONER, ARRAY_OFFDIAG_BLOCKS, ARRAY_BINBLOCK_DATA, ARRAY_INCREMENT, ARRAY_NODE_SE3) = range(23)
+ ARRAY_PRECONDITIONER, ARRAY_OFFDIAG_BLOCKS, ARRAY_BINBLOCK_DATA, ARRAY_INCREMENT, ARRAY_NODE_SE3,
+ ARRAY_DENSITY_JACOBIAN) = range(24)
 
 
 class Float4(C.Structure):
@@ -68,7 +69,7 @@ class Config(C.Structure):
         ("node_radius", C.c_float), ("precision", C.c_int32), ("mode", C.c_int32),
         ("use_foreground", C.c_int32), ("use_feature", C.c_int32), ("use_cross_view", C.c_int32),
         ("use_elastic_penalty", C.c_int32), ("num_global_iterations", C.c_int32), ("compat_flags", C.c_uint32),
-        ("penalty", Penalty),
+        ("penalty", Penalty), ("use_density", C.c_int32),
     ]
 
 
@@ -79,7 +80,15 @@ class ViewInputs(C.Structure):
         ("filtered_foreground_mask", C.c_void_p), ("foreground_mask_gradient", C.c_void_p),
         ("pitch", C.c_uint32), ("intrinsic", Intrinsic), ("world2camera", Mat34),
         ("initial_camera_se3", Mat34),
+        ("normalized_rgb_map", C.c_void_p), ("density_map", C.c_void_p), ("density_gradient_map", C.c_void_p),
     ]
+
+
+class ViewTextures(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "reference_vertex_map", "reference_normal_map", "index_map", "normalized_rgb_map", "vertex_confidence_map",
+        "normal_radius_map", "filtered_foreground_mask", "foreground_mask_gradient", "density_map",
+        "density_gradient_map")]
 
 
 class Correspondences(C.Structure):
@@ -106,13 +115,13 @@ class Counts(C.Structure):
 STRUCTS = {"mvdr_float4": Float4, "mvdr_dual_quaternion": DualQuaternion, "mvdr_mat34": Mat34,
            "mvdr_intrinsic": Intrinsic, "mvdr_penalty": Penalty, "mvdr_config": Config,
            "mvdr_view_inputs": ViewInputs, "mvdr_correspondences": Correspondences, "mvdr_inputs": Inputs,
-           "mvdr_counts": Counts}
+           "mvdr_counts": Counts, "mvdr_view_textures": ViewTextures}
 
 
 def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=480, precision=PRECISION_MIXED,
                 mode=MODE_MATERIALIZED, use_foreground=None, use_feature=None, use_cross_view=None,
                 max_surfels=None, max_feature_terms=None, max_cross_terms=None, elastic=True,
-                num_global_iterations=1 << 20, compat_flags=0, node_radius=0.025):
+                num_global_iterations=1 << 20, compat_flags=0, node_radius=0.025, use_density=None):
     """Configuration for a scene (or explicit capacities). With the elastic
     schedule on and num_global_iterations large, every iteration uses the
     global lambdas (all terms active)."""
@@ -129,6 +138,8 @@ def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=48
             use_feature = terms.get("feature", False)
         if use_cross_view is None:
             use_cross_view = terms.get("cross_view", False)
+        if use_density is None:
+            use_density = terms.get("density", False)
         max_surfels = max_surfels or scene.num_surfels
         max_feature_terms = max_feature_terms if max_feature_terms is not None else scene.feature.count
         max_cross_terms = max_cross_terms if max_cross_terms is not None else scene.cross_view.count
@@ -154,6 +165,7 @@ def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=48
     cfg.num_global_iterations = num_global_iterations
     cfg.compat_flags = compat_flags
     cfg.penalty = Penalty(2.5, 0.0, 0.0, 0.7, 0.1)  # PenaltyConstants::setDefaultValue
+    cfg.use_density = int(bool(use_density))
     return cfg
 
 
@@ -166,10 +178,12 @@ def _mat34(a):
     return m
 
 
-def fill_inputs(scene, ptr):
+def fill_inputs(scene, ptr, density=False):
     """Build an Inputs struct for `scene`; `ptr(name, array)` returns the
     address to store for each array (a host numpy pointer or a device
-    pointer). Names are stable keys so callers can cache uploads."""
+    pointer). Names are stable keys so callers can cache uploads. The density
+    maps are included only with `density` (a configuration with the density
+    term on)."""
     inp = Inputs()
     inp.num_views = scene.num_views
     inp.num_nodes = scene.num_nodes
@@ -184,6 +198,10 @@ def fill_inputs(scene, ptr):
         vi.normal_radius_map = ptr(f"v{v}.obs_n", view.normal_radius_map)
         vi.filtered_foreground_mask = ptr(f"v{v}.fg", view.filtered_foreground_mask)
         vi.foreground_mask_gradient = ptr(f"v{v}.fg_grad", view.foreground_mask_gradient)
+        if density and getattr(view, "density_map", None) is not None:
+            vi.normalized_rgb_map = ptr(f"v{v}.rgb", view.normalized_rgb_map)
+            vi.density_map = ptr(f"v{v}.dens", view.density_map)
+            vi.density_gradient_map = ptr(f"v{v}.dens_grad", view.density_gradient_map)
         vi.pitch = 0
         vi.intrinsic = Intrinsic(*[float(x) for x in view.intrinsic])
         vi.world2camera = _mat34(view.world2camera)

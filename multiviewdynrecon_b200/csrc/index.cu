@@ -246,8 +246,16 @@ __global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* ins
         } else {
             const float4 cn = V.ref_n[p];
             const float3 b = rot3(V.init, mk3(cn.x, cn.y, cn.z));
+            // the rendered grey level of the density term: rgb2density of the
+            // normalised rgb solver map (ColorTypeTransfer.h:51-56,
+            // DensityForegroundJacobianResidual.cu:51-52)
+            float geo = 0.f;
+            if (I.use_density) {
+                const float4 c = V.rgb[p];
+                geo = 0.299f * c.x + 0.587f * c.y + 0.114f * c.z;
+            }
             I.dense_cv[k] = make_float4(a.x, a.y, a.z, __uint_as_float(v));
-            I.dense_cn[k] = make_float4(b.x, b.y, b.z, 0.f);
+            I.dense_cn[k] = make_float4(b.x, b.y, b.z, geo);
         }
     }
 }

@@ -20,6 +20,10 @@
 
 namespace mvdr {
 
+// reduction region of the density term's energy partials (regions 0-3: the
+// term energy, the PCG delta by parity, d.q)
+constexpr uint32_t kRegDensityEnergy = 4;
+
 // ------------------------------------------------------- term evaluation --
 // The position chain of every term (blend, normalise, warp, camera
 // transforms, projection, residual) runs in T: float reproduces the reference
@@ -42,12 +46,15 @@ template <class T> __device__ inline V3T<T> appv(const R34T<T>& m, V3T<T> v) {
 
 // float -> double by bit manipulation (integer pipe; the FP64 conversion
 // instruction is a narrow pipe on this part). Exact for zero and normal
-// floats; float subnormals become signed zero.
+// floats; float subnormals become signed zero; Inf and NaN stay Inf and NaN
+// (their exponent field maps to the double's all-ones field, so that a NaN in
+// the inputs reaches the non-finite checks instead of a large finite value).
 __device__ inline double f2d(float f) {
     const uint32_t b = __float_as_uint(f);
     const uint32_t em = b & 0x7fffffffu, sign = b & 0x80000000u;
     const bool normal = em >= 0x00800000u;
-    const uint32_t hi = normal ? (sign | ((em >> 3) + (896u << 20))) : sign;
+    const uint32_t bias = em >= 0x7f800000u ? (1792u << 20) : (896u << 20);
+    const uint32_t hi = normal ? (sign | ((em >> 3) + bias)) : sign;
     const uint32_t lo = normal ? (em << 29) : 0u;
     return __hiloint2double((int)hi, (int)lo);
 }
@@ -107,6 +114,21 @@ __device__ inline R34T<T> blended_se3(const DQ* field, const unsigned short* nod
     m.t[1] = a3 * b1 - a0 * b2 + a1 * b3 + a2 * b0;
     m.t[2] = a3 * b2 + a0 * b1 - a1 * b0 + a2 * b3;
     return m;
+}
+
+// computeImageDensityJacobainAndResidual (density_map_jacobian.cuh:54-69): the
+// image gradient `gr` at the projected pixel, chained through the pinhole
+// projection of the camera point vc and the two rotations to a twist
+// gradient at the warped vertex wv: o0 = (rotation part, g.x), g_yz = (g.y, g.z)
+__device__ inline void image_twist_gradient(const ViewDesc& V, float3 vc, float3 wv, float2 gr, float4& o0,
+                                            float2& g_yz) {
+    float3 g;
+    g.x = gr.x * V.fx / vc.z;
+    g.y = gr.y * V.fy / vc.z;
+    g.z = -1.0f / (vc.z * vc.z) * (V.fx * vc.x * gr.x + V.fy * vc.y * gr.y);
+    g = rotT3(V.w2c, rot3(V.init, g));
+    o0 = make_float4(-g.y * wv.z + g.z * wv.y, g.x * wv.z - g.z * wv.x, -g.x * wv.y + g.y * wv.x, g.x);
+    g_yz = make_float2(g.y, g.z);
 }
 
 // 4 CTAs per SM (64 registers, a few spilled) hide the gathers of the warp
@@ -219,15 +241,11 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
             if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height && V.fg != nullptr) {
                 const size_t p = (size_t)w * V.pitch + u;
                 const float img = V.fg[p];
-                const float2 gr = V.fg_grad[p];
-                float3 g;
-                g.x = gr.x * V.fx / vc.z;
-                g.y = gr.y * V.fy / vc.z;
-                g.z = -1.0f / (vc.z * vc.z) * (V.fx * vc.x * gr.x + V.fy * vc.y * gr.y);
-                g = rotT3(V.w2c, rot3(V.init, g));
-                o0 = make_float4(-g.y * wv.z + g.z * wv.y, g.x * wv.z - g.z * wv.x, -g.x * wv.y + g.y * wv.x, g.x);
-                o1 = make_float4(g.y, g.z, img - 0.0f, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
-                nonfinite |= !isfinite(o1.z) || !isfinite(g.x) || !isfinite(g.y) || !isfinite(g.z);
+                float2 gyz;
+                image_twist_gradient(V, vc, wv, V.fg_grad[p], o0, gyz);
+                // geometry density 0 (DensityForegroundJacobianResidual.cu:103)
+                o1 = make_float4(gyz.x, gyz.y, img - 0.0f, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+                nonfinite |= !isfinite(o1.z) || !isfinite(o0.w) || !isfinite(gyz.x) || !isfinite(gyz.y);
             }
             I.term_jr[2 * (size_t)(Td + k)] = o0;
             I.term_jr[2 * (size_t)(Td + k) + 1] = o1;
@@ -270,6 +288,73 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
         double e = 0;
         for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) e += ws[w];
         I.partials[blockIdx.x] = e;
+    }
+}
+
+// computeDensityMapJacobian (DensityForegroundJacobianResidual.cu:41-91): the
+// second residual of every dense pixel, the observed grey level at the
+// projected pixel minus the rendered one, with the image-gradient Jacobian of
+// computeImageDensityJacobainAndResidual. The vertex is warped as the dense
+// term warps it (frame 0), or in its camera's frame under
+// MVDR_COMPAT_REF_FOREGROUND_FRAME. A kernel of its own, launched only when
+// the term is on, so that it adds no registers to the term evaluation. Its
+// weighted squared residuals go to reduction region kRegDensityEnergy.
+template <class T>
+__global__ void __launch_bounds__(256, 2) eval_density_kernel(const InstDesc* insts, mvdr_penalty lam) {
+    const InstDesc& I = insts[blockIdx.y];
+    const uint32_t Td = bad_inputs(I) ? 0u : I.counts->term_offset[0];
+    double energy = 0;
+    bool nonfinite = false;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < Td; k += gridDim.x * blockDim.x) {
+        const float4 cv = I.dense_cv[k], cn = I.dense_cn[k];
+        const ViewDesc& V = I.views[__float_as_uint(cv.w)];
+        const ushort4 kn = I.dense_knn[k];
+        const float4 w4 = I.dense_w[k];
+        const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
+        const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
+        const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
+        const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
+        V3T<T> p0;
+        if (I.compat & MVDR_COMPAT_REF_FOREGROUND_FRAME) {
+            const ushort4 px = I.dense_pix[k];
+            const float4 rv = V.ref_v[(size_t)px.y * V.pitch + px.x];
+            p0 = v3t(cvt<T>(rv.x), cvt<T>(rv.y), cvt<T>(rv.z));
+        } else {
+            p0 = v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z));
+            if constexpr (sizeof(T) == 8) {
+                const float4 lo = I.dense_cv_lo[k];
+                p0 = v3t(p0.x + cvt<T>(lo.x), p0.y + cvt<T>(lo.y), p0.z + cvt<T>(lo.z));
+            }
+        }
+        const V3T<T> wr = appv(se3, p0);
+        const V3T<T> vr = appv(iinv, appv(w2c, wr));
+        const float3 wvf = mk3((float)wr.x, (float)wr.y, (float)wr.z);
+        const float3 vcf = mk3((float)vr.x, (float)vr.y, (float)vr.z);
+        const int u = project_coord((float)vr.x, (float)vr.z, V.fx, V.cx);
+        const int w = project_coord((float)vr.y, (float)vr.z, V.fy, V.cy);
+        nonfinite |= !isfinite(vcf.x) || !isfinite(vcf.y) || !isfinite(vcf.z);
+        float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f), d1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
+        if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height) {
+            const size_t p = (size_t)w * V.pitch + u;
+            float2 gyz;
+            image_twist_gradient(V, vcf, wvf, V.dens_grad[p], d0, gyz);
+            d1 = make_float4(gyz.x, gyz.y, V.dens[p] - cn.w, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+            nonfinite |= !isfinite(d1.z) || !isfinite(d0.w) || !isfinite(gyz.x) || !isfinite(gyz.y);
+        }
+        I.density_jr[2 * (size_t)k] = d0;
+        I.density_jr[2 * (size_t)k + 1] = d1;
+        const float dv = lam.density * d1.z;
+        energy += (double)dv * dv;
+    }
+    if (__any_sync(0xffffffffu, nonfinite) && lane_id() == 0) set_error(I, kErrNonFinite);
+    __shared__ double ws[8];
+    energy = warp_sum(energy);
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = energy;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double e = 0;
+        for (uint32_t q = 0; q < (blockDim.x >> 5); ++q) e += ws[q];
+        I.partials[(size_t)kRegDensityEnergy * I.part_stride + blockIdx.x] = e;
     }
 }
 
@@ -505,6 +590,10 @@ __global__ void __launch_bounds__(128, 4) diag_rhs_kernel(const InstDesc* insts,
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const Acc l2_fg = (Acc)(lam.foreground * lam.foreground), l2_smooth = (Acc)(lam.smooth * lam.smooth);
     const Acc l2_feat = (Acc)(lam.feature * lam.feature), l2_cross = (Acc)(lam.cross_view * lam.cross_view);
+    // the density channel of the dense pixels (0 when the term is off or its
+    // weight is 0 in this iteration's phase)
+    const bool dens_on = I.use_density && lam.density != 0.f;
+    const Acc l2_dens = (Acc)(lam.density * lam.density);
     // the upper-triangle entry (orr, okk) of D whose total this lane receives
     uint32_t orr = 0, okk = 0;
     for (uint32_t r = 0, q = 0; r < 6; ++r)
@@ -547,14 +636,26 @@ __global__ void __launch_bounds__(128, 4) diag_rhs_kernel(const InstDesc* insts,
                 uint32_t k;
                 const TermType ty = off.typed(t, k);
                 if (ty == kDense || ty == kForeground) {
-                    if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0, r = 0
-                    const Acc l2 = ty == kDense ? (Acc)1 : l2_fg;
                     const Acc w = (Acc)wf;
-                    const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
-                    const Acc sw = l2 * w * w, rw = -l2 * w * (Acc)b.z;
+                    if (__float_as_uint(b.w) != kInvalid) {  // an invalid term has J = 0, r = 0
+                        const Acc l2 = ty == kDense ? (Acc)1 : l2_fg;
+                        const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
+                        const Acc sw = l2 * w * w, rw = -l2 * w * (Acc)b.z;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) R[q] += rw * g[q];
-                    add_scaled_outer(S, sw, g);
+                        for (int q = 0; q < 6; ++q) R[q] += rw * g[q];
+                        add_scaled_outer(S, sw, g);
+                    }
+                    if (ty == kDense && dens_on) {
+                        float4 da, db;
+                        load_record32(I.density_jr + 2 * (size_t)k, da, db);
+                        if (__float_as_uint(db.w) != kInvalid) {
+                            const Acc g[6] = {(Acc)da.x, (Acc)da.y, (Acc)da.z, (Acc)da.w, (Acc)db.x, (Acc)db.y};
+                            const Acc sw = l2_dens * w * w, rw = -l2_dens * w * (Acc)db.z;
+#pragma unroll
+                            for (int q = 0; q < 6; ++q) R[q] += rw * g[q];
+                            add_scaled_outer(S, sw, g);
+                        }
+                    }
                 } else if (ty == kSmooth) {
                     // computeSmoothTermJacobian (geometry_icp_jacobian.cuh:323-343):
                     // J_i,c = f_c(T_i x_j), J_j,c = -f_c(T_j x_j)
@@ -678,6 +779,8 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
     const uint32_t P = C->half_pairs;
     const Acc l2_fg = (Acc)(lam.foreground * lam.foreground);
     const Acc l2_feat = (Acc)(lam.feature * lam.feature), l2_cross = (Acc)(lam.cross_view * lam.cross_view);
+    const bool dens_on = I.use_density && lam.density != 0.f;
+    const Acc l2_dens = (Acc)(lam.density * lam.density);
     // pairs grouped by entry count, so the lanes of a warp loop equally long
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
         const uint32_t h = I.pair_order[i];
@@ -714,11 +817,20 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
             uint32_t k;
             const TermType ty = off.typed(t, k);
             if (ty == kDense || ty == kForeground) {
-                if (__float_as_uint(b.w) == kInvalid) continue;  // invalid term: J = 0
-                Acc s = (Acc)wij.x * (Acc)wij.y;
-                if (ty == kForeground) s *= l2_fg;
-                const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
-                add_scaled_outer(S, s, g);
+                const Acc wij2 = (Acc)wij.x * (Acc)wij.y;
+                if (__float_as_uint(b.w) != kInvalid) {  // an invalid term has J = 0
+                    const Acc s = ty == kForeground ? wij2 * l2_fg : wij2;
+                    const Acc g[6] = {(Acc)a.x, (Acc)a.y, (Acc)a.z, (Acc)a.w, (Acc)b.x, (Acc)b.y};
+                    add_scaled_outer(S, s, g);
+                }
+                if (ty == kDense && dens_on) {
+                    float4 da, db;
+                    load_record32(I.density_jr + 2 * (size_t)k, da, db);
+                    if (__float_as_uint(db.w) != kInvalid) {
+                        const Acc g[6] = {(Acc)da.x, (Acc)da.y, (Acc)da.z, (Acc)da.w, (Acc)db.x, (Acc)db.y};
+                        add_scaled_outer(S, wij2 * l2_dens, g);
+                    }
+                }
             } else if (ty == kSmooth) {
                 if (smooth_k[0] == kInvalid) smooth_k[0] = k;
                 else smooth_k[1] = k;
@@ -770,6 +882,98 @@ __global__ void __launch_bounds__(128, 4) offdiag_kernel(const InstDesc* insts, 
                     if (has[m]) v += l2_smooth * twist_rows_product<Acc>(pi[m], pj[m], r, k);
                 out[blk_idx(r, k)] = v;
             }
+    }
+}
+
+// ------------------------------------------------ scaled operator -------
+// Mixed precision, materialised: the PCG runs on A^ = L^-1 A L^-T, where
+// D_i = L_i L_i^T are the damped diagonal blocks (block-Jacobi scaling). Its
+// diagonal blocks are the identity and its off-diagonal blocks
+// A^_ij = L_i^-1 A_ij L_j^-T have entries of order one, so float storage and a
+// float SpMV perturb the increment by about 1e-6 of its size, where float
+// storage of A itself (condition numbers of the blocks up to 1e5) moves it by
+// 1e-4 to 5e-4. In exact arithmetic the iterates are those of block-Jacobi PCG
+// on A (BlockPCG.cuh:65-181): x = L^-T x^, r^ = L^-1 r, and r^.r^ = r.M^-1 r.
+// This kernel forms A^_ij from the double block A_ij (i < j) that
+// offdiag_kernel stored: 8 lanes per pair, lane k of the first six solves
+// column k of L_i Y = A_ij, the pair's lanes exchange Y through shared memory,
+// and lane k then solves L_j z = Y(k, :)^T, which is row k of A^_ij.
+constexpr uint32_t kScalePairsPerCta = 16;
+
+__device__ inline void chol_forward(const double* L, const double* b, double* y) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+        double t = b[r];
+#pragma unroll
+        for (int m = 0; m < r; ++m) t -= L[r * (r + 1) / 2 + m] * y[m];
+        y[r] = t * L[r * (r + 1) / 2 + r];  // the diagonal holds reciprocals
+    }
+}
+
+__device__ inline void chol_backward(const double* L, const double* y, double* x) {
+#pragma unroll
+    for (int r = 5; r >= 0; --r) {
+        double t = y[r];
+#pragma unroll
+        for (int m = r + 1; m < 6; ++m) t -= L[m * (m + 1) / 2 + r] * x[m];
+        x[r] = t * L[r * (r + 1) / 2 + r];
+    }
+}
+
+__global__ void __launch_bounds__(128) scale_offdiag_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (!index_complete(I)) return;
+    const uint32_t P = I.counts->half_pairs;
+    __shared__ double s_y[kScalePairsPerCta][6][7];
+    const uint32_t lp = threadIdx.x >> 3, k = threadIdx.x & 7;
+    for (uint32_t base = blockIdx.x * kScalePairsPerCta; base < P; base += gridDim.x * kScalePairsPerCta) {
+        const uint32_t h = base + lp;
+        const bool has = h < P && k < 6;
+        size_t blk = 0;
+        uint32_t j = 0;
+        if (has) {
+            const uint32_t key = I.half_key[h];
+            const uint32_t i = key / I.enc;
+            j = key % I.enc;
+            blk = 36 * (size_t)(h + i + 1);
+            double L[21], a[6], y[6];
+#pragma unroll
+            for (int q = 0; q < 21; ++q) L[q] = I.chol[21 * (size_t)i + q];
+#pragma unroll
+            for (int r = 0; r < 6; ++r) a[r] = I.bsr_d[blk + blk_idx(r, k)];
+            chol_forward(L, a, y);
+#pragma unroll
+            for (int r = 0; r < 6; ++r) s_y[lp][r][k] = y[r];
+        }
+        __syncwarp();  // the 8 lanes of a pair are in one warp
+        if (has) {
+            double L[21], yr[6], z[6];
+#pragma unroll
+            for (int q = 0; q < 21; ++q) L[q] = I.chol[21 * (size_t)j + q];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) yr[c] = s_y[lp][k][c];
+            chol_forward(L, yr, z);
+            float2* out = reinterpret_cast<float2*>(I.bsr_s + blk + 6 * k);
+            out[0] = make_float2((float)z[0], (float)z[1]);
+            out[1] = make_float2((float)z[2], (float)z[3]);
+            out[2] = make_float2((float)z[4], (float)z[5]);
+        }
+        __syncwarp();
+    }
+}
+
+// x = L^-T x^ per node: the increment of the unscaled system, in place
+__global__ void __launch_bounds__(128) pcg_unscale_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
+        double L[21], xh[6], x[6];
+#pragma unroll
+        for (int q = 0; q < 21; ++q) L[q] = I.chol[21 * (size_t)node + q];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) xh[q] = I.x_d[6 * (size_t)node + q];
+        chol_backward(L, xh, x);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) I.x_d[6 * (size_t)node + q] = x[q];
     }
 }
 
@@ -840,9 +1044,12 @@ template <class T> __device__ inline T pcg_alpha(const InstDesc& I, T delta, T d
 // ---------------------------------------------------------------- PCG -----
 
 // blockPCGZeroInitKernel (BlockPCG.cuh:65-111): r = b, s = M^-1 b, x = 0,
-// delta = r.s; the first direction is d = s (beta = 0)
-template <bool MIXED>
+// delta = r.s; the first direction is d = s (beta = 0). SCALED (the scaled
+// operator A^ of the materialised mixed mode): r^ = L^-1 b, s = r^,
+// delta = r^.r^, the same delta.
+template <bool MIXED, bool SCALED>
 __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
+    static_assert(MIXED || !SCALED, "the scaled operator is mixed precision");
     const InstDesc& I = insts[blockIdx.y];
     using T = typename std::conditional<MIXED, double, float>::type;
     using PV = PcgVec<MIXED>;
@@ -851,7 +1058,14 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
         T bv[6], sv[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) bv[i] = PV::jtr(I)[6 * (size_t)node + i];
-        if constexpr (MIXED) {
+        if constexpr (SCALED) {
+            double L[21];
+#pragma unroll
+            for (int q = 0; q < 21; ++q) L[q] = I.chol[21 * (size_t)node + q];
+            chol_forward(L, bv, sv);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) bv[i] = sv[i];
+        } else if constexpr (MIXED) {
             cholesky6_solve(I.chol + 21 * (size_t)node, bv, sv);
         } else {
 #pragma unroll
@@ -897,8 +1111,9 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
 
 // ----------------------------------------------------- PCG direction ----
 // d = s + beta d_prev (BlockPCG.cuh:167-181), formed once per iteration for
-// the whole vector, so that the SpMV reads its operand directly
-template <bool MIXED>
+// the whole vector, so that the SpMV reads its operand directly. SCALED: s is
+// r^ itself, and the float copy of d that the float SpMV reads is written too.
+template <bool MIXED, bool SCALED>
 __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* insts, int parity, int first,
                                                             uint32_t nd) {
     const InstDesc& I = insts[blockIdx.y];
@@ -907,9 +1122,14 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
     // one element per thread (the grid covers 6N), loaded before beta's sums
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     const bool has = e < 6 * I.N;
-    const T sv = has ? PV::s(I)[e] : (T)0, dp = has ? PV::d(I, !parity)[e] : (T)0;
+    const T* sp = SCALED ? PV::r(I) : PV::s(I);
+    const T sv = has ? sp[e] : (T)0, dp = has ? PV::d(I, !parity)[e] : (T)0;
     const T beta = pcg_beta<T>(I, parity, first, nd);
-    if (has) PV::d(I, parity)[e] = sv + beta * dp;
+    if (has) {
+        const T d = sv + beta * dp;
+        PV::d(I, parity)[e] = d;
+        if constexpr (SCALED) I.df[e] = (float)d;
+    }
 }
 
 // ------------------------------------------------------- tiled SpMV -----
@@ -1062,20 +1282,121 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_col_kerne
     store_block_partial<T>(I, kRegDq, part);
 }
 
+// SpMV of the scaled operator (mixed precision, materialised):
+// q^_i = d^_i + sum_{j != i} A^_ij d^_j. The identity diagonal is not read;
+// the off-diagonal blocks are float, row-major, and the product runs in
+// float on the float copy of d^ (about 1e-7 relative per row, far below the
+// 1e-4 budget of the increment); q^ and the d^.q^ partial are double. An
+// upper entry (j > i) reads row r of its stored block; a lower entry reads
+// the stored A^_ji, whose column r is row r of A^_ij: FORM 1 reads that
+// column (six 4-byte loads), FORM 0 reads row r of A^_ji and adds d^_j(r)
+// times it to all six rows, which the row's threads sum through shared
+// memory at the end. With row-major float blocks the six threads of a row
+// read one stored block as 144 contiguous bytes.
+template <uint32_t kTileRows, uint32_t kTileSplit, uint32_t kForm>
+__global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_kernel(const InstDesc* insts,
+                                                                                  int parity) {
+    static_assert((6 * kTileSplit * kTileRows) % 32 == 0, "whole warps");
+    constexpr uint32_t kSlots = kForm == 0 ? 7 : 1;  // per thread: column sums (form 0) and its row sum
+    __shared__ float s_x[(kForm == 0 || kTileSplit > 1) ? kTileRows * kTileSplit * 6 * kSlots : 1];
+    const InstDesc& I = insts[blockIdx.y];
+    const float* store = I.bsr_s;
+    const float* xf = I.df;
+    const double* xd = PcgVec<true>::d(I, parity);
+    const uint32_t t = threadIdx.x;
+    double part = 0;
+    const uint32_t r0 = blockIdx.x * kTileRows;
+    if (r0 < I.N && index_complete(I)) {
+        const uint32_t r1 = min(r0 + kTileRows, I.N);
+        const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
+        const bool computes = row < r1;
+        float acc = 0.f;
+        float col_acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (computes) {
+            // the row's first entry is its diagonal block: the identity, added below
+            const uint32_t rb = I.blkrow_offset[row] + row + 1, re = I.blkrow_offset[row + 1] + row + 1;
+#pragma unroll 2
+            for (uint32_t b = rb + half; b < re; b += kTileSplit) {
+                const uint2 ent = I.bsr_ent[b];
+                const float* blk = store + 36 * (size_t)(ent.x & ~kTransposedBlock);
+                const float2* x2 = reinterpret_cast<const float2*>(xf + 6 * (size_t)ent.y);
+                const bool lower = (ent.x & kTransposedBlock) != 0;
+                if (kForm == 0 && lower) {
+                    const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
+                    const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
+                    const float xr = xf[6 * (size_t)ent.y + rr];
+                    col_acc[0] += a01.x * xr; col_acc[1] += a01.y * xr; col_acc[2] += a23.x * xr;
+                    col_acc[3] += a23.y * xr; col_acc[4] += a45.x * xr; col_acc[5] += a45.y * xr;
+                } else {
+                    float av[6];
+                    if (lower) {
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) av[k] = blk[6 * k + rr];
+                    } else {
+                        const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
+                        const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
+                        av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y; av[4] = a45.x; av[5] = a45.y;
+                    }
+                    const float2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
+                    acc += av[0] * x01.x + av[1] * x01.y + av[2] * x23.x + av[3] * x23.y + av[4] * x45.x +
+                           av[5] * x45.y;
+                }
+            }
+        }
+        if constexpr (kForm == 0 || kTileSplit > 1) {
+            // slot 6 (form 0) / slot 0 holds a thread's row sum, slots 0-5 its column sums
+            float* mine = s_x + ((lr * kTileSplit + half) * 6 + rr) * kSlots;
+            if (computes) {
+                if constexpr (kForm == 0) {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) mine[k] = col_acc[k];
+                    mine[6] = acc;
+                } else {
+                    mine[0] = acc;
+                }
+            }
+            __syncthreads();
+            if (computes && half == 0) {
+                acc = 0.f;
+#pragma unroll
+                for (uint32_t hh = 0; hh < kTileSplit; ++hh) {
+                    const float* base = s_x + (lr * kTileSplit + hh) * 6 * kSlots;
+                    if constexpr (kForm == 0) {
+                        acc += base[rr * kSlots + 6];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) acc += base[c * kSlots + rr];
+                    } else {
+                        acc += base[rr];
+                    }
+                }
+            }
+        }
+        if (computes && half == 0) {
+            const size_t e = 6 * (size_t)row + rr;
+            const double dv = xd[e];
+            const double q = dv + (double)acc;
+            PcgVec<true>::q(I)[e] = q;
+            part += dv * q;
+        }
+    }
+    store_block_partial<double>(I, kRegDq, part);
+}
+
 // blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): alpha = delta / d.q,
 // x += alpha d, r -= alpha q, s = M^-1 r, delta_new = r.s (beta follows in
 // the next direction). A thread per node; the grid covers every node. The
 // node's vectors and preconditioner are loaded before the partial sums, so
 // their latency overlaps the sums. `nd` and `nq`: CTAs of the launches that
-// stored the delta and d.q partials.
-template <bool MIXED>
+// stored the delta and d.q partials. SCALED: the preconditioner is the
+// identity (s = r^, not stored), delta_new = r^.r^.
+template <bool MIXED, bool SCALED>
 __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity, uint32_t nd,
                                                          uint32_t nq) {
     const InstDesc& I = insts[blockIdx.y];
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
     using T2 = typename Pair<T>::type;
-    constexpr int kPre = MIXED ? 21 : 36;  // Cholesky factor / inverse entries
+    constexpr int kPre = SCALED ? 1 : (MIXED ? 21 : 36);  // Cholesky factor / inverse entries
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
     const bool has = node < I.N;
     T xv[6], dv[6], rv[6], qv[6];
@@ -1096,7 +1417,8 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
         load6(PV::q(I), qv);
 #pragma unroll
         for (int i = 0; i < kPre; ++i) {
-            if constexpr (MIXED) pre[i] = I.chol[21 * (size_t)node + i];
+            if constexpr (SCALED) pre[i] = 0;
+            else if constexpr (MIXED) pre[i] = I.chol[21 * (size_t)node + i];
             else pre[i] = I.minv[36 * (size_t)node + i];
         }
     }
@@ -1111,7 +1433,10 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
             xv[i] += alpha * dv[i];
             rv[i] -= alpha * qv[i];
         }
-        if constexpr (MIXED) {
+        if constexpr (SCALED) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) sv[i] = rv[i];
+        } else if constexpr (MIXED) {
             cholesky6_solve(pre, rv, sv);
         } else {
 #pragma unroll
@@ -1134,7 +1459,7 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
         };
         store6(PV::x(I), xv);
         store6(PV::r(I), rv);
-        store6(PV::s(I), sv);
+        if constexpr (!SCALED) store6(PV::s(I), sv);
 #pragma unroll
         for (int i = 0; i < 6; ++i) part += rv[i] * sv[i];
     }
@@ -1219,7 +1544,8 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
     uint32_t passed = 0;
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
     const bool index_ok = index_complete(I);
-    // init: r = b, s = M^-1 b, x = 0, d_prev = 0, delta_0
+    // init: r = b, s = M^-1 b, x = 0, d_prev = 0, delta_0. Mixed precision
+    // runs on the scaled operator (scale_offdiag_kernel): r^ = L^-1 b, s = r^.
     {
         T part = 0;
         for (uint32_t node = c * nt + tid; node < I.N; node += nc * nt) {
@@ -1227,7 +1553,12 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
 #pragma unroll
             for (int i = 0; i < 6; ++i) bv[i] = PV::jtr(I)[6 * (size_t)node + i];
             if constexpr (MIXED) {
-                cholesky6_solve(I.chol + 21 * (size_t)node, bv, sv);
+                double L[21];
+#pragma unroll
+                for (int q = 0; q < 21; ++q) L[q] = I.chol[21 * (size_t)node + q];
+                chol_forward(L, bv, sv);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) bv[i] = sv[i];
             } else {
 #pragma unroll
                 for (int j = 0; j < 6; ++j) {
@@ -1257,11 +1588,50 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
             const T beta = pcg_beta<T>(I, parity, it == 0, nc);
             const T* dprev = PV::d(I, !parity);
             T* dcur = PV::d(I, parity);
-            for (uint32_t e = c * nt + tid; e < 6 * I.N; e += nc * nt) dcur[e] = PV::s(I)[e] + beta * dprev[e];
+            const T* sv = MIXED ? PV::r(I) : PV::s(I);
+            for (uint32_t e = c * nt + tid; e < 6 * I.N; e += nc * nt) {
+                const T dv = sv[e] + beta * dprev[e];
+                dcur[e] = dv;
+                if constexpr (MIXED) I.df[e] = (float)dv;
+            }
         }
         if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
-        // SpMV over tiles of kPersistRows block rows, column form
-        {
+        // SpMV over tiles of kPersistRows block rows, column form (mixed
+        // precision: the scaled operator in float, as pcg_spmv_scaled_kernel)
+        if constexpr (MIXED) {
+            const double* xd = PV::d(I, parity);
+            double part = 0;
+            const uint32_t lr = tid / 6, rr = tid % 6;
+            for (uint32_t r0 = c * kPersistRows; index_ok && r0 < I.N; r0 += nc * kPersistRows) {
+                const uint32_t row = r0 + lr;
+                if (lr >= kPersistRows || row >= I.N) continue;
+                const uint32_t rb = I.blkrow_offset[row] + row + 1, re = I.blkrow_offset[row + 1] + row + 1;
+                float acc = 0.f;
+#pragma unroll 2
+                for (uint32_t b = rb; b < re; ++b) {
+                    const uint2 ent = I.bsr_ent[b];
+                    const float* blk = I.bsr_s + 36 * (size_t)(ent.x & ~kTransposedBlock);
+                    const float2* x2 = reinterpret_cast<const float2*>(I.df + 6 * (size_t)ent.y);
+                    float av[6];
+                    if (ent.x & kTransposedBlock) {
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) av[k] = blk[6 * k + rr];
+                    } else {
+                        const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
+                        const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
+                        av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y; av[4] = a45.x; av[5] = a45.y;
+                    }
+                    const float2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
+                    acc += av[0] * x01.x + av[1] * x01.y + av[2] * x23.x + av[3] * x23.y + av[4] * x45.x +
+                           av[5] * x45.y;
+                }
+                const size_t e = 6 * (size_t)row + rr;
+                const double q = xd[e] + (double)acc;
+                PV::q(I)[e] = q;
+                part += xd[e] * q;
+            }
+            store_block_partial<double>(I, kRegDq, part, c);
+        } else {
             const V* store = BlockStore<MIXED>::ptr(I);
             const V* xvec = PV::d(I, parity);
             T part = 0;
@@ -1315,7 +1685,8 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
                     PV::r(I)[e] = rv[i];
                 }
                 if constexpr (MIXED) {
-                    cholesky6_solve(I.chol + 21 * (size_t)node, rv, sv);
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) sv[i] = rv[i];  // the scaled operator: s = r^
                 } else {
 #pragma unroll
                     for (int j = 0; j < 6; ++j) {
@@ -1327,13 +1698,26 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
                 }
 #pragma unroll
                 for (int i = 0; i < 6; ++i) {
-                    PV::s(I)[6 * (size_t)node + i] = sv[i];
+                    if constexpr (!MIXED) PV::s(I)[6 * (size_t)node + i] = sv[i];
                     part += rv[i] * sv[i];
                 }
             }
             store_block_partial<T>(I, kRegDelta + (parity ^ 1), part, c);
         }
         if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
+    }
+    // mixed precision: x = L^-T x^ for this CTA's nodes (the nodes it updated)
+    if constexpr (MIXED) {
+        for (uint32_t node = c * nt + tid; node < I.N; node += nc * nt) {
+            double L[21], xh[6], x[6];
+#pragma unroll
+            for (int q = 0; q < 21; ++q) L[q] = I.chol[21 * (size_t)node + q];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) xh[q] = I.x_d[6 * (size_t)node + q];
+            chol_backward(L, xh, x);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) I.x_d[6 * (size_t)node + q] = x[q];
+        }
     }
 }
 
@@ -1382,6 +1766,16 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
 #pragma unroll
             for (int i = 0; i < 6; ++i) o += g[i] * pb[i];
             jp[t] = o;
+            if (ty == kDense && I.use_density && lam.density != 0.f) {
+                // the density channel of the pixel (channel 1)
+                float4 da, db;
+                load_record32(I.density_jr + 2 * (size_t)k, da, db);
+                const Acc gd[6] = {(Acc)da.x, (Acc)da.y, (Acc)da.z, (Acc)da.w, (Acc)db.x, (Acc)db.y};
+                Acc od = 0;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) od += gd[i] * pb[i];
+                jp[(size_t)T + t] = od;  // a zero record (invalid term) gives 0
+            }
             continue;
         }
         const int m = ty == kSmooth ? 2 : 4;
@@ -1427,6 +1821,8 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
     const T* dcur = PV::d(I, parity);
     const T* jp = reinterpret_cast<const T*>(I.jp);
     const T l2_fg = (T)(lam.foreground * lam.foreground);
+    const bool dens_on = I.use_density && lam.density != 0.f;
+    const T l2_dens = (T)(lam.density * lam.density);
     T part = 0;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
@@ -1440,11 +1836,20 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
                 const uint32_t idx = ty == kDense ? k : off.o[0] + k;
                 float4 ra, rb;
                 load_record32(I.term_jr + 2 * (size_t)idx, ra, rb);
-                const T sc = (ty == kDense ? (T)1 : l2_fg) * (T)I.n2t_w[p];
+                const T wn = (T)I.n2t_w[p];
+                const T sc = (ty == kDense ? (T)1 : l2_fg) * wn;
                 const T y = jp[t];
                 const float g[6] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y};
 #pragma unroll
                 for (int i = 0; i < 6; ++i) acc[i] += sc * (T)g[i] * y;
+                if (ty == kDense && dens_on) {
+                    float4 da, db;
+                    load_record32(I.density_jr + 2 * (size_t)k, da, db);
+                    const T sd = l2_dens * wn, yd = jp[(size_t)Tn + t];
+                    const float gd[6] = {da.x, da.y, da.z, da.w, db.x, db.y};
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) acc[i] += sd * (T)gd[i] * yd;
+                }
                 continue;
             }
             TermRows tr;
@@ -1581,11 +1986,14 @@ __global__ void __launch_bounds__(128) update_kernel(const InstDesc* insts) {
 // computeTermResidualKernel (ResidualEvaluator.cu:71-142): sum (lambda r)^2
 // The energy of the linearisation point: the term evaluation's `count`
 // per-CTA partials summed in a fixed order (one CTA per instance)
-__global__ void __launch_bounds__(256) energy_sum_kernel(const InstDesc* insts, uint32_t count, uint32_t slot) {
+__global__ void __launch_bounds__(256) energy_sum_kernel(const InstDesc* insts, uint32_t count, uint32_t slot,
+                                                         uint32_t density_count) {
     const InstDesc& I = insts[blockIdx.y];
     __shared__ double ws[8];
     double e = 0;
     for (uint32_t c = threadIdx.x; c < count; c += blockDim.x) e += I.partials[c];
+    for (uint32_t c = threadIdx.x; c < density_count; c += blockDim.x)
+        e += I.partials[(size_t)kRegDensityEnergy * I.part_stride + c];
     e = warp_sum(e);
     if (lane_id() == 0) ws[threadIdx.x >> 5] = e;
     __syncthreads();
@@ -1634,11 +2042,26 @@ static uint32_t eval_terms_grid(const LaunchCfg& lc) {
     return min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
 }
 
+// CTAs per instance of the density kernel
+static uint32_t eval_density_grid(const LaunchCfg& lc) {
+    return min((lc.cap_dense + 255) / 256, (uint32_t)lc.sm_count * 8);
+}
+
 cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, cudaStream_t st) {
     const uint32_t g = eval_terms_grid(lc);
     if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(eval_terms_kernel<double>, grid2(g, lc.B), 256, 0, st, d, lam);
     else MVDR_LAUNCH(eval_terms_kernel<float>, grid2(g, lc.B), 256, 0, st, d, lam);
+    if (lc.use_density) {
+        const uint32_t gd = eval_density_grid(lc);
+        if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(eval_density_kernel<double>, grid2(gd, lc.B), 256, 0, st, d, lam);
+        else MVDR_LAUNCH(eval_density_kernel<float>, grid2(gd, lc.B), 256, 0, st, d, lam);
+    }
     return cudaGetLastError();
+}
+
+// CTAs per instance of the operator scaling (16 pairs per CTA)
+static uint32_t scale_grid(const LaunchCfg& lc) {
+    return min((lc.cap_pairs + kScalePairsPerCta - 1) / kScalePairsPerCta, (uint32_t)lc.sm_count * 16);
 }
 
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, bool materialize,
@@ -1648,14 +2071,19 @@ cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty
     else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
     if (materialize) {
         const uint32_t gp = min((lc.cap_pairs + 127) / 128, (uint32_t)lc.sm_count * 8);
-        if (lc.precision == MVDR_PRECISION_MIXED) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, st, d, lam);
-        else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, st, d, lam);
+        if (lc.precision == MVDR_PRECISION_MIXED) {
+            MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, st, d, lam);
+            MVDR_LAUNCH(scale_offdiag_kernel, grid2(scale_grid(lc), lc.B), 128, 0, st, d);
+        } else {
+            MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, st, d, lam);
+        }
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, uint32_t slot, cudaStream_t st) {
-    MVDR_LAUNCH(energy_sum_kernel, grid2(1, lc.B), 256, 0, st, d, eval_terms_grid(lc), slot);
+    MVDR_LAUNCH(energy_sum_kernel, grid2(1, lc.B), 256, 0, st, d, eval_terms_grid(lc), slot,
+                lc.use_density ? eval_density_grid(lc) : 0u);
     return cudaGetLastError();
 }
 
@@ -1710,14 +2138,18 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gwarp = (lc.max_nodes + 7) / 8;
     const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-    if (mixed) MVDR_LAUNCH(pcg_init_kernel<true>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
-    else MVDR_LAUNCH(pcg_init_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
+    // mixed precision, materialised: PCG on the scaled operator (scale_offdiag_kernel)
+    const bool scaled = mixed && lc.mode == MVDR_MODE_MATERIALIZED;
+    if (scaled) MVDR_LAUNCH((pcg_init_kernel<true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
+    else if (mixed) MVDR_LAUNCH((pcg_init_kernel<true, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
+    else MVDR_LAUNCH((pcg_init_kernel<false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d);
     for (uint32_t it = 0; it < iters; ++it) {
         const int parity = (int)(it & 1u), first = it == 0;
         uint32_t nq;  // CTAs that store the d.q partials
         // d = s + beta d_prev, then q = A d with its d.q partials
-        if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
-        else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+        if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+        else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+        else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
             // J.d per term, then Jt per node (+ damping, q, d.q)
             if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
@@ -1730,9 +2162,11 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
             if (e != cudaSuccess) return e;
             nq = spmv_grid(lc);
         }
-        if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
-        else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
+        if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
+        else if (mixed) MVDR_LAUNCH((pcg_update_kernel<true, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
+        else MVDR_LAUNCH((pcg_update_kernel<false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
     }
+    if (scaled) MVDR_LAUNCH(pcg_unscale_kernel, grid2((lc.max_nodes + 127) / 128, lc.B), 128, 0, st, d);
     return cudaGetLastError();
 }
 
@@ -1766,14 +2200,39 @@ static void spmv_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStre
     }
 }
 
+template <uint32_t R, uint32_t S, uint32_t F>
+static void spmv_scaled_launch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
+    auto* kernel = &pcg_spmv_scaled_kernel<R, S, F>;
+    MVDR_LAUNCH(kernel, grid2((lc.max_nodes + R - 1) / R, lc.B), 6 * S * R, 0, st, d, parity);
+}
+
+// the shapes of kSpmvShapes for the scaled operator
+static void spmv_scaled_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
+    switch (lc.spmv_shape) {
+        case 1: spmv_scaled_launch<8, 2, 0>(lc, d, parity, st); break;
+        case 2: spmv_scaled_launch<16, 1, 0>(lc, d, parity, st); break;
+        case 3: spmv_scaled_launch<32, 1, 0>(lc, d, parity, st); break;
+        case 4: spmv_scaled_launch<16, 3, 0>(lc, d, parity, st); break;
+        case 5: spmv_scaled_launch<8, 4, 0>(lc, d, parity, st); break;
+        case 6: spmv_scaled_launch<32, 2, 0>(lc, d, parity, st); break;
+        case 7: spmv_scaled_launch<16, 1, 1>(lc, d, parity, st); break;
+        case 8: spmv_scaled_launch<32, 1, 1>(lc, d, parity, st); break;
+        case 9: spmv_scaled_launch<8, 2, 1>(lc, d, parity, st); break;
+        case 10: spmv_scaled_launch<16, 2, 1>(lc, d, parity, st); break;
+        case 11: spmv_scaled_launch<4, 4, 1>(lc, d, parity, st); break;
+        default: spmv_scaled_launch<16, 2, 0>(lc, d, parity, st); break;
+    }
+}
+
 cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
-    if (lc.precision == MVDR_PRECISION_MIXED) spmv_dispatch<true>(lc, d, parity, st);
+    if (lc.precision == MVDR_PRECISION_MIXED) spmv_scaled_dispatch(lc, d, parity, st);
     else spmv_dispatch<false>(lc, d, parity, st);
     return cudaGetLastError();
 }
 
 cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, int stage, cudaStream_t st) {
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
+    const bool scaled = mixed && lc.mode == MVDR_MODE_MATERIALIZED;
     const uint32_t gnode = (lc.max_nodes + kPcgNodeThreads - 1) / kPcgNodeThreads;
     const uint32_t gvec = (6 * lc.max_nodes + 255) / 256;
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
@@ -1792,12 +2251,18 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
         case MVDR_STAGE_SPMV:
             return launch_spmv(lc, d, 0, st);
         case MVDR_STAGE_DIRECTION:
-            if (mixed) MVDR_LAUNCH(pcg_direction_kernel<true>, grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
-            else MVDR_LAUNCH(pcg_direction_kernel<false>, grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
+            if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
+            else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
+            else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
             break;
         case MVDR_STAGE_PCG_UPDATE:
-            if (mixed) MVDR_LAUNCH(pcg_update_kernel<true>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
-            else MVDR_LAUNCH(pcg_update_kernel<false>, grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
+            if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
+            else if (mixed) MVDR_LAUNCH((pcg_update_kernel<true, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
+            else MVDR_LAUNCH((pcg_update_kernel<false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
+            break;
+        case MVDR_STAGE_SCALE:
+            if (!scaled) return cudaErrorInvalidValue;
+            MVDR_LAUNCH(scale_offdiag_kernel, grid2(scale_grid(lc), lc.B), 128, 0, st, d);
             break;
         case MVDR_STAGE_UPDATE: return launch_update(lc, d, st);
         case MVDR_STAGE_MATRIX_FREE: {

@@ -176,6 +176,9 @@ struct ViewDesc {
     const float4* obs_n;
     const float* fg;
     const float2* fg_grad;
+    const float4* rgb;        // density term: rendered normalised rgb (solver map)
+    const float* dens;        // density term: observed grey level
+    const float2* dens_grad;  // density term: its image gradient
     uint32_t pitch;
     float cx, cy, fx, fy;
     M34 w2c, init, init_inv;
@@ -210,6 +213,7 @@ struct InstDesc {
     uint32_t enc;         // node-pair key multiplier (4096, or 2^k >= N)
     uint32_t compat;
     uint32_t use_fg;
+    uint32_t use_density;
     float node_radius;
     ViewDesc views[MVDR_MAX_VIEWS];
     const ushort4* surfel_knn;
@@ -236,7 +240,7 @@ struct InstDesc {
     float4* dense_w;
     float4* dense_cv;       // canonical vertex in frame 0
     float4* dense_cv_lo;    // mixed precision: double transform minus dense_cv (x, y, z)
-    float4* dense_cn;       // canonical normal in frame 0
+    float4* dense_cn;       // canonical normal in frame 0; w: rendered grey level (density term)
     ushort4* fg_pix;
     ushort4* fg_knn;
     float4* fg_w;
@@ -273,6 +277,7 @@ struct InstDesc {
     float* bb_data;         // [bb cap]
     // per-iteration term data
     float4* term_jr;        // 2 float4 per dense+fg term: J(6), r, pixel bits
+    float4* density_jr;     // 2 float4 per dense term (density term): J(6), r, pixel bits
     float4* smooth;         // 3 float4 per smooth term: Ti_xj(3), Tj_xj(3), valid, 0, r(3), 0
     float4* warped;         // 2 float4 per feature+cross term: warped(3), 1, raw residual(3), 0
     // assembly
@@ -287,6 +292,13 @@ struct InstDesc {
     // of the stored block of pair (j, i).
     float* bsr;             // FP32: [(N + P cap) * 36]
     double* bsr_d;          // mixed precision: the same blocks in double
+    // mixed precision, materialised: the operator of the PCG scaled by the
+    // diagonal blocks' Cholesky factors, A^ = L^-1 A L^-T (identity diagonal
+    // blocks, not stored): its upper blocks A^_ij = L_i^-1 A_ij L_j^-T in
+    // float, row-major (element (r, k) at 6 r + k), at the half-storage block
+    // positions of bsr_d
+    float* bsr_s;
+    float* df;              // [6N] the PCG direction of the scaled system in float
     // per entry of the full (symmetric) block-row layout, row i: the diagonal,
     // then its symmetric keys in order [N + 2P cap]
     // (half-storage block | kTransposedBlock when read transposed, block column)
@@ -324,6 +336,7 @@ struct LaunchCfg {
     uint32_t max_edges, max_tp, max_tc;
     uint32_t chunks_per_view;
     int precision, mode;
+    int use_density;
     int sm_count;
     int spmv_shape;  // index into the SpMV tile shapes (chosen by the autotuner)
     // persistent PCG: one cooperative launch per PCG solve (materialised mode)

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.cuh"
 #include "kernels_common.cuh"
 
 namespace mvdr {
@@ -20,7 +21,7 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 static thread_local std::string g_last_error;
 
-static int fail(int code, const std::string& msg) {
+int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
 }
@@ -60,57 +61,11 @@ struct Arena {
     }
 };
 
-// per-instance owned device copies of the inputs (mvdr_set_inputs_host)
-struct OwnedInputs {
-    void* mem = nullptr;
-    size_t bytes = 0;
-};
-
-struct Batch {
-    mvdr_config cfg{};
-    LaunchCfg lc{};
-    uint32_t B = 0;
-    uint32_t cap_edges = 0;
-    std::vector<InstDesc> host;
-    InstDesc* d_inst = nullptr;
-    uint32_t* d_bars = nullptr;  // persistent PCG barrier counters
-    void* arena = nullptr;
-    size_t arena_bytes = 0;
-    size_t per_inst_bytes = 0;
-    std::vector<OwnedInputs> owned;
-    std::vector<uint8_t> has_inputs;
-    // the descriptor last copied to d_inst per instance: a rebind with the
-    // same buffers and sizes skips the (pageable, possibly blocking) upload
-    std::vector<InstDesc> uploaded;
-    std::vector<uint8_t> uploaded_valid;
-    uint32_t gn_iter = 0;
-    // graph cache: (gn, pcg) -> exec
-    std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;
-    std::vector<struct SolverView*> views;
-
-    ~Batch();
-};
-
-}  // namespace mvdr
-
-struct mvdr_solver {
-    mvdr::Batch* batch;
-    uint32_t inst;
-    bool owns;
-};
-struct mvdr_batch {
-    mvdr::Batch* batch;
-};
-
-namespace mvdr {
-
-struct SolverView {
-    mvdr_solver s;
-};
-
 Batch::~Batch() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     for (auto& o : owned)
+        if (o.mem) cudaFree(o.mem);
+    for (auto& o : staged)
         if (o.mem) cudaFree(o.mem);
     if (d_inst) cudaFree(d_inst);
     if (d_bars) cudaFree(d_bars);
@@ -120,7 +75,11 @@ Batch::~Batch() {
 
 static mvdr_penalty penalty_for(const mvdr_config& c, uint32_t iter) {
     mvdr_penalty p{};
-    if (!c.use_elastic_penalty) return c.penalty;
+    if (!c.use_elastic_penalty) {
+        p = c.penalty;
+        if (!c.use_density) p.density = 0.0f;
+        return p;
+    }
     if ((int64_t)iter < (int64_t)c.num_global_iterations) {  // PenaltyConstants.cpp:25-37
         p.smooth = 5.0f;
         p.density = 0.0f;
@@ -129,7 +88,7 @@ static mvdr_penalty penalty_for(const mvdr_config& c, uint32_t iter) {
         p.cross_view = c.use_cross_view ? 1.0f : 0.0f;
     } else {  // PenaltyConstants.cpp:39-51
         p.smooth = 5.0f;
-        p.density = 0.0f;
+        p.density = c.use_density ? 1e-2f : 0.0f;
         p.foreground = 0.0f;
         p.feature = 0.0f;
         p.cross_view = c.use_cross_view ? 1.0f : 0.0f;
@@ -183,6 +142,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.bb_colptr = a.take<int32_t>(lc.cap_bb / 6 + 1);
     I.bb_data = nullptr;
     I.term_jr = a.take<float4>(2 * ((size_t)lc.cap_dense + lc.cap_fg));
+    I.density_jr = lc.use_density ? a.take<float4>(2 * (size_t)lc.cap_dense) : nullptr;
     I.smooth = a.take<float4>(3 * (size_t)cap_edges);
     I.warped = a.take<float4>(2 * ((size_t)max_tp + max_tc + 1));
     I.diag = a.take<float>(36 * N);
@@ -194,6 +154,9 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.bsr = mixed ? nullptr : a.take<float>(36 * (N + (size_t)lc.cap_pairs));
     I.bsr_d = mixed ? a.take<double>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
     I.bsr_ent = a.take<uint2>(N + 2 * (size_t)lc.cap_pairs);
+    const bool scaled = mixed && lc.mode == MVDR_MODE_MATERIALIZED;
+    I.bsr_s = scaled ? a.take<float>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
+    I.df = scaled ? a.take<float>(6 * N) : nullptr;
     if (mixed) {
         I.x_d = a.take<double>(6 * N);
         I.r_d = a.take<double>(6 * N);
@@ -211,8 +174,9 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     }
     // J.p per scalar term of the matrix-free operator (double in mixed precision)
     I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
-    // region 0: energy; 1, 2: PCG delta by iteration parity; 3: d.q
-    I.partials = a.take<double>(4 * (size_t)partial_slots);
+    // region 0: energy; 1, 2: PCG delta by iteration parity; 3: d.q; 4: the
+    // density term's energy
+    I.partials = a.take<double>(5 * (size_t)partial_slots);
     I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
     I.cap_dense = lc.cap_dense;
@@ -277,6 +241,7 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     lc.chunks_per_view = (cfg->image_width * cfg->image_height + kChunkPixels - 1) / kChunkPixels;
     lc.precision = cfg->precision;
     lc.mode = cfg->mode;
+    lc.use_density = cfg->use_density ? 1 : 0;
     lc.sm_count = prop.multiProcessorCount;
 
     const size_t smem_seg = (size_t)lc.cap_seg * 4;
@@ -324,6 +289,8 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     b->lc.wait_extra_arrivals = 0;
     b->lc.pcg_grid = persistent_pcg_grid(lc.precision == MVDR_PRECISION_MIXED, lc.sm_count);
     b->owned.resize(B);
+    b->staged.resize(B);
+    b->bound.resize(B);
     b->has_inputs.assign(B, 0);
     b->uploaded.resize(B);
     b->uploaded_valid.assign(B, 0);
@@ -358,7 +325,7 @@ static M34 inverse34(const M34& a) {
     return o;
 }
 
-static int check_inputs(const Batch& b, const mvdr_inputs* in) {
+int check_inputs(const Batch& b, const mvdr_inputs* in) {
     const mvdr_config& c = b.cfg;
     if (!in) return fail(MVDR_EINVAL, "inputs is null");
     if (in->num_views == 0 || in->num_views > c.max_views) return fail(MVDR_ECAPACITY, "num_views exceeds max_views");
@@ -380,6 +347,8 @@ static int check_inputs(const Batch& b, const mvdr_inputs* in) {
         if (V.pitch && V.pitch < c.image_width) return fail(MVDR_EINVAL, "pitch smaller than image width");
         if (c.use_foreground && (!V.filtered_foreground_mask || !V.foreground_mask_gradient))
             return fail(MVDR_EINVAL, "foreground term on but mask maps missing");
+        if (c.use_density && (!V.normalized_rgb_map || !V.density_map || !V.density_gradient_map))
+            return fail(MVDR_EINVAL, "density term on but density maps missing");
     }
     if (c.use_feature && in->feature.count &&
         (!in->feature.target_vertex || !in->feature.reference_vertex || !in->feature.knn || !in->feature.knn_weight))
@@ -391,7 +360,7 @@ static int check_inputs(const Batch& b, const mvdr_inputs* in) {
     return MVDR_OK;
 }
 
-static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st) {
+int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st) {
     int rc = check_inputs(b, in);
     if (rc != MVDR_OK) return rc;
     const mvdr_config& c = b.cfg;
@@ -409,6 +378,7 @@ static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStrea
     I.enc = enc;
     I.compat = c.compat_flags;
     I.use_fg = c.use_foreground ? 1u : 0u;
+    I.use_density = c.use_density ? 1u : 0u;
     I.node_radius = c.node_radius;
     for (uint32_t v = 0; v < MVDR_MAX_VIEWS; ++v) {
         ViewDesc& V = I.views[v];
@@ -422,6 +392,9 @@ static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStrea
         V.obs_n = reinterpret_cast<const float4*>(S.normal_radius_map);
         V.fg = c.use_foreground ? S.filtered_foreground_mask : nullptr;
         V.fg_grad = c.use_foreground ? reinterpret_cast<const float2*>(S.foreground_mask_gradient) : nullptr;
+        V.rgb = c.use_density ? reinterpret_cast<const float4*>(S.normalized_rgb_map) : nullptr;
+        V.dens = c.use_density ? S.density_map : nullptr;
+        V.dens_grad = c.use_density ? reinterpret_cast<const float2*>(S.density_gradient_map) : nullptr;
         V.pitch = S.pitch ? S.pitch : c.image_width;
         V.cx = S.intrinsic.principal_x;
         V.cy = S.intrinsic.principal_y;
@@ -459,6 +432,7 @@ static int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStrea
         b.uploaded_valid[inst] = 1;
     }
     b.has_inputs[inst] = 1;
+    b.bound[inst] = *in;
     b.gn_iter = 0;
     return MVDR_OK;
 }
@@ -484,6 +458,9 @@ static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cuda
         add(V.normal_radius_map, 16 * np);
         add(c.use_foreground ? V.filtered_foreground_mask : nullptr, c.use_foreground ? 4 * np : 0);
         add(c.use_foreground ? V.foreground_mask_gradient : nullptr, c.use_foreground ? 8 * np : 0);
+        add(c.use_density ? V.normalized_rgb_map : nullptr, c.use_density ? 16 * np : 0);
+        add(c.use_density ? V.density_map : nullptr, c.use_density ? 4 * np : 0);
+        add(c.use_density ? V.density_gradient_map : nullptr, c.use_density ? 8 * np : 0);
     }
     add(in->surfel_knn, 8 * (size_t)in->num_surfels);
     add(in->surfel_knn_weight, 16 * (size_t)in->num_surfels);
@@ -555,6 +532,9 @@ static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cuda
         V.normal_radius_map = (const mvdr_float4*)dst[k++];
         V.filtered_foreground_mask = (const float*)dst[k++];
         V.foreground_mask_gradient = (const float*)dst[k++];
+        V.normalized_rgb_map = (const mvdr_float4*)dst[k++];
+        V.density_map = (const float*)dst[k++];
+        V.density_gradient_map = (const float*)dst[k++];
     }
     dev.surfel_knn = (const uint16_t*)dst[k++];
     dev.surfel_knn_weight = (const mvdr_float4*)dst[k++];
@@ -720,6 +700,9 @@ static int get_array(Batch& b, uint32_t inst, int which, void* dst, size_t cap, 
             return I.x_d ? copy_out_as_float(dst, I.x_d, 6 * N, cap, written)
                          : copy_out(dst, I.x, 4 * 6 * N, cap, written);
         case MVDR_ARRAY_NODE_SE3: return copy_out(dst, I.se3, 32 * N, cap, written);
+        case MVDR_ARRAY_DENSITY_JACOBIAN:
+            if (!I.density_jr) return fail(MVDR_EINVAL, "the density term is off");
+            return copy_out(dst, I.density_jr, 32 * (size_t)c.dense_terms, cap, written);
         case MVDR_ARRAY_PRECONDITIONER:
         case MVDR_ARRAY_OFFDIAG_BLOCKS:
         case MVDR_ARRAY_BINBLOCK_DATA: {
@@ -1023,10 +1006,12 @@ int mvdr_batch_enqueue_stage(mvdr_batch* b, int stage, void* stream) {
     int rc = all_bound(bb);
     if (rc != MVDR_OK) return rc;
     if (stage == MVDR_STAGE_INDEX) return enqueue_index(bb, (cudaStream_t)stream);
-    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_MATRIX_FREE) return fail(MVDR_EINVAL, "unknown stage");
+    if (stage < MVDR_STAGE_INDEX || stage > MVDR_STAGE_SCALE) return fail(MVDR_EINVAL, "unknown stage");
     // the J.d scratch exists only in the matrix-free mode
     if (stage == MVDR_STAGE_MATRIX_FREE && bb.cfg.mode != MVDR_MODE_MATRIX_FREE)
         return fail(MVDR_EINVAL, "the matrix-free stage needs the matrix-free mode");
+    if (stage == MVDR_STAGE_SCALE && (bb.cfg.mode != MVDR_MODE_MATERIALIZED || bb.cfg.precision != MVDR_PRECISION_MIXED))
+        return fail(MVDR_EINVAL, "the scaling stage needs mixed precision in the materialised mode");
     CU(launch_stage(bb.lc, bb.d_inst, penalty_for(bb.cfg, 0), stage, (cudaStream_t)stream));
     return MVDR_OK;
 }
@@ -1043,7 +1028,8 @@ int mvdr_abi_layout(const char* name, size_t* size) {
         {"mvdr_mat34", sizeof(mvdr_mat34)}, {"mvdr_intrinsic", sizeof(mvdr_intrinsic)},
         {"mvdr_penalty", sizeof(mvdr_penalty)}, {"mvdr_config", sizeof(mvdr_config)},
         {"mvdr_view_inputs", sizeof(mvdr_view_inputs)}, {"mvdr_correspondences", sizeof(mvdr_correspondences)},
-        {"mvdr_inputs", sizeof(mvdr_inputs)}, {"mvdr_counts", sizeof(mvdr_counts)}};
+        {"mvdr_inputs", sizeof(mvdr_inputs)}, {"mvdr_counts", sizeof(mvdr_counts)},
+        {"mvdr_view_textures", sizeof(mvdr_view_textures)}};
     for (const auto& t : table)
         if (std::strcmp(t.n, name) == 0) { *size = t.s; return MVDR_OK; }
     return MVDR_EINVAL;

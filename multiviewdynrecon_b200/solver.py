@@ -33,7 +33,7 @@ ARRAY_SPEC = {
     abi.ARRAY_DIAG_BLOCKS: (np.float32, 36), abi.ARRAY_JTR: (np.float32, 6),
     abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
     abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
-    abi.ARRAY_NODE_SE3: (np.float32, 8),
+    abi.ARRAY_NODE_SE3: (np.float32, 8), abi.ARRAY_DENSITY_JACOBIAN: (np.float32, 8),
 }
 
 
@@ -45,7 +45,7 @@ def _stream_handle(stream=None):
 class DeviceScene:
     """Device copies (torch tensors) of every array of a synthetic scene."""
 
-    def __init__(self, scene, device="cuda", pin=False):
+    def __init__(self, scene, device="cuda", pin=False, density=False):
         self.tensors = {}
         self.device = device
         self.pin = pin
@@ -57,7 +57,7 @@ class DeviceScene:
                 arrays.append((name, a.view(np.uint8).reshape(-1)))
             return None
 
-        abi.fill_inputs(scene, collect)
+        abi.fill_inputs(scene, collect, density)
         if pin:
             # one pinned arena, arrays at 256-byte offsets in input order: the
             # library's owned device copy has the same layout, so the upload
@@ -80,7 +80,7 @@ class DeviceScene:
             t = self.tensors.get(name)
             return None if t is None else t.data_ptr()
 
-        self.inputs = abi.fill_inputs(scene, ptr)
+        self.inputs = abi.fill_inputs(scene, ptr, density)
 
     @property
     def nbytes(self):
@@ -109,7 +109,7 @@ class NonRigidSolver:
 
     # SetSolverInput
     def set_solver_input(self, scene, stream=None):
-        ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene)
+        ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene, density=bool(self.config.use_density))
         self._inputs = ds
         self.num_nodes = ds.inputs.num_nodes
         check(lib().mvdr_set_inputs(self.h, C.byref(ds.inputs), _stream_handle(stream)))
@@ -169,6 +169,15 @@ class NonRigidSolver:
             out = buf[: written.value // np.dtype(dt).itemsize]
             return out.reshape(-1, width) if width > 1 else out
 
+    def node_se3_device(self):
+        """Device address of the warp field (the SolvedNodeSE3() view)."""
+        p = C.c_void_p()
+        check(lib().mvdr_node_se3_device(self.h, C.byref(p)))
+        return p.value
+
+    def save_input_bundle(self, path, stream=None):
+        check(lib().mvdr_save_input_bundle(self.h, str(path).encode(), _stream_handle(stream)))
+
     def apply_jtj(self, x, stream=None):
         x = x.contiguous().float()
         y = torch.empty_like(x)
@@ -200,7 +209,7 @@ class BatchSolver:
             pass
 
     def set_input(self, i, scene, stream=None):
-        ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene)
+        ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene, density=bool(self.config.use_density))
         self._inputs[i] = ds
         check(lib().mvdr_batch_set_inputs(self.h, i, C.byref(ds.inputs), _stream_handle(stream)))
         return ds

@@ -207,6 +207,16 @@ class Capsule:
         return t, n
 
 
+def surface_colour(p):
+    """Normalised rgb of a frame-0 surface point: smooth stripes of a few
+    centimetres, different per channel."""
+    p = np.asarray(p, np.float64)
+    r = 0.5 + 0.3 * np.sin(40.0 * p[:, 0] + 3.0 * p[:, 2])
+    g = 0.5 + 0.3 * np.cos(35.0 * p[:, 1] - 2.0 * p[:, 0])
+    b = 0.5 + 0.2 * np.sin(25.0 * (p[:, 0] + p[:, 1] + p[:, 2]))
+    return np.stack([r, g, b], 1).astype(np.float32)
+
+
 def cast(shapes, o, d):
     t = np.full(len(d), np.inf)
     n = np.zeros((len(d), 3))
@@ -234,6 +244,11 @@ class View:
     intrinsic: np.ndarray                 # (4,) principal_x, principal_y, focal_x, focal_y
     world2camera: np.ndarray              # (12,) mat34
     initial_camera_se3: np.ndarray        # (12,) mat34
+    # density (colour) term: rendered normalised rgb of the reference surface,
+    # and the observed grey level with its image gradient
+    normalized_rgb_map: np.ndarray = None     # (H, W, 4) float32
+    density_map: np.ndarray = None            # (H, W) float32
+    density_gradient_map: np.ndarray = None   # (H, W, 2) float32
 
 
 @dataclass
@@ -452,6 +467,21 @@ def _build(name, shapes, cams, W, H, fx, fy, cx, cy, num_nodes, seed, *, auto_ra
         filt = ndimage.gaussian_filter(1.0 - mask, sigma=2.0).astype(np.float32)
         gy, gx = np.gradient(filt)
         grad = np.stack([gx, gy], -1).astype(np.float32)
+        # colour: a smooth texture fixed to the surface; the reference render
+        # shows it at each surfel, the observation shows the live surface's
+        # grey level (rgb2density) with noise, blurred by 1 px
+        rgb = np.zeros((H * W, 4), np.float32)
+        rgb[vid, :3] = surface_colour(pw[vid])
+        rgb[vid, 3] = 1.0
+        grey = np.zeros(H * W, np.float32)
+        # (a generator of its own, so that the other arrays of a seed stay
+        # as they were before the colour maps existed)
+        crng = np.random.default_rng([seed, 7919, vi])
+        grey[vid] = (0.299 * rgb[vid, 0] + 0.587 * rgb[vid, 1] + 0.114 * rgb[vid, 2]
+                     + crng.normal(0, 0.005, len(vid)))
+        grey = ndimage.gaussian_filter(grey.reshape(H, W), sigma=1.0).astype(np.float32)
+        dgy, dgx = np.gradient(grey)
+        dgrad = np.stack([dgx, dgy], -1).astype(np.float32)
         views.append(View(
             reference_vertex_map=ref_v.reshape(H, W, 4),
             reference_normal_map=ref_n.reshape(H, W, 4),
@@ -463,6 +493,9 @@ def _build(name, shapes, cams, W, H, fx, fy, cx, cy, num_nodes, seed, *, auto_ra
             intrinsic=np.array([cx, cy, fx, fy], np.float32),
             world2camera=mat34_pack(Rw, tw),
             initial_camera_se3=mat34_pack(Rinit, tinit),
+            normalized_rgb_map=rgb.reshape(H, W, 4),
+            density_map=grey,
+            density_gradient_map=dgrad,
         ))
 
     def correspondences(src_surfels, tgt_points):
@@ -562,9 +595,11 @@ def torso_multi_view(seed=2, num_nodes=4096, num_views=3, width=640, height=480,
 
 
 def articulated_body(seed=5, num_nodes=32768, num_views=5, width=1280, height=720, cross_total=20000,
-                     distance=2.2, auto_radius=False):
+                     distance=2.2, auto_radius=False, focal_scale=1.0):
     """Large single solve: ellipsoid torso + 4 capsule limbs with random joint
-    bends <= 30 deg, `num_views` views, 8 GN x 20 PCG."""
+    bends <= 30 deg, `num_views` views, 8 GN x 20 PCG. `focal_scale`
+    multiplies the focal length (570 px at 640 wide): 5 frames the body so
+    that it fills about 87 % of each 1280x720 view, about 4M dense terms."""
     rng = np.random.default_rng(seed + 1000)
     center = np.array([0.0, 0.0, distance])
     shapes = [Ellipsoid(center, (0.25, 0.45, 0.15))]
@@ -587,7 +622,7 @@ def articulated_body(seed=5, num_nodes=32768, num_views=5, width=1280, height=72
         if k == 0:
             R, o = np.eye(3), np.zeros(3)
         cams.append((R, o))
-    fx = 570.0 * width / 640.0
+    fx = 570.0 * width / 640.0 * focal_scale
     per_pair = cross_total // max(1, num_views)
     return _build("articulated_5view", shapes, cams, width, height, fx, fx, width / 2.0, height / 2.0, num_nodes,
                   seed, auto_radius=auto_radius, features_per_view=0, cross_per_pair=per_pair,

@@ -45,6 +45,7 @@ def lib():
         L.orc_solve.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.orc_set_term_data.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_freeze_decisions.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_freeze_density.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_set_increment.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_set_node_se3.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_energy.restype = C.c_double
@@ -82,7 +83,7 @@ _ARRAY_SPEC = {
     abi.ARRAY_DIAG_BLOCKS: (np.float32, 36), abi.ARRAY_JTR: (np.float32, 6),
     abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
     abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
-    abi.ARRAY_NODE_SE3: (np.float32, 8),
+    abi.ARRAY_NODE_SE3: (np.float32, 8), abi.ARRAY_DENSITY_JACOBIAN: (np.float32, 8),
 }
 REAL_ARRAYS = {abi.ARRAY_DIAG_BLOCKS, abi.ARRAY_JTR, abi.ARRAY_PRECONDITIONER, abi.ARRAY_OFFDIAG_BLOCKS,
                abi.ARRAY_BINBLOCK_DATA, abi.ARRAY_INCREMENT, abi.ARRAY_NODE_SE3}
@@ -101,7 +102,7 @@ class Oracle:
             self._keep.append(a)
             return a.ctypes.data
 
-        self.inputs = abi.fill_inputs(scene, ptr)
+        self.inputs = abi.fill_inputs(scene, ptr, bool(config.use_density))
         self.h = lib().orc_create(C.byref(config), C.byref(self.inputs), int(fp64))
         if not self.h:
             raise ValueError("oracle rejected the inputs")
@@ -139,12 +140,17 @@ class Oracle:
         keep = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (term_jr, smooth, warped)]
         lib().orc_set_term_data(self.h, *[None if a is None else _p(a) for a in keep])
 
-    def freeze(self, term_jr, smooth):
-        """Freeze projected pixels / validity from another run's term data."""
+    def freeze(self, term_jr, smooth, density_jr=None):
+        """Freeze projected pixels / validity from another run's term data
+        (and the density term's pixels when its records are given)."""
         jr = np.ascontiguousarray(term_jr, np.float32).reshape(-1, 8)
         pix = np.ascontiguousarray(jr[:, 7].view(np.uint32))
         sv = np.ascontiguousarray((np.asarray(smooth, np.float32).reshape(-1, 12)[:, 6] != 0).astype(np.uint8))
         lib().orc_freeze_decisions(self.h, _p(pix), _p(sv))
+        if density_jr is not None:
+            dj = np.ascontiguousarray(density_jr, np.float32).reshape(-1, 8)
+            dp = np.ascontiguousarray(dj[:, 7].view(np.uint32))
+            lib().orc_freeze_density(self.h, _p(dp))
 
     def unfreeze(self):
         lib().orc_unfreeze(self.h)

@@ -265,6 +265,8 @@ struct ViewData {
     std::vector<mvdr_float4> ref_v, ref_n, obs_v, obs_n;
     std::vector<u32> index;
     std::vector<float> fg_mask, fg_grad;
+    std::vector<mvdr_float4> rgb;          // density term: rendered normalised rgb
+    std::vector<float> dens, dens_grad;    // density term: observed grey level, gradient
     mvdr_intrinsic intr;
     mvdr_mat34 w2c, init;
 };
@@ -305,6 +307,8 @@ struct Oracle {
 
     // term data (float layout of the ABI)
     std::vector<float> term_jr;   // 8 per dense+fg term
+    std::vector<float> density_jr;  // 8 per dense term: density J (6), residual, pixel (use_density)
+    std::vector<u32> frozen_density;  // frozen projected pixels of the density term
     std::vector<float> smooth;    // 8 per smooth term
     std::vector<float> warped;    // 4 per feature+cross term
     // frozen decisions: per dense+fg term the projected pixel (v*W+u) or invalid
@@ -326,6 +330,7 @@ struct Oracle {
     void penalty_for(int iter) {
         if (!cfg.use_elastic_penalty) {
             lambda = cfg.penalty;
+            if (!cfg.use_density) lambda.density = 0.0f;
             return;
         }
         if (iter < cfg.num_global_iterations) {  // PenaltyConstants.cpp:25-37
@@ -336,7 +341,7 @@ struct Oracle {
             lambda.cross_view = cfg.use_cross_view ? 1.0f : 0.0f;
         } else {  // PenaltyConstants.cpp:39-51
             lambda.smooth = 5.0f;
-            lambda.density = 0.0f;
+            lambda.density = cfg.use_density ? 1e-2f : 0.0f;
             lambda.foreground = 0.0f;
             lambda.feature = 0.0f;
             lambda.cross_view = cfg.use_cross_view ? 1.0f : 0.0f;
@@ -378,6 +383,19 @@ struct Oracle {
                         d.fg_mask[t] = vi.filtered_foreground_mask[s];
                         d.fg_grad[2 * t] = vi.foreground_mask_gradient[2 * s];
                         d.fg_grad[2 * t + 1] = vi.foreground_mask_gradient[2 * s + 1];
+                    }
+            }
+            if (c->use_density && vi.normalized_rgb_map && vi.density_map && vi.density_gradient_map) {
+                d.rgb.resize(P);
+                d.dens.resize(P);
+                d.dens_grad.resize(2 * P);
+                for (u32 y = 0; y < H; ++y)
+                    for (u32 x = 0; x < W; ++x) {
+                        const size_t s = (size_t)y * pitch + x, t = (size_t)y * W + x;
+                        d.rgb[t] = vi.normalized_rgb_map[s];
+                        d.dens[t] = vi.density_map[s];
+                        d.dens_grad[2 * t] = vi.density_gradient_map[2 * s];
+                        d.dens_grad[2 * t + 1] = vi.density_gradient_map[2 * s + 1];
                     }
             }
             d.intr = vi.intrinsic;
@@ -798,6 +816,53 @@ struct Oracle {
             }
             std::memcpy(&out[7], &pix_choice, 4);
         }
+        // density: computeDensityMapJacobian (DensityForegroundJacobianResidual.cu:41-91)
+        // with computeImageDensityJacobainAndResidual (density_map_jacobian.cuh:12-79):
+        // per dense pixel, observed minus rendered grey level (rgb2density,
+        // ColorTypeTransfer.h:51-56); the vertex warped as the dense term warps
+        // it, or in its camera's frame under MVDR_COMPAT_REF_FOREGROUND_FRAME
+        density_jr.assign(cfg.use_density ? 8 * (size_t)Td : 0, 0.0f);
+        for (u32 idx = 0; cfg.use_density && idx < Td; ++idx) {
+            const u16* px = &dense_pix[4 * (size_t)idx];
+            const u32 v = view_of(idx, dense_pix.data(), dense_view_count);
+            const ViewData& d = views[v];
+            if (d.dens.empty()) continue;
+            const size_t p = (size_t)px[1] * W + px[0];
+            const V3<R> cv{(R)d.ref_v[p].x, (R)d.ref_v[p].y, (R)d.ref_v[p].z};
+            const V3<R> p0 = raw_frame ? cv : init[v].apply(cv);
+            const M34<R> se3 = se3_matrix(blend(f, &dense_knn[4 * (size_t)idx], &dense_w[idx].x));
+            const V3<R> wv = se3.apply(p0);
+            const V3<R> vc = inv[v].apply(w2c[v].apply(wv));
+            u32 pix_choice = MVDR_INVALID_INDEX;
+            if (!frozen_density.empty()) {
+                pix_choice = frozen_density[idx];
+            } else {
+                const int u = rint_even((float)(((double)vc.x / ((double)vc.z + 1e-10)) * (double)d.intr.focal_x +
+                                                (double)d.intr.principal_x));
+                const int vv = rint_even((float)(((double)vc.y / ((double)vc.z + 1e-10)) * (double)d.intr.focal_y +
+                                                 (double)d.intr.principal_y));
+                if (u >= 0 && u < (int)W && vv >= 0 && vv < (int)H) pix_choice = (u32)((size_t)vv * W + u);
+            }
+            float* out = &density_jr[8 * (size_t)idx];
+            if (pix_choice != MVDR_INVALID_INDEX) {
+                const mvdr_float4 c = d.rgb[p];
+                const float geo = 0.299f * c.x + 0.587f * c.y + 0.114f * c.z;
+                const R img = (R)d.dens[pix_choice];
+                const R gx = (R)d.dens_grad[2 * (size_t)pix_choice], gy = (R)d.dens_grad[2 * (size_t)pix_choice + 1];
+                const R fx = (R)d.intr.focal_x, fy = (R)d.intr.focal_y;
+                V3<R> g;
+                g.x = gx * fx / vc.z;
+                g.y = gy * fy / vc.z;
+                g.z = (R)(-1.0f) / (vc.z * vc.z) * (fx * vc.x * gx + fy * vc.y * gy);
+                g = w2c[v].rotT(init[v].rot(g));
+                out[0] = (float)(-g.y * wv.z + g.z * wv.y);
+                out[1] = (float)(g.x * wv.z - g.z * wv.x);
+                out[2] = (float)(-g.x * wv.y + g.y * wv.x);
+                out[3] = (float)g.x; out[4] = (float)g.y; out[5] = (float)g.z;
+                out[6] = (float)(img - (R)geo);
+            }
+            std::memcpy(&out[7], &pix_choice, 4);
+        }
         // sparse feature / cross view: forwardWarpFeatureVertexKernel
         // (SparseCorrespondenceHandler.cu:202-220)
         // record: warped vertex, 1, raw residual warped - target (in R), 0
@@ -834,6 +899,16 @@ struct Oracle {
                 r[0] = jr[6];
                 lam2 = t == kDense ? 1.0 : (double)lambda.foreground * lambda.foreground;
                 wnode = weight_of(knn_of(t, k), w_of(t, k));
+                if (t == kDense && !density_jr.empty() && lambda.density != 0.0f) {
+                    // the density residual of the same pixel (the reference adds
+                    // it in the DenseImage slot, PreconditionerBlocked.cu:216-219),
+                    // as a second channel scaled by lambda_density (lam2 = 1 here)
+                    const float* dj = &density_jr[8 * (size_t)k];
+                    const double ld = (double)lambda.density;
+                    for (int i = 0; i < 6; ++i) J[1][i] = ld * dj[i];
+                    r[1] = ld * dj[6];
+                    return 2;
+                }
                 return 1;
             }
             case kSmooth: {
@@ -1077,6 +1152,10 @@ struct Oracle {
     double compute_energy() const {
         double e = 0;
         for (u32 k = 0; k < Td; ++k) { const double r = term_jr[8 * (size_t)k + 6]; e += r * r; }
+        for (size_t k = 0; k < density_jr.size() / 8; ++k) {  // ResidualEvaluator.cu:94-99
+            const double r = (double)(lambda.density * density_jr[8 * k + 6]);
+            e += r * r;
+        }
         for (u32 k = 0; k < Ts; ++k) {
             const float* s = &smooth[12 * (size_t)k];
             if (s[6] == 0.0f) continue;
@@ -1152,7 +1231,16 @@ void orc_freeze_decisions(void* h, const uint32_t* pixels, const uint8_t* smooth
     o->frozen_smooth.assign(smooth_valid, smooth_valid + o->Ts);
     o->frozen = true;
 }
-void orc_unfreeze(void* h) { ((Oracle*)h)->frozen = false; }
+void orc_unfreeze(void* h) {
+    ((Oracle*)h)->frozen = false;
+    ((Oracle*)h)->frozen_density.clear();
+}
+
+/* Freeze the density term's projected pixels (one per dense term). */
+void orc_freeze_density(void* h, const uint32_t* pixels) {
+    Oracle* o = (Oracle*)h;
+    o->frozen_density.assign(pixels, pixels + o->Td);
+}
 
 void orc_assemble(void* h) { ((Oracle*)h)->gn_assemble(); }
 void orc_pcg(void* h, uint32_t iters) { ((Oracle*)h)->gn_solve(iters); }
@@ -1241,6 +1329,7 @@ long long orc_get(void* h, int which, void* dst, size_t cap, int as_double) {
         case MVDR_ARRAY_BINBLOCK_ROWPTR: return put(o->rowptr.data(), o->rowptr.size() * 4);
         case MVDR_ARRAY_BINBLOCK_COLPTR: return put(o->colptr.data(), o->colptr.size() * 4);
         case MVDR_ARRAY_TERM_JACOBIAN: return put(o->term_jr.data(), o->term_jr.size() * 4);
+        case MVDR_ARRAY_DENSITY_JACOBIAN: return put(o->density_jr.data(), o->density_jr.size() * 4);
         case MVDR_ARRAY_SMOOTH_TERMS: return put(o->smooth.data(), o->smooth.size() * 4);
         case MVDR_ARRAY_WARPED_CORRESPONDENCE: return put(o->warped.data(), o->warped.size() * 4);
         case MVDR_ARRAY_DIAG_BLOCKS: return put_real(o->D);

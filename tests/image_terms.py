@@ -47,6 +47,50 @@ def dq_blend_se3(dq, knn, w):
     return R, t
 
 
+def _image_terms(scene, pixels, frame0, image, gradient, geometry):
+    W, H = scene.width, scene.height
+    out = np.zeros((len(pixels), 8))
+    for k, (x, y, v, _) in enumerate(np.asarray(pixels, np.int64)):
+        view = scene.views[v]
+        s = int(view.index_map[y, x])
+        Rw, tw = unpack34(view.world2camera)
+        Ri, ti = unpack34(view.initial_camera_se3)
+        ref = view.reference_vertex_map[y, x, :3].astype(np.float64)
+        if frame0:
+            ref = Ri @ ref + ti
+        R, t = dq_blend_se3(scene.node_se3, scene.surfel_knn[s], scene.surfel_knn_weight[s])
+        wv = R @ ref + t
+        vc = Ri.T @ (Rw @ wv + tw - ti)
+        cx, cy, fx, fy = (float(a) for a in view.intrinsic)
+        u = int(np.rint(np.float32(vc[0] / (vc[2] + 1e-10) * fx + cx)))
+        r = int(np.rint(np.float32(vc[1] / (vc[2] + 1e-10) * fy + cy)))
+        out[k, 7] = -1
+        if 0 <= u < W and 0 <= r < H:
+            img = float(image(view)[r, u])
+            gx, gy = (float(a) for a in gradient(view)[r, u])
+            d = np.array([gx * fx / vc[2], gy * fy / vc[2],
+                          -1.0 / (vc[2] * vc[2]) * (fx * vc[0] * gx + fy * vc[1] * gy)])
+            d = Rw.T @ (Ri @ d)
+            out[k, :3] = [-d[1] * wv[2] + d[2] * wv[1], d[0] * wv[2] - d[2] * wv[0],
+                          -d[0] * wv[1] + d[1] * wv[0]]
+            out[k, 3:6] = d
+            out[k, 6] = img - geometry(view, x, y)
+            out[k, 7] = r * W + u
+    return out
+
+
+def density_terms(scene, pixels, frame0):
+    """The density term (computeDensityMapJacobian,
+    DensityForegroundJacobianResidual.cu:41-91) at the dense pixels: the
+    observed grey level and its gradient, minus rgb2density of the rendered
+    normalised rgb at the pixel (ColorTypeTransfer.h:51-56). Rows as in
+    foreground_terms."""
+    def geometry(view, x, y):
+        c = view.normalized_rgb_map[y, x].astype(np.float32)
+        return float(np.float32(0.299) * c[0] + np.float32(0.587) * c[1] + np.float32(0.114) * c[2])
+    return _image_terms(scene, pixels, frame0, lambda v: v.density_map, lambda v: v.density_gradient_map, geometry)
+
+
 def foreground_terms(scene, pixels, frame0):
     """(T, 8) float64 rows of the foreground terms at the compacted `pixels`
     ((T, 4) x, y, view, 0): the twist gradient (6), the residual, and the

@@ -156,11 +156,15 @@ def test_index_definitions(oracle_mod, kind):
     assert np.array_equal(blk, np.searchsorted(rows, np.arange(scene.num_nodes + 1)))
 
 
-def _sparse_jacobian(scene, o):
-    """Independent assembly: sparse J (scalar rows x 6N), lambda^2 per row, r."""
+def _sparse_jacobian(scene, o, cfg=None, lam=None, density=0.0):
+    """Independent assembly: sparse J (scalar rows x 6N), lambda^2 per row, r.
+    `lam` = (smooth, foreground, feature, cross) weights (the global phase by
+    default); `density` > 0 adds each dense pixel's density row with that
+    weight."""
     c = o.counts()
-    cfg = abi.make_config(scene)
-    lam = (5.0, 2e-3 if cfg.use_foreground else 0.0, 1.0, 1.0 if cfg.use_cross_view else 0.0)
+    cfg = cfg or abi.make_config(scene)
+    if lam is None:
+        lam = (5.0, 2e-3 if cfg.use_foreground else 0.0, 1.0, 1.0 if cfg.use_cross_view else 0.0)
     jr = o.get(abi.ARRAY_TERM_JACOBIAN)
     sm = o.get(abi.ARRAY_SMOOTH_TERMS)
     wv = o.get(abi.ARRAY_WARPED_CORRESPONDENCE)
@@ -185,6 +189,11 @@ def _sparse_jacobian(scene, o):
     for t in range(Td):
         J = jr[t, :6].astype(np.float64)
         add_row([(int(knn_d[t, k]), w_d[t, k] * J) for k in range(4)], 1.0, float(jr[t, 6]))
+    if density:
+        dj = o.get(abi.ARRAY_DENSITY_JACOBIAN)
+        for t in range(Td):
+            J = dj[t, :6].astype(np.float64)
+            add_row([(int(knn_d[t, k]), w_d[t, k] * J) for k in range(4)], density ** 2, float(dj[t, 6]))
 
     def skew_rows(p):
         return np.array([[0, p[2], -p[1]], [-p[2], 0, p[0]], [p[1], -p[0], 0]], np.float64)
@@ -251,6 +260,66 @@ def test_assembly_matches_sparse_jacobian(oracle_mod, kind):
     nz_blocks = {(r // 6, c // 6) for r, c in zip(*A.nonzero())}
     idx_blocks = {(k // 4096, k % 4096) for k in sym} | {(n, n) for n in range(N)}
     assert nz_blocks <= idx_blocks
+
+
+@pytest.mark.parametrize("compat", [False, True])
+def test_density_terms_match_the_reference_formula(oracle_mod, compat):
+    """The oracle's density terms (one per dense pixel) against an independent
+    restatement of computeDensityMapJacobian / computeImageDensityJacobainAndResidual."""
+    from image_terms import density_terms
+    scene = small_scene("torso")
+    flags = abi.COMPAT_REF_FOREGROUND_FRAME if compat else 0
+    o = oracle_mod.Oracle(scene, abi.make_config(scene, compat_flags=flags, use_density=True), fp64=True)
+    o.build_index()
+    o.eval_terms()
+    dj = o.get(abi.ARRAY_DENSITY_JACOBIAN)
+    assert len(dj) == o.counts().dense_terms
+    want = density_terms(scene, o.get(abi.ARRAY_DENSE_PIXELS), frame0=not compat)
+    pix = np.ascontiguousarray(dj[:, 7]).view(np.uint32).astype(np.int64)
+    pix = np.where(pix == abi.MVDR_INVALID_INDEX, -1, pix)
+    same = pix == want[:, 7].astype(np.int64)
+    assert same.mean() > 0.999
+    got = dj.astype(np.float64)
+    assert max_relative_error(got[same, :7], want[same, :7], 1e-6 * np.abs(want[:, :7]).max()) < 1e-5
+    assert np.abs(want[:, 6]).max() > 0.01  # the term is not trivially zero
+
+
+def test_density_assembly_matches_sparse_jacobian(oracle_mod):
+    """With the density term in the local phase (lambda_density = 1e-2 from
+    the first iteration; foreground and feature weights 0), the assembled
+    blocks and Jt r equal the independent sparse Jacobian's."""
+    scene = small_scene("torso")
+    cfg = abi.make_config(scene, use_density=True, num_global_iterations=0)
+    o = oracle_mod.Oracle(scene, cfg, fp64=True)
+    o.build_index()
+    o.eval_terms()
+    o.assemble()
+    A, b = _sparse_jacobian(scene, o, cfg=cfg, lam=(5.0, 0.0, 0.0, 1.0), density=1e-2)
+    N = scene.num_nodes
+    Ad = A.toarray()
+    D = o.get(abi.ARRAY_DIAG_BLOCKS, as_double=True).reshape(N, 6, 6)
+    for n in range(N):
+        ref = Ad[6 * n:6 * n + 6, 6 * n:6 * n + 6]
+        assert max_relative_error(D[n], ref, 1e-9 * max(1.0, np.abs(ref).max())) < 1e-9
+    bo = o.get(abi.ARRAY_JTR, as_double=True).reshape(-1)
+    assert max_relative_error(bo, b, 1e-9 * np.abs(b).max()) < 1e-8
+    sym = o.get(abi.ARRAY_NODEPAIR_KEY)
+    off = o.get(abi.ARRAY_OFFDIAG_BLOCKS, as_double=True)
+    for s_, key in enumerate(sym):
+        i, j = key // 4096, key % 4096
+        ref = Ad[6 * i:6 * i + 6, 6 * j:6 * j + 6]
+        assert max_relative_error(off[s_].reshape(6, 6).T, ref, 1e-9 * max(1.0, np.abs(ref).max())) < 1e-8
+    # the density rows changed the system
+    A0, b0 = _sparse_jacobian(scene, o, cfg=cfg, lam=(5.0, 0.0, 0.0, 1.0), density=0.0)
+    assert np.abs(b - b0).max() > 1e-6 * np.abs(b).max()
+    # and the energy counts them: sum (lambda_d r_d)^2 on top of the others
+    dj = o.get(abi.ARRAY_DENSITY_JACOBIAN).astype(np.float64)
+    o2 = oracle_mod.Oracle(scene, abi.make_config(scene, use_density=False, num_global_iterations=0), fp64=True)
+    o2.build_index()
+    o2.eval_terms()
+    o2.assemble()
+    # (the kernels and the oracle weight the residual in float: ~1e-7 relative)
+    assert math.isclose(o.energy() - o2.energy(), float(((1e-2 * dj[:, 6]) ** 2).sum()), rel_tol=1e-6)
 
 
 @pytest.mark.parametrize("kind", ["sphere", "torso"])

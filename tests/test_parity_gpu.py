@@ -470,3 +470,58 @@ def test_matrix_free_stage_only_in_matrix_free_mode():
         assert lib().mvdr_kernel_launch_count() - k0 == (2 if want == abi.MVDR_OK else 0)
         assert b.instance(0).counts().error_flags == 0
         b.close()
+
+
+@pytest.mark.parametrize("flags", [0, abi.COMPAT_REF_FOREGROUND_FRAME])
+@pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_FP32])
+def test_density_term_parity(oracle_mod, flags, precision):
+    """The density (colour) term of every dense pixel: the kernel's records
+    equal the oracle's and an independent restatement of
+    computeDensityMapJacobian (DensityForegroundJacobianResidual.cu:41-91)."""
+    from image_terms import density_terms
+    scene = small_scene("torso")
+    g, cfg = make_gpu(scene, precision=precision, compat_flags=flags, use_density=True, num_global_iterations=0)
+    g.build_index()
+    g.gn_iteration(scene.pcg_iterations)
+    torch.cuda.synchronize()
+    o = oracle_mod.Oracle(scene, cfg)
+    o.build_index()
+    o.eval_terms()
+    gd, od = g.get_array(abi.ARRAY_DENSITY_JACOBIAN), o.get(abi.ARRAY_DENSITY_JACOBIAN)
+    assert gd.shape == od.shape and len(gd) == g.counts().dense_terms
+    same = gd[:, 7].view(np.uint32) == od[:, 7].view(np.uint32)
+    assert (~same).sum() <= max(2, int(1e-3 * len(same)))
+    scale = np.abs(od[same, :7]).max()
+    assert max_relative_error(gd[same, :7], od[same, :7], 1e-6 * scale) < 1e-4
+    want = density_terms(scene, g.get_array(abi.ARRAY_DENSE_PIXELS), frame0=not flags)
+    gp = np.ascontiguousarray(gd[:, 7]).view(np.uint32).astype(np.int64)
+    gp = np.where(gp == abi.MVDR_INVALID_INDEX, -1, gp)
+    ok = gp == want[:, 7].astype(np.int64)
+    assert ok.mean() > 0.999
+    assert max_relative_error(gd[ok, :7].astype(np.float64), want[ok, :7],
+                              1e-6 * np.abs(want[:, :7]).max()) < 1e-4
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_MATERIALIZED, abi.MODE_MATRIX_FREE])
+def test_density_solve_vs_fp64_oracle(oracle_mod, mode):
+    """Gauss-Newton increments with the density term active (lambda 1e-2 from
+    the first iteration) against the FP64 oracle from the same warp field, with
+    the GPU's pixel decisions for both image terms."""
+    scene = small_scene("torso")
+    g, cfg = make_gpu(scene, mode=mode, use_density=True, num_global_iterations=0)
+    g.build_index()
+    o64 = oracle_mod.Oracle(scene, cfg, fp64=True)
+    o64.build_index()
+    for it in range(3):
+        o64.set_node_se3(g.get_array(abi.ARRAY_NODE_SE3))
+        g.gn_iteration(scene.pcg_iterations)
+        torch.cuda.synchronize()
+        o64.freeze(g.get_array(abi.ARRAY_TERM_JACOBIAN), g.get_array(abi.ARRAY_SMOOTH_TERMS),
+                   g.get_array(abi.ARRAY_DENSITY_JACOBIAN))
+        o64.eval_terms()
+        o64.assemble()
+        assert abs(g.energy() - o64.energy()) <= 1e-4 * abs(o64.energy()), it
+        o64.pcg(scene.pcg_iterations)
+        o64.update()
+        assert rel_norm_error(g.get_array(abi.ARRAY_INCREMENT), o64.get(abi.ARRAY_INCREMENT, as_double=True)) < 1e-4, it
+    assert g.counts().error_flags == 0
