@@ -4,9 +4,13 @@ Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import
 this package. It restates the reference NonRigidSolver algorithm on the CPU
 (oracle/oracle.cpp) and is used as the checker, never as the product.
 
-Parity unpinned: the reference cannot be built here and ships no golden
-vectors; the restatement is pinned by known-answer tests instead
-(tests/test_oracle.py).
+The reference cannot be built whole and ships no golden vectors. Its
+header-only solver math (dual quaternions, the ICP and smooth-term Jacobians,
+the 6x6 Gauss-Jordan inverse, the node-pair encoding, the term offsets, the
+image-term Jacobian) is compiled from the reference tree into
+oracle/_ref/libref_pin.so (oracle/Makefile, target `ref`) and the oracle is
+checked against it (tests/test_ref_pin.py, tests/golden/ref_vectors.npz);
+the rest is pinned by known-answer tests (tests/test_oracle.py).
 """
 from __future__ import annotations
 
@@ -23,8 +27,39 @@ _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 _lib = None
 
 
+REFERENCE_TREE = "/root/reference"
+_REF_PATH = os.path.join(_HERE, "_ref", "libref_pin.so")
+_ref_lib = None
+
+
 def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    # the reference-pinning harness needs the reference tree; elsewhere the
+    # library built here (oracle/_ref) is used as it is
+    if os.path.isdir(REFERENCE_TREE):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={REFERENCE_TREE}"], check=True)
+
+
+def ref_lib():
+    """The reference's own header math compiled by oracle/Makefile (target
+    `ref`), or None when it has not been built."""
+    global _ref_lib
+    if _ref_lib is None and os.path.exists(_REF_PATH):
+        L = C.CDLL(_REF_PATH)
+        vp, u16, u32, i32, f32 = C.c_void_p, C.c_uint16, C.c_uint32, C.c_int, C.c_float
+        for name, argt in (("ref_blend_se3", [vp, vp, vp, vp]), ("ref_dq_to_mat34", [vp, vp]),
+                           ("ref_mat34_to_dq", [vp, vp]), ("ref_gauss_jordan6", [vp, vp]),
+                           ("ref_p2p_jacobian", [vp, vp, vp]), ("ref_p2p_jt_residual", [vp, vp, vp]),
+                           ("ref_smooth_jacobian", [vp, vp, i32, vp]), ("ref_smooth_jt_residual", [vp, vp, i32, vp]),
+                           ("ref_term_offsets", [vp, vp, vp, vp])):
+            getattr(L, name).argtypes = argt
+            getattr(L, name).restype = None
+        L.ref_huber.argtypes, L.ref_huber.restype = [f32], f32
+        L.ref_encode_nodepair.argtypes, L.ref_encode_nodepair.restype = [u16, u16], u32
+        L.ref_image_terms.argtypes = [u32, u32, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp]
+        L.ref_image_terms.restype = i32
+        _ref_lib = L
+    return _ref_lib
 
 
 def lib():
@@ -61,6 +96,10 @@ def lib():
         L.orc_apply_twist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_set_node_se3_f64.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_gauss_jordan_inverse.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_blend_se3.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_huber.argtypes, L.orc_huber.restype = [C.c_float], C.c_float
+        L.orc_smooth_rows.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_p2p_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
         _lib = L
     return _lib

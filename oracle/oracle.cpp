@@ -882,6 +882,38 @@ struct Oracle {
         warp_corr(cross, Tc, Tp);
     }
 
+    // computeSmoothTermJacobian (geometry_icp_jacobian.cuh:359-382) for the
+    // record s (Ti xj, Tj xj, validity, 0, residual Ti xj - Tj xj, 0): the
+    // rows of node i (is_i) or node j; 0 channels for an invalid edge
+    static int smooth_rows(const float* s, bool is_i, double J[3][6], double r[3]) {
+        if (s[6] == 0.0f) return 0;
+        const double a[3] = {s[0], s[1], s[2]}, bq[3] = {s[3], s[4], s[5]};
+        const double sg = is_i ? 1.0 : -1.0;
+        const double* p = is_i ? a : bq;
+        const double rot[3][3] = {{0, p[2], -p[1]}, {-p[2], 0, p[0]}, {p[1], -p[0], 0}};
+        for (int c = 0; c < 3; ++c) {
+            for (int i = 0; i < 3; ++i) J[c][i] = sg * rot[c][i];
+            for (int i = 0; i < 3; ++i) J[c][3 + i] = (c == i) ? sg : 0.0;
+            r[c] = s[8 + c];
+        }
+        return 3;
+    }
+
+    // computePointToPointICPTermJacobian / residual (geometry_icp_jacobian.cuh:50-120)
+    // for the record wv (warped vertex, 1, raw residual warped - target, 0):
+    // Huber-weighted rows and residuals
+    static int p2p_rows(const float* wv, double J[3][6], double r[3]) {
+        const float raw[3] = {wv[4], wv[5], wv[6]};
+        const double rot[3][3] = {{0, wv[2], -wv[1]}, {-wv[2], 0, wv[0]}, {wv[1], -wv[0], 0}};
+        for (int ch = 0; ch < 3; ++ch) {
+            const double hw = huber<float>(raw[ch]);
+            for (int i = 0; i < 3; ++i) J[ch][i] = hw * rot[ch][i];
+            for (int i = 0; i < 3; ++i) J[ch][3 + i] = (ch == i) ? hw : 0.0;
+            r[ch] = hw * raw[ch];
+        }
+        return 3;
+    }
+
     // per-term weighted Jacobian rows of term `term` for node `node`:
     // returns channel count (0 invalid) and fills J[ch][6], r[ch], lambda^2
     int term_rows(u32 term, u32 node, double J[3][6], double r[3], double& lam2, double& wnode) const {
@@ -912,41 +944,16 @@ struct Oracle {
                 return 1;
             }
             case kSmooth: {
-                const float* s = &smooth[12 * (size_t)k];
                 lam2 = (double)lambda.smooth * lambda.smooth;
                 wnode = 1.0;
-                if (s[6] == 0.0f) return 0;
-                const bool is_i = node == graph[2 * (size_t)k];
-                // computeSmoothTermJacobian (geometry_icp_jacobian.cuh:359-382)
-                const double a[3] = {s[0], s[1], s[2]}, bq[3] = {s[3], s[4], s[5]};
-                const double sg = is_i ? 1.0 : -1.0;
-                const double* p = is_i ? a : bq;
-                const double rot[3][3] = {{0, p[2], -p[1]}, {-p[2], 0, p[0]}, {p[1], -p[0], 0}};
-                for (int c = 0; c < 3; ++c) {
-                    for (int i = 0; i < 3; ++i) J[c][i] = sg * rot[c][i];
-                    for (int i = 0; i < 3; ++i) J[c][3 + i] = (c == i) ? sg : 0.0;
-                    r[c] = s[8 + c];
-                }
-                return 3;
+                return smooth_rows(&smooth[12 * (size_t)k], node == graph[2 * (size_t)k], J, r);
             }
             case kFeature:
             case kCross: {
-                const Corr& c = t == kFeature ? feat : cross;
-                const float* wv = &warped[8 * (size_t)(t == kFeature ? k : Tp + k)];
-                (void)c;
                 lam2 = t == kFeature ? (double)lambda.feature * lambda.feature
                                      : (double)lambda.cross_view * lambda.cross_view;
                 wnode = weight_of(knn_of(t, k), w_of(t, k));
-                // computePointToPointICPTermJacobian / residual (geometry_icp_jacobian.cuh:50-120)
-                const float raw[3] = {wv[4], wv[5], wv[6]};
-                const double rot[3][3] = {{0, wv[2], -wv[1]}, {-wv[2], 0, wv[0]}, {wv[1], -wv[0], 0}};
-                for (int ch = 0; ch < 3; ++ch) {
-                    const double hw = huber<float>(raw[ch]);
-                    for (int i = 0; i < 3; ++i) J[ch][i] = hw * rot[ch][i];
-                    for (int i = 0; i < 3; ++i) J[ch][3 + i] = (ch == i) ? hw : 0.0;
-                    r[ch] = hw * raw[ch];
-                }
-                return 3;
+                return p2p_rows(&warped[8 * (size_t)(t == kFeature ? k : Tp + k)], J, r);
             }
             default: return 0;
         }
@@ -1360,9 +1367,10 @@ void orc_apply_jtj(void* h, const double* xin, double* y) {
 }
 
 /* Known-answer helpers over the restated math. */
+/* DualQuaternion::operator mat34 (DualQuaternion.h:309-319) in float. */
 void orc_dq_to_mat34(const float* dq8, float* m12) {
     const DQ<float> d{{dq8[0], dq8[1], dq8[2], dq8[3]}, {dq8[4], dq8[5], dq8[6], dq8[7]}};
-    const M34<float> m = se3_matrix(d);
+    const M34<float> m = dq_to_mat34(d);
     for (int c = 0; c < 3; ++c)
         for (int r = 0; r < 3; ++r) m12[3 * c + r] = m.m[r][c];
     for (int r = 0; r < 3; ++r) m12[9 + r] = m.t[r];
@@ -1383,6 +1391,45 @@ void orc_apply_twist(const double* dq8, const double* tw6, double* out8) {
     std::memcpy(out8, a, 64);
 }
 void orc_gauss_jordan_inverse(const double* A36, double* out36) { Oracle::inverse_gauss_jordan(A36, out36); }
+
+/* The oracle's float DQ blend of four nodes and its se3 matrix, in the
+ * mvdr_mat34 layout (rotation columns, translation). */
+void orc_blend_se3(const float* field, const uint16_t* knn, const float* w, float* mat12) {
+    std::vector<DQ<float>> f(4);
+    for (int k = 0; k < 4; ++k) {
+        const float* d = field + 8 * (size_t)knn[k];
+        f[k] = {{d[0], d[1], d[2], d[3]}, {d[4], d[5], d[6], d[7]}};
+    }
+    const u16 local[4] = {0, 1, 2, 3};
+    const M34<float> m = se3_matrix(blend(f, local, w));
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) mat12[3 * c + r] = m.m[r][c];
+    for (int r = 0; r < 3; ++r) mat12[9 + r] = m.t[r];
+}
+
+float orc_huber(float r) { return huber<float>(r); }
+
+/* The oracle's Jacobian rows (3 x 6) and residuals of a smooth-term record
+ * (12 floats) for node i (is_i) or j, and of a point-to-point record (8
+ * floats). Returns the channel count. */
+int orc_smooth_rows(const float* s12, int is_i, double* J18, double* r3) {
+    double J[3][6], r[3];
+    const int ch = Oracle::smooth_rows(s12, is_i != 0, J, r);
+    for (int c = 0; c < 3; ++c) {
+        for (int i = 0; i < 6; ++i) J18[6 * c + i] = ch ? J[c][i] : 0.0;
+        r3[c] = ch ? r[c] : 0.0;
+    }
+    return ch;
+}
+int orc_p2p_rows(const float* wv8, double* J18, double* r3) {
+    double J[3][6], r[3];
+    const int ch = Oracle::p2p_rows(wv8, J, r);
+    for (int c = 0; c < 3; ++c) {
+        for (int i = 0; i < 6; ++i) J18[6 * c + i] = J[c][i];
+        r3[c] = r[c];
+    }
+    return ch;
+}
 void orc_cholesky_inverse(const double* A36, double* out36) { Oracle::inverse_cholesky(A36, out36); }
 
 }  // extern "C"
