@@ -305,6 +305,65 @@ MVDR_API int mvdr_set_inputs_textures(mvdr_solver* solver, const mvdr_inputs* in
  * not checked here: read error_flags with mvdr_get_counts. */
 MVDR_API int mvdr_node_se3_device(mvdr_solver* solver, const mvdr_dual_quaternion** device_ptr);
 
+/* ---- solver maps (the renderer's solver-map pass, on CUDA) ---------------
+ * The reference renders its solver maps with OpenGL: every surfel is a point
+ * (render/shaders/SolverMap.vert, SolverMapSized.vert, SolverMapIndexMap.vert,
+ * SolverMap.frag; drawn by RendererDraw.cpp:384-480), depth-tested with
+ * GL_LESS against a float depth buffer cleared to 1, into float4 vertex,
+ * normal and rgb maps and an unsigned index map. mvdr_render_solver_maps
+ * produces the same maps with CUDA kernels on the caller's buffers. */
+typedef struct mvdr_surfel_geometry {
+    uint32_t num_surfels;
+    const mvdr_float4* reference_vertex_confid;  /* canonical vertex (frame 0), confidence */
+    const mvdr_float4* reference_normal_radius;  /* canonical normal, radius (mm)          */
+    const mvdr_float4* live_vertex_confid;       /* warped (live) vertex                   */
+    const mvdr_float4* live_normal_radius;       /* warped normal                          */
+    const mvdr_float4* color_time;               /* x: packed 0xRRGGBB as float bits,
+                                                    y: written to the rgb map's w,
+                                                    z: time last observed               */
+} mvdr_surfel_geometry;
+
+typedef struct mvdr_solver_map_params {
+    uint32_t width, height;        /* map size in pixels                                   */
+    float max_depth;               /* widthHeightMaxMinDepth.z: points beyond max_depth + 0.05 m are dropped */
+    float current_time;            /* the frame's time                                     */
+    float confidence_threshold;    /* kStableSurfelConfidenceThreshold                      */
+    float time_threshold;          /* kRenderingRecentTimeThreshold; a negative value drops
+                                      every surfel below the confidence threshold
+                                      (DrawSolverMapsConfidentObservation)                 */
+} mvdr_solver_map_params;
+
+typedef struct mvdr_solver_map_view {
+    mvdr_mat34 world2camera;       /* the view's world2camera                              */
+    mvdr_mat34 initial_camera_se3; /* camera v -> frame 0 (identity for view 0); the maps
+                                      hold its inverse applied to the surfel attributes   */
+    mvdr_intrinsic intrinsic;      /* the renderer's intrinsic of this view                */
+    int32_t sized_points;          /* 1: each point covers the projected surfel disc
+                                      (SolverMapSized.vert, view 0 with USE_DENSE_SOLVER_MAPS);
+                                      0: one-pixel points (SolverMapIndexMap.vert)         */
+    uint32_t pitch;                /* row pitch of the outputs in elements (0 = width)     */
+    /* outputs, device memory, height x pitch elements each (any may be NULL
+       except index_map and depth_index) */
+    mvdr_float4* reference_vertex_map;
+    mvdr_float4* reference_normal_map;
+    mvdr_float4* live_vertex_map;
+    mvdr_float4* live_normal_map;
+    uint32_t* index_map;           /* surfel id, MVDR_INVALID_INDEX where nothing lands    */
+    mvdr_float4* normalized_rgb_map;
+    uint64_t* depth_index;         /* caller-owned scratch: the depth test's (depth, id)
+                                      words, height x pitch                               */
+} mvdr_solver_map_view;
+
+/* Render the solver maps of num_views views (<= MVDR_MAX_VIEWS) on `stream`.
+ * No allocation and no host synchronisation. Equal depths resolve to the
+ * smaller surfel id, as the first point drawn wins GL_LESS. Points whose
+ * centre falls outside the image are dropped, as GL clips points by their
+ * centre. The rasteriser's sub-pixel snapping is not reproduced: a point
+ * covers the pixels whose centres lie in the square of its size around its
+ * projection. */
+MVDR_API int mvdr_render_solver_maps(const mvdr_surfel_geometry* surfels, const mvdr_solver_map_params* params,
+                                     const mvdr_solver_map_view* views, uint32_t num_views, void* stream);
+
 /* ---- input bundles (replay of one solve's inputs) -----------------------
  * mvdr_save_input_bundle writes the configuration and every input array
  * bound to the solver (device or owned copies) to a file; it synchronises

@@ -71,6 +71,8 @@ def _declare(L):
         "mvdr_batch_set_pcg_persistent": (i32, [vp, i32]),
         "mvdr_batch_set_wait_limit": (i32, [vp, C.c_uint64, u32]),
         "mvdr_batch_enqueue_stage": (i32, [vp, i32, vp]),
+        "mvdr_render_solver_maps": (i32, [P(abi.SurfelGeometry), P(abi.SolverMapParams), P(abi.SolverMapView), u32,
+                                          vp]),
         "mvdr_last_error_string": (C.c_char_p, []),
         "mvdr_kernel_launch_count": (C.c_uint64, []),
         "mvdr_abi_layout": (i32, [C.c_char_p, P(C.c_size_t)]),

@@ -112,10 +112,30 @@ class Counts(C.Structure):
         "nodepair_entries", "half_pairs", "num_bins", "binblock_nnz", "error_flags", "reserved")]
 
 
+class SurfelGeometry(C.Structure):
+    _fields_ = [("num_surfels", C.c_uint32), ("reference_vertex_confid", C.c_void_p),
+                ("reference_normal_radius", C.c_void_p), ("live_vertex_confid", C.c_void_p),
+                ("live_normal_radius", C.c_void_p), ("color_time", C.c_void_p)]
+
+
+class SolverMapParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("max_depth", C.c_float),
+                ("current_time", C.c_float), ("confidence_threshold", C.c_float), ("time_threshold", C.c_float)]
+
+
+class SolverMapView(C.Structure):
+    _fields_ = [("world2camera", Mat34), ("initial_camera_se3", Mat34), ("intrinsic", Intrinsic),
+                ("sized_points", C.c_int32), ("pitch", C.c_uint32), ("reference_vertex_map", C.c_void_p),
+                ("reference_normal_map", C.c_void_p), ("live_vertex_map", C.c_void_p),
+                ("live_normal_map", C.c_void_p), ("index_map", C.c_void_p), ("normalized_rgb_map", C.c_void_p),
+                ("depth_index", C.c_void_p)]
+
+
 STRUCTS = {"mvdr_float4": Float4, "mvdr_dual_quaternion": DualQuaternion, "mvdr_mat34": Mat34,
            "mvdr_intrinsic": Intrinsic, "mvdr_penalty": Penalty, "mvdr_config": Config,
            "mvdr_view_inputs": ViewInputs, "mvdr_correspondences": Correspondences, "mvdr_inputs": Inputs,
-           "mvdr_counts": Counts, "mvdr_view_textures": ViewTextures}
+           "mvdr_counts": Counts, "mvdr_view_textures": ViewTextures, "mvdr_surfel_geometry": SurfelGeometry,
+           "mvdr_solver_map_params": SolverMapParams, "mvdr_solver_map_view": SolverMapView}
 
 
 def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=480, precision=PRECISION_MIXED,
@@ -218,3 +238,39 @@ def fill_inputs(scene, ptr, density=False):
         dst.knn = ptr(f"{name}.knn", corr.knn)
         dst.knn_weight = ptr(f"{name}.w", corr.knn_weight)
     return inp
+
+
+SOLVER_MAP_OUTPUTS = ("reference_vertex_map", "reference_normal_map", "live_vertex_map", "live_normal_map",
+                      "index_map", "normalized_rgb_map", "depth_index")
+SURFEL_ARRAYS = ("reference_vertex_confid", "reference_normal_radius", "live_vertex_confid", "live_normal_radius",
+                 "color_time")
+
+
+def surfel_geometry(num_surfels, ptrs):
+    """mvdr_surfel_geometry over the five arrays `ptrs[name]` (addresses)."""
+    g = SurfelGeometry()
+    g.num_surfels = num_surfels
+    for name in SURFEL_ARRAYS:
+        setattr(g, name, ptrs[name])
+    return g
+
+
+def solver_map_params(width, height, max_depth=3.0, current_time=10.0, confidence_threshold=10.0,
+                      time_threshold=3.0):
+    return SolverMapParams(width, height, max_depth, current_time, confidence_threshold, time_threshold)
+
+
+def solver_map_view(view, ptrs, sized_points=False, pitch=0):
+    """mvdr_solver_map_view for a scene view's camera (world2camera,
+    initial_camera_se3, intrinsic); `ptrs` maps SOLVER_MAP_OUTPUTS names to
+    addresses (absent or None: that map is not written)."""
+    mv = SolverMapView()
+    mv.world2camera = _mat34(view.world2camera)
+    mv.initial_camera_se3 = _mat34(view.initial_camera_se3)
+    mv.intrinsic = Intrinsic(*[float(x) for x in view.intrinsic])
+    mv.sized_points = int(bool(sized_points))
+    mv.pitch = pitch
+    for name in SOLVER_MAP_OUTPUTS:
+        setattr(mv, name, ptrs.get(name))
+    return mv
+

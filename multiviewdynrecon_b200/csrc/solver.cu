@@ -1029,7 +1029,9 @@ int mvdr_abi_layout(const char* name, size_t* size) {
         {"mvdr_penalty", sizeof(mvdr_penalty)}, {"mvdr_config", sizeof(mvdr_config)},
         {"mvdr_view_inputs", sizeof(mvdr_view_inputs)}, {"mvdr_correspondences", sizeof(mvdr_correspondences)},
         {"mvdr_inputs", sizeof(mvdr_inputs)}, {"mvdr_counts", sizeof(mvdr_counts)},
-        {"mvdr_view_textures", sizeof(mvdr_view_textures)}};
+        {"mvdr_view_textures", sizeof(mvdr_view_textures)}, {"mvdr_surfel_geometry", sizeof(mvdr_surfel_geometry)},
+        {"mvdr_solver_map_params", sizeof(mvdr_solver_map_params)},
+        {"mvdr_solver_map_view", sizeof(mvdr_solver_map_view)}};
     for (const auto& t : table)
         if (std::strcmp(t.n, name) == 0) { *size = t.s; return MVDR_OK; }
     return MVDR_EINVAL;

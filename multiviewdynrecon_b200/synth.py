@@ -283,6 +283,9 @@ class Scene:
     cross_view: Correspondences
     node_radius: float = 0.025
     terms: dict = field(default_factory=dict)   # which terms the config asks for
+    # the surfels behind the index maps, in frame 0 (surfel id = row)
+    surfel_position: np.ndarray = None   # (S, 3) float64
+    surfel_normal: np.ndarray = None     # (S, 3) float64
     gn_iterations: int = 3
     pcg_iterations: int = 10
 
@@ -551,7 +554,74 @@ def _build(name, shapes, cams, W, H, fx, fy, cx, cy, num_nodes, seed, *, auto_ra
     return Scene(name=name, width=W, height=H, views=views, surfel_knn=surfel_knn,
                  surfel_knn_weight=surfel_w, node_se3=node_se3, canonical_nodes=canonical_nodes,
                  node_graph=graph, feature=cat(feats), cross_view=cat(cross), node_radius=node_radius,
-                 terms=terms or {}, gn_iterations=gn, pcg_iterations=pcg)
+                 terms=terms or {}, gn_iterations=gn, pcg_iterations=pcg, surfel_position=surfels,
+                 surfel_normal=surfel_normals)
+
+
+# --------------------------------------------------------------------------
+# surfel geometry for the solver-map renderer
+# --------------------------------------------------------------------------
+
+def blend_warp(node_se3, knn, w):
+    """Surfel-wise rigid motions of the blended warp field (DQ blend,
+    normalise, se3 matrix) in float64: returns R (S, 3, 3), t (S, 3)."""
+    q = np.einsum("sk,skc->sc", np.asarray(w, np.float64), np.asarray(node_se3, np.float64)[knn.astype(np.int64)])
+    q0, q1 = q[:, :4], q[:, 4:]
+    inv = 1.0 / np.linalg.norm(q0, axis=1)
+    q0, q1 = q0 * inv[:, None], q1 * inv[:, None]
+    q1 = q1 - np.einsum("sc,sc->s", q0, q1)[:, None] * q0
+    x, y, z, ww = q0.T
+    R = np.stack([np.stack([1 - 2 * y * y - 2 * z * z, 2 * x * y - 2 * z * ww, 2 * x * z + 2 * y * ww], -1),
+                  np.stack([2 * x * y + 2 * z * ww, 1 - 2 * x * x - 2 * z * z, 2 * y * z - 2 * x * ww], -1),
+                  np.stack([2 * x * z - 2 * y * ww, 2 * y * z + 2 * x * ww, 1 - 2 * x * x - 2 * y * y], -1)], 1)
+    a = 2 * q1
+    t = np.stack([a[:, 3] * -x + a[:, 0] * ww + a[:, 1] * -z - a[:, 2] * -y,
+                  a[:, 3] * -y - a[:, 0] * -z + a[:, 1] * ww + a[:, 2] * -x,
+                  a[:, 3] * -z + a[:, 0] * -y - a[:, 1] * -x + a[:, 2] * ww], -1)
+    return R, t
+
+
+def pack_rgb(rgb):
+    """Colour packed as the renderer reads it: 8-bit r, g, b in bits 16-23,
+    8-15 and 0-7 of color_time.x's float bits (the top byte is 0)."""
+    c = np.clip(np.rint(np.asarray(rgb, np.float64) * 255.0), 0, 255).astype(np.uint32)
+    return ((c[:, 0] << 16) | (c[:, 1] << 8) | c[:, 2]).view(np.float32)
+
+
+def solver_map_geometry(scene, seed=0, current_time=10.0, warped=True):
+    """The scene's surfels as the renderer's five float4 arrays: reference
+    vertex + confidence, reference normal + radius (mm), live vertex and
+    normal (the reference surfels moved by the scene's warp field, or copies
+    when `warped` is False) and (packed colour, initial time, last observed
+    time, 0). Confidence in [0, 20) and observation times in
+    [current_time - 6, current_time] so that the stable/recent cull of the
+    renderer has both outcomes."""
+    rng = np.random.default_rng([seed, 104729])
+    S = scene.num_surfels
+    p = np.asarray(scene.surfel_position, np.float64)
+    n = np.asarray(scene.surfel_normal, np.float64)
+    # a disc about as wide as the pixel footprint in view 0 (mm): 1.4 to 4.2
+    # pixels across there
+    m = np.asarray(scene.views[0].initial_camera_se3, np.float64)
+    depth = np.abs((p - m[9:12]) @ m[:9].reshape(3, 3).T[:, 2])
+    fx = float(scene.views[0].intrinsic[2])
+    radius = depth / fx * 1000.0 * rng.uniform(0.5, 1.5, S)
+    ref_v = np.concatenate([p, rng.uniform(0.0, 20.0, (S, 1))], 1).astype(np.float32)
+    ref_n = np.concatenate([n, radius[:, None]], 1).astype(np.float32)
+    if warped:
+        R, t = blend_warp(scene.node_se3, scene.surfel_knn, scene.surfel_knn_weight)
+        lp = np.einsum("sij,sj->si", R, p) + t
+        ln = np.einsum("sij,sj->si", R, n)
+    else:
+        lp, ln = p, n
+    live_v = np.concatenate([lp, ref_v[:, 3:4]], 1).astype(np.float32)
+    live_n = np.concatenate([ln, radius[:, None]], 1).astype(np.float32)
+    ct = np.zeros((S, 4), np.float32)
+    ct[:, 0] = pack_rgb(surface_colour(p))
+    ct[:, 1] = rng.integers(0, int(current_time) + 1, S).astype(np.float32)
+    ct[:, 2] = (current_time - rng.integers(0, 7, S)).astype(np.float32)
+    return dict(reference_vertex_confid=ref_v, reference_normal_radius=ref_n, live_vertex_confid=live_v,
+                live_normal_radius=live_n, color_time=ct)
 
 
 # --------------------------------------------------------------------------

@@ -101,6 +101,7 @@ def lib():
         L.orc_smooth_rows.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_p2p_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_render_solver_maps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
         _lib = L
     return _lib
 
@@ -271,3 +272,25 @@ def cholesky_inverse(A):
     out = np.empty(36, np.float64)
     lib().orc_cholesky_inverse(_p(A), _p(out))
     return out.reshape(6, 6)
+
+
+def render_solver_maps(geometry, params, views, sized=None):
+    """The oracle's restatement of the solver-map pass. `geometry`: dict of
+    the five (S, 4) float32 surfel arrays; `params`: abi.SolverMapParams;
+    `views`: scene views (cameras). Returns per view a dict of host maps
+    (the names of abi.SOLVER_MAP_OUTPUTS minus depth_index)."""
+    arrs = {k: np.ascontiguousarray(geometry[k], np.float32) for k in abi.SURFEL_ARRAYS}
+    n = len(arrs["live_vertex_confid"])
+    g = abi.surfel_geometry(n, {k: a.ctypes.data for k, a in arrs.items()})
+    H, W = params.height, params.width
+    out, mv = [], (abi.SolverMapView * len(views))()
+    for v, view in enumerate(views):
+        maps = {k: np.zeros((H, W, 4), np.float32) for k in ("reference_vertex_map", "reference_normal_map",
+                                                            "live_vertex_map", "live_normal_map",
+                                                            "normalized_rgb_map")}
+        maps["index_map"] = np.zeros((H, W), np.uint32)
+        out.append(maps)
+        mv[v] = abi.solver_map_view(view, {k: a.ctypes.data for k, a in maps.items()},
+                                     sized_points=bool(sized[v]) if sized is not None else False)
+    lib().orc_render_solver_maps(C.byref(g), C.byref(params), mv, len(views))
+    return out

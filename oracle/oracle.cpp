@@ -1392,6 +1392,133 @@ void orc_apply_twist(const double* dq8, const double* tw6, double* out8) {
 }
 void orc_gauss_jordan_inverse(const double* A36, double* out36) { Oracle::inverse_gauss_jordan(A36, out36); }
 
+/* The renderer's solver-map pass (render/shaders/SolverMap.vert,
+ * SolverMapSized.vert, SolverMapIndexMap.vert, SolverMap.frag; drawn by
+ * RendererDraw.cpp:384-480) restated as the GL pipeline runs it: points drawn
+ * in surfel order, each covering the pixels whose centres lie in the square of
+ * its size around its projection, kept where their depth is strictly below
+ * the depth buffer's (GL_LESS, buffer cleared to 1 = nothing drawn). Every
+ * pointer is HOST memory; depth_index is not used. Float arithmetic without
+ * contraction, in the kernel's operation order. */
+void orc_render_solver_maps(const mvdr_surfel_geometry* g, const mvdr_solver_map_params* prm,
+                            const mvdr_solver_map_view* views, uint32_t num_views) {
+    const uint32_t W = prm->width, H = prm->height;
+    auto rows = [](const mvdr_mat34& m, float* o) {
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) o[3 * r + c] = m.rot[3 * c + r];
+        for (int r = 0; r < 3; ++r) o[9 + r] = m.trans[r];
+    };
+    auto pt = [](const float* m, const float* p, float* o) {
+        for (int r = 0; r < 3; ++r) o[r] = m[3 * r] * p[0] + m[3 * r + 1] * p[1] + m[3 * r + 2] * p[2] + m[9 + r];
+    };
+    auto dir = [](const float* m, const float* p, float* o) {
+        for (int r = 0; r < 3; ++r) o[r] = m[3 * r] * p[0] + m[3 * r + 1] * p[1] + m[3 * r + 2] * p[2];
+    };
+    auto nrm = [](float* v) {
+        const float inv = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int k = 0; k < 3; ++k) v[k] *= inv;
+    };
+    for (uint32_t v = 0; v < num_views; ++v) {
+        const mvdr_solver_map_view& V = views[v];
+        const uint32_t pitch = V.pitch ? V.pitch : W;
+        float w2c[12], init[12], inv[12];
+        rows(V.world2camera, w2c);
+        rows(V.initial_camera_se3, init);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) inv[3 * r + c] = init[3 * c + r];
+        for (int r = 0; r < 3; ++r) inv[9 + r] = -(inv[3 * r] * init[9] + inv[3 * r + 1] * init[10] + inv[3 * r + 2] * init[11]);
+        const float fx = V.intrinsic.focal_x, fy = V.intrinsic.focal_y, cx = V.intrinsic.principal_x,
+                    cy = V.intrinsic.principal_y;
+        std::vector<float> depth((size_t)W * H, INFINITY);
+        std::vector<uint32_t> who((size_t)W * H, MVDR_INVALID_INDEX);
+        for (uint32_t s = 0; s < g->num_surfels; ++s) {
+            const mvdr_float4 lv = g->live_vertex_confid[s];
+            const float l3[3] = {lv.x, lv.y, lv.z};
+            float p1[3], pc[3];
+            pt(inv, l3, p1);
+            pt(w2c, p1, pc);
+            const mvdr_float4 ct = g->color_time[s];
+            if (pc[2] > prm->max_depth + 0.05f || !(pc[2] > 0.0f) ||
+                (g->reference_vertex_confid[s].w < prm->confidence_threshold &&
+                 std::fabs(ct.z - prm->current_time) >= prm->time_threshold))
+                continue;
+            const float xw = (fx * pc[0]) / pc[2] + cx, yw = (fy * pc[1]) / pc[2] + cy;
+            if (!(xw >= 0.0f && xw <= (float)W && yw >= 0.0f && yw <= (float)H)) continue;
+            float size = 1.0f;
+            if (V.sized_points) {
+                const mvdr_float4 ln = g->live_normal_radius[s];
+                const float l4[3] = {ln.x, ln.y, ln.z};
+                float t[3], n[3];
+                dir(inv, l4, t);
+                dir(w2c, t, n);
+                nrm(n);
+                const float scale = g->reference_normal_radius[s].w * 1.41421356f * 0.001f;
+                float x0[3] = {n[1] - n[2], -n[0], n[0]};
+                nrm(x0);
+                const float x1[3] = {x0[0] * scale, x0[1] * scale, x0[2] * scale};
+                const float y1[3] = {n[1] * x1[2] - n[2] * x1[1], n[2] * x1[0] - n[0] * x1[2], n[0] * x1[1] - n[1] * x1[0]};
+                float px[4], py[4];
+                const float* ds[4] = {x1, y1, y1, x1};
+                const float sg[4] = {1.f, 1.f, -1.f, -1.f};
+                for (int k = 0; k < 4; ++k) {
+                    const float q[3] = {sg[k] > 0 ? pc[0] + ds[k][0] : pc[0] - ds[k][0],
+                                        sg[k] > 0 ? pc[1] + ds[k][1] : pc[1] - ds[k][1],
+                                        sg[k] > 0 ? pc[2] + ds[k][2] : pc[2] - ds[k][2]};
+                    px[k] = (fx * q[0]) / q[2] + cx;
+                    py[k] = (fy * q[1]) / q[2] + cy;
+                }
+                const float xd = std::max(px[0], std::max(px[1], std::max(px[2], px[3]))) -
+                                 std::min(px[0], std::min(px[1], std::min(px[2], px[3])));
+                const float yd = std::max(py[0], std::max(py[1], std::max(py[2], py[3]))) -
+                                 std::min(py[0], std::min(py[1], std::min(py[2], py[3])));
+                size = std::min(std::max(std::max(0.0f, std::min(std::fabs(xd), std::fabs(yd))), 1.0f), 2047.0f);
+            }
+            const float h = 0.5f * size;
+            const int u0 = std::max(0, (int)std::ceil(xw - h - 0.5f)), u1 = std::min((int)W, (int)std::ceil(xw + h - 0.5f));
+            const int w0 = std::max(0, (int)std::ceil(yw - h - 0.5f)), w1 = std::min((int)H, (int)std::ceil(yw + h - 0.5f));
+            for (int w = w0; w < w1; ++w)
+                for (int u = u0; u < u1; ++u) {
+                    const size_t q = (size_t)w * W + u;
+                    if (pc[2] < depth[q]) {  // GL_LESS: an equal depth keeps the point drawn first
+                        depth[q] = pc[2];
+                        who[q] = s;
+                    }
+                }
+        }
+        for (uint32_t w = 0; w < H; ++w)
+            for (uint32_t u = 0; u < W; ++u) {
+                const uint32_t id = who[(size_t)w * W + u];
+                const size_t o = (size_t)w * pitch + u;
+                mvdr_float4 rv{0, 0, 0, 0}, rn{0, 0, 0, 0}, lv{0, 0, 0, 0}, ln{0, 0, 0, 0}, rgb{0, 0, 0, 0};
+                if (id != MVDR_INVALID_INDEX) {
+                    const mvdr_float4 a0 = g->reference_vertex_confid[id], a1 = g->reference_normal_radius[id],
+                                      a2 = g->live_vertex_confid[id], a3 = g->live_normal_radius[id];
+                    const float i0[3] = {a0.x, a0.y, a0.z}, i1[3] = {a1.x, a1.y, a1.z}, i2[3] = {a2.x, a2.y, a2.z},
+                                i3[3] = {a3.x, a3.y, a3.z};
+                    float q0[3], q1[3], q2[3], q3[3];
+                    pt(inv, i0, q0);
+                    dir(inv, i1, q1);
+                    pt(inv, i2, q2);
+                    dir(inv, i3, q3);
+                    rv = {q0[0], q0[1], q0[2], 1.0f};
+                    rn = {q1[0], q1[1], q1[2], 0.0f};
+                    lv = {q2[0], q2[1], q2[2], 1.0f};
+                    ln = {q3[0], q3[1], q3[2], 0.0f};
+                    uint32_t bits;
+                    std::memcpy(&bits, &g->color_time[id].x, 4);
+                    rgb = {(float)((bits & 0x00FF0000u) >> 16) / 255.f, (float)((bits & 0x0000FF00u) >> 8) / 255.f,
+                           (float)(bits & 0x000000FFu) / 255.f, V.sized_points ? 1.0f : g->color_time[id].y};
+                }
+                if (V.reference_vertex_map) V.reference_vertex_map[o] = rv;
+                if (V.reference_normal_map) V.reference_normal_map[o] = rn;
+                if (V.live_vertex_map) V.live_vertex_map[o] = lv;
+                if (V.live_normal_map) V.live_normal_map[o] = ln;
+                if (V.normalized_rgb_map) V.normalized_rgb_map[o] = rgb;
+                V.index_map[o] = id;
+            }
+    }
+}
+
 /* The oracle's float DQ blend of four nodes and its se3 matrix, in the
  * mvdr_mat34 layout (rotation columns, translation). */
 void orc_blend_se3(const float* field, const uint16_t* knn, const float* w, float* mat12) {
