@@ -61,10 +61,11 @@ def parse():
                    help="use this SpMV tile shape (index into abi.SPMV_SHAPES) instead of the autotuner's")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="torso", choices=["torso", "sphere", "uneven", "body"],
+    p.add_argument("--workload", default="torso", choices=["torso", "sphere", "uneven", "body", "solver_maps"],
                    help="torso: the headline batch (default); sphere: the 1-view 2048-node plain-method "
                         "configuration; uneven: 16 instances with 1024-16384 nodes and 1-4 views; body: one "
-                        "32768-node, 5-view 1280x720 solve")
+                        "32768-node, 5-view 1280x720 solve; solver_maps: the renderer's solver maps of the "
+                        "body workload's surfels in its 5 views")
     p.add_argument("--no-accuracy", action="store_true", help="skip the FP64 check of the timed configuration")
     p.add_argument("--no-e2e", action="store_true",
                    help="skip the end-to-end leg (for profiler captures only; the bench line then has no e2e)")
@@ -594,6 +595,68 @@ def spmv_stage(lib, abi, batch, stream, reps=20):
     return a.elapsed_time(b) / reps
 
 
+def solver_map_bytes(S, V, W, H, drawn, any_sized):
+    """Algorithmic DRAM bytes of one render of V views: every surfel's live
+    vertex, colour/time and reference vertex (for its confidence; a float4
+    component costs its whole 16-byte element, the sector size being 32) and,
+    when a view draws sized points, its live normal and reference normal (for
+    the radius) read once; per pixel the depth-index word cleared and read
+    back and the five float4 maps and the index written; per drawn pixel the
+    winner's five float4 attributes gathered. The depth test's atomics stay
+    in L2 (a view's depth-index buffer is W*H*8 bytes)."""
+    surfel = S * (16 * 3 + (16 * 2 if any_sized else 0))
+    pixels = V * W * H * (8 + 8 + 5 * 16 + 4)
+    return surfel + pixels + drawn * 5 * 16
+
+
+def run_solver_maps(args):
+    """Times mvdr_render_solver_maps on the body workload's surfels (moved by
+    its warp field) in its five 1280x720 views, view 0 with sized points;
+    checks the maps bit for bit against the oracle and times the oracle's
+    render on one host thread."""
+    import torch
+    from multiviewdynrecon_b200 import abi, synth
+    from multiviewdynrecon_b200.solver_maps import SolverMapRenderer, geometry_to_device
+    import oracle
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    t0 = time.perf_counter()
+    scene = synth.articulated_body(auto_radius=True, focal_scale=5.0)
+    g = synth.solver_map_geometry(scene)
+    gen_s = time.perf_counter() - t0
+    S, V, W, H = scene.num_surfels, scene.num_views, scene.width, scene.height
+    r = SolverMapRenderer(W, H, V, sized_view0=True)
+    dg = geometry_to_device(g)
+    with torch.cuda.stream(stream):
+        step = lambda: r.draw_solver_maps_with_recent_observation(dg, 10.0, scene.views, stream=stream)  # noqa
+        ms = time_solves(step, args.steps, max(3, args.warmup), stream)
+    got = [{k: t.cpu().numpy() for k, t in r.maps(v).items()} for v in range(V)]
+    prm = abi.solver_map_params(W, H)
+    oracle.lib()
+    t1 = time.perf_counter()
+    want = oracle.render_solver_maps(g, prm, scene.views, sized=[v == 0 for v in range(V)])
+    cpu_s = time.perf_counter() - t1
+    same = all(np.array_equal(np.ascontiguousarray(got[v][k]).view(np.uint32),
+                              np.ascontiguousarray(want[v][k]).view(np.uint32))
+               for v in range(V) for k in want[v])
+    drawn = int(sum((w["index_map"] != 0xFFFFFFFF).sum() for w in want))
+    nbytes = solver_map_bytes(S, V, W, H, drawn, True)
+    peak, peak_kind = load_peaks()
+    gbs = nbytes / 1e9 / (ms / 1e3)
+    line = {"workload": "solver_maps", "metric": "solver-map renders/s", "unit": "renders/s",
+            "value": round(1e3 / ms, 2), "ms_per_step": round(ms, 4), "steps": args.steps,
+            "config": {"surfels": S, "views": V, "image": [W, H], "sized_view0": True,
+                       "l2": "surfel arrays and maps well above the 126 MB L2; no flush"},
+            "drawn_pixels": drawn, "bit_exact_vs_oracle": bool(same), "generation_s": round(gen_s, 1),
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "peak_kind": peak_kind, "algorithmic_bytes": nbytes,
+                         "kernels": "splat_kernel + resolve_kernel + the depth-index clears"},
+            "cpu_baseline": {"value": round(1.0 / cpu_s, 3), "unit": "renders/s", "cores": 1, "kind": "port",
+                             "sample": "one whole render of the workload by the oracle"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_extra_workload(args):
     """The uneven batch and the large single solve: one JSON line each,
     documenting configurations beside the headline."""
@@ -776,6 +839,8 @@ def main():
         print(json.dumps(line), flush=True)
         return 0
 
+    if args.workload == "solver_maps":
+        return run_solver_maps(args) if rank == 0 else 0
     if args.workload != "torso":
         return run_extra_workload(args) if rank == 0 else 0
 

@@ -4,17 +4,17 @@
 // (render/shaders/SolverMap.vert, SolverMapSized.vert, SolverMapIndexMap.vert,
 // SolverMap.frag, drawn by RendererDraw.cpp:384-480) with a GL_LESS depth test
 // against a float depth buffer cleared to 1 (GLRenderMaps.cpp:207-218). Here
-// that is two kernels per view:
-//   splat   - a thread per surfel: cull, project, size the point, and for every
-//             pixel the point covers an atomicMin of (camera z bits << 32 | id)
-//             into a 64-bit depth-index word. Positive floats order as their
-//             bit patterns, so the minimum is the nearest surfel and, among
-//             equal depths, the smallest id: the point drawn first, which is
-//             the one GL_LESS keeps. The result does not depend on the order in
-//             which threads run.
-//   resolve - a thread per pixel: write the winning surfel's attributes (a
-//             point's fragments all carry its vertex outputs) or the clear
-//             values.
+// that is two kernels:
+//   splat   - a thread per surfel, for every view: cull, project, size the
+//             point, and for every pixel the point covers an atomicMin of
+//             (camera z bits << 32 | id) into a 64-bit depth-index word.
+//             Positive floats order as their bit patterns, so the minimum is
+//             the nearest surfel and, among equal depths, the smallest id:
+//             the point drawn first, which is the one GL_LESS keeps. The
+//             result does not depend on the order in which threads run.
+//   resolve - a thread per pixel of each view: write the winning surfel's
+//             attributes (a point's fragments all carry its vertex outputs)
+//             or the clear values.
 // This file is compiled with -fmad=false: every float operation is a single
 // IEEE operation, as in the CPU restatement the tests compare it with.
 #include <algorithm>
@@ -46,6 +46,7 @@ struct SplatView {
 
 struct SplatArgs {
     SplatView v[MVDR_MAX_VIEWS];
+    uint32_t num_views, any_sized;
     uint32_t num_surfels, width, height;
     float max_depth, now, conf_thr, time_thr;
     const float4* ref_vc;
@@ -72,45 +73,58 @@ __device__ inline float2 image_point(const SplatView& V, float3 p) {
     return make_float2((V.fx * p.x) / p.z + V.cx, (V.fy * p.y) / p.z + V.cy);
 }
 
+// One thread per surfel, every view: the surfel's attributes are read once
+// and splatted into each view's depth-index buffer.
 __global__ void __launch_bounds__(256) splat_kernel(const __grid_constant__ SplatArgs a) {
-    const SplatView& V = a.v[blockIdx.y];
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.num_surfels) return;
     const float4 lv = a.live_v[s];
-    // the point in the view's camera: world2camera * initialCameraSE3^-1 * live
-    const float3 pc = mat_point(V.w2c, mat_point(V.inv, make_float3(lv.x, lv.y, lv.z)));
     const float4 ct = a.color_time[s];
     const float conf = a.ref_vc[s].w;
-    if (pc.z > a.max_depth + 0.05f || !(pc.z > 0.0f) ||
-        (conf < a.conf_thr && fabsf(ct.z - a.now) >= a.time_thr))
-        return;  // culled (the shaders move the point out of the clip volume)
-    const float2 c = image_point(V, pc);
-    // GL clips a point by its centre: the window position must be in the image
-    if (!(c.x >= 0.0f && c.x <= (float)a.width && c.y >= 0.0f && c.y <= (float)a.height)) return;
-    float size = 1.0f;
-    if (V.sized) {
-        // SolverMapSized.vert: the extent of the surfel's disc in the image
-        const float4 ln = a.live_n[s];
-        const float3 n = normalized3(mat_dir(V.w2c, mat_dir(V.inv, make_float3(ln.x, ln.y, ln.z))));
-        const float scale = a.ref_nr[s].w * 1.41421356f * 0.001f;
-        const float3 x0 = normalized3(make_float3(n.y - n.z, -n.x, n.x));
-        const float3 x1 = make_float3(x0.x * scale, x0.y * scale, x0.z * scale);
-        const float3 y1 = make_float3(n.y * x1.z - n.z * x1.y, n.z * x1.x - n.x * x1.z, n.x * x1.y - n.y * x1.x);
-        const float2 p1 = image_point(V, make_float3(pc.x + x1.x, pc.y + x1.y, pc.z + x1.z));
-        const float2 p2 = image_point(V, make_float3(pc.x + y1.x, pc.y + y1.y, pc.z + y1.z));
-        const float2 p3 = image_point(V, make_float3(pc.x - y1.x, pc.y - y1.y, pc.z - y1.z));
-        const float2 p4 = image_point(V, make_float3(pc.x - x1.x, pc.y - x1.y, pc.z - x1.z));
-        const float xd = fmaxf(p1.x, fmaxf(p2.x, fmaxf(p3.x, p4.x))) - fminf(p1.x, fminf(p2.x, fminf(p3.x, p4.x)));
-        const float yd = fmaxf(p1.y, fmaxf(p2.y, fmaxf(p3.y, p4.y))) - fminf(p1.y, fminf(p2.y, fminf(p3.y, p4.y)));
-        size = fminf(fmaxf(fmaxf(0.0f, fminf(fabsf(xd), fabsf(yd))), 1.0f), kMaxPointSize);
+    // the culling test that does not depend on the view: unstable and not
+    // recently observed
+    if (conf < a.conf_thr && fabsf(ct.z - a.now) >= a.time_thr) return;
+    float4 ln = make_float4(0.f, 0.f, 0.f, 0.f);
+    float radius = 0.0f;
+    if (a.any_sized) {
+        ln = a.live_n[s];
+        radius = a.ref_nr[s].w;
     }
-    // the pixels whose centres lie in [c - size/2, c + size/2)
-    const float h = 0.5f * size;
-    const int u0 = max(0, (int)ceilf(c.x - h - 0.5f)), u1 = min((int)a.width, (int)ceilf(c.x + h - 0.5f));
-    const int w0 = max(0, (int)ceilf(c.y - h - 0.5f)), w1 = min((int)a.height, (int)ceilf(c.y + h - 0.5f));
-    const unsigned long long key = ((unsigned long long)__float_as_uint(pc.z) << 32) | s;
-    for (int w = w0; w < w1; ++w)
-        for (int u = u0; u < u1; ++u) atomicMin(V.zbuf + (size_t)w * V.pitch + u, key);
+    for (uint32_t v = 0; v < a.num_views; ++v) {
+        const SplatView& V = a.v[v];
+        // the point in the view's camera: world2camera * initialCameraSE3^-1 * live
+        const float3 pc = mat_point(V.w2c, mat_point(V.inv, make_float3(lv.x, lv.y, lv.z)));
+        if (pc.z > a.max_depth + 0.05f || !(pc.z > 0.0f)) continue;  // culled (moved out of the clip volume)
+        const float2 c = image_point(V, pc);
+        // GL clips a point by its centre: the window position must be in the image
+        if (!(c.x >= 0.0f && c.x <= (float)a.width && c.y >= 0.0f && c.y <= (float)a.height)) continue;
+        float size = 1.0f;
+        if (V.sized) {
+            // SolverMapSized.vert: the extent of the surfel's disc in the image
+            const float3 n = normalized3(mat_dir(V.w2c, mat_dir(V.inv, make_float3(ln.x, ln.y, ln.z))));
+            const float scale = radius * 1.41421356f * 0.001f;
+            const float3 x0 = normalized3(make_float3(n.y - n.z, -n.x, n.x));
+            const float3 x1 = make_float3(x0.x * scale, x0.y * scale, x0.z * scale);
+            const float3 y1 =
+                make_float3(n.y * x1.z - n.z * x1.y, n.z * x1.x - n.x * x1.z, n.x * x1.y - n.y * x1.x);
+            const float2 p1 = image_point(V, make_float3(pc.x + x1.x, pc.y + x1.y, pc.z + x1.z));
+            const float2 p2 = image_point(V, make_float3(pc.x + y1.x, pc.y + y1.y, pc.z + y1.z));
+            const float2 p3 = image_point(V, make_float3(pc.x - y1.x, pc.y - y1.y, pc.z - y1.z));
+            const float2 p4 = image_point(V, make_float3(pc.x - x1.x, pc.y - x1.y, pc.z - x1.z));
+            const float xd =
+                fmaxf(p1.x, fmaxf(p2.x, fmaxf(p3.x, p4.x))) - fminf(p1.x, fminf(p2.x, fminf(p3.x, p4.x)));
+            const float yd =
+                fmaxf(p1.y, fmaxf(p2.y, fmaxf(p3.y, p4.y))) - fminf(p1.y, fminf(p2.y, fminf(p3.y, p4.y)));
+            size = fminf(fmaxf(fmaxf(0.0f, fminf(fabsf(xd), fabsf(yd))), 1.0f), kMaxPointSize);
+        }
+        // the pixels whose centres lie in [c - size/2, c + size/2)
+        const float h = 0.5f * size;
+        const int u0 = max(0, (int)ceilf(c.x - h - 0.5f)), u1 = min((int)a.width, (int)ceilf(c.x + h - 0.5f));
+        const int w0 = max(0, (int)ceilf(c.y - h - 0.5f)), w1 = min((int)a.height, (int)ceilf(c.y + h - 0.5f));
+        const unsigned long long key = ((unsigned long long)__float_as_uint(pc.z) << 32) | s;
+        for (int w = w0; w < w1; ++w)
+            for (int u = u0; u < u1; ++u) atomicMin(V.zbuf + (size_t)w * V.pitch + u, key);
+    }
 }
 
 __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ SplatArgs a) {
@@ -172,6 +186,7 @@ extern "C" int mvdr_render_solver_maps(const mvdr_surfel_geometry* g, const mvdr
     if (g->num_surfels == 0xFFFFFFFFu) return fail(MVDR_ECAPACITY, "mvdr_render_solver_maps: too many surfels");
     SplatArgs a;
     std::memset(&a, 0, sizeof(a));
+    a.num_views = num_views;
     a.num_surfels = g->num_surfels;
     a.width = prm->width;
     a.height = prm->height;
@@ -205,6 +220,7 @@ extern "C" int mvdr_render_solver_maps(const mvdr_surfel_geometry* g, const mvdr
         V.fx = in.intrinsic.focal_x;
         V.fy = in.intrinsic.focal_y;
         V.sized = in.sized_points ? 1 : 0;
+        a.any_sized |= (uint32_t)V.sized;
         V.ref_v = reinterpret_cast<float4*>(in.reference_vertex_map);
         V.ref_n = reinterpret_cast<float4*>(in.reference_normal_map);
         V.live_v = reinterpret_cast<float4*>(in.live_vertex_map);
@@ -221,7 +237,7 @@ extern "C" int mvdr_render_solver_maps(const mvdr_surfel_geometry* g, const mvdr
         if (e != cudaSuccess) return fail(MVDR_ECUDA, std::string("mvdr_render_solver_maps: ") + cudaGetErrorString(e));
     }
     if (g->num_surfels)
-        MVDR_LAUNCH(splat_kernel, dim3((g->num_surfels + 255) / 256, num_views), 256, 0, st, a);
+        MVDR_LAUNCH(splat_kernel, dim3((g->num_surfels + 255) / 256), 256, 0, st, a);
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
