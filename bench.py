@@ -61,11 +61,12 @@ def parse():
                    help="use this SpMV tile shape (index into abi.SPMV_SHAPES) instead of the autotuner's")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="torso", choices=["torso", "sphere", "uneven", "body", "solver_maps"],
+    p.add_argument("--workload", default="torso", choices=["torso", "sphere", "uneven", "body", "solver_maps", "deform"],
                    help="torso: the headline batch (default); sphere: the 1-view 2048-node plain-method "
                         "configuration; uneven: 16 instances with 1024-16384 nodes and 1-4 views; body: one "
                         "32768-node, 5-view 1280x720 solve; solver_maps: the renderer's solver maps of the "
-                        "body workload's surfels in its 5 views")
+                        "body workload's surfels in its 5 views; deform: the post-solve warp, node error and "
+                        "correction on the body workload")
     p.add_argument("--no-accuracy", action="store_true", help="skip the FP64 check of the timed configuration")
     p.add_argument("--no-e2e", action="store_true",
                    help="skip the end-to-end leg (for profiler captures only; the bench line then has no e2e)")
@@ -657,6 +658,83 @@ def run_solver_maps(args):
     return 0
 
 
+def run_deform(args):
+    """Times the post-solve path on the body workload (4.0M surfels, 32,768
+    nodes, 5 views of 1280x720): the forward warp of surfels and nodes, the
+    node alignment error with both error maps, and the large-error
+    correction, each with CUDA events over --steps calls; algorithmic bytes
+    per call from the sizes (stated beside each figure)."""
+    import torch
+    from multiviewdynrecon_b200 import abi, synth
+    from multiviewdynrecon_b200.deform import SurfelNodeDeformer
+    from multiviewdynrecon_b200.solver import NonRigidSolver
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    scene = synth.articulated_body(auto_radius=True, focal_scale=5.0)
+    g = synth.solver_map_geometry(scene, warped=False)
+    nk, nw = synth.node_skinning(scene)
+    nodes = synth.node_views(scene)
+    guides = synth.correction_guides(scene)
+    gen_s = time.perf_counter() - t0
+
+    def dev(a):
+        a = np.ascontiguousarray(a)
+        return torch.from_numpy(a.view(np.int16) if a.dtype == np.uint16 else a.copy()).cuda()
+
+    S, N, V, W, H = scene.num_surfels, scene.num_nodes, scene.num_views, scene.width, scene.height
+    field, knn, w = dev(scene.node_se3), dev(scene.surfel_knn), dev(scene.surfel_knn_weight)
+    cv, cn = dev(g["reference_vertex_confid"]), dev(g["reference_normal_radius"])
+    dnk, dnw, dnodes = dev(nk), dev(nw), dev(nodes)
+    solver = NonRigidSolver(abi.make_config(scene))
+    solver.set_solver_input(scene)
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = load_peaks()
+    out = {}
+
+    def timed(name, fn, nbytes):
+        ms = time_solves(fn, args.steps, max(3, args.warmup), stream)
+        out[name] = {"ms": round(ms, 4), "algorithmic_bytes": int(nbytes),
+                     "GBps": round(nbytes / 1e9 / (ms / 1e3), 1),
+                     "frac_of_measured_hbm": round(nbytes / 1e9 / (ms / 1e3) / peak, 4)}
+
+    res = {}
+
+    def fwd():
+        res["fwd"] = SurfelNodeDeformer.forward_warp_surfels_and_nodes(field, knn, w, cv, cn, dnk, dnw, dnodes)
+
+    # per surfel: knn 8 + weights 16 + vertex and normal in 32 + out 32; per node 8 + 16 + 16 + 16
+    timed("forward_warp", fwd, S * 88 + N * 56)
+    lv, ln, live = res["fwd"]
+    drawn = sum(int((v.index_map != 0xFFFFFFFF).sum()) for v in scene.views)
+
+    def node_err():
+        res["err"] = solver.compute_alignment_error_on_nodes(maps=True)
+
+    # per pixel: index 4 + two map writes 8; per rendered pixel: reference
+    # vertex and normal 32, skinning 24, the observed window (once) 32, mask 4,
+    # the node-map pass's index 4, skinning 24 and node sums 32
+    timed("node_error", node_err, V * W * H * 12 + drawn * (32 + 24 + 32 + 4 + 4 + 24 + 32))
+    united = res["err"]["united_error"]
+    dg = [tuple(dev(a) for a in gd) for gd in guides]
+    se3 = field.clone()
+    live_v, live_n, live_nodes = lv.clone(), ln.clone(), live.clone()
+
+    def correct():
+        solver.correct_large_error_node(dg, united, live_nodes, dnk, dnw, live_v, live_n, knn, w, node_se3=se3)
+
+    # per surfel: knn 8 + weights 16 + vertex and normal in 32 and out 32;
+    # per node: the same plus the field (32 in, 32 out) and the guide windows
+    large = int((united > 0.2).sum().item())
+    timed("correction", correct, S * 88 + N * (88 + 64) + large * 25 * (48 + 1 + 16))
+    torch.cuda.synchronize()
+    line = {"workload": "deform", "config": {"surfels": S, "nodes": N, "views": V, "image": [W, H],
+                                            "rendered_pixels": drawn, "large_error_nodes": large},
+            "peak": peak, "peak_kind": peak_kind, "generation_s": round(gen_s, 1), "stages": out}
+    solver.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_extra_workload(args):
     """The uneven batch and the large single solve: one JSON line each,
     documenting configurations beside the headline."""
@@ -841,6 +919,8 @@ def main():
 
     if args.workload == "solver_maps":
         return run_solver_maps(args) if rank == 0 else 0
+    if args.workload == "deform":
+        return run_deform(args) if rank == 0 else 0
     if args.workload != "torso":
         return run_extra_workload(args) if rank == 0 else 0
 

@@ -364,6 +364,117 @@ typedef struct mvdr_solver_map_view {
 MVDR_API int mvdr_render_solver_maps(const mvdr_surfel_geometry* surfels, const mvdr_solver_map_params* params,
                                      const mvdr_solver_map_view* views, uint32_t num_views, void* stream);
 
+/* ---- after the solve: moving the surfels and nodes, node errors, and the
+ * correction of badly aligned nodes ----------------------------------------
+ * The reference's SurfelNodeDeformer (core/Geometry/SurfelNodeDeformer.cu)
+ * moves the canonical surfels and nodes with the solved warp field and back;
+ * DenseDepthHandler (core/NonRigidSolver/DenseDepthAlignmentError.cu:97-370)
+ * measures how well each node's surface matches the depth observation; and
+ * NonRigidSolver::CorrectLargeErrorNode (NonRigidSolver.cu:93-227,377-425)
+ * pulls nodes with a large error towards guiding correspondences. */
+
+/* Surfels to move: forward (canonical -> live) or inverse (live -> canonical).
+ * A surfel whose KNN names a node at or past the node count gets NaN outputs
+ * (no out-of-range read). */
+typedef struct mvdr_deform_surfels {
+    uint32_t num_surfels;
+    const uint16_t* knn;            /* ushort4 per surfel */
+    const mvdr_float4* knn_weight;
+    const mvdr_float4* in_vertex;   /* xyz + confidence (w kept) */
+    const mvdr_float4* in_normal;   /* xyz + radius (w kept) */
+    mvdr_float4* out_vertex;
+    mvdr_float4* out_normal;
+} mvdr_deform_surfels;
+
+/* Nodes moved by the forward warp: live = blend(nodes' own KNN) applied to
+ * the canonical coordinate, its w (which encodes the node's view) kept. */
+typedef struct mvdr_deform_nodes {
+    uint32_t num_nodes;
+    const uint16_t* knn;            /* ushort4 per node: nodesKNN */
+    const mvdr_float4* knn_weight;
+    const mvdr_float4* canonical_nodes;
+    mvdr_float4* live_nodes;
+} mvdr_deform_nodes;
+
+/* SurfelNodeDeformer::ForwardWarpSurfelsAndNodes (SurfelNodeDeformer.cu:9-206):
+ * out = se3(blend) * in for every surfel and (when `nodes` is not NULL) every
+ * node. node_se3 holds num_node_se3 dual quaternions (device). */
+MVDR_API int mvdr_forward_warp(const mvdr_dual_quaternion* node_se3, uint32_t num_node_se3,
+                               const mvdr_deform_surfels* surfels, const mvdr_deform_nodes* nodes, void* stream);
+/* SurfelNodeDeformer::InverseWarpSurfels (SurfelNodeDeformer.cu:63-119,
+ * 229-318): out = se3(blend)^-1 * in, then, when correct_se3 (one mat34 per
+ * surfel, device) is not NULL, out = correct_se3^-1 * out. */
+MVDR_API int mvdr_inverse_warp(const mvdr_dual_quaternion* node_se3, uint32_t num_node_se3,
+                               const mvdr_mat34* correct_se3, const mvdr_deform_surfels* surfels, void* stream);
+
+/* Node alignment errors of the solver's bound inputs under its current warp
+ * field (NonRigidSolver::ComputeAlignmentErrorOnNodes ->
+ * DenseDepthHandler::ComputeNodewiseError). Per rendered pixel of every view
+ * the error is the smallest L1 distance between the warped reference vertex
+ * (camera frame) and the observed vertices of the 3x3 window at its
+ * projection, at most 0.1 m; without a compatible observed vertex (normal dot
+ * > 0.7) it is 0.03 x the filtered foreground mask when that is below 0.9,
+ * else 0.1. Errors above 1e-6 are added with the pixel's skinning weights to
+ * its four nodes. The sums are kept in 2^-32 fixed point, so they do not
+ * depend on the order of the additions. Outputs (device, N = bound nodes):
+ * the sums, united_error = (sum_err / (sum_w + 1e-4)) / 0.1 (1 for a node
+ * with no error), and large_error_mark = united_error > threshold (or no
+ * error); optional per-view maps: the per-pixel error
+ * (ComputeAlignmentErrorMapDirect) and the node errors interpolated back to
+ * the pixels (ComputeAlignmentErrorMapFromNode). Maps are width x height
+ * floats, rows `width` apart. */
+typedef struct mvdr_node_error {
+    float* accumulated_error;   /* [N] */
+    float* accumulated_weight;  /* [N] */
+    float* united_error;        /* [N] */
+    uint32_t* large_error_mark; /* [N] 1 = large */
+    float threshold;            /* the reference passes 0.2 */
+    float* alignment_error_map[MVDR_MAX_VIEWS];  /* optional */
+    float* node_error_map[MVDR_MAX_VIEWS];       /* optional */
+} mvdr_node_error;
+MVDR_API int mvdr_compute_node_error(mvdr_solver* solver, const mvdr_node_error* out, void* stream);
+
+/* Guides of one view for the correction: the correspondence SE3 map
+ * (previous frame -> current frame, camera frame), its validity (1 = valid)
+ * and the previous frame's vertex map, each width x height with rows `pitch`
+ * elements apart (0 = width). */
+typedef struct mvdr_correction_view {
+    const mvdr_mat34* se3_map;
+    const uint8_t* valid_map;
+    const mvdr_float4* previous_vertex_map;
+    uint32_t pitch;
+} mvdr_correction_view;
+
+/* NonRigidSolver::CorrectLargeErrorNode, correspondence form
+ * (NonRigidSolver.cu:93-139,154-227,377-425). For every node whose united
+ * error is above error_threshold, the node's live coordinate is projected into
+ * the view its w names (i < w <= i + 1); within the 5x5 window there, the
+ * valid guide whose previous vertex is nearest (squared distance below 1e-4)
+ * and that moves the node by less than 2 node radii gives the node's
+ * correction, brought to frame 0 and scaled by the error
+ * (DualQuaternion::operator*(float)). Other nodes get the identity. The
+ * corrections are then blended at every surfel and node: live surfels and
+ * live nodes are moved, and each node's SE3 becomes blend * SE3. The
+ * corrected warp field is written to node_se3 and becomes the solver's
+ * current warp field. Cameras come from the solver's bound inputs. */
+typedef struct mvdr_correction {
+    uint32_t width, height;                         /* of the guide maps */
+    mvdr_correction_view views[MVDR_MAX_VIEWS];     /* the bound views' guides */
+    const float* united_error;                      /* [N], from mvdr_compute_node_error */
+    float error_threshold;                          /* the reference uses 0.2 */
+    mvdr_dual_quaternion* node_se3;                 /* [N] in/out; NULL: the solver's current field */
+    mvdr_float4* live_nodes;                        /* [N] in/out */
+    const uint16_t* node_knn;                       /* ushort4 [N] */
+    const mvdr_float4* node_knn_weight;             /* [N] */
+    uint32_t num_surfels;
+    mvdr_float4* live_vertex;                       /* [S] in/out */
+    mvdr_float4* live_normal;                       /* [S] in/out */
+    const uint16_t* surfel_knn;                     /* ushort4 [S] */
+    const mvdr_float4* surfel_knn_weight;           /* [S] */
+    mvdr_dual_quaternion* correction;               /* [N] out: each node's correction */
+} mvdr_correction;
+MVDR_API int mvdr_correct_large_error_nodes(mvdr_solver* solver, const mvdr_correction* c, void* stream);
+
 /* ---- input bundles (replay of one solve's inputs) -----------------------
  * mvdr_save_input_bundle writes the configuration and every input array
  * bound to the solver (device or owned copies) to a file; it synchronises

@@ -73,6 +73,10 @@ def _declare(L):
         "mvdr_batch_enqueue_stage": (i32, [vp, i32, vp]),
         "mvdr_render_solver_maps": (i32, [P(abi.SurfelGeometry), P(abi.SolverMapParams), P(abi.SolverMapView), u32,
                                           vp]),
+        "mvdr_forward_warp": (i32, [vp, u32, P(abi.DeformSurfels), P(abi.DeformNodes), vp]),
+        "mvdr_inverse_warp": (i32, [vp, u32, vp, P(abi.DeformSurfels), vp]),
+        "mvdr_compute_node_error": (i32, [vp, P(abi.NodeError), vp]),
+        "mvdr_correct_large_error_nodes": (i32, [vp, P(abi.Correction), vp]),
         "mvdr_last_error_string": (C.c_char_p, []),
         "mvdr_kernel_launch_count": (C.c_uint64, []),
         "mvdr_abi_layout": (i32, [C.c_char_p, P(C.c_size_t)]),

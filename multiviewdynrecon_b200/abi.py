@@ -131,11 +131,43 @@ class SolverMapView(C.Structure):
                 ("depth_index", C.c_void_p)]
 
 
+class DeformSurfels(C.Structure):
+    _fields_ = [("num_surfels", C.c_uint32), ("knn", C.c_void_p), ("knn_weight", C.c_void_p),
+                ("in_vertex", C.c_void_p), ("in_normal", C.c_void_p), ("out_vertex", C.c_void_p),
+                ("out_normal", C.c_void_p)]
+
+
+class DeformNodes(C.Structure):
+    _fields_ = [("num_nodes", C.c_uint32), ("knn", C.c_void_p), ("knn_weight", C.c_void_p),
+                ("canonical_nodes", C.c_void_p), ("live_nodes", C.c_void_p)]
+
+
+class NodeError(C.Structure):
+    _fields_ = [("accumulated_error", C.c_void_p), ("accumulated_weight", C.c_void_p),
+                ("united_error", C.c_void_p), ("large_error_mark", C.c_void_p), ("threshold", C.c_float),
+                ("alignment_error_map", C.c_void_p * MVDR_MAX_VIEWS), ("node_error_map", C.c_void_p * MVDR_MAX_VIEWS)]
+
+
+class CorrectionView(C.Structure):
+    _fields_ = [("se3_map", C.c_void_p), ("valid_map", C.c_void_p), ("previous_vertex_map", C.c_void_p),
+                ("pitch", C.c_uint32)]
+
+
+class Correction(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("views", CorrectionView * MVDR_MAX_VIEWS),
+                ("united_error", C.c_void_p), ("error_threshold", C.c_float), ("node_se3", C.c_void_p),
+                ("live_nodes", C.c_void_p), ("node_knn", C.c_void_p), ("node_knn_weight", C.c_void_p),
+                ("num_surfels", C.c_uint32), ("live_vertex", C.c_void_p), ("live_normal", C.c_void_p),
+                ("surfel_knn", C.c_void_p), ("surfel_knn_weight", C.c_void_p), ("correction", C.c_void_p)]
+
+
 STRUCTS = {"mvdr_float4": Float4, "mvdr_dual_quaternion": DualQuaternion, "mvdr_mat34": Mat34,
            "mvdr_intrinsic": Intrinsic, "mvdr_penalty": Penalty, "mvdr_config": Config,
            "mvdr_view_inputs": ViewInputs, "mvdr_correspondences": Correspondences, "mvdr_inputs": Inputs,
            "mvdr_counts": Counts, "mvdr_view_textures": ViewTextures, "mvdr_surfel_geometry": SurfelGeometry,
-           "mvdr_solver_map_params": SolverMapParams, "mvdr_solver_map_view": SolverMapView}
+           "mvdr_solver_map_params": SolverMapParams, "mvdr_solver_map_view": SolverMapView,
+           "mvdr_deform_surfels": DeformSurfels, "mvdr_deform_nodes": DeformNodes, "mvdr_node_error": NodeError,
+           "mvdr_correction_view": CorrectionView, "mvdr_correction": Correction}
 
 
 def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=480, precision=PRECISION_MIXED,

@@ -323,6 +323,7 @@ struct InstDesc {
     uint32_t part_stride;   // >= the CTAs per instance of any launch
     uint32_t* pcg_bar;      // persistent PCG: this instance's barrier counter (batch-owned)
     double* energy;         // [max GN iterations + 1]
+    unsigned long long* node_err_acc;  // [2N] node alignment error and weight sums, 2^-32 fixed point
 
     // capacities
     uint32_t cap_dense, cap_fg, cap_k1, cap_k2, cap_pairs, cap_seg, cap_bb;

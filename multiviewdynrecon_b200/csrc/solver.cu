@@ -179,6 +179,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.partials = a.take<double>(5 * (size_t)partial_slots);
     I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
+    I.node_err_acc = a.take<unsigned long long>(2 * N);
     I.cap_dense = lc.cap_dense;
     I.cap_fg = lc.cap_fg;
     I.cap_k1 = lc.cap_k1;
@@ -1031,7 +1032,9 @@ int mvdr_abi_layout(const char* name, size_t* size) {
         {"mvdr_inputs", sizeof(mvdr_inputs)}, {"mvdr_counts", sizeof(mvdr_counts)},
         {"mvdr_view_textures", sizeof(mvdr_view_textures)}, {"mvdr_surfel_geometry", sizeof(mvdr_surfel_geometry)},
         {"mvdr_solver_map_params", sizeof(mvdr_solver_map_params)},
-        {"mvdr_solver_map_view", sizeof(mvdr_solver_map_view)}};
+        {"mvdr_solver_map_view", sizeof(mvdr_solver_map_view)}, {"mvdr_deform_surfels", sizeof(mvdr_deform_surfels)},
+        {"mvdr_deform_nodes", sizeof(mvdr_deform_nodes)}, {"mvdr_node_error", sizeof(mvdr_node_error)},
+        {"mvdr_correction_view", sizeof(mvdr_correction_view)}, {"mvdr_correction", sizeof(mvdr_correction)}};
     for (const auto& t : table)
         if (std::strcmp(t.n, name) == 0) { *size = t.s; return MVDR_OK; }
     return MVDR_EINVAL;

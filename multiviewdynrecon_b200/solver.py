@@ -178,6 +178,58 @@ class NonRigidSolver:
     def save_input_bundle(self, path, stream=None):
         check(lib().mvdr_save_input_bundle(self.h, str(path).encode(), _stream_handle(stream)))
 
+    # NonRigidSolver::ComputeAlignmentErrorOnNodes (+ the error maps)
+    def compute_alignment_error_on_nodes(self, threshold=0.2, maps=False, stream=None):
+        """Node alignment errors of the bound inputs under the current warp
+        field: a dict of device tensors (accumulated_error, accumulated_weight,
+        united_error, large_error_mark; with `maps`, per-view
+        alignment_error_map and node_error_map of (H, W))."""
+        N = self.num_nodes
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = {k: torch.empty(N, dtype=torch.float32, device=dev)
+               for k in ("accumulated_error", "accumulated_weight", "united_error")}
+        out["large_error_mark"] = torch.empty(N, dtype=torch.int32, device=dev)
+        ne = abi.NodeError()
+        ne.accumulated_error = out["accumulated_error"].data_ptr()
+        ne.accumulated_weight = out["accumulated_weight"].data_ptr()
+        ne.united_error = out["united_error"].data_ptr()
+        ne.large_error_mark = out["large_error_mark"].data_ptr()
+        ne.threshold = threshold
+        if maps:
+            V, H, W = self._inputs.inputs.num_views, self.config.image_height, self.config.image_width
+            out["alignment_error_map"] = torch.empty((V, H, W), dtype=torch.float32, device=dev)
+            out["node_error_map"] = torch.empty((V, H, W), dtype=torch.float32, device=dev)
+            for v in range(V):
+                ne.alignment_error_map[v] = out["alignment_error_map"][v].data_ptr()
+                ne.node_error_map[v] = out["node_error_map"][v].data_ptr()
+        check(lib().mvdr_compute_node_error(self.h, C.byref(ne), _stream_handle(stream)))
+        return out
+
+    # NonRigidSolver::CorrectLargeErrorNode (correspondence form)
+    def correct_large_error_node(self, guides, united_error, live_nodes, node_knn, node_weight, live_vertex,
+                                 live_normal, surfel_knn, surfel_weight, threshold=0.2, node_se3=None, stream=None):
+        """`guides`: per bound view (se3 map (H, W, 12), valid (H, W) uint8,
+        previous vertex map (H, W, 4)) device tensors. live_* are corrected in
+        place, node_se3 too (None: the solver's own warp field); the
+        corrected field becomes the solver's current one. Returns the
+        per-node corrections (N, 8)."""
+        corr = torch.empty((self.num_nodes, 8), dtype=torch.float32, device=live_nodes.device)
+        c = abi.Correction()
+        H, W = guides[0][1].shape
+        c.width, c.height = W, H
+        for v, (se3, valid, prev) in enumerate(guides):
+            c.views[v].se3_map, c.views[v].valid_map = se3.data_ptr(), valid.data_ptr()
+            c.views[v].previous_vertex_map, c.views[v].pitch = prev.data_ptr(), 0
+        c.united_error, c.error_threshold = united_error.data_ptr(), threshold
+        c.node_se3 = None if node_se3 is None else node_se3.data_ptr()
+        c.live_nodes, c.node_knn, c.node_knn_weight = live_nodes.data_ptr(), node_knn.data_ptr(), node_weight.data_ptr()
+        c.num_surfels = live_vertex.shape[0]
+        c.live_vertex, c.live_normal = live_vertex.data_ptr(), live_normal.data_ptr()
+        c.surfel_knn, c.surfel_knn_weight = surfel_knn.data_ptr(), surfel_weight.data_ptr()
+        c.correction = corr.data_ptr()
+        check(lib().mvdr_correct_large_error_nodes(self.h, C.byref(c), _stream_handle(stream)))
+        return corr
+
     def apply_jtj(self, x, stream=None):
         x = x.contiguous().float()
         y = torch.empty_like(x)

@@ -625,6 +625,55 @@ def solver_map_geometry(scene, seed=0, current_time=10.0, warped=True):
 
 
 # --------------------------------------------------------------------------
+# inputs of the post-solve deformation and correction
+# --------------------------------------------------------------------------
+
+def node_skinning(scene):
+    """Each node's 4 nearest nodes (itself first) and their weights, as the
+    warp field's nodesKNN / nodesKNNWeight."""
+    p = np.asarray(scene.canonical_nodes, np.float64)[:, :3]
+    d, i = cKDTree(p).query(p, k=4)
+    return i.astype(np.uint16), _knn_weights(d * d, scene.node_radius)
+
+
+def node_views(scene):
+    """Canonical nodes with w encoding the view that sees each one best
+    (i + 1 for view i, decoded as i < w <= i + 1): the view in whose camera
+    the node is nearest."""
+    nodes = np.asarray(scene.canonical_nodes, np.float32).copy()
+    best = np.full(len(nodes), np.inf)
+    for v, view in enumerate(scene.views):
+        m = np.asarray(view.initial_camera_se3, np.float64)
+        z = ((nodes[:, :3] - m[9:12]) @ m[:9].reshape(3, 3).T)[:, 2]
+        z = np.where(z > 0, z, np.inf)
+        better = z < best
+        nodes[better, 3] = v + 1
+        best[better] = z[better]
+    return nodes
+
+
+def correction_guides(scene, seed=0, valid_fraction=0.5, step_mm=4.0):
+    """Per view: a correspondence SE3 map (previous -> current frame, camera
+    frame; a small rotation and a translation of a few millimetres, varying
+    per pixel), its validity (valid_fraction of the observed pixels) and the
+    previous frame's vertex map (the observation)."""
+    rng = np.random.default_rng([seed, 3571])
+    H, W = scene.height, scene.width
+    out = []
+    for view in scene.views:
+        prev = np.ascontiguousarray(view.vertex_confidence_map, np.float32)
+        observed = np.abs(prev[..., 2]) > 0
+        valid = (observed & (rng.random((H, W)) < valid_fraction)).astype(np.uint8)
+        se3 = np.zeros((H, W, 12), np.float32)
+        w = rng.normal(0, np.radians(0.5), (H * W, 3))
+        R = rodrigues_batch(w).reshape(H, W, 3, 3)
+        se3[..., :9] = np.transpose(R, (0, 1, 3, 2)).reshape(H, W, 9)  # rotation columns
+        se3[..., 9:] = rng.normal(0, step_mm * 1e-3, (H, W, 3))
+        out.append((se3, valid, prev))
+    return out
+
+
+# --------------------------------------------------------------------------
 # the workloads
 # --------------------------------------------------------------------------
 

@@ -102,6 +102,11 @@ def lib():
         L.orc_p2p_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_render_solver_maps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        L.orc_forward_warp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32] + [C.c_void_p] * 6 + \
+            [C.c_uint32] + [C.c_void_p] * 4
+        L.orc_inverse_warp.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32] + [C.c_void_p] * 6
+        L.orc_node_error.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_float] + [C.c_void_p] * 6
+        L.orc_correct_large_error_nodes.argtypes = [C.c_void_p, C.c_float, C.c_void_p]
         _lib = L
     return _lib
 
@@ -294,3 +299,106 @@ def render_solver_maps(geometry, params, views, sized=None):
                                      sized_points=bool(sized[v]) if sized is not None else False)
     lib().orc_render_solver_maps(C.byref(g), C.byref(params), mv, len(views))
     return out
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, np.float32)
+    return a if shape is None else a.reshape(shape)
+
+
+def forward_warp(field, knn, weight, vertex, normal, node_knn=None, node_weight=None, nodes=None):
+    """SurfelNodeDeformer::ForwardWarpSurfelsAndNodes on host arrays: returns
+    live vertices, live normals and (with nodes) live nodes."""
+    field = _f32(field, (-1, 8))
+    knn = np.ascontiguousarray(knn, np.uint16)
+    w, v, n = _f32(weight), _f32(vertex), _f32(normal)
+    S = len(knn)
+    ov, on = np.zeros((S, 4), np.float32), np.zeros((S, 4), np.float32)
+    N = 0 if nodes is None else len(nodes)
+    nk = np.ascontiguousarray(node_knn if N else np.zeros((0, 4)), np.uint16)
+    nw, nd = _f32(node_weight if N else np.zeros((0, 4))), _f32(nodes if N else np.zeros((0, 4)))
+    live = np.zeros((N, 4), np.float32)
+    lib().orc_forward_warp(_p(field), len(field), S, _p(knn), _p(w), _p(v), _p(n), _p(ov), _p(on), N, _p(nk),
+                           _p(nw), _p(nd), _p(live))
+    return ov, on, live
+
+
+def inverse_warp(field, knn, weight, vertex, normal, correct=None):
+    """SurfelNodeDeformer::InverseWarpSurfels on host arrays; `correct` is
+    (S, 12) mat34 (rotation columns, translation) or None."""
+    field = _f32(field, (-1, 8))
+    knn = np.ascontiguousarray(knn, np.uint16)
+    w, v, n = _f32(weight), _f32(vertex), _f32(normal)
+    S = len(knn)
+    ov, on = np.zeros((S, 4), np.float32), np.zeros((S, 4), np.float32)
+    cs = None if correct is None else _f32(correct, (-1, 12))
+    lib().orc_inverse_warp(_p(field), len(field), None if cs is None else _p(cs), S, _p(knn), _p(w), _p(v), _p(n),
+                           _p(ov), _p(on))
+    return ov, on
+
+
+def node_error(scene, field, threshold=0.2, maps=False):
+    """DenseDepthHandler::ComputeNodewiseError (+ the two error maps) on the
+    scene's maps with the warp field `field` (N, 8)."""
+    keep = []
+
+    def ptr(name, arr):
+        a = np.ascontiguousarray(arr)
+        keep.append(a)
+        return a.ctypes.data
+
+    inp = abi.fill_inputs(scene, ptr)
+    field = _f32(field, (-1, 8))
+    N, V, W, H = scene.num_nodes, scene.num_views, scene.width, scene.height
+    out = {k: np.zeros(N, np.float32) for k in ("accumulated_error", "accumulated_weight", "united_error")}
+    out["large_error_mark"] = np.zeros(N, np.uint32)
+    am = [np.zeros((H, W), np.float32) for _ in range(V)] if maps else []
+    nm = [np.zeros((H, W), np.float32) for _ in range(V)] if maps else []
+    amp = (C.c_void_p * V)(*[a.ctypes.data for a in am]) if maps else None
+    nmp = (C.c_void_p * V)(*[a.ctypes.data for a in nm]) if maps else None
+    lib().orc_node_error(C.byref(inp), W, H, _p(field), threshold, _p(out["accumulated_error"]),
+                         _p(out["accumulated_weight"]), _p(out["united_error"]), _p(out["large_error_mark"]),
+                         C.cast(amp, C.c_void_p) if maps else None, C.cast(nmp, C.c_void_p) if maps else None)
+    if maps:
+        out["alignment_error_map"], out["node_error_map"] = am, nm
+    return out
+
+
+def correct_large_error_nodes(scene, guides, united_error, node_se3, live_nodes, node_knn, node_weight, live_vertex,
+                              live_normal, surfel_knn, surfel_weight, threshold=0.2, node_radius=None):
+    """NonRigidSolver::CorrectLargeErrorNode (correspondence form) on host
+    arrays; `guides` per view (se3 map (H, W, 12), valid (H, W) uint8,
+    previous vertex map (H, W, 4)). Returns the corrected arrays and the
+    per-node corrections."""
+    keep = []
+
+    def ptr(name, arr):
+        a = np.ascontiguousarray(arr)
+        keep.append(a)
+        return a.ctypes.data
+
+    inp = abi.fill_inputs(scene, ptr)
+    res = {"node_se3": _f32(node_se3, (-1, 8)).copy(), "live_nodes": _f32(live_nodes).copy(),
+           "live_vertex": _f32(live_vertex).copy(), "live_normal": _f32(live_normal).copy(),
+           "correction": np.zeros((scene.num_nodes, 8), np.float32)}
+    c = abi.Correction()
+    c.width, c.height = scene.width, scene.height
+    for v, (se3, valid, prev) in enumerate(guides):
+        arrs = (_f32(se3), np.ascontiguousarray(valid, np.uint8), _f32(prev))
+        keep.extend(arrs)
+        c.views[v].se3_map, c.views[v].valid_map, c.views[v].previous_vertex_map = [a.ctypes.data for a in arrs]
+        c.views[v].pitch = 0
+    ue = _f32(united_error)
+    nk, nw = np.ascontiguousarray(node_knn, np.uint16), _f32(node_weight)
+    sk, sw = np.ascontiguousarray(surfel_knn, np.uint16), _f32(surfel_weight)
+    keep.extend([ue, nk, nw, sk, sw])
+    c.united_error, c.error_threshold = ue.ctypes.data, threshold
+    c.node_se3, c.live_nodes = res["node_se3"].ctypes.data, res["live_nodes"].ctypes.data
+    c.node_knn, c.node_knn_weight = nk.ctypes.data, nw.ctypes.data
+    c.num_surfels = len(sk)
+    c.live_vertex, c.live_normal = res["live_vertex"].ctypes.data, res["live_normal"].ctypes.data
+    c.surfel_knn, c.surfel_knn_weight = sk.ctypes.data, sw.ctypes.data
+    c.correction = res["correction"].ctypes.data
+    lib().orc_correct_large_error_nodes(C.byref(inp), scene.node_radius if node_radius is None else node_radius,
+                                        C.byref(c))
+    return res

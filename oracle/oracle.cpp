@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -1391,6 +1392,362 @@ void orc_apply_twist(const double* dq8, const double* tw6, double* out8) {
     std::memcpy(out8, a, 64);
 }
 void orc_gauss_jordan_inverse(const double* A36, double* out36) { Oracle::inverse_gauss_jordan(A36, out36); }
+
+/* ---- after the solve (the oracle's restatement of csrc/deform.cu) ------- */
+
+// __float2int_rn / __float2uint_rn: round to nearest even, NaN -> 0,
+// saturating at the type's range
+static int f2i_rn_sat(float v) {
+    if (v != v) return 0;
+    if (v >= 2147483648.0f) return 2147483647;
+    if (v < -2147483648.0f) return (-2147483647 - 1);
+    return (int)std::nearbyint(v);
+}
+static uint32_t f2u_rn_sat(float v) {
+    if (v != v) return 0;
+    if (v >= 4294967296.0f) return 0xFFFFFFFFu;
+    const float r = std::nearbyint(v);
+    return r <= 0.0f ? 0u : (uint32_t)r;
+}
+
+static M34<float> normalized_se3(DQ<float> d, DQ<float>* normalized_out = nullptr) {
+    const float inv = 1.0f / std::sqrt(qdot(d.q0, d.q0));
+    d.q0 = qscale(inv, d.q0);
+    d.q1 = qscale(inv, d.q1);
+    const float dd = qdot(d.q0, d.q1);
+    d.q1 = {d.q1.x - dd * d.q0.x, d.q1.y - dd * d.q0.y, d.q1.z - dd * d.q0.z, d.q1.w - dd * d.q0.w};
+    if (normalized_out) *normalized_out = d;
+    const Q<float> q = d.q0;
+    M34<float> m;  // Quaternion::rotation_matrix(false), Quaternion.h:207-220
+    m.m[0][0] = 1 - 2 * q.y * q.y - 2 * q.z * q.z;
+    m.m[0][1] = 2 * q.x * q.y - 2 * q.z * q.w;
+    m.m[0][2] = 2 * q.x * q.z + 2 * q.y * q.w;
+    m.m[1][0] = 2 * q.x * q.y + 2 * q.z * q.w;
+    m.m[1][1] = 1 - 2 * q.x * q.x - 2 * q.z * q.z;
+    m.m[1][2] = 2 * q.y * q.z - 2 * q.x * q.w;
+    m.m[2][0] = 2 * q.x * q.z - 2 * q.y * q.w;
+    m.m[2][1] = 2 * q.y * q.z + 2 * q.x * q.w;
+    m.m[2][2] = 1 - 2 * q.x * q.x - 2 * q.y * q.y;
+    const Q<float> tp = qmul(qscale(2.0f, d.q1), qconj(d.q0));
+    m.t[0] = tp.x;
+    m.t[1] = tp.y;
+    m.t[2] = tp.z;
+    return m;
+}
+
+static DQ<float> blend_f(const mvdr_dual_quaternion* field, const uint16_t* knn, const mvdr_float4& w) {
+    const float ws[4] = {w.x, w.y, w.z, w.w};
+    DQ<float> a;
+    for (int k = 0; k < 4; ++k) {
+        const DQ<float> d = load_dq<float>(field[knn[k]]);
+        const float s = ws[k];
+        if (k == 0) {
+            a.q0 = qscale(s, d.q0);
+            a.q1 = qscale(s, d.q1);
+        } else {
+            a.q0 = {a.q0.x + s * d.q0.x, a.q0.y + s * d.q0.y, a.q0.z + s * d.q0.z, a.q0.w + s * d.q0.w};
+            a.q1 = {a.q1.x + s * d.q1.x, a.q1.y + s * d.q1.y, a.q1.z + s * d.q1.z, a.q1.w + s * d.q1.w};
+        }
+    }
+    return a;
+}
+
+static bool knn_in(const uint16_t* k, uint32_t n) { return k[0] < n && k[1] < n && k[2] < n && k[3] < n; }
+
+static M34<float> mul34f(const M34<float>& a, const M34<float>& b) {  // mat34::operator*
+    M34<float> o;
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) o.m[r][c] = a.m[r][0] * b.m[0][c] + a.m[r][1] * b.m[1][c] + a.m[r][2] * b.m[2][c];
+        o.t[r] = (a.m[r][0] * b.t[0] + a.m[r][1] * b.t[1] + a.m[r][2] * b.t[2]) + a.t[r];
+    }
+    return o;
+}
+
+/* SurfelNodeDeformer::ForwardWarpSurfelsAndNodes (SurfelNodeDeformer.cu:9-57):
+ * HOST arrays. */
+void orc_forward_warp(const mvdr_dual_quaternion* field, uint32_t num_field, uint32_t S, const uint16_t* knn,
+                      const mvdr_float4* w, const mvdr_float4* in_v, const mvdr_float4* in_n, mvdr_float4* out_v,
+                      mvdr_float4* out_n, uint32_t N, const uint16_t* node_knn, const mvdr_float4* node_w,
+                      const mvdr_float4* nodes, mvdr_float4* live_nodes) {
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    for (uint32_t i = 0; i < S + N; ++i) {
+        const bool surfel = i < S;
+        const uint32_t k = surfel ? i : i - S;
+        const uint16_t* kk = surfel ? knn + 4 * (size_t)k : node_knn + 4 * (size_t)k;
+        const mvdr_float4 ww = surfel ? w[k] : node_w[k];
+        const mvdr_float4 v = surfel ? in_v[k] : nodes[k];
+        const mvdr_float4 n = surfel ? in_n[k] : mvdr_float4{0, 0, 0, 0};
+        mvdr_float4 ov{nan, nan, nan, v.w}, on{nan, nan, nan, n.w};
+        if (knn_in(kk, num_field)) {
+            const M34<float> se3 = normalized_se3(blend_f(field, kk, ww));
+            const V3<float> p = se3.apply({v.x, v.y, v.z}), q = se3.rot({n.x, n.y, n.z});
+            ov = {p.x, p.y, p.z, v.w};
+            on = {q.x, q.y, q.z, n.w};
+        }
+        if (surfel) {
+            out_v[k] = ov;
+            out_n[k] = on;
+        } else {
+            live_nodes[k] = ov;
+        }
+    }
+}
+
+/* SurfelNodeDeformer::InverseWarpSurfels (SurfelNodeDeformer.cu:63-119):
+ * HOST arrays; correct may be NULL. */
+void orc_inverse_warp(const mvdr_dual_quaternion* field, uint32_t num_field, const mvdr_mat34* correct, uint32_t S,
+                      const uint16_t* knn, const mvdr_float4* w, const mvdr_float4* in_v, const mvdr_float4* in_n,
+                      mvdr_float4* out_v, mvdr_float4* out_n) {
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    for (uint32_t i = 0; i < S; ++i) {
+        const mvdr_float4 v = in_v[i], n = in_n[i];
+        V3<float> p{nan, nan, nan}, q = p;
+        if (knn_in(knn + 4 * (size_t)i, num_field)) {
+            const M34<float> se3 = normalized_se3(blend_f(field, knn + 4 * (size_t)i, w[i]));
+            p = se3.rotT({v.x - se3.t[0], v.y - se3.t[1], v.z - se3.t[2]});
+            q = se3.rotT({n.x, n.y, n.z});
+            if (correct) {
+                const M34<float> ci = inverse34(load_mat34<float>(correct[i]));
+                p = ci.apply(p);
+                q = ci.rot(q);
+            }
+        }
+        out_v[i] = {p.x, p.y, p.z, v.w};
+        out_n[i] = {q.x, q.y, q.z, n.w};
+    }
+}
+
+static bool zero_vertex_f(const mvdr_float4& v) {
+    return (double)std::fabs(v.x) < 1e-3 && (double)std::fabs(v.y) < 1e-3 && (double)std::fabs(v.z) < 1e-3;
+}
+
+static uint64_t to_fixed_f(float v) {
+    float s = v * 4294967296.0f;
+    if (s != s) s = 0.0f;
+    s = std::fmin(std::fmax(s, -4.611686e18f), 4.611686e18f);
+    return (uint64_t)(int64_t)std::llrint(s);
+}
+
+/* DenseDepthHandler::ComputeNodewiseError, ComputeAlignmentErrorMapDirect and
+ * ComputeAlignmentErrorMapFromNode (DenseDepthAlignmentError.cu:16-238) on
+ * HOST inputs: `in` with host map pointers (rows `pitch` or W apart), the
+ * warp field `field` (in->num_nodes dual quaternions). Node sums in 2^-32
+ * fixed point. Maps (optional, W x H) per view. */
+void orc_node_error(const mvdr_inputs* in, uint32_t W, uint32_t H, const mvdr_dual_quaternion* field, float threshold,
+                    float* acc_error, float* acc_weight, float* united, uint32_t* mark, float* const* align_maps,
+                    float* const* node_maps) {
+    const uint32_t N = in->num_nodes, S = in->num_surfels;
+    std::vector<uint64_t> acc(2 * (size_t)N, 0);
+    const uint16_t* sk = in->surfel_knn;
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        const mvdr_view_inputs& vi = in->views[v];
+        const uint32_t pitch = vi.pitch ? vi.pitch : W;
+        const M34<float> w2c = load_mat34<float>(vi.world2camera), init = load_mat34<float>(vi.initial_camera_se3);
+        const M34<float> iinv = inverse34(init);
+        for (uint32_t y = 0; y < H; ++y)
+            for (uint32_t x = 0; x < W; ++x) {
+                const size_t o = (size_t)y * pitch + x;
+                float err = 0.0f;
+                const uint32_t s = vi.index_map[o];
+                const uint16_t* kk = nullptr;
+                mvdr_float4 ww{0, 0, 0, 0};
+                if (s != MVDR_INVALID_INDEX && s < S && knn_in(sk + 4 * (size_t)s, N)) {
+                    kk = sk + 4 * (size_t)s;
+                    ww = in->surfel_knn_weight[s];
+                    const mvdr_float4 rv = vi.reference_vertex_map[o], rn = vi.reference_normal_map[o];
+                    const V3<float> cv = init.apply({rv.x, rv.y, rv.z}), cn = init.rot({rn.x, rn.y, rn.z});
+                    const M34<float> se3 = normalized_se3(blend_f(field, kk, ww));
+                    const V3<float> wv = se3.apply(cv), wn = se3.rot(cn);
+                    const V3<float> c1 = iinv.apply(w2c.apply(wv)), n1 = iinv.rot(w2c.rot(wn));
+                    const mvdr_intrinsic& K = vi.intrinsic;
+                    int ix = f2i_rn_sat((float)(((double)c1.x / ((double)c1.z + 1e-10)) * (double)K.focal_x +
+                                                (double)K.principal_x));
+                    int iy = f2i_rn_sat((float)(((double)c1.y / ((double)c1.z + 1e-10)) * (double)K.focal_y +
+                                                (double)K.principal_y));
+                    ix = std::min(std::max(ix, -2), (int)W + 1);
+                    iy = std::min(std::max(iy, -2), (int)H + 1);
+                    err = 0.1f;
+                    bool found = false;
+                    for (int dy = iy - 1; dy <= iy + 1; ++dy)
+                        for (int dx = ix - 1; dx <= ix + 1; ++dx) {
+                            mvdr_float4 dv{0, 0, 0, 0}, dn{0, 0, 0, 0};
+                            if (dx >= 0 && dy >= 0 && dx < (int)W && dy < (int)H) {
+                                dv = vi.vertex_confidence_map[(size_t)dy * pitch + dx];
+                                dn = vi.normal_radius_map[(size_t)dy * pitch + dx];
+                            }
+                            if (!zero_vertex_f(dv) && (n1.x * dn.x + n1.y * dn.y + n1.z * dn.z) > 0.7f) found = true;
+                            const float e = std::fabs(c1.x - dv.x) + std::fabs(c1.y - dv.y) + std::fabs(c1.z - dv.z);
+                            if (e < err) err = e;
+                        }
+                    if (!found) {
+                        float fg = 0.0f;
+                        if (ix >= 0 && iy >= 0 && ix < (int)W && iy < (int)H)
+                            fg = vi.filtered_foreground_mask[(size_t)iy * pitch + ix];
+                        err = fg < 0.9f ? 0.03f * fg : 0.1f;
+                    }
+                }
+                if (align_maps && align_maps[v]) align_maps[v][(size_t)y * W + x] = err;
+                if (err > 1e-6f) {
+                    const float wk[4] = {ww.x, ww.y, ww.z, ww.w};
+                    for (int k = 0; k < 4; ++k) {
+                        acc[kk[k]] += to_fixed_f(wk[k] * err);
+                        acc[N + kk[k]] += to_fixed_f(wk[k]);
+                    }
+                }
+            }
+    }
+    for (uint32_t n = 0; n < N; ++n) {
+        const float e = (float)((double)(int64_t)acc[n] * (1.0 / 4294967296.0));
+        const float w = (float)((double)(int64_t)acc[N + n] * (1.0 / 4294967296.0));
+        float u = (e / (w + 1e-4f)) / 0.1f;
+        uint32_t m = u > threshold ? 1u : 0u;
+        if (e < 1e-10f) {
+            m = 1u;
+            u = 1.0f;
+        }
+        acc_error[n] = e;
+        acc_weight[n] = w;
+        united[n] = u;
+        mark[n] = m;
+    }
+    if (!node_maps) return;
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        if (!node_maps[v]) continue;
+        const mvdr_view_inputs& vi = in->views[v];
+        const uint32_t pitch = vi.pitch ? vi.pitch : W;
+        for (uint32_t y = 0; y < H; ++y)
+            for (uint32_t x = 0; x < W; ++x) {
+                const uint32_t s = vi.index_map[(size_t)y * pitch + x];
+                float f = 0.0f;
+                if (s != MVDR_INVALID_INDEX && s < S && knn_in(sk + 4 * (size_t)s, N)) {
+                    const uint16_t* kk = sk + 4 * (size_t)s;
+                    const mvdr_float4 ww = in->surfel_knn_weight[s];
+                    const float wk[4] = {ww.x, ww.y, ww.z, ww.w};
+                    float ae = 0.0f, aw = 0.0f;
+                    for (int k = 0; k < 4; ++k) {
+                        const float unit = acc_error[kk[k]] / acc_weight[kk[k]];
+                        ae += unit * wk[k];
+                        aw += wk[k];
+                    }
+                    f = ae / (aw + 1e-4f);
+                }
+                node_maps[v][(size_t)y * W + x] = f;
+            }
+    }
+}
+
+/* NonRigidSolver::CorrectLargeErrorNode, correspondence form
+ * (NonRigidSolver.cu:93-227): cameras from `in` (host), every array of `c`
+ * HOST memory; c->node_se3 must be given (corrected in place). */
+void orc_correct_large_error_nodes(const mvdr_inputs* in, float node_radius, const mvdr_correction* c) {
+    const uint32_t N = in->num_nodes, V = in->num_views;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    const float four_r2 = 4.0f * node_radius * node_radius;
+    std::vector<DQ<float>> corr(N);
+    for (uint32_t n = 0; n < N; ++n) {
+        DQ<float> d{{0, 0, 0, 1}, {0, 0, 0, 0}};
+        const float err = c->united_error[n];
+        if (err > c->error_threshold) {
+            const mvdr_float4 node = c->live_nodes[n];
+            int view = -1;
+            for (uint32_t i = 0; i < V; ++i)
+                if ((float)i < node.w && node.w <= (float)(i + 1)) { view = (int)i; break; }
+            if (view >= 0) {
+                const mvdr_view_inputs& vi = in->views[view];
+                const mvdr_correction_view& g = c->views[view];
+                const uint32_t pitch = g.pitch ? g.pitch : c->width;
+                const M34<float> w2c = load_mat34<float>(vi.world2camera), init = load_mat34<float>(vi.initial_camera_se3);
+                const M34<float> iinv = inverse34(init);
+                const V3<float> cc = iinv.apply(w2c.apply({node.x, node.y, node.z}));
+                const mvdr_intrinsic& K = vi.intrinsic;
+                const uint32_t ux = f2u_rn_sat((float)(((double)cc.x / ((double)cc.z + 1e-10)) * (double)K.focal_x +
+                                                       (double)K.principal_x));
+                const uint32_t uy = f2u_rn_sat((float)(((double)cc.y / ((double)cc.z + 1e-10)) * (double)K.focal_y +
+                                                       (double)K.principal_y));
+                M34<float> sel;
+                for (int r = 0; r < 3; ++r) {
+                    for (int k = 0; k < 3; ++k) sel.m[r][k] = r == k ? 1.0f : 0.0f;
+                    sel.t[r] = 0.0f;
+                }
+                const uint32_t h = 2;
+                if (!(ux >= c->width - h || ux < h || uy >= c->height - h || uy < h)) {
+                    float best = 1e6f;
+                    for (uint32_t i = ux - h; i <= ux + h; ++i)
+                        for (uint32_t j = uy - h; j <= uy + h; ++j) {
+                            const size_t o = (size_t)j * pitch + i;
+                            const mvdr_float4 pv = g.previous_vertex_map[o];
+                            if (g.valid_map[o] == 1 && !zero_vertex_f(pv)) {
+                                const M34<float> gm = load_mat34<float>(g.se3_map[o]);
+                                const float dx = cc.x - pv.x, dy = cc.y - pv.y, dz = cc.z - pv.z;
+                                const float dist = dx * dx + dy * dy + dz * dz;
+                                const V3<float> mv = gm.apply(cc);
+                                const float ex = mv.x - cc.x, ey = mv.y - cc.y, ez = mv.z - cc.z;
+                                if (best > dist && dist < 1e-4f && (ex * ex + ey * ey + ez * ez) < four_r2) {
+                                    best = dist;
+                                    sel = gm;
+                                }
+                            }
+                        }
+                    sel = mul34f(mul34f(mul34f(mul34f(inverse34(w2c), init), sel), iinv), w2c);
+                }
+                // DualQuaternion(mat34), then operator*(float) via Quaternion::pow
+                const DQ<float> m = mat34_to_dq(sel);
+                float t = err;
+                if (t > 1.0f) t = 1.0f;
+                else if (t < 1e-10f) t = 1e-10f;
+                const Q<float> q0 = m.q0;
+                const float norm = std::sqrt(q0.x * q0.x + q0.y * q0.y + q0.z * q0.z);
+                const float nt = std::atan2(norm, q0.w) * t;
+                const float sn = std::sin(nt);
+                Q<float> p;
+                if (std::fabs(norm) < 1e-6f) {
+                    p = {0.0f, 0.0f, 0.0f, std::cos(nt)};
+                } else {
+                    const float scale = sn / norm;
+                    p = {q0.x * scale, q0.y * scale, q0.z * scale, std::cos(nt)};
+                }
+                d.q0 = p;
+                d.q1 = qmul(qscale(t, qmul(m.q1, qconj(q0))), p);
+            }
+        }
+        corr[n] = d;
+        c->correction[n] = {{d.q0.x, d.q0.y, d.q0.z, d.q0.w}, {d.q1.x, d.q1.y, d.q1.z, d.q1.w}};
+    }
+    const uint32_t S = c->num_surfels;
+    for (uint32_t i = 0; i < S + N; ++i) {
+        const bool surfel = i < S;
+        const uint32_t k = surfel ? i : i - S;
+        const uint16_t* kk = surfel ? c->surfel_knn + 4 * (size_t)k : c->node_knn + 4 * (size_t)k;
+        const mvdr_float4 ww = surfel ? c->surfel_knn_weight[k] : c->node_knn_weight[k];
+        const mvdr_float4 v = surfel ? c->live_vertex[k] : c->live_nodes[k];
+        const mvdr_float4 nr = surfel ? c->live_normal[k] : mvdr_float4{0, 0, 0, 0};
+        mvdr_float4 ov{nan, nan, nan, v.w}, on{nan, nan, nan, nr.w};
+        const bool ok = knn_in(kk, N);
+        DQ<float> avg{};
+        if (ok) {
+            const M34<float> se3 = normalized_se3(blend_f(c->correction, kk, ww), &avg);
+            const V3<float> p = se3.apply({v.x, v.y, v.z}), q = se3.rot({nr.x, nr.y, nr.z});
+            ov = {p.x, p.y, p.z, v.w};
+            on = {q.x, q.y, q.z, nr.w};
+        }
+        if (surfel) {
+            c->live_vertex[k] = ov;
+            c->live_normal[k] = on;
+            continue;
+        }
+        c->live_nodes[k] = ov;
+        mvdr_dual_quaternion& f = c->node_se3[k];
+        if (!ok) {
+            for (int j = 0; j < 4; ++j) f.q0[j] = f.q1[j] = nan;
+            continue;
+        }
+        const DQ<float> cur = load_dq<float>(f);
+        const Q<float> a0 = qmul(avg.q0, cur.q0);
+        const Q<float> b1 = qmul(avg.q1, cur.q0), b2 = qmul(avg.q0, cur.q1);
+        const Q<float> a1{b1.x + b2.x, b1.y + b2.y, b1.z + b2.z, b1.w + b2.w};
+        f = {{a0.x, a0.y, a0.z, a0.w}, {a1.x, a1.y, a1.z, a1.w}};
+    }
+}
 
 /* The renderer's solver-map pass (render/shaders/SolverMap.vert,
  * SolverMapSized.vert, SolverMapIndexMap.vert, SolverMap.frag; drawn by
