@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define MVDR_ABI_VERSION 2u
+#define MVDR_ABI_VERSION 3u
 #define MVDR_MAX_VIEWS 8u
 #define MVDR_INVALID_INDEX 0xFFFFFFFFu
 
@@ -205,6 +205,28 @@ typedef struct mvdr_correspondences {
     const mvdr_float4* knn_weight;
 } mvdr_correspondences;
 
+/* Raw sparse-feature pixel pairs per view, as CameraObservation carries them
+ * (CameraObservation.h:53-56), for the solver to select and compact on the
+ * device (SparseCorrespondenceHandler.cu:100-199, the nearest-distance form
+ * that solver_constants.h:9 enables). A pair (x, y, z, w) names a pixel of
+ * the rendered solver maps and a pixel of the observation. Per pair the
+ * observed pixel is the first non-zero depth vertex of the 3x3 window at
+ * (z, w) in row order, the centre preferred, dropped on an edge pixel; the
+ * rendered pixel is the 3x3 window pixel at (x, y) with a surfel whose live
+ * vertex is nearest the observed vertex; the pair is kept when the reference
+ * vertex there is within 5 cm (squared distance 2.5e-3) of the observed
+ * vertex. Kept pairs become the feature terms in candidate order: target =
+ * camera2world (the inverse of world2camera) of the observed vertex moved to
+ * frame 0, reference = the reference vertex moved to frame 0, skinning of
+ * the rendered pixel's surfel. The count of kept pairs stays on the device.
+ * When any view has pairs, `feature` must be empty. */
+typedef struct mvdr_feature_pairs {
+    uint32_t count[MVDR_MAX_VIEWS];                     /* candidate pairs per view */
+    const uint16_t* pixel_pairs[MVDR_MAX_VIEWS];        /* ushort4 per pair          */
+    const mvdr_float4* live_vertex_map[MVDR_MAX_VIEWS]; /* SolverMaps::warp_vertex_map, the view's pitch */
+    const uint8_t* edge_mask[MVDR_MAX_VIEWS];           /* 1 = edge; NULL: no edges  */
+} mvdr_feature_pairs;
+
 typedef struct mvdr_inputs {
     uint32_t num_views;
     uint32_t num_nodes;
@@ -220,6 +242,7 @@ typedef struct mvdr_inputs {
     const uint16_t* node_graph;            /* ushort2 (i, j) per edge */
     mvdr_correspondences feature;          /* SparseCorrespondenceHandler output */
     mvdr_correspondences cross_view;       /* CrossViewCorrespondenceHandler output */
+    mvdr_feature_pairs feature_pairs;      /* raw pairs, selected on the device (optional) */
 } mvdr_inputs;
 
 /* Sizes produced by the index build (host-readable after a stream sync). */

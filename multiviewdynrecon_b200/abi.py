@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-MVDR_ABI_VERSION = 2
+MVDR_ABI_VERSION = 3
 MVDR_MAX_VIEWS = 8
 MVDR_INVALID_INDEX = 0xFFFFFFFF
 
@@ -96,13 +96,18 @@ class Correspondences(C.Structure):
                 ("knn", C.c_void_p), ("knn_weight", C.c_void_p)]
 
 
+class FeaturePairs(C.Structure):
+    _fields_ = [("count", C.c_uint32 * MVDR_MAX_VIEWS), ("pixel_pairs", C.c_void_p * MVDR_MAX_VIEWS),
+                ("live_vertex_map", C.c_void_p * MVDR_MAX_VIEWS), ("edge_mask", C.c_void_p * MVDR_MAX_VIEWS)]
+
+
 class Inputs(C.Structure):
     _fields_ = [
         ("num_views", C.c_uint32), ("num_nodes", C.c_uint32), ("num_surfels", C.c_uint32),
         ("num_graph_edges", C.c_uint32), ("views", ViewInputs * MVDR_MAX_VIEWS),
         ("surfel_knn", C.c_void_p), ("surfel_knn_weight", C.c_void_p), ("node_se3", C.c_void_p),
         ("canonical_node_coords", C.c_void_p), ("node_graph", C.c_void_p),
-        ("feature", Correspondences), ("cross_view", Correspondences),
+        ("feature", Correspondences), ("cross_view", Correspondences), ("feature_pairs", FeaturePairs),
     ]
 
 
@@ -164,7 +169,8 @@ class Correction(C.Structure):
 STRUCTS = {"mvdr_float4": Float4, "mvdr_dual_quaternion": DualQuaternion, "mvdr_mat34": Mat34,
            "mvdr_intrinsic": Intrinsic, "mvdr_penalty": Penalty, "mvdr_config": Config,
            "mvdr_view_inputs": ViewInputs, "mvdr_correspondences": Correspondences, "mvdr_inputs": Inputs,
-           "mvdr_counts": Counts, "mvdr_view_textures": ViewTextures, "mvdr_surfel_geometry": SurfelGeometry,
+           "mvdr_counts": Counts, "mvdr_view_textures": ViewTextures, "mvdr_feature_pairs": FeaturePairs,
+           "mvdr_surfel_geometry": SurfelGeometry,
            "mvdr_solver_map_params": SolverMapParams, "mvdr_solver_map_view": SolverMapView,
            "mvdr_deform_surfels": DeformSurfels, "mvdr_deform_nodes": DeformNodes, "mvdr_node_error": NodeError,
            "mvdr_correction_view": CorrectionView, "mvdr_correction": Correction}
@@ -193,7 +199,8 @@ def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=48
         if use_density is None:
             use_density = terms.get("density", False)
         max_surfels = max_surfels or scene.num_surfels
-        max_feature_terms = max_feature_terms if max_feature_terms is not None else scene.feature.count
+        pairs = sum(len(p[0]) for p in (getattr(scene, "feature_pairs", None) or []))
+        max_feature_terms = max_feature_terms if max_feature_terms is not None else max(scene.feature.count, pairs)
         max_cross_terms = max_cross_terms if max_cross_terms is not None else scene.cross_view.count
         node_radius = scene.node_radius
     cfg.max_nodes = max_nodes
@@ -269,6 +276,11 @@ def fill_inputs(scene, ptr, density=False):
         dst.reference_vertex = ptr(f"{name}.ref", corr.reference_vertex)
         dst.knn = ptr(f"{name}.knn", corr.knn)
         dst.knn_weight = ptr(f"{name}.w", corr.knn_weight)
+    for v, (pairs, live, edge) in enumerate(getattr(scene, "feature_pairs", None) or []):
+        inp.feature_pairs.count[v] = len(pairs)
+        inp.feature_pairs.pixel_pairs[v] = ptr(f"v{v}.fp_pairs", pairs)
+        inp.feature_pairs.live_vertex_map[v] = ptr(f"v{v}.fp_live", live)
+        inp.feature_pairs.edge_mask[v] = None if edge is None else ptr(f"v{v}.fp_edge", edge)
     return inp
 
 

@@ -118,9 +118,13 @@ const char* const kMapNames[kNumMaps] = {"reference_vertex_map", "reference_norm
                                          "filtered_foreground_mask", "foreground_mask_gradient", "density_map",
                                          "density_gradient_map"};
 
-bool map_used(const mvdr_config& c, int k) {
+// Maps a configuration needs; the filtered foreground mask is also carried
+// when it is given with the foreground term off (the post-solve node error
+// reads it).
+bool map_used(const mvdr_config& c, int k, bool given) {
     if (k == 3 || k == 8 || k == 9) return c.use_density != 0;
-    if (k == 6 || k == 7) return c.use_foreground != 0;
+    if (k == 6) return c.use_foreground != 0 || given;
+    if (k == 7) return c.use_foreground != 0;
     return true;
 }
 
@@ -128,7 +132,7 @@ bool map_used(const mvdr_config& c, int k) {
 // File: magic, config, inputs (pointer fields meaningless), then every input
 // array as (uint64 byte count, bytes) in the order of input_arrays().
 
-constexpr char kBundleMagic[8] = {'M', 'V', 'D', 'R', 'I', 'B', 0, 1};
+constexpr char kBundleMagic[8] = {'M', 'V', 'D', 'R', 'I', 'B', 0, 2};
 
 struct InputArray {
     void* field;  // address of the pointer field in the mvdr_inputs
@@ -143,7 +147,8 @@ std::vector<InputArray> input_arrays(const mvdr_config& c, mvdr_inputs& in) {
         mvdr_view_inputs& V = in.views[k];
         const size_t np = (size_t)(V.pitch ? V.pitch : c.image_width) * H;
         for (int m = 0; m < kNumMaps; ++m)
-            add(map_field(V, kMaps[m]), map_used(c, m) ? (size_t)kMaps[m].elem_bytes * np : 0);
+            add(map_field(V, kMaps[m]),
+                map_used(c, m, get_ptr(map_field(V, kMaps[m])) != nullptr) ? (size_t)kMaps[m].elem_bytes * np : 0);
     }
     const uint32_t tp = c.use_feature ? in.feature.count : 0, tc = c.use_cross_view ? in.cross_view.count : 0;
     add(&in.surfel_knn, 8 * (size_t)in.num_surfels);
@@ -157,6 +162,14 @@ std::vector<InputArray> input_arrays(const mvdr_config& c, mvdr_inputs& in) {
         add(&cc->reference_vertex, 16 * n);
         add(&cc->knn, 8 * n);
         add(&cc->knn_weight, 16 * n);
+    }
+    for (uint32_t k = 0; k < in.num_views && k < MVDR_MAX_VIEWS; ++k) {
+        mvdr_feature_pairs& fp = in.feature_pairs;
+        const size_t n = c.use_feature ? fp.count[k] : 0;
+        const size_t np = (size_t)(in.views[k].pitch ? in.views[k].pitch : c.image_width) * H;
+        add(&fp.pixel_pairs[k], 8 * n);
+        add(&fp.live_vertex_map[k], n ? 16 * np : 0);
+        add(&fp.edge_mask[k], n && fp.edge_mask[k] ? np : 0);
     }
     return v;
 }
@@ -185,7 +198,8 @@ int mvdr_set_inputs_textures(mvdr_solver* s, const mvdr_inputs* in, const mvdr_v
     size_t total = 0;
     for (uint32_t v = 0; v < in->num_views; ++v)
         for (int m = 0; m < kNumMaps; ++m)
-            if (map_used(c, m)) total += ((size_t)kMaps[m].elem_bytes * np + 255) & ~(size_t)255;
+            if (map_used(c, m, tex_of(tex[v], kMaps[m]) != 0))
+                total += ((size_t)kMaps[m].elem_bytes * np + 255) & ~(size_t)255;
     OwnedInputs& o = b.staged[s->inst];
     if (o.bytes < total) {
         if (o.mem) CU(cudaFree(o.mem));
@@ -201,8 +215,8 @@ int mvdr_set_inputs_textures(mvdr_solver* s, const mvdr_inputs* in, const mvdr_v
         V.pitch = 0;
         for (int m = 0; m < kNumMaps; ++m) {
             set_ptr(map_field(V, kMaps[m]), nullptr);
-            if (!map_used(c, m)) continue;
             const uint64_t h = tex_of(tex[v], kMaps[m]);
+            if (!map_used(c, m, h != 0)) continue;
             if (!h) return fail(MVDR_EINVAL, std::string(kMapNames[m]) + " texture missing for view " + std::to_string(v));
             void* dst = static_cast<char*>(o.mem) + off;
             const int rc = stage_map(h, kMaps[m], c.image_width, c.image_height, dst, st, kMapNames[m]);

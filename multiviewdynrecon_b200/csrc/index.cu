@@ -36,7 +36,9 @@ __global__ void __launch_bounds__(256) input_check_kernel(const InstDesc* insts,
         const ushort2 e = I.graph[i];
         bad |= e.x >= I.N || e.y >= I.N;
     }
-    for (uint32_t i = t0; i < I.Tp; i += stride) {
+    // selected feature terms take their skinning from the (checked) surfels
+    const uint32_t tp = I.feat_select ? 0u : I.Tp;
+    for (uint32_t i = t0; i < tp; i += stride) {
         const ushort4 k = I.feat_knn[i];
         bad |= k.x >= I.N || k.y >= I.N || k.z >= I.N || k.w >= I.N;
     }
@@ -260,13 +262,126 @@ __global__ void __launch_bounds__(256) prepare_pixels_kernel(const InstDesc* ins
     }
 }
 
+// ------------------------------------------- sparse feature selection -----
+// SparseCorrespondenceHandler (SparseCorrespondenceHandler.cu:18-199), the
+// nearest-distance form (USE_NEAREST_DISTANCE_PAIRS, solver_constants.h:9).
+// Maps are read with the reference's border addressing: outside the image a
+// float4 map reads zero and the index map reads 0, which counts as a surfel
+// (it is not 0xFFFFFFFF); such a pixel's coordinate then wraps to 0xFFFF as
+// an unsigned short and fails the image-size test, as in the reference.
+
+__device__ inline float4 border4(const float4* m, int x, int y, uint32_t W, uint32_t H, uint32_t pitch) {
+    if (x < 0 || y < 0 || x >= (int)W || y >= (int)H) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return m[(size_t)y * pitch + x];
+}
+
+// is_zero_vertex (VectorUtils.h:214-216): the 1e-3 bound is a double
+__device__ inline bool zero_vertex4(float4 v) {
+    return (double)fabsf(v.x) < 1e-3 && (double)fabsf(v.y) < 1e-3 && (double)fabsf(v.z) < 1e-3;
+}
+
+__device__ inline float sq_dist3(float4 a, float4 b) {
+    return (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
+}
+
+// chooseValidPixelKernel: one thread per candidate pair
+__global__ void __launch_bounds__(256) feat_choose_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (!I.feat_select) return;
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= I.fp_offset[MVDR_MAX_VIEWS]) return;
+    uint32_t v = 0;
+    while (v + 1 < I.num_views && idx >= I.fp_offset[v + 1]) ++v;
+    const ViewDesc& V = I.views[v];
+    const uint32_t W = I.width, H = I.height, P = V.pitch;
+    const ushort4 pair = I.fp_pairs[v][idx - I.fp_offset[v]];
+    // validDepthPixelInWindow: the last row's first non-zero vertex, the
+    // centre preferred
+    ushort2 dp = make_ushort2(0xFFFF, 0xFFFF);
+    for (int y = (int)pair.w - 1; y <= (int)pair.w + 1; ++y)
+        for (int x = (int)pair.z - 1; x <= (int)pair.z + 1; ++x)
+            if (!zero_vertex4(border4(V.obs_v, x, y, W, H, P))) {
+                dp = make_ushort2((unsigned short)x, (unsigned short)y);
+                break;
+            }
+    if (!zero_vertex4(border4(V.obs_v, pair.z, pair.w, W, H, P))) dp = make_ushort2(pair.z, pair.w);
+    uint32_t keep = 0;
+    ushort4 chosen = make_ushort4(0, 0, 0, 0);
+    const uint8_t* edge = I.fp_edge[v];
+    const bool on_edge = edge && dp.x < W && dp.y < H && edge[(size_t)dp.y * P + dp.x] == 1;
+    if (dp.x < W && dp.y < H && !on_edge) {
+        const float4 ov = V.obs_v[(size_t)dp.y * P + dp.x];
+        // validGeometryPixelInWindow (nearest form): the window pixel with a
+        // surfel whose live vertex is nearest the observed vertex
+        ushort2 gp = make_ushort2(0xFFFF, 0xFFFF);
+        float best = 100.0f;
+        for (int y = (int)pair.y - 1; y <= (int)pair.y + 1; ++y)
+            for (int x = (int)pair.x - 1; x <= (int)pair.x + 1; ++x) {
+                const bool in = x >= 0 && y >= 0 && x < (int)W && y < (int)H;
+                const uint32_t s = in ? V.index[(size_t)y * P + x] : 0u;
+                if (s != kInvalid) {
+                    const float d = sq_dist3(ov, border4(I.fp_live[v], x, y, W, H, P));
+                    if (d < best) {
+                        gp = make_ushort2((unsigned short)x, (unsigned short)y);
+                        best = d;
+                    }
+                }
+            }
+        if (gp.x < W && gp.y < H) {
+            const size_t o = (size_t)gp.y * P + gp.x;
+            const uint32_t s = V.index[o];
+            // a pixel without a valid surfel id cannot give a skinning
+            if (s < I.S && sq_dist3(V.ref_v[o], ov) < 2.5e-3f) {
+                keep = 1;
+                chosen = make_ushort4(gp.x, gp.y, dp.x, dp.y);
+            }
+        }
+    }
+    I.fp_keep[idx] = keep;
+    I.fp_chosen[idx] = chosen;
+}
+
+// compactQueryValidPairsKernel: kept pairs in candidate order (one CTA of
+// 1024 threads per instance: an exclusive scan of the keep flags, then each
+// kept pair written at its prefix)
+__global__ void __launch_bounds__(1024) feat_compact_kernel(const InstDesc* insts) {
+    const InstDesc& I = insts[blockIdx.y];
+    if (!I.feat_select) return;
+    const uint32_t n = I.fp_offset[MVDR_MAX_VIEWS];
+    __shared__ uint32_t total;
+    block_exclusive_scan_inplace(I.fp_keep, n, &total);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t o = I.fp_keep[i];
+        const uint32_t next = i + 1 < n ? I.fp_keep[i + 1] : total;
+        if (next == o) continue;
+        uint32_t v = 0;
+        while (v + 1 < I.num_views && i >= I.fp_offset[v + 1]) ++v;
+        const ViewDesc& V = I.views[v];
+        const ushort4 c = I.fp_chosen[i];
+        const size_t og = (size_t)c.y * V.pitch + c.x, oo = (size_t)c.w * V.pitch + c.z;
+        const float4 rv = V.ref_v[og];
+        const float3 r0 = apply3(V.init, mk3(rv.x, rv.y, rv.z));
+        const float4 dv = V.obs_v[oo];
+        const float3 t0 = apply3(V.c2w, apply3(V.init, mk3(dv.x, dv.y, dv.z)));
+        const uint32_t s = V.index[og];
+        I.fp_target[o] = make_float4(t0.x, t0.y, t0.z, 1.0f);
+        I.fp_ref[o] = make_float4(r0.x, r0.y, r0.z, rv.w);
+        I.fp_knn[o] = I.surfel_knn[s];
+        I.fp_w[o] = I.surfel_w[s];
+    }
+    if (threadIdx.x == 0) I.counts->feature_terms = total;
+}
+
 // size2offset (term_offset_types.h:44-64) on the device
 __global__ void term_offsets_kernel(const InstDesc* insts) {
     const InstDesc& I = insts[blockIdx.y];
     if (threadIdx.x != 0) return;
     DeviceCounts* C = I.counts;
     C->smooth_terms = I.E;
-    C->feature_terms = I.Tp;
+    // selected feature terms: their count was written by feat_compact_kernel
+    const uint32_t tp = I.feat_select ? C->feature_terms : I.Tp;
+    C->feature_terms = tp;
     C->cross_terms = I.Tc;
     uint32_t o = C->dense_terms;
     C->term_offset[0] = o;
@@ -274,7 +389,7 @@ __global__ void term_offsets_kernel(const InstDesc* insts) {
     C->term_offset[1] = o;
     o += C->foreground_terms;
     C->term_offset[2] = o;
-    o += I.Tp;
+    o += tp;
     C->term_offset[3] = o;
     o += I.Tc;
     C->term_offset[4] = o;
@@ -913,6 +1028,10 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d, cudaStream_t st
     MVDR_LAUNCH(compact_scan_kernel, grid2(1, B), 1024, 0, st, d, cpv, lc.max_views, 1);
     MVDR_LAUNCH(compact_write_kernel<ForegroundPred>, grid2(cpv * lc.max_views, B), 256, 0, st, d, lc.width, lc.height, cpv, 1);
     MVDR_LAUNCH(prepare_pixels_kernel, grid2(spread, B), 256, 0, st, d, lc.precision == MVDR_PRECISION_MIXED);
+    if (lc.max_tp) {
+        MVDR_LAUNCH(feat_choose_kernel, grid2((lc.max_tp + 255) / 256, B), 256, 0, st, d);
+        MVDR_LAUNCH(feat_compact_kernel, grid2(1, B), 1024, 0, st, d);
+    }
     MVDR_LAUNCH(term_offsets_kernel, grid2(1, B), 32, 0, st, d);
     // node -> term
     MVDR_LAUNCH(n2t_count_kernel, grid2(spread, B), 256, 0, st, d);

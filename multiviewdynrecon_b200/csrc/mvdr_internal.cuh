@@ -182,6 +182,7 @@ struct ViewDesc {
     uint32_t pitch;
     float cx, cy, fx, fy;
     M34 w2c, init, init_inv;
+    M34 c2w;  // the inverse of w2c (camera2World of the sparse feature selection)
     // the same transforms in double, for the mixed-precision residual chain
     double w2c_d[12], init_d[12], init_inv_d[12];  // row-major rotation, then translation
 };
@@ -228,6 +229,20 @@ struct InstDesc {
     const float4* cross_ref;
     const ushort4* cross_knn;
     const float4* cross_w;
+    // device-side selection of the feature terms from raw pixel pairs
+    // (mvdr_feature_pairs); feat_* then point at the fp_* outputs and Tp is
+    // the capacity (the layout stride), the count being counts->feature_terms
+    uint32_t feat_select;
+    uint32_t fp_offset[MVDR_MAX_VIEWS + 1];  // candidate pairs before each view
+    const ushort4* fp_pairs[MVDR_MAX_VIEWS];
+    const float4* fp_live[MVDR_MAX_VIEWS];
+    const uint8_t* fp_edge[MVDR_MAX_VIEWS];
+    uint32_t* fp_keep;       // [max_tp] 1 = kept, then its exclusive prefix
+    ushort4* fp_chosen;      // [max_tp] (rendered x, y, observed x, y)
+    float4* fp_target;       // [max_tp]
+    float4* fp_ref;
+    ushort4* fp_knn;
+    float4* fp_w;
 
     // ---- workspace (solver-owned) ----
     DeviceCounts* counts;

@@ -180,6 +180,14 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
     I.node_err_acc = a.take<unsigned long long>(2 * N);
+    if (max_tp) {  // device-side feature selection
+        I.fp_keep = a.take<uint32_t>(max_tp);
+        I.fp_chosen = a.take<ushort4>(max_tp);
+        I.fp_target = a.take<float4>(max_tp);
+        I.fp_ref = a.take<float4>(max_tp);
+        I.fp_knn = a.take<ushort4>(max_tp);
+        I.fp_w = a.take<float4>(max_tp);
+    }
     I.cap_dense = lc.cap_dense;
     I.cap_fg = lc.cap_fg;
     I.cap_k1 = lc.cap_k1;
@@ -354,6 +362,20 @@ int check_inputs(const Batch& b, const mvdr_inputs* in) {
     if (c.use_feature && in->feature.count &&
         (!in->feature.target_vertex || !in->feature.reference_vertex || !in->feature.knn || !in->feature.knn_weight))
         return fail(MVDR_EINVAL, "missing feature arrays");
+    uint64_t pairs = 0;
+    for (uint32_t v = 0; v < MVDR_MAX_VIEWS; ++v) {
+        const uint32_t n = in->feature_pairs.count[v];
+        if (!n) continue;
+        if (v >= in->num_views) return fail(MVDR_EINVAL, "feature pixel pairs given for a view that is not bound");
+        if (!in->feature_pairs.pixel_pairs[v] || !in->feature_pairs.live_vertex_map[v])
+            return fail(MVDR_EINVAL, "feature pixel pairs need their pairs and the live vertex map");
+        pairs += n;
+    }
+    if (pairs) {
+        if (!c.use_feature) return fail(MVDR_EINVAL, "feature pixel pairs given with the feature term off");
+        if (in->feature.count) return fail(MVDR_EINVAL, "give either feature pixel pairs or feature correspondences");
+        if (pairs > c.max_feature_terms) return fail(MVDR_ECAPACITY, "feature pixel pairs exceed max_feature_terms");
+    }
     if (c.use_cross_view && in->cross_view.count &&
         (!in->cross_view.target_vertex || !in->cross_view.reference_vertex || !in->cross_view.knn ||
          !in->cross_view.knn_weight))
@@ -391,7 +413,8 @@ int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st)
         V.index = S.index_map;
         V.obs_v = reinterpret_cast<const float4*>(S.vertex_confidence_map);
         V.obs_n = reinterpret_cast<const float4*>(S.normal_radius_map);
-        V.fg = c.use_foreground ? S.filtered_foreground_mask : nullptr;
+        // the mask is bound whenever given: the post-solve node error reads it
+        V.fg = S.filtered_foreground_mask;
         V.fg_grad = c.use_foreground ? reinterpret_cast<const float2*>(S.foreground_mask_gradient) : nullptr;
         V.rgb = c.use_density ? reinterpret_cast<const float4*>(S.normalized_rgb_map) : nullptr;
         V.dens = c.use_density ? S.density_map : nullptr;
@@ -404,6 +427,7 @@ int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st)
         V.w2c = load34(S.world2camera);
         V.init = load34(S.initial_camera_se3);
         V.init_inv = inverse34(V.init);
+        V.c2w = inverse34(V.w2c);
         // double copies for the mixed-precision residual chain
         const M34* src[3] = {&V.w2c, &V.init, &V.init_inv};
         double* dst[3] = {V.w2c_d, V.init_d, V.init_inv_d};
@@ -424,6 +448,26 @@ int bind_inputs(Batch& b, uint32_t inst, const mvdr_inputs* in, cudaStream_t st)
     I.cross_ref = reinterpret_cast<const float4*>(in->cross_view.reference_vertex);
     I.cross_knn = reinterpret_cast<const ushort4*>(in->cross_view.knn);
     I.cross_w = reinterpret_cast<const float4*>(in->cross_view.knn_weight);
+    uint32_t pairs = 0;
+    for (uint32_t v = 0; v < MVDR_MAX_VIEWS; ++v) {
+        I.fp_offset[v] = pairs;
+        const bool on = v < in->num_views && c.use_feature;
+        const uint32_t n = on ? in->feature_pairs.count[v] : 0;
+        I.fp_pairs[v] = n ? reinterpret_cast<const ushort4*>(in->feature_pairs.pixel_pairs[v]) : nullptr;
+        I.fp_live[v] = n ? reinterpret_cast<const float4*>(in->feature_pairs.live_vertex_map[v]) : nullptr;
+        I.fp_edge[v] = n ? in->feature_pairs.edge_mask[v] : nullptr;
+        pairs += n;
+    }
+    I.fp_offset[MVDR_MAX_VIEWS] = pairs;
+    I.feat_select = pairs ? 1u : 0u;
+    if (pairs) {
+        // the selected terms live in the solver's arrays; Tp is the capacity
+        I.Tp = c.max_feature_terms;
+        I.feat_target = I.fp_target;
+        I.feat_ref = I.fp_ref;
+        I.feat_knn = I.fp_knn;
+        I.feat_w = I.fp_w;
+    }
     // SolverIterationData::SetWarpFieldInitialValue (SolverIterationData.cpp:37-50)
     CU(cudaMemcpyAsync(I.se3, in->node_se3, sizeof(DQ) * I.N, cudaMemcpyDefault, st));
     CU(cudaMemsetAsync(I.counts, 0, sizeof(DeviceCounts), st));
@@ -457,7 +501,7 @@ static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cuda
         add(V.index_map, 4 * np);
         add(V.vertex_confidence_map, 16 * np);
         add(V.normal_radius_map, 16 * np);
-        add(c.use_foreground ? V.filtered_foreground_mask : nullptr, c.use_foreground ? 4 * np : 0);
+        add(V.filtered_foreground_mask, V.filtered_foreground_mask ? 4 * np : 0);
         add(c.use_foreground ? V.foreground_mask_gradient : nullptr, c.use_foreground ? 8 * np : 0);
         add(c.use_density ? V.normalized_rgb_map : nullptr, c.use_density ? 16 * np : 0);
         add(c.use_density ? V.density_map : nullptr, c.use_density ? 4 * np : 0);
@@ -477,6 +521,13 @@ static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cuda
     add(in->cross_view.reference_vertex, 16 * (size_t)tc);
     add(in->cross_view.knn, 8 * (size_t)tc);
     add(in->cross_view.knn_weight, 16 * (size_t)tc);
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        const uint32_t n = c.use_feature ? in->feature_pairs.count[v] : 0;
+        const size_t np = (size_t)(in->views[v].pitch ? in->views[v].pitch : W) * H;
+        add(n ? in->feature_pairs.pixel_pairs[v] : nullptr, 8 * (size_t)n);
+        add(n ? in->feature_pairs.live_vertex_map[v] : nullptr, n ? 16 * np : 0);
+        add(n ? in->feature_pairs.edge_mask[v] : nullptr, n && in->feature_pairs.edge_mask[v] ? np : 0);
+    }
     size_t total = 0;
     for (auto& it : items) total += (it.bytes + 255) & ~(size_t)255;
     OwnedInputs& o = b.owned[inst];
@@ -550,6 +601,11 @@ static int bind_inputs_host(Batch& b, uint32_t inst, const mvdr_inputs* in, cuda
     dev.cross_view.reference_vertex = (const mvdr_float4*)dst[k++];
     dev.cross_view.knn = (const uint16_t*)dst[k++];
     dev.cross_view.knn_weight = (const mvdr_float4*)dst[k++];
+    for (uint32_t v = 0; v < in->num_views; ++v) {
+        dev.feature_pairs.pixel_pairs[v] = (const uint16_t*)dst[k++];
+        dev.feature_pairs.live_vertex_map[v] = (const mvdr_float4*)dst[k++];
+        dev.feature_pairs.edge_mask[v] = (const uint8_t*)dst[k++];
+    }
     return bind_inputs(b, inst, &dev, st);
 }
 
@@ -1030,7 +1086,8 @@ int mvdr_abi_layout(const char* name, size_t* size) {
         {"mvdr_penalty", sizeof(mvdr_penalty)}, {"mvdr_config", sizeof(mvdr_config)},
         {"mvdr_view_inputs", sizeof(mvdr_view_inputs)}, {"mvdr_correspondences", sizeof(mvdr_correspondences)},
         {"mvdr_inputs", sizeof(mvdr_inputs)}, {"mvdr_counts", sizeof(mvdr_counts)},
-        {"mvdr_view_textures", sizeof(mvdr_view_textures)}, {"mvdr_surfel_geometry", sizeof(mvdr_surfel_geometry)},
+        {"mvdr_view_textures", sizeof(mvdr_view_textures)}, {"mvdr_feature_pairs", sizeof(mvdr_feature_pairs)},
+        {"mvdr_surfel_geometry", sizeof(mvdr_surfel_geometry)},
         {"mvdr_solver_map_params", sizeof(mvdr_solver_map_params)},
         {"mvdr_solver_map_view", sizeof(mvdr_solver_map_view)}, {"mvdr_deform_surfels", sizeof(mvdr_deform_surfels)},
         {"mvdr_deform_nodes", sizeof(mvdr_deform_nodes)}, {"mvdr_node_error", sizeof(mvdr_node_error)},

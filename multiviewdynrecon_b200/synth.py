@@ -286,6 +286,10 @@ class Scene:
     # the surfels behind the index maps, in frame 0 (surfel id = row)
     surfel_position: np.ndarray = None   # (S, 3) float64
     surfel_normal: np.ndarray = None     # (S, 3) float64
+    # raw sparse-feature pixel pairs per view, selected by the solver: a list
+    # of (pairs (n, 4) uint16, live vertex map (H, W, 4), edge mask (H, W)
+    # uint8); `feature` is then empty
+    feature_pairs: list = None
     gn_iterations: int = 3
     pcg_iterations: int = 10
 
@@ -622,6 +626,50 @@ def solver_map_geometry(scene, seed=0, current_time=10.0, warped=True):
     ct[:, 2] = (current_time - rng.integers(0, 7, S)).astype(np.float32)
     return dict(reference_vertex_confid=ref_v, reference_normal_radius=ref_n, live_vertex_confid=live_v,
                 live_normal_radius=live_n, color_time=ct)
+
+
+# --------------------------------------------------------------------------
+# raw sparse-feature pixel pairs
+# --------------------------------------------------------------------------
+
+def with_feature_pairs(scene, per_view=400, seed=0, outlier_fraction=0.1):
+    """A copy of `scene` whose feature term comes from raw pixel pairs: per
+    view, pairs (x, y, z, w) of a rendered pixel with a surfel and a nearby
+    observed pixel (jitter of one pixel, `outlier_fraction` of them up to
+    six pixels away), the rendered live vertex map (the reference surface
+    moved by the scene's warp field, camera frame) and the observation's
+    silhouette edges."""
+    import dataclasses
+    rng = np.random.default_rng([seed, 7349])
+    H, W = scene.height, scene.width
+    out = []
+    for view in scene.views:
+        idx = view.index_map
+        ys, xs = np.nonzero(idx != INVALID_INDEX)
+        pick = rng.choice(len(xs), size=min(per_view, len(xs)), replace=False)
+        x, y = xs[pick], ys[pick]
+        far = rng.random(len(x)) < outlier_fraction
+        jx = np.where(far, rng.integers(-6, 7, len(x)), rng.integers(-1, 2, len(x)))
+        jy = np.where(far, rng.integers(-6, 7, len(x)), rng.integers(-1, 2, len(x)))
+        z, w = np.clip(x + jx, 0, W - 1), np.clip(y + jy, 0, H - 1)
+        pairs = np.stack([x, y, z, w], 1).astype(np.uint16)
+        # live vertex map: warp(init * reference) brought back to the camera
+        m = np.asarray(view.initial_camera_se3, np.float64)
+        Ri, ti = m[:9].reshape(3, 3).T, m[9:12]
+        live = np.zeros((H, W, 4), np.float32)
+        s = idx[ys, xs]
+        R, t = blend_warp(scene.node_se3, scene.surfel_knn[s], scene.surfel_knn_weight[s])
+        ref0 = view.reference_vertex_map[ys, xs, :3].astype(np.float64) @ Ri.T + ti
+        lv = np.einsum("sij,sj->si", R, ref0) + t
+        live[ys, xs, :3] = (lv - ti) @ Ri
+        live[ys, xs, 3] = 1.0
+        observed = np.abs(view.vertex_confidence_map[..., 2]) > 0
+        pad = np.pad(observed, 1, constant_values=False)
+        inner = pad[:-2, 1:-1] & pad[2:, 1:-1] & pad[1:-1, :-2] & pad[1:-1, 2:]
+        edge = (observed & ~inner).astype(np.uint8)
+        out.append((pairs, live, edge))
+    return dataclasses.replace(scene, feature=Correspondences.empty(), feature_pairs=out,
+                               terms={**scene.terms, "feature": True})
 
 
 # --------------------------------------------------------------------------

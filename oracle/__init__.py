@@ -102,6 +102,8 @@ def lib():
         L.orc_p2p_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_render_solver_maps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        L.orc_feature_terms.restype = C.c_uint32
+        L.orc_feature_terms.argtypes = [C.c_void_p] * 5
         L.orc_forward_warp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32] + [C.c_void_p] * 6 + \
             [C.c_uint32] + [C.c_void_p] * 4
         L.orc_inverse_warp.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32] + [C.c_void_p] * 6
@@ -160,6 +162,15 @@ class Oracle:
             self.h = None
 
     # stages
+    def feature_terms(self):
+        """The feature terms (bound, or selected from raw pixel pairs):
+        target (T, 4), reference (T, 4), knn (T, 4) uint16, weights (T, 4)."""
+        n = lib().orc_feature_terms(self.h, None, None, None, None)
+        t, r, w = (np.zeros((n, 4), np.float32) for _ in range(3))
+        k = np.zeros((n, 4), np.uint16)
+        lib().orc_feature_terms(self.h, _p(t), _p(r), _p(k), _p(w))
+        return t, r, k, w
+
     def build_index(self):
         lib().orc_build_index(self.h)
 

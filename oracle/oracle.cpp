@@ -417,11 +417,91 @@ struct Oracle {
         };
         copy_corr(feat, in->feature, cfg.use_feature != 0);
         copy_corr(cross, in->cross_view, cfg.use_cross_view != 0);
+        if (cfg.use_feature) select_features(in);
         se3d.resize(N);
         for (u32 i = 0; i < N; ++i) se3d[i] = load_dq<double>(node_se3_init[i]);
         gn_iter = 0;
         frozen = false;
         return MVDR_OK;
+    }
+
+    // SparseCorrespondenceHandler (SparseCorrespondenceHandler.cu:18-199), the
+    // nearest-distance form: raw pixel pairs -> feature terms, in candidate
+    // order. Border addressing: outside the image a float4 map reads zero and
+    // the index map reads 0 (a "surfel"); such a pixel's coordinate wraps to
+    // 0xFFFF and fails the image-size test.
+    void select_features(const mvdr_inputs* in) {
+        const mvdr_feature_pairs& fp = in->feature_pairs;
+        bool any = false;
+        for (u32 v = 0; v < V; ++v) any |= fp.count[v] != 0;
+        if (!any) return;
+        feat = Corr();
+        auto zero = [](const mvdr_float4& a) {
+            return (double)std::fabs(a.x) < 1e-3 && (double)std::fabs(a.y) < 1e-3 && (double)std::fabs(a.z) < 1e-3;
+        };
+        auto sq = [](const mvdr_float4& a, const mvdr_float4& b) {
+            return (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
+        };
+        for (u32 v = 0; v < V; ++v) {
+            const ViewData& d = views[v];
+            const mvdr_view_inputs& vi = in->views[v];
+            const u32 pitch = vi.pitch ? vi.pitch : W;
+            auto at4 = [&](const std::vector<mvdr_float4>& m, int x, int y) {
+                if (x < 0 || y < 0 || x >= (int)W || y >= (int)H) return mvdr_float4{0, 0, 0, 0};
+                return m[(size_t)y * W + x];
+            };
+            auto live = [&](int x, int y) {
+                if (x < 0 || y < 0 || x >= (int)W || y >= (int)H) return mvdr_float4{0, 0, 0, 0};
+                return fp.live_vertex_map[v][(size_t)y * pitch + x];
+            };
+            const M34<float> init = load_mat34<float>(d.init);
+            const M34<float> c2w = inverse34(load_mat34<float>(d.w2c));
+            for (u32 k = 0; k < fp.count[v]; ++k) {
+                const u16* pr = fp.pixel_pairs[v] + 4 * (size_t)k;
+                u16 dx = 0xFFFF, dy = 0xFFFF;
+                for (int y = (int)pr[3] - 1; y <= (int)pr[3] + 1; ++y)
+                    for (int x = (int)pr[2] - 1; x <= (int)pr[2] + 1; ++x)
+                        if (!zero(at4(d.obs_v, x, y))) {
+                            dx = (u16)x;
+                            dy = (u16)y;
+                            break;
+                        }
+                if (!zero(at4(d.obs_v, pr[2], pr[3]))) {
+                    dx = pr[2];
+                    dy = pr[3];
+                }
+                if (!(dx < W && dy < H)) continue;
+                if (fp.edge_mask[v] && fp.edge_mask[v][(size_t)dy * pitch + dx] == 1) continue;
+                const mvdr_float4 ov = d.obs_v[(size_t)dy * W + dx];
+                u16 gx = 0xFFFF, gy = 0xFFFF;
+                float best = 100.0f;
+                for (int y = (int)pr[1] - 1; y <= (int)pr[1] + 1; ++y)
+                    for (int x = (int)pr[0] - 1; x <= (int)pr[0] + 1; ++x) {
+                        const bool inside = x >= 0 && y >= 0 && x < (int)W && y < (int)H;
+                        const u32 s = inside ? d.index[(size_t)y * W + x] : 0u;
+                        if (s != MVDR_INVALID_INDEX) {
+                            const float dd = sq(ov, live(x, y));
+                            if (dd < best) {
+                                gx = (u16)x;
+                                gy = (u16)y;
+                                best = dd;
+                            }
+                        }
+                    }
+                if (!(gx < W && gy < H)) continue;
+                const size_t og = (size_t)gy * W + gx;
+                const u32 s = d.index[og];
+                if (!(s < S && sq(d.ref_v[og], ov) < 2.5e-3f)) continue;
+                const mvdr_float4 rv = d.ref_v[og];
+                const V3<float> r0 = init.apply({rv.x, rv.y, rv.z});
+                const mvdr_float4 dv = ov;  // the observed vertex at the chosen depth pixel
+                const V3<float> t0 = c2w.apply(init.apply({dv.x, dv.y, dv.z}));
+                feat.target.push_back({t0.x, t0.y, t0.z, 1.0f});
+                feat.ref.push_back({r0.x, r0.y, r0.z, rv.w});
+                feat.w.push_back(surfel_w[s]);
+                for (int j = 0; j < 4; ++j) feat.knn.push_back(surfel_knn[4 * (size_t)s + j]);
+            }
+        }
     }
 
     template <class R> std::vector<DQ<R>> field() const {
@@ -1218,6 +1298,19 @@ void* orc_create(const mvdr_config* cfg, const mvdr_inputs* host_inputs, int fp6
 void orc_destroy(void* h) { delete (Oracle*)h; }
 
 void orc_build_index(void* h) { ((Oracle*)h)->build_index(); }
+
+/* The feature terms as bound or selected from raw pixel pairs: returns their
+ * count and, when the pointers are not NULL, copies target, reference,
+ * ushort4 knn and weights. */
+uint32_t orc_feature_terms(void* h, mvdr_float4* target, mvdr_float4* ref, uint16_t* knn, mvdr_float4* w) {
+    const Oracle* o = (const Oracle*)h;
+    const size_t n = o->feat.w.size();
+    if (target) std::memcpy(target, o->feat.target.data(), 16 * n);
+    if (ref) std::memcpy(ref, o->feat.ref.data(), 16 * n);
+    if (knn) std::memcpy(knn, o->feat.knn.data(), 8 * n);
+    if (w) std::memcpy(w, o->feat.w.data(), 16 * n);
+    return (uint32_t)n;
+}
 
 /* Evaluate the terms of the current Gauss-Newton iteration (penalty schedule
  * of that iteration included). */
