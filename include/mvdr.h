@@ -578,8 +578,10 @@ enum {
     MVDR_ARRAY_BINBLOCK_DATA = 20,      /* float [binblock_nnz] bin-block CSR values        */
     MVDR_ARRAY_INCREMENT = 21,          /* float [6N] PCG solution of the last iteration     */
     MVDR_ARRAY_NODE_SE3 = 22,           /* dual quaternion [N] current warp field            */
-    MVDR_ARRAY_DENSITY_JACOBIAN = 23    /* float [T_d][8]: density twist gradient (6), residual,
+    MVDR_ARRAY_DENSITY_JACOBIAN = 23,   /* float [T_d][8]: density twist gradient (6), residual,
                                            projected pixel (use_density only)                */
+    MVDR_ARRAY_FEATURE_TERMS = 24       /* float [T_p][8]: target vertex (4), reference vertex
+                                           (4) of the feature terms (bound or selected)      */
 };
 MVDR_API int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t capacity_bytes,
                    size_t* written_bytes, void* stream);

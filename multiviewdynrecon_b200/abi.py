@@ -34,7 +34,7 @@ NUM_SPMV_SHAPES = len(SPMV_SHAPES)
  ARRAY_NODEPAIR_TERM_RANGE, ARRAY_BLKROW_OFFSET, ARRAY_BINBLOCK_ROWPTR, ARRAY_BINBLOCK_COLPTR,
  ARRAY_TERM_JACOBIAN, ARRAY_SMOOTH_TERMS, ARRAY_WARPED_CORRESPONDENCE, ARRAY_DIAG_BLOCKS, ARRAY_JTR,
  ARRAY_PRECONDITIONER, ARRAY_OFFDIAG_BLOCKS, ARRAY_BINBLOCK_DATA, ARRAY_INCREMENT, ARRAY_NODE_SE3,
- ARRAY_DENSITY_JACOBIAN) = range(24)
+ ARRAY_DENSITY_JACOBIAN, ARRAY_FEATURE_TERMS) = range(25)
 
 
 class Float4(C.Structure):

@@ -280,8 +280,24 @@ __device__ inline bool zero_vertex4(float4 v) {
     return (double)fabsf(v.x) < 1e-3 && (double)fabsf(v.y) < 1e-3 && (double)fabsf(v.z) < 1e-3;
 }
 
+// The selection's float arithmetic is written with round-to-nearest
+// intrinsics, which the compiler does not contract into FMAs: the kept pairs
+// and the term positions are then the CPU restatement's to the bit (a one-ulp
+// shift of a target moves the small late-iteration residuals measurably).
 __device__ inline float sq_dist3(float4 a, float4 b) {
-    return (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
+    const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// m * p + t, uncontracted (mat34 applied as the reference writes it)
+__device__ inline float3 apply3_rn(const M34& m, float3 p) {
+    float o[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        o[r] = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.r[3 * r], p.x), __fmul_rn(m.r[3 * r + 1], p.y)),
+                                   __fmul_rn(m.r[3 * r + 2], p.z)),
+                         m.t[r]);
+    return mk3(o[0], o[1], o[2]);
 }
 
 // chooseValidPixelKernel: one thread per candidate pair
@@ -361,9 +377,9 @@ __global__ void __launch_bounds__(1024) feat_compact_kernel(const InstDesc* inst
         const ushort4 c = I.fp_chosen[i];
         const size_t og = (size_t)c.y * V.pitch + c.x, oo = (size_t)c.w * V.pitch + c.z;
         const float4 rv = V.ref_v[og];
-        const float3 r0 = apply3(V.init, mk3(rv.x, rv.y, rv.z));
+        const float3 r0 = apply3_rn(V.init, mk3(rv.x, rv.y, rv.z));
         const float4 dv = V.obs_v[oo];
-        const float3 t0 = apply3(V.c2w, apply3(V.init, mk3(dv.x, dv.y, dv.z)));
+        const float3 t0 = apply3_rn(V.c2w, apply3_rn(V.init, mk3(dv.x, dv.y, dv.z)));
         const uint32_t s = V.index[og];
         I.fp_target[o] = make_float4(t0.x, t0.y, t0.z, 1.0f);
         I.fp_ref[o] = make_float4(r0.x, r0.y, r0.z, rv.w);

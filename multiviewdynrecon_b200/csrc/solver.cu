@@ -760,6 +760,22 @@ static int get_array(Batch& b, uint32_t inst, int which, void* dst, size_t cap, 
         case MVDR_ARRAY_DENSITY_JACOBIAN:
             if (!I.density_jr) return fail(MVDR_EINVAL, "the density term is off");
             return copy_out(dst, I.density_jr, 32 * (size_t)c.dense_terms, cap, written);
+        case MVDR_ARRAY_FEATURE_TERMS: {
+            // (target, reference) per term, interleaved on the host
+            const size_t n = c.feature_terms;
+            *written = 32 * n;
+            if (cap < 32 * n) return fail(MVDR_ECAPACITY, "destination too small");
+            if (n == 0) return MVDR_OK;
+            std::vector<float4> t(n), r(n);
+            CU(cudaMemcpy(t.data(), I.feat_target, 16 * n, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(r.data(), I.feat_ref, 16 * n, cudaMemcpyDeviceToHost));
+            float4* out = static_cast<float4*>(dst);
+            for (size_t k = 0; k < n; ++k) {
+                out[2 * k] = t[k];
+                out[2 * k + 1] = r[k];
+            }
+            return MVDR_OK;
+        }
         case MVDR_ARRAY_PRECONDITIONER:
         case MVDR_ARRAY_OFFDIAG_BLOCKS:
         case MVDR_ARRAY_BINBLOCK_DATA: {

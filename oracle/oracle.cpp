@@ -1431,6 +1431,14 @@ long long orc_get(void* h, int which, void* dst, size_t cap, int as_double) {
         case MVDR_ARRAY_BINBLOCK_COLPTR: return put(o->colptr.data(), o->colptr.size() * 4);
         case MVDR_ARRAY_TERM_JACOBIAN: return put(o->term_jr.data(), o->term_jr.size() * 4);
         case MVDR_ARRAY_DENSITY_JACOBIAN: return put(o->density_jr.data(), o->density_jr.size() * 4);
+        case MVDR_ARRAY_FEATURE_TERMS: {
+            std::vector<mvdr_float4> tr;
+            for (size_t k = 0; k < o->feat.w.size(); ++k) {
+                tr.push_back(o->feat.target[k]);
+                tr.push_back(o->feat.ref[k]);
+            }
+            return put(tr.data(), tr.size() * 16);
+        }
         case MVDR_ARRAY_SMOOTH_TERMS: return put(o->smooth.data(), o->smooth.size() * 4);
         case MVDR_ARRAY_WARPED_CORRESPONDENCE: return put(o->warped.data(), o->warped.size() * 4);
         case MVDR_ARRAY_DIAG_BLOCKS: return put_real(o->D);

@@ -46,6 +46,8 @@ def test_selected_index_bit_exact(oracle_mod, kind):
         assert getattr(gc, f) == getattr(oc, f), f
     for which in INDEX_ARRAYS:
         assert np.array_equal(bits(g.get_array(which)), bits(o.get(which))), which
+    # the selected terms' positions, to the bit
+    assert np.array_equal(bits(g.get_array(abi.ARRAY_FEATURE_TERMS)), bits(o.get(abi.ARRAY_FEATURE_TERMS)))
     # the warped feature records: the GPU keeps the capacity as the stride
     g.gn_iteration(1)
     torch.cuda.synchronize()
