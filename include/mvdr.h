@@ -169,6 +169,14 @@ typedef struct mvdr_config {
      * penalty.density without the schedule. Needs the three density maps of
      * every view. */
     int32_t use_density;
+    /* Convergence check of every PCG solve (BlockPCG::SolveConvergeChecked,
+     * BlockPCG.cuh:339-377): the solve stops after the first iteration whose
+     * delta = r.M^-1 r is below pcg_tolerance^2 times the initial delta, the
+     * test made on the device (the later iterations' kernels of that instance
+     * return at once), so solves stay capturable in a CUDA graph. 0 (the
+     * default) runs the fixed iteration count (BlockPCG::Solve). The launched
+     * PCG form only: with a tolerance the persistent form is not used. */
+    float pcg_tolerance;
 } mvdr_config;
 
 /* Per-view inputs: the rendered solver maps (Renderer::SolverMaps,
@@ -580,9 +588,14 @@ enum {
     MVDR_ARRAY_NODE_SE3 = 22,           /* dual quaternion [N] current warp field            */
     MVDR_ARRAY_DENSITY_JACOBIAN = 23,   /* float [T_d][8]: density twist gradient (6), residual,
                                            projected pixel (use_density only)                */
-    MVDR_ARRAY_FEATURE_TERMS = 24       /* float [T_p][8]: target vertex (4), reference vertex
+    MVDR_ARRAY_FEATURE_TERMS = 24,      /* float [T_p][8]: target vertex (4), reference vertex
                                            (4) of the feature terms (bound or selected)      */
+    MVDR_ARRAY_PCG_RESIDUALS = 25       /* double [G][MVDR_PCG_HISTORY]: per Gauss-Newton
+                                           iteration g < 64 of the last solve, delta_k of
+                                           each PCG iteration k (delta_0 first); NaN after
+                                           the last iteration run                            */
 };
+#define MVDR_PCG_HISTORY 257u /* delta_0 and up to 256 PCG iterations per Gauss-Newton iteration */
 MVDR_API int mvdr_get_array(mvdr_solver* solver, int which, void* dst, size_t capacity_bytes,
                    size_t* written_bytes, void* stream);
 

@@ -34,7 +34,8 @@ NUM_SPMV_SHAPES = len(SPMV_SHAPES)
  ARRAY_NODEPAIR_TERM_RANGE, ARRAY_BLKROW_OFFSET, ARRAY_BINBLOCK_ROWPTR, ARRAY_BINBLOCK_COLPTR,
  ARRAY_TERM_JACOBIAN, ARRAY_SMOOTH_TERMS, ARRAY_WARPED_CORRESPONDENCE, ARRAY_DIAG_BLOCKS, ARRAY_JTR,
  ARRAY_PRECONDITIONER, ARRAY_OFFDIAG_BLOCKS, ARRAY_BINBLOCK_DATA, ARRAY_INCREMENT, ARRAY_NODE_SE3,
- ARRAY_DENSITY_JACOBIAN, ARRAY_FEATURE_TERMS) = range(25)
+ ARRAY_DENSITY_JACOBIAN, ARRAY_FEATURE_TERMS, ARRAY_PCG_RESIDUALS) = range(26)
+MVDR_PCG_HISTORY = 257
 
 
 class Float4(C.Structure):
@@ -69,7 +70,7 @@ class Config(C.Structure):
         ("node_radius", C.c_float), ("precision", C.c_int32), ("mode", C.c_int32),
         ("use_foreground", C.c_int32), ("use_feature", C.c_int32), ("use_cross_view", C.c_int32),
         ("use_elastic_penalty", C.c_int32), ("num_global_iterations", C.c_int32), ("compat_flags", C.c_uint32),
-        ("penalty", Penalty), ("use_density", C.c_int32),
+        ("penalty", Penalty), ("use_density", C.c_int32), ("pcg_tolerance", C.c_float),
     ]
 
 
@@ -179,7 +180,8 @@ STRUCTS = {"mvdr_float4": Float4, "mvdr_dual_quaternion": DualQuaternion, "mvdr_
 def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=480, precision=PRECISION_MIXED,
                 mode=MODE_MATERIALIZED, use_foreground=None, use_feature=None, use_cross_view=None,
                 max_surfels=None, max_feature_terms=None, max_cross_terms=None, elastic=True,
-                num_global_iterations=1 << 20, compat_flags=0, node_radius=0.025, use_density=None):
+                num_global_iterations=1 << 20, compat_flags=0, node_radius=0.025, use_density=None,
+                pcg_tolerance=0.0):
     """Configuration for a scene (or explicit capacities). With the elastic
     schedule on and num_global_iterations large, every iteration uses the
     global lambdas (all terms active)."""
@@ -225,6 +227,7 @@ def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=48
     cfg.compat_flags = compat_flags
     cfg.penalty = Penalty(2.5, 0.0, 0.0, 0.7, 0.1)  # PenaltyConstants::setDefaultValue
     cfg.use_density = int(bool(use_density))
+    cfg.pcg_tolerance = pcg_tolerance
     return cfg
 
 

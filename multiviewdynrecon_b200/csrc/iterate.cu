@@ -1022,13 +1022,21 @@ __device__ inline void sum_two_block_partials(const InstDesc& I, uint32_t ra, ui
 }
 
 // beta = delta_k / delta_(k-1) of iteration k (0 for the first), from the
-// `nd` partials of the init / update launches
+// `nd` partials of the init / update launches; *delta receives delta_k
 template <class T>
-__device__ inline T pcg_beta(const InstDesc& I, int parity, int first, uint32_t nd) {
+__device__ inline T pcg_beta(const InstDesc& I, int parity, int first, uint32_t nd, T* delta = nullptr) {
     T dk, dkm1;
     sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDelta + (parity ^ 1), nd, &dk, &dkm1);
+    if (delta) *delta = dk;
     // a zero delta_(k-1) (the residual vanished) restarts with d = s
     return first || dkm1 == (T)0 ? (T)0 : dk / dkm1;
+}
+
+// The convergence check (BlockPCG::SolveConvergeChecked, BlockPCG.cuh:
+// 339-377) stopped this instance's PCG solve: its later iterations' kernels
+// return at once. Only with a tolerance; the flag is cleared by pcg_init.
+__device__ inline bool pcg_stopped(const InstDesc& I) {
+    return I.pcg_tol > 0.f && *(volatile const uint32_t*)&I.counts->pcg_stop != 0u;
 }
 
 // alpha = delta / d.q; a zero d.q (an exactly zero right-hand side) gives a
@@ -1054,6 +1062,7 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const InstDesc* insts) {
     using T = typename std::conditional<MIXED, double, float>::type;
     using PV = PcgVec<MIXED>;
     T part = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) I.counts->pcg_stop = 0u;
     for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < I.N; node += gridDim.x * blockDim.x) {
         T bv[6], sv[6];
 #pragma unroll
@@ -1113,18 +1122,41 @@ __device__ inline float bsr_row(const InstDesc& I, uint32_t br, uint32_t r, cons
 // d = s + beta d_prev (BlockPCG.cuh:167-181), formed once per iteration for
 // the whole vector, so that the SpMV reads its operand directly. SCALED: s is
 // r^ itself, and the float copy of d that the float SpMV reads is written too.
+// Every CTA sums the same partials in the same order, so all reach the same
+// delta_k and the same convergence decision; CTA 0 records delta_k in the
+// residual history of GN iteration `gn` and, on convergence, the stop.
 template <bool MIXED, bool SCALED>
 __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* insts, int parity, int first,
-                                                            uint32_t nd) {
+                                                            uint32_t nd, uint32_t gn, uint32_t it) {
     const InstDesc& I = insts[blockIdx.y];
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
+    if (pcg_stopped(I)) return;
     // one element per thread (the grid covers 6N), loaded before beta's sums
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     const bool has = e < 6 * I.N;
     const T* sp = SCALED ? PV::r(I) : PV::s(I);
     const T sv = has ? sp[e] : (T)0, dp = has ? PV::d(I, !parity)[e] : (T)0;
-    const T beta = pcg_beta<T>(I, parity, first, nd);
+    T dk;
+    const T beta = pcg_beta<T>(I, parity, first, nd, &dk);
+    DeviceCounts* C = I.counts;
+    double* hist = gn < kPcgHistRows ? I.pcg_hist + (size_t)gn * MVDR_PCG_HISTORY : nullptr;
+    if (blockIdx.x == 0) {
+        if (first) {
+            if (threadIdx.x == 0) C->pcg_delta0 = (double)dk;
+            if (hist)
+                for (uint32_t k = 1 + threadIdx.x; k < MVDR_PCG_HISTORY; k += blockDim.x) hist[k] = __longlong_as_double(0x7ff8000000000000ll);
+        }
+        if (hist && threadIdx.x == 0 && it < MVDR_PCG_HISTORY) hist[it] = (double)dk;
+    }
+    if (!first && I.pcg_tol > 0.f) {
+        const double d0 = first ? (double)dk : C->pcg_delta0;
+        const double tol2 = (double)I.pcg_tol * (double)I.pcg_tol;
+        if (fabs((double)dk) < tol2 * fabs(d0)) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) C->pcg_stop = it;
+            return;
+        }
+    }
     if (has) {
         const T d = sv + beta * dp;
         PV::d(I, parity)[e] = d;
@@ -1169,6 +1201,7 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_kernel(co
     const uint32_t t = threadIdx.x;
     T part = 0;
     const uint32_t r0 = blockIdx.x * kTileRows;
+    if (pcg_stopped(I)) return;
     if (r0 < I.N && index_complete(I)) {
         const uint32_t r1 = min(r0 + kTileRows, I.N);
         const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
@@ -1236,6 +1269,7 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_col_kerne
     const uint32_t t = threadIdx.x;
     T part = 0;
     const uint32_t r0 = blockIdx.x * kTileRows;
+    if (pcg_stopped(I)) return;
     if (r0 < I.N && index_complete(I)) {
         const uint32_t r1 = min(r0 + kTileRows, I.N);
         const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
@@ -1306,6 +1340,7 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
     const uint32_t t = threadIdx.x;
     double part = 0;
     const uint32_t r0 = blockIdx.x * kTileRows;
+    if (pcg_stopped(I)) return;
     if (r0 < I.N && index_complete(I)) {
         const uint32_t r1 = min(r0 + kTileRows, I.N);
         const uint32_t lr = t / (6 * kTileSplit), half = (t / 6) % kTileSplit, rr = t % 6, row = r0 + lr;
@@ -1393,6 +1428,7 @@ template <bool MIXED, bool SCALED>
 __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity, uint32_t nd,
                                                          uint32_t nq) {
     const InstDesc& I = insts[blockIdx.y];
+    if (pcg_stopped(I)) return;
     using PV = PcgVec<MIXED>;
     using T = typename PV::T;
     using T2 = typename Pair<T>::type;
@@ -1732,7 +1768,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
                                                       mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
-    if (bad_inputs(I)) return;
+    if (bad_inputs(I) || (fused && pcg_stopped(I))) return;
     TermOffsets off;
     off.load(I.counts);
     const uint32_t T = off.o[4];
@@ -1813,6 +1849,7 @@ template <bool MIXED>
 __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
                                                        int parity, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
+    if (pcg && pcg_stopped(I)) return;
     using T = typename std::conditional<MIXED, double, float>::type;
     TermOffsets off;
     off.load(I.counts);
@@ -2130,8 +2167,11 @@ static cudaError_t launch_pcg_persistent(const LaunchCfg& lc, InstDesc* d, uint3
     return e;
 }
 
-cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, cudaStream_t st) {
-    if (lc.pcg_persistent && lc.mode == MVDR_MODE_MATERIALIZED) return launch_pcg_persistent(lc, d, iters, st);
+cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, uint32_t iters, uint32_t gn,
+                       cudaStream_t st) {
+    // the convergence check runs in the launched form only
+    if (lc.pcg_persistent && lc.mode == MVDR_MODE_MATERIALIZED && lc.pcg_tol == 0.f)
+        return launch_pcg_persistent(lc, d, iters, st);
     const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
     // the update's and direction's grids cover every node / element
     const uint32_t gnode = (lc.max_nodes + kPcgNodeThreads - 1) / kPcgNodeThreads;
@@ -2147,9 +2187,9 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
         const int parity = (int)(it & 1u), first = it == 0;
         uint32_t nq;  // CTAs that store the d.q partials
         // d = s + beta d_prev, then q = A d with its d.q partials
-        if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
-        else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
-        else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode);
+        if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
+        else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
+        else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
             // J.d per term, then Jt per node (+ damping, q, d.q)
             if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
@@ -2251,9 +2291,10 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
         case MVDR_STAGE_SPMV:
             return launch_spmv(lc, d, 0, st);
         case MVDR_STAGE_DIRECTION:
-            if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
-            else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
-            else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode);
+            // (no residual history, no convergence test: an iteration past the first)
+            if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode, ~0u, 1u);
+            else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode, ~0u, 1u);
+            else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode, ~0u, 1u);
             break;
         case MVDR_STAGE_PCG_UPDATE:
             if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));

@@ -204,7 +204,9 @@ struct DeviceCounts {
     uint32_t term_offset[5];  // prefix ends of Dense, Smooth, Foreground, Feature, Cross
     uint32_t dense_view_count[MVDR_MAX_VIEWS];
     uint32_t fg_view_count[MVDR_MAX_VIEWS];
-    uint32_t reduce_ticket[4];  // unused (keeps the record's layout)
+    uint32_t pcg_stop;          // PCG iteration at which the convergence check stopped (0: running)
+    uint32_t reserved2[3];
+    double pcg_delta0;          // delta_0 of the current PCG solve
 };
 
 struct InstDesc {
@@ -339,6 +341,8 @@ struct InstDesc {
     uint32_t* pcg_bar;      // persistent PCG: this instance's barrier counter (batch-owned)
     double* energy;         // [max GN iterations + 1]
     unsigned long long* node_err_acc;  // [2N] node alignment error and weight sums, 2^-32 fixed point
+    double* pcg_hist;       // [kPcgHistRows][MVDR_PCG_HISTORY] delta_k per GN iteration
+    float pcg_tol;          // convergence tolerance (0: fixed iteration count)
 
     // capacities
     uint32_t cap_dense, cap_fg, cap_k1, cap_k2, cap_pairs, cap_seg, cap_bb;
@@ -364,7 +368,10 @@ struct LaunchCfg {
     // CTAs (non-zero only to exercise the timeout path)
     uint64_t wait_limit_ns;
     uint32_t wait_extra_arrivals;
+    float pcg_tol;  // PCG convergence tolerance (0: fixed iteration count)
 };
+
+constexpr uint32_t kPcgHistRows = 64;  // GN iterations whose PCG residuals are kept
 
 constexpr uint64_t kDefaultWaitLimitNs = 500ull * 1000 * 1000;  // a barrier step takes microseconds
 constexpr uint64_t kMaxWaitLimitNs = 10ull * 1000 * 1000 * 1000;
@@ -396,7 +403,7 @@ cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, bool materialize,
                             cudaStream_t st);
 cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d_inst, uint32_t slot, cudaStream_t st);
-cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t iters,
+cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t iters, uint32_t gn,
                        cudaStream_t st);
 cudaError_t launch_update(const LaunchCfg& lc, InstDesc* d_inst, cudaStream_t st);
 cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, int stage, cudaStream_t st);

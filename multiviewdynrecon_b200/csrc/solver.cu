@@ -180,6 +180,8 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
     I.node_err_acc = a.take<unsigned long long>(2 * N);
+    I.pcg_hist = a.take<double>((size_t)kPcgHistRows * MVDR_PCG_HISTORY);
+    I.pcg_tol = lc.pcg_tol;
     if (max_tp) {  // device-side feature selection
         I.fp_keep = a.take<uint32_t>(max_tp);
         I.fp_chosen = a.take<ushort4>(max_tp);
@@ -210,6 +212,8 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
         return fail(MVDR_EINVAL, "unknown precision");
     if (cfg->mode != MVDR_MODE_MATERIALIZED && cfg->mode != MVDR_MODE_MATRIX_FREE)
         return fail(MVDR_EINVAL, "unknown mode");
+    if (!(cfg->pcg_tolerance >= 0.0f && cfg->pcg_tolerance < 1.0f))
+        return fail(MVDR_EINVAL, "pcg_tolerance must be in [0, 1)");
     int dev = 0;
     CU(cudaGetDevice(&dev));
     cudaDeviceProp prop;
@@ -251,6 +255,7 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     lc.precision = cfg->precision;
     lc.mode = cfg->mode;
     lc.use_density = cfg->use_density ? 1 : 0;
+    lc.pcg_tol = cfg->pcg_tolerance;
     lc.sm_count = prop.multiProcessorCount;
 
     const size_t smem_seg = (size_t)lc.cap_seg * 4;
@@ -631,7 +636,7 @@ static int enqueue_iteration(Batch& b, uint32_t iter, uint32_t pcg, cudaStream_t
     CU(launch_eval_terms(b.lc, b.d_inst, lam, st));
     CU(launch_energy(b.lc, b.d_inst, std::min<uint32_t>(iter, 63), st));
     CU(launch_assemble(b.lc, b.d_inst, lam, b.cfg.mode == MVDR_MODE_MATERIALIZED, st));
-    CU(launch_pcg(b.lc, b.d_inst, lam, pcg, st));
+    CU(launch_pcg(b.lc, b.d_inst, lam, pcg, iter, st));
     CU(launch_update(b.lc, b.d_inst, st));
     return MVDR_OK;
 }
@@ -760,6 +765,10 @@ static int get_array(Batch& b, uint32_t inst, int which, void* dst, size_t cap, 
         case MVDR_ARRAY_DENSITY_JACOBIAN:
             if (!I.density_jr) return fail(MVDR_EINVAL, "the density term is off");
             return copy_out(dst, I.density_jr, 32 * (size_t)c.dense_terms, cap, written);
+        case MVDR_ARRAY_PCG_RESIDUALS: {
+            const size_t rows = std::min<size_t>(b.gn_iter, kPcgHistRows);
+            return copy_out(dst, I.pcg_hist, sizeof(double) * MVDR_PCG_HISTORY * rows, cap, written);
+        }
         case MVDR_ARRAY_FEATURE_TERMS: {
             // (target, reference) per term, interleaved on the host
             const size_t n = c.feature_terms;
@@ -1085,6 +1094,9 @@ int mvdr_batch_enqueue_stage(mvdr_batch* b, int stage, void* stream) {
         return fail(MVDR_EINVAL, "the matrix-free stage needs the matrix-free mode");
     if (stage == MVDR_STAGE_SCALE && (bb.cfg.mode != MVDR_MODE_MATERIALIZED || bb.cfg.precision != MVDR_PRECISION_MIXED))
         return fail(MVDR_EINVAL, "the scaling stage needs mixed precision in the materialised mode");
+    // a stage runs in full even when the last solve's convergence check stopped its PCG
+    for (uint32_t i = 0; i < bb.B; ++i)
+        CU(cudaMemsetAsync(&bb.host[i].counts->pcg_stop, 0, sizeof(uint32_t), (cudaStream_t)stream));
     CU(launch_stage(bb.lc, bb.d_inst, penalty_for(bb.cfg, 0), stage, (cudaStream_t)stream));
     return MVDR_OK;
 }

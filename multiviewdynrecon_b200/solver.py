@@ -34,7 +34,7 @@ ARRAY_SPEC = {
     abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
     abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
     abi.ARRAY_NODE_SE3: (np.float32, 8), abi.ARRAY_DENSITY_JACOBIAN: (np.float32, 8),
-    abi.ARRAY_FEATURE_TERMS: (np.float32, 8),
+    abi.ARRAY_FEATURE_TERMS: (np.float32, 8), abi.ARRAY_PCG_RESIDUALS: (np.float64, abi.MVDR_PCG_HISTORY),
 }
 
 

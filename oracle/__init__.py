@@ -102,6 +102,8 @@ def lib():
         L.orc_p2p_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_cholesky_inverse.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_render_solver_maps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        L.orc_pcg_history.restype = C.c_uint32
+        L.orc_pcg_history.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
         L.orc_feature_terms.restype = C.c_uint32
         L.orc_feature_terms.argtypes = [C.c_void_p] * 5
         L.orc_forward_warp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32] + [C.c_void_p] * 6 + \
@@ -131,7 +133,7 @@ _ARRAY_SPEC = {
     abi.ARRAY_PRECONDITIONER: (np.float32, 36), abi.ARRAY_OFFDIAG_BLOCKS: (np.float32, 36),
     abi.ARRAY_BINBLOCK_DATA: (np.float32, 1), abi.ARRAY_INCREMENT: (np.float32, 6),
     abi.ARRAY_NODE_SE3: (np.float32, 8), abi.ARRAY_DENSITY_JACOBIAN: (np.float32, 8),
-    abi.ARRAY_FEATURE_TERMS: (np.float32, 8),
+    abi.ARRAY_FEATURE_TERMS: (np.float32, 8), abi.ARRAY_PCG_RESIDUALS: (np.float64, abi.MVDR_PCG_HISTORY),
 }
 REAL_ARRAYS = {abi.ARRAY_DIAG_BLOCKS, abi.ARRAY_JTR, abi.ARRAY_PRECONDITIONER, abi.ARRAY_OFFDIAG_BLOCKS,
                abi.ARRAY_BINBLOCK_DATA, abi.ARRAY_INCREMENT, abi.ARRAY_NODE_SE3}
@@ -163,6 +165,13 @@ class Oracle:
             self.h = None
 
     # stages
+    def pcg_history(self):
+        """delta at the start of each PCG iteration of the last PCG solve."""
+        n = lib().orc_pcg_history(self.h, None, 0)
+        out = np.zeros(n, np.float64)
+        lib().orc_pcg_history(self.h, _p(out), n)
+        return out
+
     def feature_terms(self):
         """The feature terms (bound, or selected from raw pixel pairs):
         target (T, 4), reference (T, 4), knn (T, 4) uint16, weights (T, 4)."""

@@ -291,6 +291,7 @@ struct Oracle {
 
     // current warp field, kept in double; rounded to float at each update
     std::vector<DQ<double>> se3d;
+    std::vector<double> pcg_history;  // delta at the start of each PCG iteration of the last solve
     int gn_iter = 0;
 
     // compaction
@@ -1200,7 +1201,15 @@ struct Oracle {
         r = bb;
         precond(r, d);
         R delta = vdot(r, d);
+        const R delta0 = delta;
+        const double tol2 = (double)cfg.pcg_tolerance * (double)cfg.pcg_tolerance;
+        pcg_history.clear();
         for (u32 it = 0; it < iters; ++it) {
+            // SolveConvergeChecked (BlockPCG.cuh:339-377): delta at the start of
+            // each iteration against tol^2 delta_0
+            pcg_history.push_back((double)delta);
+            if (it > 0 && cfg.pcg_tolerance > 0.0f && std::fabs((double)delta) < tol2 * std::fabs((double)delta0))
+                break;
             spmv<R>(d, q);
             const R dq = vdot(d, q);
             // a zero d.q (a right-hand side that is exactly zero) gives a zero
@@ -1298,6 +1307,15 @@ void* orc_create(const mvdr_config* cfg, const mvdr_inputs* host_inputs, int fp6
 void orc_destroy(void* h) { delete (Oracle*)h; }
 
 void orc_build_index(void* h) { ((Oracle*)h)->build_index(); }
+
+/* delta at the start of each PCG iteration of the last PCG solve (delta_0
+ * first); returns how many, copying at most `cap`. */
+uint32_t orc_pcg_history(void* h, double* out, uint32_t cap) {
+    const Oracle* o = (const Oracle*)h;
+    const uint32_t n = (uint32_t)o->pcg_history.size();
+    for (uint32_t k = 0; k < n && k < cap; ++k) out[k] = o->pcg_history[k];
+    return n;
+}
 
 /* The feature terms as bound or selected from raw pixel pairs: returns their
  * count and, when the pointers are not NULL, copies target, reference,
