@@ -227,7 +227,15 @@ def algorithmic_bytes(counts, N, mixed=True, materialized=True):
         spmv = 36 * elem * (N + P) + 8 * (N + 2 * P) + 4 * (N + 1) + 2 * 6 * elem * N
         direction = 3 * 6 * elem * N          # s and d_prev read, d written
         pcg_update = 7 * 6 * elem * N + precond  # x rw, r rw, d, q read, s written
+    # index build (once per solve), the per-unit bytes of a radix-sort build:
+    # the node -> term pairs (6 B) read and written once per 8-bit pass over
+    # ceil(log2 N) key bits, their scan; the node-pair pairs (8 B) over
+    # 2 ceil(log2 N) key bits; the symmetric pass over 2P entries of 12 B
+    lg = max(1, math.ceil(math.log2(max(N, 2))))
+    K1, K2 = counts.node2term_entries, counts.nodepair_entries
+    index = (6 * K1 * 2 * math.ceil(lg / 8) + 8 * K1 + 8 * K2 * 2 * math.ceil(2 * lg / 8) + 2 * (2 * P) * 12)
     return {
+        "index": index,
         "terms": 122 * Td + 86 * Tf + 29 * Ts + 72 * (Tp + Tc) + 32 * N,
         "diag": term_data + 4 * counts.node2term_entries + 144 * N + 36 * elem * N + 24 * N + precond,
         "offdiag": term_data + 4 * counts.nodepair_entries + 12 * P + 36 * elem * P,
@@ -477,6 +485,21 @@ def run_ours(args, rank, world, dist):
                                   "form": f"plain FP32, {B} instances per launch, CUDA graph (as the headline)"}
         pb.close()
 
+    # the PCG residual history of instance 0's last timed solve: delta_k /
+    # delta_0 at the start of every PCG iteration, first and last GN iteration
+    pcg_history = None
+    with torch.cuda.stream(stream):
+        bind_all()
+        batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+        stream.synchronize()
+    hist = batch.instance(0).get_array(abi.ARRAY_PCG_RESIDUALS)
+    if len(hist):
+        def ratios(row):
+            row = row[np.isfinite(row)]
+            return [float("%.3g" % (v / row[0])) for v in row] if len(row) else []
+        pcg_history = {"delta_over_delta0_gn_first": ratios(hist[0]), "delta_over_delta0_gn_last": ratios(hist[-1]),
+                       "instance": "0 of the timed batch", "iterations": args.pcg}
+
     # accuracy of the timed configuration: instance 0's solve, every
     # Gauss-Newton increment against the FP64 oracle (after the timed region)
     accuracy = None
@@ -495,7 +518,8 @@ def run_ours(args, rank, world, dist):
                 spmv_tile=dict(spmv_tile_desc(spmv_shape),
                                candidates_ms={spmv_tile_label(sh): round(t, 5)
                                               for sh, t in zip(abi.SPMV_SHAPES, spmv_shape_ms)}),
-                roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base, accuracy=accuracy)
+                roofline=roofline, e2e=e2e, plain=plain, counts=counts, base=base, accuracy=accuracy,
+                pcg_history=pcg_history)
 
 
 def first_increment_errors(scenes, cfg_for, gpu_increments, pcg, threads):
@@ -960,6 +984,7 @@ def main():
             "speedup_vs_plain_fp32_batched": (round(r["value"] / r["plain"]["batched_graph"]["value"], 3)
                                               if r["plain"] else None),
             "accuracy": r["accuracy"],
+            "pcg_history": r["pcg_history"],
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
