@@ -38,6 +38,15 @@ ARRAY_SPEC = {
 }
 
 
+def _check_image_size(config, ds):
+    """The library reads every map as image_height rows of image_width (or
+    pitch) elements and cannot see a buffer's size: maps of another size would
+    be read past their end."""
+    if ds.image_size != (config.image_width, config.image_height):
+        raise ValueError(f"scene maps are {ds.image_size[0]}x{ds.image_size[1]}, the solver was created for "
+                         f"{config.image_width}x{config.image_height}")
+
+
 def _stream_handle(stream=None):
     s = stream if stream is not None else torch.cuda.current_stream()
     return C.c_void_p(s.cuda_stream)
@@ -50,6 +59,7 @@ class DeviceScene:
         self.tensors = {}
         self.device = device
         self.pin = pin
+        self.image_size = (scene.width, scene.height)
         arrays = []
 
         def collect(name, arr):
@@ -111,6 +121,7 @@ class NonRigidSolver:
     # SetSolverInput
     def set_solver_input(self, scene, stream=None):
         ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene, density=bool(self.config.use_density))
+        _check_image_size(self.config, ds)
         self._inputs = ds
         self.num_nodes = ds.inputs.num_nodes
         check(lib().mvdr_set_inputs(self.h, C.byref(ds.inputs), _stream_handle(stream)))
@@ -118,6 +129,7 @@ class NonRigidSolver:
 
     def set_solver_input_host(self, host_scene, stream=None):
         """`host_scene`: a DeviceScene built with pin=True (host pointers)."""
+        _check_image_size(self.config, host_scene)
         self._inputs = host_scene
         self.num_nodes = host_scene.inputs.num_nodes
         check(lib().mvdr_set_inputs_host(self.h, C.byref(host_scene.inputs), _stream_handle(stream)))
@@ -263,11 +275,13 @@ class BatchSolver:
 
     def set_input(self, i, scene, stream=None):
         ds = scene if isinstance(scene, DeviceScene) else DeviceScene(scene, density=bool(self.config.use_density))
+        _check_image_size(self.config, ds)
         self._inputs[i] = ds
         check(lib().mvdr_batch_set_inputs(self.h, i, C.byref(ds.inputs), _stream_handle(stream)))
         return ds
 
     def set_input_host(self, i, host_scene, stream=None):
+        _check_image_size(self.config, host_scene)
         self._inputs[i] = host_scene
         check(lib().mvdr_batch_set_inputs_host(self.h, i, C.byref(host_scene.inputs), _stream_handle(stream)))
 

@@ -77,9 +77,10 @@ def test_stop_equals_fixed_count(oracle_mod, kind, precision):
 
 
 def test_instances_stop_independently():
-    """Two instances of a batch reach the tolerance at their own iterations;
-    each equals its single-instance solve, inside a replayed graph too."""
-    a, b = small_scene("torso"), small_scene("torso_rigid")
+    """Two instances of a batch (both 160x120, as one batch needs) reach the
+    tolerance at their own iterations; each equals its single-instance
+    solve, inside a replayed graph too."""
+    a, b = small_scene("torso"), small_scene("sphere")
     caps = dict(max_nodes=max(a.num_nodes, b.num_nodes), max_views=3, width=a.width, height=a.height,
                 use_foreground=False, use_feature=True, use_cross_view=True,
                 max_surfels=max(a.num_surfels, b.num_surfels),
