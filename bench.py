@@ -181,11 +181,14 @@ def measured_traffic(args):
     path = os.path.join(ROOT, PROFILE_SPMV)
     if not default or not os.path.exists(path):
         return None, None
+    import re
     with open(path) as f:
         for line in f:
             if line.startswith("| DRAM read + write |"):
-                parts = line.split("|")[2].replace("MB", "").split("+")
-                return int(sum(float(p) for p in parts) * 1e6), PROFILE_SPMV
+                # "R + W MB ...": the first two numbers of the cell
+                nums = re.findall(r"[0-9]+(?:\.[0-9]+)?", line.split("|")[2])
+                if len(nums) >= 2:
+                    return int((float(nums[0]) + float(nums[1])) * 1e6), PROFILE_SPMV
     return None, None
 
 

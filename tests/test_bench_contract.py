@@ -42,3 +42,14 @@ def test_reference_arm_other_ranks_exit_without_output():
     p = run_bench({"RANK": "1", "WORLD_SIZE": "2"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert not [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_committed_spmv_profile_parses():
+    """The headline line's roofline.traffic comes from the committed ncu
+    summary; its DRAM row must parse to the read + write bytes."""
+    import argparse
+    sys.path.insert(0, ROOT)
+    import bench
+    a = argparse.Namespace(batch=16, nodes=4096, width=640, height=480, precision="mixed", mode="materialized")
+    traffic, src = bench.measured_traffic(a)
+    assert src is not None and 1e7 < traffic < 1e9
