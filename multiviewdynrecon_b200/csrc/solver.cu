@@ -1094,9 +1094,11 @@ int mvdr_batch_enqueue_stage(mvdr_batch* b, int stage, void* stream) {
         return fail(MVDR_EINVAL, "the matrix-free stage needs the matrix-free mode");
     if (stage == MVDR_STAGE_SCALE && (bb.cfg.mode != MVDR_MODE_MATERIALIZED || bb.cfg.precision != MVDR_PRECISION_MIXED))
         return fail(MVDR_EINVAL, "the scaling stage needs mixed precision in the materialised mode");
-    // a stage runs in full even when the last solve's convergence check stopped its PCG
-    for (uint32_t i = 0; i < bb.B; ++i)
-        CU(cudaMemsetAsync(&bb.host[i].counts->pcg_stop, 0, sizeof(uint32_t), (cudaStream_t)stream));
+    // a stage runs in full even when the last solve's convergence check
+    // stopped its PCG (the flag is read only with a tolerance)
+    if (bb.cfg.pcg_tolerance > 0.0f)
+        for (uint32_t i = 0; i < bb.B; ++i)
+            CU(cudaMemsetAsync(&bb.host[i].counts->pcg_stop, 0, sizeof(uint32_t), (cudaStream_t)stream));
     CU(launch_stage(bb.lc, bb.d_inst, penalty_for(bb.cfg, 0), stage, (cudaStream_t)stream));
     return MVDR_OK;
 }
