@@ -195,14 +195,13 @@ def measured_traffic(args):
 def spmv_tile_desc(shape):
     """The SpMV tile shape (rows, split, form) in words."""
     rows, split, form = shape
-    lower = {0: "row reads, shared-memory exchange", 1: "column reads",
-             2: "16-byte vector reads of whole blocks, fixed-table exchange"}[form]
-    return {"rows_per_cta": rows, "threads_per_row": 6 * split, "lower_blocks": lower}
+    return {"rows_per_cta": rows, "threads_per_row": 6 * split,
+            "lower_blocks": "row reads, shared-memory exchange" if form == 0 else "column reads"}
 
 
 def spmv_tile_label(shape):
     rows, split, form = shape
-    return f"{('row', 'col', 'vec')[form]}{rows}x{6 * split}"
+    return f"{'row' if form == 0 else 'col'}{rows}x{6 * split}"
 
 
 def algorithmic_bytes(counts, N, mixed=True, materialized=True):

@@ -665,7 +665,7 @@ MVDR_API int mvdr_batch_autotune(mvdr_batch* batch, void* stream, double* times_
 /* Use SpMV tile shape `shape` (0 .. MVDR_NUM_SPMV_SHAPES - 1, the
  * autotuner's candidate order) for later solves of this batch, in place of
  * the autotuner's choice; drops the captured graphs. */
-#define MVDR_NUM_SPMV_SHAPES 14u
+#define MVDR_NUM_SPMV_SHAPES 12u
 MVDR_API int mvdr_batch_set_spmv_shape(mvdr_batch* batch, uint32_t shape);
 /* on != 0: run each PCG solve of a materialised batch as one persistent
  * cooperative launch (the CTAs split among the instances, each instance's

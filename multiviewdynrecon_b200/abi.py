@@ -26,7 +26,7 @@ COMPAT_REF_FOREGROUND_FRAME = 2
 # the autotuner's order. Form 0 reads a lower block's row and exchanges the
 # column sums through shared memory; form 1 reads its column.
 SPMV_SHAPES = [(16, 2, 0), (8, 2, 0), (16, 1, 0), (32, 1, 0), (16, 3, 0), (8, 4, 0), (32, 2, 0),
-               (16, 1, 1), (32, 1, 1), (8, 2, 1), (16, 2, 1), (4, 4, 1), (16, 1, 2), (32, 1, 2)]
+               (16, 1, 1), (32, 1, 1), (8, 2, 1), (16, 2, 1), (4, 4, 1)]
 NUM_SPMV_SHAPES = len(SPMV_SHAPES)
 
 (ARRAY_DENSE_PIXELS, ARRAY_DENSE_KNN, ARRAY_DENSE_KNN_WEIGHT, ARRAY_FOREGROUND_PIXELS, ARRAY_NODE2TERM_OFFSET,

@@ -1160,8 +1160,7 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
     if (has) {
         const T d = sv + beta * dp;
         PV::d(I, parity)[e] = d;
-        // the float copy of the scaled path: 8 floats per node (16-byte rows)
-        if constexpr (SCALED) I.df[kDfStride * (e / 6) + e % 6] = (float)d;
+        if constexpr (SCALED) I.df[e] = (float)d;
     }
 }
 
@@ -1177,9 +1176,8 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
 // sequential (position, column) entries, so many loads stay in flight. The
 // stored transpose of a lower block belongs to a row of this or an earlier
 // tile, so it is usually still in L2.
-const SpmvShape kSpmvShapes[kNumSpmvShapes] = {{16, 2, 0}, {8, 2, 0},  {16, 1, 0}, {32, 1, 0}, {16, 3, 0},
-                                                {8, 4, 0},  {32, 2, 0}, {16, 1, 1}, {32, 1, 1}, {8, 2, 1},
-                                                {16, 2, 1}, {4, 4, 1},  {16, 1, 2}, {32, 1, 2}};
+const SpmvShape kSpmvShapes[kNumSpmvShapes] = {{16, 2, 0}, {8, 2, 0},  {16, 1, 0}, {32, 1, 0}, {16, 3, 0}, {8, 4, 0},
+                                                {32, 2, 0}, {16, 1, 1}, {32, 1, 1}, {8, 2, 1},  {16, 2, 1}, {4, 4, 1}};
 
 template <class V> struct Pair;
 template <> struct Pair<double> { using type = double2; };
@@ -1356,12 +1354,12 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
             for (uint32_t b = rb + half; b < re; b += kTileSplit) {
                 const uint2 ent = I.bsr_ent[b];
                 const float* blk = store + 36 * (size_t)(ent.x & ~kTransposedBlock);
-                const float2* x2 = reinterpret_cast<const float2*>(xf + kDfStride * (size_t)ent.y);
+                const float2* x2 = reinterpret_cast<const float2*>(xf + 6 * (size_t)ent.y);
                 const bool lower = (ent.x & kTransposedBlock) != 0;
                 if (kForm == 0 && lower) {
                     const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
                     const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
-                    const float xr = xf[kDfStride * (size_t)ent.y + rr];
+                    const float xr = xf[6 * (size_t)ent.y + rr];
                     col_acc[0] += a01.x * xr; col_acc[1] += a01.y * xr; col_acc[2] += a23.x * xr;
                     col_acc[3] += a23.y * xr; col_acc[4] += a45.x * xr; col_acc[5] += a45.y * xr;
                 } else {
@@ -1418,102 +1416,6 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
     }
     store_block_partial<double>(I, kRegDq, part);
 }
-
-// SpMV of the scaled operator, vector form: the six threads of a block row
-// read each stored block as 16-byte vectors, thread k the floats 4k..4k+3
-// and, for k < 3, 24+4k..24+4k+3, so that a row's threads sweep the block in
-// two contiguous loads (the row forms read it as 24-byte rows, three 8-byte
-// loads each). A thread's elements have fixed (row, column) positions: it
-// keeps up to four partial row sums for upper blocks and four partial column
-// sums for lower ones (read transposed), and the row's threads combine them
-// through shared memory at the end by a fixed table, in a fixed order. The
-// direction is read as 16 + 8 bytes from its padded float copy.
-__constant__ unsigned char kV4RowOut[6][2][2] = {  // row r: (thread, slot) of its two upper partials
-    {{0, 0}, {1, 0}}, {{1, 1}, {2, 0}}, {{3, 0}, {4, 0}}, {{4, 1}, {5, 0}}, {{0, 2}, {1, 2}}, {{1, 3}, {2, 2}}};
-__constant__ unsigned char kV4ColOut[6][4][2] = {  // column c: (thread, m) of its four lower partials
-    {{0, 0}, {3, 0}, {1, 2}, {4, 2}}, {{0, 1}, {3, 1}, {1, 3}, {4, 3}}, {{0, 2}, {3, 2}, {2, 0}, {5, 0}},
-    {{0, 3}, {3, 3}, {2, 1}, {5, 1}}, {{1, 0}, {4, 0}, {2, 2}, {5, 2}}, {{1, 1}, {4, 1}, {2, 3}, {5, 3}}};
-
-template <uint32_t kTileRows>
-__global__ void __launch_bounds__(6 * kTileRows) pcg_spmv_scaled_v4_kernel(const InstDesc* insts, int parity) {
-    static_assert((6 * kTileRows) % 32 == 0, "whole warps");
-    __shared__ float s_part[kTileRows][6][8];  // per thread: 4 row partials, 4 column partials
-    const InstDesc& I = insts[blockIdx.y];
-    if (pcg_stopped(I)) return;
-    const float* store = I.bsr_s;
-    const float* xf = I.df;
-    const double* xd = PcgVec<true>::d(I, parity);
-    const uint32_t t = threadIdx.x;
-    double part = 0;
-    const uint32_t r0 = blockIdx.x * kTileRows;
-    if (r0 < I.N && index_complete(I)) {
-        const uint32_t lr = t / 6, k = t % 6, row = r0 + lr;
-        const bool computes = row < I.N;
-        // the thread's element pattern: start column cs of its first vector,
-        // split (its four elements span two rows: cs = 4), second vector (k < 3)
-        const uint32_t k3 = k % 3;
-        const bool split = k3 == 1, second = k < 3;
-        const uint32_t ra = (4 * k) / 6;  // row of the first element
-        float u0 = 0.f, u1 = 0.f, u2 = 0.f, u3 = 0.f;  // upper: rows ra, ra+1 (split), ra+4, ra+5 (split)
-        float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;  // lower: columns (cs + m) % 6
-        if (computes) {
-            const uint32_t rb = I.blkrow_offset[row] + row + 1, re = I.blkrow_offset[row + 1] + row + 1;
-#pragma unroll 2
-            for (uint32_t b = rb; b < re; ++b) {
-                const uint2 ent = I.bsr_ent[b];
-                const float4* blk = reinterpret_cast<const float4*>(store + 36 * (size_t)(ent.x & ~kTransposedBlock));
-                const float4* xv = reinterpret_cast<const float4*>(xf + kDfStride * (size_t)ent.y);
-                const float4 f1 = blk[k];
-                const float4 f2 = second ? blk[6 + k] : make_float4(0.f, 0.f, 0.f, 0.f);
-                const float4 x03 = xv[0];
-                const float2 x45 = *reinterpret_cast<const float2*>(xv + 1);
-                if (ent.x & kTransposedBlock) {
-                    // lower: element (r, c) adds a x_j[r] to column c; x_j at
-                    // the elements' rows ra (ra + 1 for the split pair) and ra + 4
-                    const float xa = ra == 0 ? x03.x : ra == 1 ? x03.y : ra == 2 ? x03.z : x03.w;
-                    const float xb = ra == 0 ? x03.y : ra == 1 ? x03.z : x03.w;  // row ra + 1 (split threads)
-                    const float xc = ra == 0 ? x45.x : x45.y;                   // row ra + 4 (k < 3)
-                    const float xd2 = x45.y;                                    // row ra + 5 (k = 1)
-                    l0 += f1.x * xa + f2.x * xc;
-                    l1 += f1.y * xa + f2.y * xc;
-                    l2 += f1.z * (split ? xb : xa) + f2.z * (split ? xd2 : xc);
-                    l3 += f1.w * (split ? xb : xa) + f2.w * (split ? xd2 : xc);
-                } else {
-                    // upper: x_j at the elements' columns (cs + m) % 6
-                    const float s0 = k3 == 0 ? x03.x : k3 == 1 ? x45.x : x03.z;
-                    const float s1 = k3 == 0 ? x03.y : k3 == 1 ? x45.y : x03.w;
-                    const float s2 = k3 == 0 ? x03.z : k3 == 1 ? x03.x : x45.x;
-                    const float s3 = k3 == 0 ? x03.w : k3 == 1 ? x03.y : x45.y;
-                    const float pa = f1.x * s0 + f1.y * s1, pb = f1.z * s2 + f1.w * s3;
-                    const float qa = f2.x * s0 + f2.y * s1, qb = f2.z * s2 + f2.w * s3;
-                    u0 += split ? pa : pa + pb;
-                    u1 += split ? pb : 0.f;
-                    u2 += split ? qa : qa + qb;
-                    u3 += split ? qb : 0.f;
-                }
-            }
-            float* mine = s_part[lr][k];
-            mine[0] = u0; mine[1] = u1; mine[2] = u2; mine[3] = u3;
-            mine[4] = l0; mine[5] = l1; mine[6] = l2; mine[7] = l3;
-        }
-        __syncthreads();
-        if (computes) {
-            // thread k outputs q^_i[k]: its two upper partials (row k) and its
-            // four lower partials (column k), in a fixed order
-            float acc = s_part[lr][kV4RowOut[k][0][0]][kV4RowOut[k][0][1]] +
-                        s_part[lr][kV4RowOut[k][1][0]][kV4RowOut[k][1][1]];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc += s_part[lr][kV4ColOut[k][q][0]][4 + kV4ColOut[k][q][1]];
-            const size_t e = 6 * (size_t)row + k;
-            const double dv = xd[e];
-            const double qv = dv + (double)acc;
-            PcgVec<true>::q(I)[e] = qv;
-            part += dv * qv;
-        }
-    }
-    store_block_partial<double>(I, kRegDq, part);
-}
-
 
 // blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): alpha = delta / d.q,
 // x += alpha d, r -= alpha q, s = M^-1 r, delta_new = r.s (beta follows in
@@ -1726,7 +1628,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
             for (uint32_t e = c * nt + tid; e < 6 * I.N; e += nc * nt) {
                 const T dv = sv[e] + beta * dprev[e];
                 dcur[e] = dv;
-                if constexpr (MIXED) I.df[kDfStride * (e / 6) + e % 6] = (float)dv;
+                if constexpr (MIXED) I.df[e] = (float)dv;
             }
         }
         if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
@@ -1745,7 +1647,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
                 for (uint32_t b = rb; b < re; ++b) {
                     const uint2 ent = I.bsr_ent[b];
                     const float* blk = I.bsr_s + 36 * (size_t)(ent.x & ~kTransposedBlock);
-                    const float2* x2 = reinterpret_cast<const float2*>(I.df + kDfStride * (size_t)ent.y);
+                    const float2* x2 = reinterpret_cast<const float2*>(I.df + 6 * (size_t)ent.y);
                     float av[6];
                     if (ent.x & kTransposedBlock) {
 #pragma unroll
@@ -2344,11 +2246,6 @@ static void spmv_scaled_launch(const LaunchCfg& lc, InstDesc* d, int parity, cud
     MVDR_LAUNCH(kernel, grid2((lc.max_nodes + R - 1) / R, lc.B), 6 * S * R, 0, st, d, parity);
 }
 
-template <uint32_t R>
-static void spmv_scaled_v4_launch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
-    MVDR_LAUNCH(pcg_spmv_scaled_v4_kernel<R>, grid2((lc.max_nodes + R - 1) / R, lc.B), 6 * R, 0, st, d, parity);
-}
-
 // the shapes of kSpmvShapes for the scaled operator
 static void spmv_scaled_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st) {
     switch (lc.spmv_shape) {
@@ -2363,8 +2260,6 @@ static void spmv_scaled_dispatch(const LaunchCfg& lc, InstDesc* d, int parity, c
         case 9: spmv_scaled_launch<8, 2, 1>(lc, d, parity, st); break;
         case 10: spmv_scaled_launch<16, 2, 1>(lc, d, parity, st); break;
         case 11: spmv_scaled_launch<4, 4, 1>(lc, d, parity, st); break;
-        case 12: spmv_scaled_v4_launch<16>(lc, d, parity, st); break;
-        case 13: spmv_scaled_v4_launch<32>(lc, d, parity, st); break;
         default: spmv_scaled_launch<16, 2, 0>(lc, d, parity, st); break;
     }
 }

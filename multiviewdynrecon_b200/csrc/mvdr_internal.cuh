@@ -315,7 +315,7 @@ struct InstDesc {
     // float, row-major (element (r, k) at 6 r + k), at the half-storage block
     // positions of bsr_d
     float* bsr_s;
-    float* df;              // [8N] the PCG direction of the scaled system in float, 8 floats per node
+    float* df;              // [6N] the PCG direction of the scaled system in float
     // per entry of the full (symmetric) block-row layout, row i: the diagonal,
     // then its symmetric keys in order [N + 2P cap]
     // (half-storage block | kTransposedBlock when read transposed, block column)
@@ -392,10 +392,7 @@ cudaError_t set_index_smem_limits(size_t seg_bytes);
 struct SpmvShape {
     uint32_t rows, split, form;
 };
-constexpr int kNumSpmvShapes = 14;
-// floats per node of the float direction copy of the scaled PCG (six used,
-// padded so that a node's values are one 16-byte and one 8-byte load)
-constexpr uint32_t kDfStride = 8;
+constexpr int kNumSpmvShapes = 12;
 extern const SpmvShape kSpmvShapes[kNumSpmvShapes];
 // one PCG SpMV (q = A d, d.q) with the shape lc.spmv_shape
 cudaError_t launch_spmv(const LaunchCfg& lc, InstDesc* d, int parity, cudaStream_t st);
