@@ -797,7 +797,8 @@ def run_extra_workload(args):
         caps = None
         cfg_for = lambda sc: abi.make_config(sc)  # noqa: E731
         modes = [("materialized", abi.MODE_MATERIALIZED, abi.PRECISION_MIXED),
-                 ("matrix_free", abi.MODE_MATRIX_FREE, abi.PRECISION_MIXED)]
+                 ("matrix_free", abi.MODE_MATRIX_FREE, abi.PRECISION_MIXED),
+                 ("matrix_free_recompute", abi.MODE_MATRIX_FREE, abi.PRECISION_MIXED)]
     gen_s = time.perf_counter() - t0
     dev = [DeviceScene(sc) for sc in scenes]
     B = len(scenes)
@@ -806,9 +807,14 @@ def run_extra_workload(args):
             "gn": gn, "pcg": pcg, "generation_s": round(gen_s, 1), "modes": {}}
     incs = None
     for name, mode, prec in modes:
-        cfg = (abi.make_config(None, precision=prec, mode=mode, **caps) if caps
-               else abi.make_config(scenes[0], precision=prec, mode=mode))
+        rec = name.endswith("_recompute")
+        cfg = (abi.make_config(None, precision=prec, mode=mode, recompute_jacobians=rec, **caps) if caps
+               else abi.make_config(scenes[0], precision=prec, mode=mode, recompute_jacobians=rec))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         batch = BatchSolver(cfg, B)
+        torch.cuda.synchronize()
+        solver_mb = round((free0 - torch.cuda.mem_get_info()[0]) / 2**20, 1)
 
         def bind():
             for i, ds in enumerate(dev):
@@ -819,7 +825,8 @@ def run_extra_workload(args):
             shape = batch.autotune(stream=stream)[0] if mode == abi.MODE_MATERIALIZED else None
             ms = time_solves(lambda: (bind(), batch.solve(gn, pcg, use_graph=True, stream=stream)), args.steps,
                              max(3, args.warmup), stream)
-            entry = {"solves_per_s": round(B / (ms / 1e3), 3), "ms_per_step": round(ms, 3)}
+            entry = {"solves_per_s": round(B / (ms / 1e3), 3), "ms_per_step": round(ms, 3),
+                     "solver_device_mb": solver_mb}
             if mode == abi.MODE_MATERIALIZED:
                 bind()
                 batch.solve(gn, pcg, use_graph=False, stream=stream)

@@ -177,6 +177,13 @@ typedef struct mvdr_config {
      * default) runs the fixed iteration count (BlockPCG::Solve). The launched
      * PCG form only: with a tolerance the persistent form is not used. */
     float pcg_tolerance;
+    /* Matrix-free mode only: the J.d / Jt.y products of every PCG iteration
+     * evaluate each dense and foreground pixel term again from the maps and
+     * the warp field (as ApplyJtJMatrixFreeIndexed.cu:222-348 does) instead
+     * of reading the 32-byte record the term evaluation stored. The records
+     * are still kept, for the preconditioner's diagonal blocks, so this saves
+     * no memory; it trades their reads for the evaluation's arithmetic. */
+    int32_t recompute_jacobians;
 } mvdr_config;
 
 /* Per-view inputs: the rendered solver maps (Renderer::SolverMaps,

@@ -71,6 +71,7 @@ class Config(C.Structure):
         ("use_foreground", C.c_int32), ("use_feature", C.c_int32), ("use_cross_view", C.c_int32),
         ("use_elastic_penalty", C.c_int32), ("num_global_iterations", C.c_int32), ("compat_flags", C.c_uint32),
         ("penalty", Penalty), ("use_density", C.c_int32), ("pcg_tolerance", C.c_float),
+        ("recompute_jacobians", C.c_int32),
     ]
 
 
@@ -181,7 +182,7 @@ def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=48
                 mode=MODE_MATERIALIZED, use_foreground=None, use_feature=None, use_cross_view=None,
                 max_surfels=None, max_feature_terms=None, max_cross_terms=None, elastic=True,
                 num_global_iterations=1 << 20, compat_flags=0, node_radius=0.025, use_density=None,
-                pcg_tolerance=0.0):
+                pcg_tolerance=0.0, recompute_jacobians=False):
     """Configuration for a scene (or explicit capacities). With the elastic
     schedule on and num_global_iterations large, every iteration uses the
     global lambdas (all terms active)."""
@@ -228,6 +229,7 @@ def make_config(scene=None, *, max_nodes=4096, max_views=3, width=640, height=48
     cfg.penalty = Penalty(2.5, 0.0, 0.0, 0.7, 0.1)  # PenaltyConstants::setDefaultValue
     cfg.use_density = int(bool(use_density))
     cfg.pcg_tolerance = pcg_tolerance
+    cfg.recompute_jacobians = int(bool(recompute_jacobians))
     return cfg
 
 

@@ -133,6 +133,95 @@ __device__ inline void image_twist_gradient(const ViewDesc& V, float3 vc, float3
 
 // 4 CTAs per SM (64 registers, a few spilled) hide the gathers of the warp
 // field and the maps better than 2 (-32 % measured)
+// The dense-depth term of compacted pixel k under the current warp field
+// (computeDenseDepthJacobianKernel, DenseDepthJacobianResidual.cu:24-104): the
+// 32-byte record (twist gradient, residual, projected pixel; J = 0 and the
+// pixel 0xFFFFFFFF when the correspondence is invalid). The term evaluation
+// stores it; the matrix-free products recompute it when asked to.
+template <class T>
+__device__ inline void dense_record(const InstDesc& I, uint32_t k, float4& o0, float4& o1, bool& nonfinite) {
+    const float4 cv = I.dense_cv[k], cn = I.dense_cn[k];
+    const uint32_t v = __float_as_uint(cv.w);
+    const ViewDesc& V = I.views[v];
+    const ushort4 kn = I.dense_knn[k];
+    const float4 w4 = I.dense_w[k];
+    const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
+    const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
+    const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
+    const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
+    V3T<T> cvt3 = v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z));
+    if constexpr (sizeof(T) == 8) {
+        const float4 lo = I.dense_cv_lo[k];
+        cvt3 = v3t(cvt3.x + cvt<T>(lo.x), cvt3.y + cvt<T>(lo.y), cvt3.z + cvt<T>(lo.z));
+    }
+    const V3T<T> wv = appv(se3, cvt3);
+    const V3T<T> wn = rotv(se3, v3t(cvt<T>(cn.x), cvt<T>(cn.y), cvt<T>(cn.z)));
+    const V3T<T> vc = appv(iinv, appv(w2c, wv));
+    const V3T<T> nc = rotv(iinv, rotv(w2c, wn));
+    const int u = project_coord((float)vc.x, (float)vc.z, V.fx, V.cx);
+    const int w = project_coord((float)vc.y, (float)vc.z, V.fy, V.cy);
+    nonfinite |= !isfinite((float)vc.x) || !isfinite((float)vc.y) || !isfinite((float)vc.z);
+    o0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
+    if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height) {
+        const size_t p = (size_t)w * V.pitch + u;
+        const float4 dv4 = V.obs_v[p], dn4 = V.obs_n[p];
+        const V3T<T> dv = v3t(cvt<T>(dv4.x), cvt<T>(dv4.y), cvt<T>(dv4.z));
+        const V3T<T> dn = v3t(cvt<T>(dn4.x), cvt<T>(dn4.y), cvt<T>(dn4.z));
+        bool valid = true;
+        if (fabsf(dv4.x) < 1e-3f && fabsf(dv4.y) < 1e-3f && fabsf(dv4.z) < 1e-3f) valid = false;
+        if (dotv(dn, nc) < (T)0.7f) valid = false;
+        const V3T<T> df = sub(dv, vc);
+        if (dotv(df, df) > (T)(0.075f * 0.075f)) valid = false;
+        if (valid) {
+            const float r = (float)dotv(dn, sub(vc, dv));
+            nonfinite |= !isfinite(r);
+            const float3 dnf = mk3(dn4.x, dn4.y, dn4.z);
+            const float3 tr = rotT3(V.w2c, rot3(V.init, dnf));
+            const float3 ro = cross3(mk3((float)wv.x, (float)wv.y, (float)wv.z), tr);
+            o0 = make_float4(ro.x, ro.y, ro.z, tr.x);
+            o1 = make_float4(tr.y, tr.z, r, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+        }
+    }
+}
+
+// The foreground-mask term of compacted pixel k
+// (computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual,
+// DensityForegroundJacobianResidual.cu:93-142); fg_cv holds the canonical
+// vertex in frame 0, as the dense term uses it, or with
+// MVDR_COMPAT_REF_FOREGROUND_FRAME in its own camera's frame, as
+// density_map_jacobian.cuh:32-36 warps it.
+template <class T>
+__device__ inline void fg_record(const InstDesc& I, uint32_t k, float4& o0, float4& o1, bool& nonfinite) {
+    const float4 cv = I.fg_cv[k];
+    const uint32_t v = __float_as_uint(cv.w);
+    const ViewDesc& V = I.views[v];
+    const ushort4 kn = I.fg_knn[k];
+    const float4 w4 = I.fg_w[k];
+    const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
+    const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
+    const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
+    const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
+    const V3T<T> wvt = appv(se3, v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z)));
+    const V3T<T> vct = appv(iinv, appv(w2c, wvt));
+    const float3 wv = mk3((float)wvt.x, (float)wvt.y, (float)wvt.z);
+    const float3 vc = mk3((float)vct.x, (float)vct.y, (float)vct.z);
+    const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
+    const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
+    nonfinite |= !isfinite(vc.x) || !isfinite(vc.y) || !isfinite(vc.z);
+    o0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
+    if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height && V.fg != nullptr) {
+        const size_t p = (size_t)w * V.pitch + u;
+        const float img = V.fg[p];
+        float2 gyz;
+        image_twist_gradient(V, vc, wv, V.fg_grad[p], o0, gyz);
+        // geometry density 0 (DensityForegroundJacobianResidual.cu:103)
+        o1 = make_float4(gyz.x, gyz.y, img - 0.0f, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
+        nonfinite |= !isfinite(o1.z) || !isfinite(o0.w) || !isfinite(gyz.x) || !isfinite(gyz.y);
+    }
+}
+
 template <class T>
 __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* insts, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
@@ -151,49 +240,8 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
         uint32_t k;
         const TermType ty = off.typed(t, k);
         if (ty == kDense) {
-            // computeDenseDepthJacobianKernel (DenseDepthJacobianResidual.cu:24-104)
-            const float4 cv = I.dense_cv[k], cn = I.dense_cn[k];
-            const uint32_t v = __float_as_uint(cv.w);
-            const ViewDesc& V = I.views[v];
-            const ushort4 kn = I.dense_knn[k];
-            const float4 w4 = I.dense_w[k];
-            const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
-            const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
-            const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
-            const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
-            V3T<T> cvt3 = v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z));
-            if constexpr (sizeof(T) == 8) {
-                const float4 lo = I.dense_cv_lo[k];
-                cvt3 = v3t(cvt3.x + cvt<T>(lo.x), cvt3.y + cvt<T>(lo.y), cvt3.z + cvt<T>(lo.z));
-            }
-            const V3T<T> wv = appv(se3, cvt3);
-            const V3T<T> wn = rotv(se3, v3t(cvt<T>(cn.x), cvt<T>(cn.y), cvt<T>(cn.z)));
-            const V3T<T> vc = appv(iinv, appv(w2c, wv));
-            const V3T<T> nc = rotv(iinv, rotv(w2c, wn));
-            const int u = project_coord((float)vc.x, (float)vc.z, V.fx, V.cx);
-            const int w = project_coord((float)vc.y, (float)vc.z, V.fy, V.cy);
-            nonfinite |= !isfinite((float)vc.x) || !isfinite((float)vc.y) || !isfinite((float)vc.z);
-            float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
-            if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height) {
-                const size_t p = (size_t)w * V.pitch + u;
-                const float4 dv4 = V.obs_v[p], dn4 = V.obs_n[p];
-                const V3T<T> dv = v3t(cvt<T>(dv4.x), cvt<T>(dv4.y), cvt<T>(dv4.z));
-                const V3T<T> dn = v3t(cvt<T>(dn4.x), cvt<T>(dn4.y), cvt<T>(dn4.z));
-                bool valid = true;
-                if (fabsf(dv4.x) < 1e-3f && fabsf(dv4.y) < 1e-3f && fabsf(dv4.z) < 1e-3f) valid = false;
-                if (dotv(dn, nc) < (T)0.7f) valid = false;
-                const V3T<T> df = sub(dv, vc);
-                if (dotv(df, df) > (T)(0.075f * 0.075f)) valid = false;
-                if (valid) {
-                    const float r = (float)dotv(dn, sub(vc, dv));
-                    nonfinite |= !isfinite(r);
-                    const float3 dnf = mk3(dn4.x, dn4.y, dn4.z);
-                    const float3 tr = rotT3(V.w2c, rot3(V.init, dnf));
-                    const float3 ro = cross3(mk3((float)wv.x, (float)wv.y, (float)wv.z), tr);
-                    o0 = make_float4(ro.x, ro.y, ro.z, tr.x);
-                    o1 = make_float4(tr.y, tr.z, r, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
-                }
-            }
+            float4 o0, o1;
+            dense_record<T>(I, k, o0, o1, nonfinite);
             I.term_jr[2 * (size_t)k] = o0;
             I.term_jr[2 * (size_t)k + 1] = o1;
             energy += (double)o1.z * o1.z;
@@ -217,36 +265,8 @@ __global__ void __launch_bounds__(256, 4) eval_terms_kernel(const InstDesc* inst
                 energy += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
             }
         } else if (ty == kForeground) {
-            // computeForegroundMaskJacobian + computeImageDensityJacobainAndResidual;
-            // fg_cv holds the canonical vertex in frame 0, as the dense term
-            // uses it, or with MVDR_COMPAT_REF_FOREGROUND_FRAME in its own
-            // camera's frame, as density_map_jacobian.cuh:32-36 warps it
-            const float4 cv = I.fg_cv[k];
-            const uint32_t v = __float_as_uint(cv.w);
-            const ViewDesc& V = I.views[v];
-            const ushort4 kn = I.fg_knn[k];
-            const float4 w4 = I.fg_w[k];
-            const unsigned short nodes[4] = {kn.x, kn.y, kn.z, kn.w};
-            const float wts[4] = {w4.x, w4.y, w4.z, w4.w};
-            const R34T<T> se3 = blended_se3<T>(I.se3, nodes, wts, 4);
-            const R34T<T> w2c = view_mat<T>(V, 0), iinv = view_mat<T>(V, 2);
-            const V3T<T> wvt = appv(se3, v3t(cvt<T>(cv.x), cvt<T>(cv.y), cvt<T>(cv.z)));
-            const V3T<T> vct = appv(iinv, appv(w2c, wvt));
-            const float3 wv = mk3((float)wvt.x, (float)wvt.y, (float)wvt.z);
-            const float3 vc = mk3((float)vct.x, (float)vct.y, (float)vct.z);
-            const int u = project_coord(vc.x, vc.z, V.fx, V.cx);
-            const int w = project_coord(vc.y, vc.z, V.fy, V.cy);
-            nonfinite |= !isfinite(vc.x) || !isfinite(vc.y) || !isfinite(vc.z);
-            float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInvalid));
-            if (u >= 0 && u < (int)I.width && w >= 0 && w < (int)I.height && V.fg != nullptr) {
-                const size_t p = (size_t)w * V.pitch + u;
-                const float img = V.fg[p];
-                float2 gyz;
-                image_twist_gradient(V, vc, wv, V.fg_grad[p], o0, gyz);
-                // geometry density 0 (DensityForegroundJacobianResidual.cu:103)
-                o1 = make_float4(gyz.x, gyz.y, img - 0.0f, __uint_as_float((uint32_t)w * I.width + (uint32_t)u));
-                nonfinite |= !isfinite(o1.z) || !isfinite(o0.w) || !isfinite(gyz.x) || !isfinite(gyz.y);
-            }
+            float4 o0, o1;
+            fg_record<T>(I, k, o0, o1, nonfinite);
             I.term_jr[2 * (size_t)(Td + k)] = o0;
             I.term_jr[2 * (size_t)(Td + k) + 1] = o1;
             {
@@ -1758,6 +1778,22 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
 }
 
 // ------------------------------------------------------ matrix-free JtJ ---
+// A pixel term's record for the matrix-free products: the one the term
+// evaluation stored, or (recompute_jacobians) evaluated again from the maps
+// and the current warp field, as ApplyJtJMatrixFreeIndexed.cu:222-348
+// re-derives every term in every PCG iteration. The same function computes
+// both, so the two forms use the same values.
+template <class T>
+__device__ inline void pixel_record(const InstDesc& I, TermType ty, uint32_t k, uint32_t idx, float4& a, float4& b) {
+    if (I.recompute_jr) {
+        bool nonfinite = false;  // flagged by the term evaluation of this iteration
+        if (ty == kDense) dense_record<T>(I, k, a, b, nonfinite);
+        else fg_record<T>(I, k, a, b, nonfinite);
+    } else {
+        load_record32(I.term_jr + 2 * (size_t)idx, a, b);
+    }
+}
+
 // J.p per term (ApplyJacobianDot.cu:127-198), stored channel-major:
 // jp[c * T + t], T the solve's term count. A pixel term's rows for its nodes
 // are one Jacobian row scaled by each node's skinning weight, so its J.p is
@@ -1783,7 +1819,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
         if (ty == kDense || ty == kForeground) {
             const uint32_t idx = ty == kDense ? k : off.o[0] + k;
             float4 ra, rb;
-            load_record32(I.term_jr + 2 * (size_t)idx, ra, rb);
+            pixel_record<Acc>(I, ty, k, idx, ra, rb);
             const float4 w4 = term_weights(I, ty, k);
             Acc pb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -1872,7 +1908,7 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
             if (ty == kDense || ty == kForeground) {
                 const uint32_t idx = ty == kDense ? k : off.o[0] + k;
                 float4 ra, rb;
-                load_record32(I.term_jr + 2 * (size_t)idx, ra, rb);
+                pixel_record<T>(I, ty, k, idx, ra, rb);
                 const T wn = (T)I.n2t_w[p];
                 const T sc = (ty == kDense ? (T)1 : l2_fg) * wn;
                 const T y = jp[t];

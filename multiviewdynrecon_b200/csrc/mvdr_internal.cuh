@@ -343,6 +343,7 @@ struct InstDesc {
     unsigned long long* node_err_acc;  // [2N] node alignment error and weight sums, 2^-32 fixed point
     double* pcg_hist;       // [kPcgHistRows][MVDR_PCG_HISTORY] delta_k per GN iteration
     float pcg_tol;          // convergence tolerance (0: fixed iteration count)
+    uint32_t recompute_jr;  // matrix-free products re-derive the pixel terms' records
 
     // capacities
     uint32_t cap_dense, cap_fg, cap_k1, cap_k2, cap_pairs, cap_seg, cap_bb;
@@ -369,6 +370,7 @@ struct LaunchCfg {
     uint64_t wait_limit_ns;
     uint32_t wait_extra_arrivals;
     float pcg_tol;  // PCG convergence tolerance (0: fixed iteration count)
+    int recompute_jr;  // matrix-free products re-derive the pixel terms' records
 };
 
 constexpr uint32_t kPcgHistRows = 64;  // GN iterations whose PCG residuals are kept

@@ -182,6 +182,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.node_err_acc = a.take<unsigned long long>(2 * N);
     I.pcg_hist = a.take<double>((size_t)kPcgHistRows * MVDR_PCG_HISTORY);
     I.pcg_tol = lc.pcg_tol;
+    I.recompute_jr = (uint32_t)lc.recompute_jr;
     if (max_tp) {  // device-side feature selection
         I.fp_keep = a.take<uint32_t>(max_tp);
         I.fp_chosen = a.take<ushort4>(max_tp);
@@ -214,6 +215,8 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
         return fail(MVDR_EINVAL, "unknown mode");
     if (!(cfg->pcg_tolerance >= 0.0f && cfg->pcg_tolerance < 1.0f))
         return fail(MVDR_EINVAL, "pcg_tolerance must be in [0, 1)");
+    if (cfg->recompute_jacobians && cfg->mode != MVDR_MODE_MATRIX_FREE)
+        return fail(MVDR_EINVAL, "recompute_jacobians needs the matrix-free mode");
     int dev = 0;
     CU(cudaGetDevice(&dev));
     cudaDeviceProp prop;
@@ -256,6 +259,7 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     lc.mode = cfg->mode;
     lc.use_density = cfg->use_density ? 1 : 0;
     lc.pcg_tol = cfg->pcg_tolerance;
+    lc.recompute_jr = cfg->recompute_jacobians ? 1 : 0;
     lc.sm_count = prop.multiProcessorCount;
 
     const size_t smem_seg = (size_t)lc.cap_seg * 4;

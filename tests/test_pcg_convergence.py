@@ -50,3 +50,13 @@ def test_tolerance_validation():
         h = C.c_void_p()
         assert lib().mvdr_create(C.byref(cfg), C.byref(h)) == abi.MVDR_EINVAL
         assert b"pcg_tolerance" in lib().mvdr_last_error_string()
+
+
+def test_recompute_needs_the_matrix_free_mode():
+    """recompute_jacobians with the materialised operator is refused at create."""
+    from multiviewdynrecon_b200 import lib
+    scene = small_scene("sphere")
+    cfg = abi.make_config(scene, mode=abi.MODE_MATERIALIZED, recompute_jacobians=True)
+    h = C.c_void_p()
+    assert lib().mvdr_create(C.byref(cfg), C.byref(h)) == abi.MVDR_EINVAL
+    assert b"matrix-free" in lib().mvdr_last_error_string()
