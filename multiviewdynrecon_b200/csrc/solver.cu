@@ -9,6 +9,8 @@
 #include <cstring>
 #include <map>
 #include <string>
+
+#include <nvtx3/nvToolsExt.h>
 #include <vector>
 
 #include "batch.cuh"
@@ -624,7 +626,16 @@ static int all_bound(const Batch& b) {
     return MVDR_OK;
 }
 
+// NVTX ranges around the enqueued stages, for profilers (`ncu --nvtx
+// --nvtx-include "mvdr/pcg/"` takes one stage's kernels); without a tool
+// attached the calls return at once
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
 static int enqueue_index(Batch& b, cudaStream_t st) {
+    NvtxRange range("mvdr/index");
     // zero the per-build counters of every instance
     for (uint32_t i = 0; i < b.B; ++i) {
         const InstDesc& I = b.host[i];
@@ -636,16 +647,30 @@ static int enqueue_index(Batch& b, cudaStream_t st) {
 }
 
 static int enqueue_iteration(Batch& b, uint32_t iter, uint32_t pcg, cudaStream_t st) {
+    NvtxRange range("mvdr/gn_iteration");
     const mvdr_penalty lam = penalty_for(b.cfg, iter);
-    CU(launch_eval_terms(b.lc, b.d_inst, lam, st));
-    CU(launch_energy(b.lc, b.d_inst, std::min<uint32_t>(iter, 63), st));
-    CU(launch_assemble(b.lc, b.d_inst, lam, b.cfg.mode == MVDR_MODE_MATERIALIZED, st));
-    CU(launch_pcg(b.lc, b.d_inst, lam, pcg, iter, st));
-    CU(launch_update(b.lc, b.d_inst, st));
+    {
+        NvtxRange r("mvdr/terms");
+        CU(launch_eval_terms(b.lc, b.d_inst, lam, st));
+        CU(launch_energy(b.lc, b.d_inst, std::min<uint32_t>(iter, 63), st));
+    }
+    {
+        NvtxRange r("mvdr/assemble");
+        CU(launch_assemble(b.lc, b.d_inst, lam, b.cfg.mode == MVDR_MODE_MATERIALIZED, st));
+    }
+    {
+        NvtxRange r("mvdr/pcg");
+        CU(launch_pcg(b.lc, b.d_inst, lam, pcg, iter, st));
+    }
+    {
+        NvtxRange r("mvdr/update");
+        CU(launch_update(b.lc, b.d_inst, st));
+    }
     return MVDR_OK;
 }
 
 static int solve_batch(Batch& b, uint32_t gn, uint32_t pcg, bool graph, cudaStream_t st) {
+    NvtxRange range("mvdr/solve");
     int rc = all_bound(b);
     if (rc != MVDR_OK) return rc;
     if (gn > 63) return fail(MVDR_EINVAL, "at most 63 Gauss-Newton iterations per solve");
