@@ -9,9 +9,9 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <vector>
 
 #include <nvtx3/nvToolsExt.h>
-#include <vector>
 
 #include "batch.cuh"
 #include "kernels_common.cuh"
