@@ -973,10 +973,9 @@ __global__ void __launch_bounds__(128) scale_offdiag_kernel(const InstDesc* inst
 #pragma unroll
             for (int c = 0; c < 6; ++c) yr[c] = s_y[lp][k][c];
             chol_forward(L, yr, z);
-            float2* out = reinterpret_cast<float2*>(I.bsr_s + blk + 6 * k);
-            out[0] = make_float2((float)z[0], (float)z[1]);
-            out[1] = make_float2((float)z[2], (float)z[3]);
-            out[2] = make_float2((float)z[4], (float)z[5]);
+            float4* out = reinterpret_cast<float4*>(I.bsr_s + (blk / 36) * kScaledBlock + kScaledRow * k);
+            out[0] = make_float4((float)z[0], (float)z[1], (float)z[2], (float)z[3]);
+            out[1] = make_float4((float)z[4], (float)z[5], 0.f, 0.f);
         }
         __syncwarp();
     }
@@ -1180,7 +1179,7 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(const InstDesc* inst
     if (has) {
         const T d = sv + beta * dp;
         PV::d(I, parity)[e] = d;
-        if constexpr (SCALED) I.df[e] = (float)d;
+        if constexpr (SCALED) I.df[df_pos(e)] = (float)d;
     }
 }
 
@@ -1345,8 +1344,10 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_col_kerne
 // the stored A^_ji, whose column r is row r of A^_ij: FORM 1 reads that
 // column (six 4-byte loads), FORM 0 reads row r of A^_ji and adds d^_j(r)
 // times it to all six rows, which the row's threads sum through shared
-// memory at the end. With row-major float blocks the six threads of a row
-// read one stored block as 144 contiguous bytes.
+// memory at the end. The float blocks are row-major with each row padded to
+// 32 bytes (kScaledRow), so a thread reads its block row, and the column's
+// float direction, in one 256-bit load each, and the six threads of a row
+// read one stored block as 192 contiguous bytes.
 template <uint32_t kTileRows, uint32_t kTileSplit, uint32_t kForm>
 __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_kernel(const InstDesc* insts,
                                                                                   int parity) {
@@ -1373,28 +1374,26 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
 #pragma unroll 2
             for (uint32_t b = rb + half; b < re; b += kTileSplit) {
                 const uint2 ent = I.bsr_ent[b];
-                const float* blk = store + 36 * (size_t)(ent.x & ~kTransposedBlock);
-                const float2* x2 = reinterpret_cast<const float2*>(xf + 6 * (size_t)ent.y);
+                const float* blk = store + kScaledBlock * (size_t)(ent.x & ~kTransposedBlock);
+                const float* xc = xf + kScaledRow * (size_t)ent.y;
                 const bool lower = (ent.x & kTransposedBlock) != 0;
                 if (kForm == 0 && lower) {
-                    const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
-                    const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
-                    const float xr = xf[6 * (size_t)ent.y + rr];
-                    col_acc[0] += a01.x * xr; col_acc[1] += a01.y * xr; col_acc[2] += a23.x * xr;
-                    col_acc[3] += a23.y * xr; col_acc[4] += a45.x * xr; col_acc[5] += a45.y * xr;
+                    float av[8];
+                    load8f(blk + kScaledRow * rr, av);
+                    const float xr = xc[rr];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) col_acc[k] += av[k] * xr;
                 } else {
-                    float av[6];
+                    float av[8], xv[8];
                     if (lower) {
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) av[k] = blk[6 * k + rr];
+                        for (int k = 0; k < 6; ++k) av[k] = blk[kScaledRow * k + rr];
                     } else {
-                        const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
-                        const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
-                        av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y; av[4] = a45.x; av[5] = a45.y;
+                        load8f(blk + kScaledRow * rr, av);
                     }
-                    const float2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
-                    acc += av[0] * x01.x + av[1] * x01.y + av[2] * x23.x + av[3] * x23.y + av[4] * x45.x +
-                           av[5] * x45.y;
+                    load8f(xc, xv);
+                    acc += av[0] * xv[0] + av[1] * xv[1] + av[2] * xv[2] + av[3] * xv[3] + av[4] * xv[4] +
+                           av[5] * xv[5];
                 }
             }
         }
@@ -1648,7 +1647,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
             for (uint32_t e = c * nt + tid; e < 6 * I.N; e += nc * nt) {
                 const T dv = sv[e] + beta * dprev[e];
                 dcur[e] = dv;
-                if constexpr (MIXED) I.df[e] = (float)dv;
+                if constexpr (MIXED) I.df[df_pos(e)] = (float)dv;
             }
         }
         if (!instance_barrier(I, bar, ++passed * nc + extra, limit_ns)) return;
@@ -1666,20 +1665,17 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
 #pragma unroll 2
                 for (uint32_t b = rb; b < re; ++b) {
                     const uint2 ent = I.bsr_ent[b];
-                    const float* blk = I.bsr_s + 36 * (size_t)(ent.x & ~kTransposedBlock);
-                    const float2* x2 = reinterpret_cast<const float2*>(I.df + 6 * (size_t)ent.y);
-                    float av[6];
+                    const float* blk = I.bsr_s + kScaledBlock * (size_t)(ent.x & ~kTransposedBlock);
+                    float av[8], xv[8];
                     if (ent.x & kTransposedBlock) {
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) av[k] = blk[6 * k + rr];
+                        for (int k = 0; k < 6; ++k) av[k] = blk[kScaledRow * k + rr];
                     } else {
-                        const float2* b2 = reinterpret_cast<const float2*>(blk + 6 * rr);
-                        const float2 a01 = b2[0], a23 = b2[1], a45 = b2[2];
-                        av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y; av[4] = a45.x; av[5] = a45.y;
+                        load8f(blk + kScaledRow * rr, av);
                     }
-                    const float2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
-                    acc += av[0] * x01.x + av[1] * x01.y + av[2] * x23.x + av[3] * x23.y + av[4] * x45.x +
-                           av[5] * x45.y;
+                    load8f(I.df + kScaledRow * (size_t)ent.y, xv);
+                    acc += av[0] * xv[0] + av[1] * xv[1] + av[2] * xv[2] + av[3] * xv[3] + av[4] * xv[4] +
+                           av[5] * xv[5];
                 }
                 const size_t e = 6 * (size_t)row + rr;
                 const double q = xd[e] + (double)acc;

@@ -232,6 +232,16 @@ __device__ inline void load_record32(const float4* p, float4& a, float4& b) {
                  : "l"(p));
 }
 
+// Eight floats at a 32-byte-aligned address in one 256-bit load
+__device__ inline void load8f(const float* p, float (&v)[8]) {
+    asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "l"(p));
+}
+
+// the float direction's position of vector element e (node e / 6, row e % 6)
+__device__ inline size_t df_pos(size_t e) { return e + 2 * (e / 6); }
+
 // true when the input check found an out-of-range node or surfel id
 __device__ inline bool bad_inputs(const InstDesc& I) {
     return (*(volatile const uint32_t*)&I.counts->error_flags & kErrBadNodeIndex) != 0;

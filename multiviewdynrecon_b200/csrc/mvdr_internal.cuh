@@ -33,6 +33,12 @@ __host__ __device__ constexpr uint32_t len_bucket_of(uint32_t len) {
 // another instruction's read).
 __host__ __device__ constexpr uint32_t blk_idx(uint32_t r, uint32_t k) { return 12 * (k >> 1) + 2 * r + (k & 1); }
 
+// The scaled operator's float blocks and the float copy of the PCG direction
+// keep each row of six values in 32 bytes (two padding floats), so that a
+// thread reads a block row or a node's direction in one 256-bit load.
+constexpr uint32_t kScaledRow = 8;                  // floats per stored row
+constexpr uint32_t kScaledBlock = 6 * kScaledRow;   // floats per stored block
+
 constexpr uint32_t kChunkPixels = 2048;  // pixels per compaction CTA (256 threads x 8)
 
 // error flag bits (DeviceCounts::error_flags)
@@ -312,10 +318,11 @@ struct InstDesc {
     // mixed precision, materialised: the operator of the PCG scaled by the
     // diagonal blocks' Cholesky factors, A^ = L^-1 A L^-T (identity diagonal
     // blocks, not stored): its upper blocks A^_ij = L_i^-1 A_ij L_j^-T in
-    // float, row-major (element (r, k) at 6 r + k), at the half-storage block
+    // float, row-major with rows of kScaledRow floats (element (r, k) at
+    // 8 r + k), kScaledBlock floats per block at the half-storage block
     // positions of bsr_d
     float* bsr_s;
-    float* df;              // [6N] the PCG direction of the scaled system in float
+    float* df;              // [8N] the PCG direction of the scaled system in float, 8 floats per node
     // per entry of the full (symmetric) block-row layout, row i: the diagonal,
     // then its symmetric keys in order [N + 2P cap]
     // (half-storage block | kTransposedBlock when read transposed, block column)

@@ -157,8 +157,8 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.bsr_d = mixed ? a.take<double>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
     I.bsr_ent = a.take<uint2>(N + 2 * (size_t)lc.cap_pairs);
     const bool scaled = mixed && lc.mode == MVDR_MODE_MATERIALIZED;
-    I.bsr_s = scaled ? a.take<float>(36 * (N + (size_t)lc.cap_pairs)) : nullptr;
-    I.df = scaled ? a.take<float>(6 * N) : nullptr;
+    I.bsr_s = scaled ? a.take<float>(kScaledBlock * (N + (size_t)lc.cap_pairs)) : nullptr;
+    I.df = scaled ? a.take<float>(kScaledRow * N) : nullptr;
     if (mixed) {
         I.x_d = a.take<double>(6 * N);
         I.r_d = a.take<double>(6 * N);
