@@ -697,7 +697,8 @@ __global__ void __launch_bounds__(256) np_row_count_kernel(const InstDesc* insts
 // each distinct partner j (ascending, found by a warp minimum) one sweep of
 // the list emits the terms that contain j, in t order, and finds the next
 // partner. The first kRowCache * 32 terms stay in registers (the term id and
-// its partners, packed 16-bit); longer lists re-read the rest each sweep. A
+// its partners, packed 16-bit), the next kRowSpill * 32 in shared memory;
+// longer lists re-derive the rest each sweep. A
 // term that lists a partner twice contributes two adjacent entries, like the
 // duplicate keys of a sort. Writes np_index, the per-pair (key, start) of the
 // row and upper_count.
@@ -716,16 +717,23 @@ __device__ inline uint2 packed_partners(const InstDesc& I, const TermOffsets& of
     return make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
 }
 
+// terms kRowCache * 32 .. kRowCache * 32 + kRowSpill * 32 of a node's list
+// wait in shared memory (the same (term, partners) pairs), so that the sweeps
+// re-read them without re-deriving their partners
+constexpr int kRowSpill = 8;
+
 __global__ void __launch_bounds__(256, 4) np_row_build_kernel(const InstDesc* insts) {
+    __shared__ uint32_t s_t[8][kRowSpill * 32];
+    __shared__ uint2 s_pk[8][kRowSpill * 32];
     const InstDesc& I = insts[blockIdx.y];
     const DeviceCounts* C = I.counts;
     if (C->node2term_entries > I.cap_k1 || C->nodepair_entries > I.cap_k2) return;
     TermOffsets off;
     off.load(I.counts);
-    const uint32_t lane = lane_id();
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < I.N; node += warps) {
+    for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + w; node < I.N; node += warps) {
         const uint32_t b0 = I.n2t_offset[node], b1 = I.n2t_offset[node + 1];
         const uint32_t out = I.row_offset[node], len = I.row_count[node];
         uint32_t ct[kRowCache];
@@ -736,6 +744,18 @@ __global__ void __launch_bounds__(256, 4) np_row_build_kernel(const InstDesc* in
             ct[m] = p < b1 ? I.n2t_index[p] : kInvalid;
             cj[m] = p < b1 ? packed_partners(I, off, node, ct[m]) : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         }
+        // the spill slices in shared memory (entries past b1 hold no partners)
+        const uint32_t spill0 = b0 + 32u * kRowCache;
+        const uint32_t spill1 = min(b1, spill0 + 32u * kRowSpill);
+        __syncwarp();
+        const uint32_t nspill = spill1 > spill0 ? (spill1 - spill0 + 31u) / 32u : 0u;  // whole slices
+        for (uint32_t q = lane; q < 32u * nspill; q += 32) {
+            const uint32_t p = spill0 + q;
+            const uint32_t t = p < b1 ? I.n2t_index[p] : kInvalid;
+            s_t[w][q] = t;
+            s_pk[w][q] = p < b1 ? packed_partners(I, off, node, t) : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+        }
+        __syncwarp();
         // emit the slice's entries for partner j at out + pos; returns the
         // smallest partner above j seen in the slice
         auto slice = [&](uint32_t t, uint2 pk, uint32_t j, uint32_t& pos) -> uint32_t {
@@ -781,7 +801,7 @@ __global__ void __launch_bounds__(256, 4) np_row_build_kernel(const InstDesc* in
             }
             for (uint32_t p = b0 + 32u * kRowCache + lane; p < b1; p += 32) {
                 uint32_t js[4];
-                unpack_partners(packed_partners(I, off, node, I.n2t_index[p]), js);
+                unpack_partners(p < spill1 ? s_pk[w][p - spill0] : packed_partners(I, off, node, I.n2t_index[p]), js);
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                     if (js[q] != 0xFFFFu) mn = min(mn, js[q]);
@@ -802,8 +822,15 @@ __global__ void __launch_bounds__(256, 4) np_row_build_kernel(const InstDesc* in
             }
             for (uint32_t base = b0 + 32u * kRowCache; base < b1; base += 32) {
                 const uint32_t p = base + lane;
-                const uint32_t t = p < b1 ? I.n2t_index[p] : kInvalid;
-                const uint2 pk = p < b1 ? packed_partners(I, off, node, t) : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+                uint32_t t;
+                uint2 pk;
+                if (base < spill1) {  // warp-uniform: a spilled slice
+                    t = s_t[w][p - spill0];
+                    pk = s_pk[w][p - spill0];
+                } else {
+                    t = p < b1 ? I.n2t_index[p] : kInvalid;
+                    pk = p < b1 ? packed_partners(I, off, node, t) : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+                }
                 nxt = min(nxt, slice(t, pk, j, pos));
             }
             ++runs;
