@@ -44,23 +44,9 @@ template <class T> __device__ inline V3T<T> appv(const R34T<T>& m, V3T<T> v) {
     return {a.x + m.t[0], a.y + m.t[1], a.z + m.t[2]};
 }
 
-// float -> double by bit manipulation (integer pipe; the FP64 conversion
-// instruction is a narrow pipe on this part). Exact for zero and normal
-// floats; float subnormals become signed zero; Inf and NaN stay Inf and NaN
-// (their exponent field maps to the double's all-ones field, so that a NaN in
-// the inputs reaches the non-finite checks instead of a large finite value).
-__device__ inline double f2d(float f) {
-    const uint32_t b = __float_as_uint(f);
-    const uint32_t em = b & 0x7fffffffu, sign = b & 0x80000000u;
-    const bool normal = em >= 0x00800000u;
-    const uint32_t bias = em >= 0x7f800000u ? (1792u << 20) : (896u << 20);
-    const uint32_t hi = normal ? (sign | ((em >> 3) + bias)) : sign;
-    const uint32_t lo = normal ? (em << 29) : 0u;
-    return __hiloint2double((int)hi, (int)lo);
-}
 template <class T> __device__ inline T cvt(float x);
 template <> __device__ inline float cvt<float>(float x) { return x; }
-template <> __device__ inline double cvt<double>(float x) { return f2d(x); }
+template <> __device__ inline double cvt<double>(float x) { return (double)x; }
 template <class T> __device__ inline T rsqrt_t(T x);
 template <> __device__ inline float rsqrt_t<float>(float x) { return rsqrtf(x); }
 template <> __device__ inline double rsqrt_t<double>(double x) { return rsqrt(x); }
