@@ -505,11 +505,8 @@ __device__ inline void cholesky6_solve(const double* L, const double* b, double*
 // Mixed precision keeps the assembled JtJ blocks in double: rounding them to
 // float moves the PCG increment by 1.3e-4 to 5e-4 on these blocks, whose
 // condition numbers reach 1e5, and rounding only the off-diagonal blocks still
-// moves it by up to 1.5e-4. Double storage also spares the SpMV every
-// float-to-double conversion (B200 runs FP64 FMAs at half the FP32 rate, but
-// conversions go through a much slower pipe). The half storage (diagonal and
-// upper blocks) keeps the bytes per SpMV below those of full float storage
-// with a 16-bit correction.
+// moves it by up to 1.5e-4. The PCG itself runs on the float blocks of the
+// scaled operator (scale_offdiag_kernel), whose entries are of order one.
 template <bool MIXED> struct BlockStore;
 template <> struct BlockStore<true> {
     using V = double;
