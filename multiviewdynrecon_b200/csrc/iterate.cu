@@ -1773,6 +1773,21 @@ __device__ inline void pixel_record(const InstDesc& I, TermType ty, uint32_t k, 
     }
 }
 
+// a node's six direction components: the PCG direction d (fused) in pair
+// loads (the solver's own 16-byte-aligned vector), or the float operand xin
+template <class Acc>
+__device__ inline void load_node6(int fused, const Acc* dv, const float* xin, uint32_t node, Acc (&x)[6]) {
+    if (fused) {
+        using P = typename std::conditional<sizeof(Acc) == 8, double2, float2>::type;
+        const P* p2 = reinterpret_cast<const P*>(dv + 6 * (size_t)node);
+        const P a = p2[0], b = p2[1], c = p2[2];
+        x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y; x[4] = c.x; x[5] = c.y;
+    } else {  // a caller's vector: no alignment beyond 4 bytes assumed
+#pragma unroll
+        for (int i = 0; i < 6; ++i) x[i] = (Acc)xin[6 * (size_t)node + i];
+    }
+}
+
 // J.p per term (ApplyJacobianDot.cu:127-198), stored channel-major:
 // jp[c * T + t], T the solve's term count. A pixel term's rows for its nodes
 // are one Jacobian row scaled by each node's skinning weight, so its J.p is
@@ -1806,11 +1821,10 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
                 const uint32_t node = nodes[q];
                 if (node >= I.N) continue;
                 const Acc w = (Acc)weight_of(nn, w4, node);
+                Acc x6[6];
+                load_node6<Acc>(fused, dv, xin, node, x6);
 #pragma unroll
-                for (int i = 0; i < 6; ++i) {
-                    const size_t e = 6 * (size_t)node + i;
-                    pb[i] += w * (fused ? (Acc)dv[e] : (Acc)xin[e]);
-                }
+                for (int i = 0; i < 6; ++i) pb[i] += w * x6[i];
             }
             const Acc g[6] = {(Acc)ra.x, (Acc)ra.y, (Acc)ra.z, (Acc)ra.w, (Acc)rb.x, (Acc)rb.y};
             Acc o = 0;
@@ -1837,11 +1851,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
             TermRows tr;
             const int ch = term_rows(I, off, lam, t, node, tr);
             Acc p[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                const size_t e = 6 * (size_t)node + i;
-                p[i] = fused ? (Acc)dv[e] : (Acc)xin[e];
-            }
+            load_node6<Acc>(fused, dv, xin, node, p);
             for (int c = 0; c < ch; ++c) {
                 Acc a = 0;
 #pragma unroll
