@@ -1761,10 +1761,13 @@ __global__ void __launch_bounds__(kPersistThreads, 3) pcg_persistent_kernel(cons
 // evaluation stored, or (recompute_jacobians) evaluated again from the maps
 // and the current warp field, as ApplyJtJMatrixFreeIndexed.cu:222-348
 // re-derives every term in every PCG iteration. The same function computes
-// both, so the two forms use the same values.
-template <class T>
+// both, so the two forms use the same values. The kernels are instantiated
+// for stored records only (RECOMP false: no registers for the
+// re-derivation) and for the per-instance choice (RECOMP true), which the
+// solver launches when the configuration asks for re-derived terms.
+template <class T, bool RECOMP>
 __device__ inline void pixel_record(const InstDesc& I, TermType ty, uint32_t k, uint32_t idx, float4& a, float4& b) {
-    if (I.recompute_jr) {
+    if (RECOMP && I.recompute_jr) {
         bool nonfinite = false;  // flagged by the term evaluation of this iteration
         if (ty == kDense) dense_record<T>(I, k, a, b, nonfinite);
         else fg_record<T>(I, k, a, b, nonfinite);
@@ -1793,7 +1796,7 @@ __device__ inline void load_node6(int fused, const Acc* dv, const float* xin, ui
 // are one Jacobian row scaled by each node's skinning weight, so its J.p is
 // that row times the weight-blended p (one record load per term). With
 // `fused` set p is the PCG direction d of this iteration, else xin.
-template <bool MIXED>
+template <bool MIXED, bool RECOMP>
 __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
                                                       mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
@@ -1813,7 +1816,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
         if (ty == kDense || ty == kForeground) {
             const uint32_t idx = ty == kDense ? k : off.o[0] + k;
             float4 ra, rb;
-            pixel_record<Acc>(I, ty, k, idx, ra, rb);
+            pixel_record<Acc, RECOMP>(I, ty, k, idx, ra, rb);
             const float4 w4 = term_weights(I, ty, k);
             Acc pb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -1870,7 +1873,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
 // scaled by the entry's recorded skinning weight. With `pcg` set the operand
 // is this iteration's direction d; the kernel stores q and the d.q partial,
 // like pcg_spmv_kernel.
-template <bool MIXED>
+template <bool MIXED, bool RECOMP>
 __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
                                                        int parity, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
@@ -1897,7 +1900,7 @@ __global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, co
             if (ty == kDense || ty == kForeground) {
                 const uint32_t idx = ty == kDense ? k : off.o[0] + k;
                 float4 ra, rb;
-                pixel_record<T>(I, ty, k, idx, ra, rb);
+                pixel_record<T, RECOMP>(I, ty, k, idx, ra, rb);
                 const T wn = (T)I.n2t_w[p];
                 const T sc = (ty == kDense ? (T)1 : l2_fg) * wn;
                 const T y = jp[t];
@@ -2126,6 +2129,26 @@ static uint32_t scale_grid(const LaunchCfg& lc) {
     return min((lc.cap_pairs + kScalePairsPerCta - 1) / kScalePairsPerCta, (uint32_t)lc.sm_count * 16);
 }
 
+// J.d then Jt.(J.d) (+ damping): `fused` takes the PCG direction of `parity`
+// as the operand and stores q with its d.q partials, else x -> y
+static void launch_apply_pair(const LaunchCfg& lc, InstDesc* d, const float* x, float* y, int parity, int fused,
+                              uint32_t gterm, uint32_t gwarp, uint32_t B, const mvdr_penalty& lam, cudaStream_t st) {
+    const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
+    if (mixed && lc.recompute_jr) {
+        MVDR_LAUNCH((apply_j_kernel<true, true>), grid2(gterm, B), 256, 0, st, d, x, parity, fused, lam);
+        MVDR_LAUNCH((apply_jt_kernel<true, true>), grid2(gwarp, B), 256, 0, st, d, x, y, fused, parity, lam);
+    } else if (mixed) {
+        MVDR_LAUNCH((apply_j_kernel<true, false>), grid2(gterm, B), 256, 0, st, d, x, parity, fused, lam);
+        MVDR_LAUNCH((apply_jt_kernel<true, false>), grid2(gwarp, B), 256, 0, st, d, x, y, fused, parity, lam);
+    } else if (lc.recompute_jr) {
+        MVDR_LAUNCH((apply_j_kernel<false, true>), grid2(gterm, B), 256, 0, st, d, x, parity, fused, lam);
+        MVDR_LAUNCH((apply_jt_kernel<false, true>), grid2(gwarp, B), 256, 0, st, d, x, y, fused, parity, lam);
+    } else {
+        MVDR_LAUNCH((apply_j_kernel<false, false>), grid2(gterm, B), 256, 0, st, d, x, parity, fused, lam);
+        MVDR_LAUNCH((apply_jt_kernel<false, false>), grid2(gwarp, B), 256, 0, st, d, x, y, fused, parity, lam);
+    }
+}
+
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, bool materialize,
                             cudaStream_t st) {
     const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
@@ -2217,10 +2240,7 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
         else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
             // J.d per term, then Jt per node (+ damping, q, d.q)
-            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
-            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, parity, 1, lam);
-            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
-            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, parity, lam);
+            launch_apply_pair(lc, d, nullptr, nullptr, parity, 1, gterm, gwarp, lc.B, lam, st);
             nq = gwarp;
         } else {
             const cudaError_t e = launch_spmv(lc, d, parity, st);
@@ -2335,10 +2355,7 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             // the launches of one matrix-free PCG iteration after its direction
             const uint32_t gwarp = (lc.max_nodes + 7) / 8;
             const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-            if (mixed) MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, 0, 1, lam);
-            else MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, lc.B), 256, 0, st, d, (const float*)nullptr, 0, 1, lam);
-            if (mixed) MVDR_LAUNCH(apply_jt_kernel<true>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, 0, lam);
-            else MVDR_LAUNCH(apply_jt_kernel<false>, grid2(gwarp, lc.B), 256, 0, st, d, nullptr, nullptr, 1, 0, lam);
+            launch_apply_pair(lc, d, nullptr, nullptr, 0, 1, gterm, gwarp, lc.B, lam, st);
             break;
         }
         default: return cudaErrorInvalidValue;
@@ -2358,13 +2375,7 @@ cudaError_t launch_apply_jtj(const LaunchCfg& lc, InstDesc* d, const mvdr_penalt
     // single instance view: d points at the instance's descriptor, B = 1
     if (lc.mode == MVDR_MODE_MATRIX_FREE) {
         const uint32_t gterm = min((lc.cap_terms + 255) / 256, (uint32_t)lc.sm_count * 8);
-        if (lc.precision == MVDR_PRECISION_MIXED) {
-            MVDR_LAUNCH(apply_j_kernel<true>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
-            MVDR_LAUNCH(apply_jt_kernel<true>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
-        } else {
-            MVDR_LAUNCH(apply_j_kernel<false>, grid2(gterm, 1), 256, 0, st, d, x, 0, 0, lam);
-            MVDR_LAUNCH(apply_jt_kernel<false>, grid2((lc.max_nodes + 7) / 8, 1), 256, 0, st, d, x, y, 0, 0, lam);
-        }
+        launch_apply_pair(lc, d, x, y, 0, 0, gterm, (lc.max_nodes + 7) / 8, 1, lam, st);
     } else {
         if (lc.precision == MVDR_PRECISION_MIXED)
             MVDR_LAUNCH(bsr_apply_kernel<true>, grid2((lc.max_nodes + 31) / 32, 1), 192, 0, st, d, x, y);
