@@ -1791,13 +1791,17 @@ __device__ inline void load_node6(int fused, const Acc* dv, const float* xin, ui
     }
 }
 
+// The stored-record kernels run 4 CTAs per SM (64 registers, a few spilled):
+// measured faster than 3 (0.42 against 0.36 ms per PCG iteration on the
+// 16-instance torso batch) and than 6 (0.37 ms); the re-deriving kernels run
+// 2 CTAs per SM (up to 128 registers: the term evaluation's chain inline).
 // J.p per term (ApplyJacobianDot.cu:127-198), stored channel-major:
 // jp[c * T + t], T the solve's term count. A pixel term's rows for its nodes
 // are one Jacobian row scaled by each node's skinning weight, so its J.p is
 // that row times the weight-blended p (one record load per term). With
 // `fused` set p is the PCG direction d of this iteration, else xin.
 template <bool MIXED, bool RECOMP>
-__global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
+__global__ void __launch_bounds__(256, RECOMP ? 2 : 4) apply_j_kernel(const InstDesc* insts, const float* xin, int parity, int fused,
                                                       mvdr_penalty lam) {
     using Acc = typename std::conditional<MIXED, double, float>::type;
     const InstDesc& I = insts[blockIdx.y];
@@ -1874,7 +1878,7 @@ __global__ void __launch_bounds__(256) apply_j_kernel(const InstDesc* insts, con
 // is this iteration's direction d; the kernel stores q and the d.q partial,
 // like pcg_spmv_kernel.
 template <bool MIXED, bool RECOMP>
-__global__ void __launch_bounds__(256) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
+__global__ void __launch_bounds__(256, RECOMP ? 2 : 4) apply_jt_kernel(const InstDesc* insts, const float* xin, float* yout, int pcg,
                                                        int parity, mvdr_penalty lam) {
     const InstDesc& I = insts[blockIdx.y];
     if (pcg && pcg_stopped(I)) return;
