@@ -170,25 +170,37 @@ class ClockSampler:
 
 
 PROFILE_SPMV = "profiles/pcg_spmv_scaled_torso_3view_4096nodes_16inst.md"
+PROFILE_MATRIX_FREE = "profiles/apply_pair_matrix_free_torso_3view_4096nodes_8inst.md"
 
 
 def measured_traffic(args):
-    """DRAM bytes (read + write) per launch of the headline SpMV kernel
-    (pcg_spmv_scaled_kernel) from the ncu capture of this workload summarised
-    in PROFILE_SPMV; None for other workloads or when no summary exists."""
+    """DRAM bytes (read + write) per launch of the roofline kernel from the ncu
+    capture of this workload summarised under profiles/: the headline SpMV
+    (pcg_spmv_scaled_kernel, PROFILE_SPMV) or, in the matrix-free mode, the
+    product pair (PROFILE_MATRIX_FREE, an 8-instance capture scaled to the
+    batch: each instance moves the same bytes); None for other workloads or
+    when no summary exists."""
     default = (args.batch == 16 and args.nodes == 4096 and args.width == 640 and args.height == 480
-               and args.precision == "mixed" and args.mode == "materialized")
-    path = os.path.join(ROOT, PROFILE_SPMV)
-    if not default or not os.path.exists(path):
+               and args.precision == "mixed")
+    if not default:
         return None, None
     import re
+    if args.mode == "materialized":
+        rel, row, scale = PROFILE_SPMV, "| DRAM read + write |", 1.0
+    else:
+        rel, row, scale = PROFILE_MATRIX_FREE, "| DRAM bytes (rate x duration) |", args.batch / 8.0
+    path = os.path.join(ROOT, rel)
+    if not os.path.exists(path):
+        return None, None
     with open(path) as f:
         for line in f:
-            if line.startswith("| DRAM read + write |"):
-                # "R + W MB ...": the first two numbers of the cell
-                nums = re.findall(r"[0-9]+(?:\.[0-9]+)?", line.split("|")[2])
+            if line.startswith(row):
+                # the first number of each of the next two cells (SpMV: "R + W MB";
+                # matrix-free: one cell per kernel)
+                cells = line.split("|")[2:4] if rel == PROFILE_MATRIX_FREE else [line.split("|")[2]]
+                nums = [float(x) for c in cells for x in re.findall(r"[0-9]+(?:\.[0-9]+)?", c)[:2]]
                 if len(nums) >= 2:
-                    return int((float(nums[0]) + float(nums[1])) * 1e6), PROFILE_SPMV
+                    return int((nums[0] + nums[1]) * 1e6 * scale), rel
     return None, None
 
 
@@ -373,11 +385,10 @@ def run_ours(args, rank, world, dist):
             kernel = "pcg_spmv_col_kernel" if spmv_shape[2] == 1 else "pcg_spmv_kernel"
         traffic, traffic_src = measured_traffic(args)
     else:
-        # no ncu capture of the matrix-free pair is committed
         spmv = stages["matrix_free"]
         spmv_bytes = B * abytes["matrix_free"]
         kernel = "apply_j_kernel + apply_jt_kernel"
-        traffic, traffic_src = None, None
+        traffic, traffic_src = measured_traffic(args)
     roofline = {"kernel": kernel, "bound": "hbm", "achieved": spmv["GBps"], "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s", "frac": round(spmv["GBps"] / peak, 4),
                 "traffic": traffic, "traffic_source": traffic_src, "algorithmic_bytes_per_launch": spmv_bytes,

@@ -53,3 +53,20 @@ def test_committed_spmv_profile_parses():
     a = argparse.Namespace(batch=16, nodes=4096, width=640, height=480, precision="mixed", mode="materialized")
     traffic, src = bench.measured_traffic(a)
     assert src is not None and 1e7 < traffic < 1e9
+
+
+def test_committed_profiles_give_the_summed_dram_bytes():
+    """The SpMV summary's row is "R + W MB" for the 16-instance launch; the
+    matrix-free summary has one DRAM figure per kernel for 8 instances, which
+    the bench sums and scales to its batch."""
+    import argparse
+    sys.path.insert(0, ROOT)
+    import bench
+    a = argparse.Namespace(batch=16, nodes=4096, width=640, height=480, precision="mixed", mode="materialized")
+    assert bench.measured_traffic(a)[0] == int((107.5 + 2.76) * 1e6)
+    a.mode = "matrix_free"
+    traffic, src = bench.measured_traffic(a)
+    assert src.endswith("apply_pair_matrix_free_torso_3view_4096nodes_8inst.md")
+    assert traffic == int((130 + 165) * 1e6 * 2)
+    a.batch = 8
+    assert bench.measured_traffic(a)[0] is None  # only the headline batch size
