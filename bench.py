@@ -224,9 +224,11 @@ def algorithmic_bytes(counts, N, mixed=True, materialized=True):
     the scaling turns the P upper blocks into float blocks of the
     block-Jacobi scaled operator, whose identity diagonal the SpMV does not
     read; the SpMV reads the float copy of the direction (24 B per node) and
-    the double direction (48 B), and writes the double product (48 B); the PCG
-    update needs no preconditioner. Plain FP32: float blocks with the
-    diagonal, float vectors, the 6x6 inverse per node."""
+    the double direction (48 B) and the residual (48 B, for r.q), and writes
+    the double product (48 B); the PCG update needs no preconditioner and
+    forms the next direction (the direction kernel runs once per solve).
+    Plain FP32: float blocks with the diagonal, float vectors, the 6x6
+    inverse per node."""
     Td, Ts, Tf, Tp, Tc = (counts.dense_terms, counts.smooth_terms, counts.foreground_terms, counts.feature_terms,
                           counts.cross_terms)
     P = counts.half_pairs
@@ -235,9 +237,9 @@ def algorithmic_bytes(counts, N, mixed=True, materialized=True):
     term_data = 52 * (Td + Tf) + 29 * Ts + 88 * (Tp + Tc)
     precond = 168 * N if mixed else 144 * N
     if scaled:
-        spmv = 144 * P + 8 * 2 * P + 4 * (N + 1) + 24 * N + 48 * N + 48 * N
+        spmv = 144 * P + 8 * 2 * P + 4 * (N + 1) + 24 * N + 48 * N + 48 * N + 48 * N
         direction = 3 * 48 * N + 24 * N      # r and d_prev read, d and its float copy written
-        pcg_update = 6 * 48 * N               # x rw, r rw, d, q read
+        pcg_update = 7 * 48 * N + 32 * N      # x rw, r rw, d, q read; next d and its padded float copy written
     else:
         spmv = 36 * elem * (N + P) + 8 * (N + 2 * P) + 4 * (N + 1) + 2 * 6 * elem * N
         direction = 3 * 6 * elem * N          # s and d_prev read, d written

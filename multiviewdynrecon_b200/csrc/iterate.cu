@@ -987,8 +987,9 @@ __global__ void __launch_bounds__(128) pcg_unscale_kernel(const InstDesc* insts)
 // the others (no ticket, fence or atomic on the SpMV's critical path).
 // Regions: kRegDelta + parity holds delta = r.s of the iteration with that
 // parity (pcg_init writes iteration 0's, pcg_update the next one's), kRegDq
-// holds d.q of the current iteration.
-constexpr uint32_t kRegDelta = 1, kRegDq = 3;
+// holds d.q of the current iteration; the scaled SpMV also stores r.q and q.q
+// (kRegRq, kRegQq), from which the fused update forms the next delta.
+constexpr uint32_t kRegDelta = 1, kRegDq = 3, kRegRq = 5, kRegQq = 6;
 
 template <class T>
 __device__ inline void store_block_partial(const InstDesc& I, uint32_t region, T v, uint32_t slot = 0xFFFFFFFFu) {
@@ -1001,6 +1002,47 @@ __device__ inline void store_block_partial(const InstDesc& I, uint32_t region, T
         for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += ws[w];
         I.partials[(size_t)region * I.part_stride + (slot == 0xFFFFFFFFu ? blockIdx.x : slot)] = (double)s;
     }
+}
+
+// three block sums at once (one barrier), to three regions
+template <class T>
+__device__ inline void store_block_partials3(const InstDesc& I, uint32_t r0, T v0, uint32_t r1, T v1, uint32_t r2,
+                                             T v2) {
+    __shared__ T ws3[3][32];
+    v0 = warp_sum(v0);
+    v1 = warp_sum(v1);
+    v2 = warp_sum(v2);
+    if (lane_id() == 0) {
+        ws3[0][threadIdx.x >> 5] = v0;
+        ws3[1][threadIdx.x >> 5] = v1;
+        ws3[2][threadIdx.x >> 5] = v2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        T s = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += ws3[threadIdx.x][w];
+        const uint32_t r = threadIdx.x == 0 ? r0 : (threadIdx.x == 1 ? r1 : r2);
+        I.partials[(size_t)r * I.part_stride + blockIdx.x] = (double)s;
+    }
+}
+
+// The sums of the partials of four regions (warp w sums regions w, w + warps,
+// ...; each in a fixed order), in every thread. blockDim.x >= 64.
+template <class T>
+__device__ inline void sum_four_block_partials(const InstDesc& I, const uint32_t (&reg)[4], const uint32_t (&cnt)[4],
+                                               T (&out)[4]) {
+    __shared__ T total[4];
+    const uint32_t warps = blockDim.x >> 5;
+    for (uint32_t q = threadIdx.x >> 5; q < 4; q += warps) {
+        const double* p = I.partials + (size_t)reg[q] * I.part_stride;
+        T s = 0;
+        for (uint32_t c = lane_id(); c < cnt[q]; c += 32) s += (T)__ldcg(p + c);
+        s = warp_sum(s);
+        if (lane_id() == 0) total[q] = s;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) out[q] = total[q];
 }
 
 // The sums of the partials of two regions (warp 0 sums region a, warp 1
@@ -1342,7 +1384,7 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
     const float* xf = I.df;
     const double* xd = PcgVec<true>::d(I, parity);
     const uint32_t t = threadIdx.x;
-    double part = 0;
+    double part = 0, prq = 0, pqq = 0;  // d.q, r.q, q.q
     const uint32_t r0 = blockIdx.x * kTileRows;
     if (pcg_stopped(I)) return;
     if (r0 < I.N && index_complete(I)) {
@@ -1414,9 +1456,11 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
             const double q = dv + (double)acc;
             PcgVec<true>::q(I)[e] = q;
             part += dv * q;
+            prq += PcgVec<true>::r(I)[e] * q;
+            pqq += q * q;
         }
     }
-    store_block_partial<double>(I, kRegDq, part);
+    store_block_partials3<double>(I, kRegDq, part, kRegRq, prq, kRegQq, pqq);
 }
 
 // blockPCGSecondUpdateKernel (BlockPCG.cuh:120-161): alpha = delta / d.q,
@@ -1426,9 +1470,21 @@ __global__ void __launch_bounds__(6 * kTileSplit * kTileRows) pcg_spmv_scaled_ke
 // their latency overlaps the sums. `nd` and `nq`: CTAs of the launches that
 // stored the delta and d.q partials. SCALED: the preconditioner is the
 // identity (s = r^, not stored), delta_new = r^.r^.
-template <bool MIXED, bool SCALED>
+// FUSE (the scaled form): the kernel also forms the next direction
+// d_(k+1) = r^_(k+1) + beta d_k, so that no direction kernel runs between
+// iterations. beta = delta_(k+1) / delta_k needs delta_(k+1) before any CTA
+// has finished, so it is taken from the identity
+// r_(k+1).r_(k+1) = delta_k - 2 alpha r_k.q_k + alpha^2 q_k.q_k, with the
+// r.q and q.q sums that the SpMV stored; the directly summed delta_(k+1)
+// (this kernel's partials) still gives the next alpha and the residual
+// history, recorded here for iteration `it` of GN iteration `gn`. With a
+// tolerance the convergence test of iteration `it` (the direction kernel's)
+// is made here: on a stop no CTA applies the step, so the solve equals the
+// fixed-count solve of `it` iterations.
+template <bool MIXED, bool SCALED, bool FUSE>
 __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, int parity, uint32_t nd,
-                                                         uint32_t nq) {
+                                                         uint32_t nq, uint32_t gn, uint32_t it) {
+    static_assert(!FUSE || SCALED, "the fused direction is the scaled form's");
     const InstDesc& I = insts[blockIdx.y];
     if (pcg_stopped(I)) return;
     using PV = PcgVec<MIXED>;
@@ -1460,8 +1516,26 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
             else pre[i] = I.minv[36 * (size_t)node + i];
         }
     }
-    T delta, dq;
-    sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDq, nq, &delta, &dq);
+    T delta, dq, rq = 0, qq = 0;
+    if constexpr (FUSE) {
+        T sums[4];
+        sum_four_block_partials<T>(I, {kRegDelta + (uint32_t)parity, kRegDq, kRegRq, kRegQq}, {nd, nq, nq, nq}, sums);
+        delta = sums[0];
+        dq = sums[1];
+        rq = sums[2];
+        qq = sums[3];
+        double* hist = gn < kPcgHistRows ? I.pcg_hist + (size_t)gn * MVDR_PCG_HISTORY : nullptr;
+        if (blockIdx.x == 0 && threadIdx.x == 0 && hist && it < MVDR_PCG_HISTORY) hist[it] = (double)delta;
+        if (it > 0 && I.pcg_tol > 0.f) {
+            const double tol2 = (double)I.pcg_tol * (double)I.pcg_tol;
+            if (fabs((double)delta) < tol2 * fabs(I.counts->pcg_delta0)) {
+                if (blockIdx.x == 0 && threadIdx.x == 0) I.counts->pcg_stop = it;
+                return;  // the same decision in every thread of every CTA
+            }
+        }
+    } else {
+        sum_two_block_partials<T>(I, kRegDelta + parity, nd, kRegDq, nq, &delta, &dq);
+    }
     const T alpha = pcg_alpha<T>(I, delta, dq, blockIdx.x == 0);
     T part = 0;
     if (has) {
@@ -1500,6 +1574,17 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(const InstDesc* insts, 
         if constexpr (!SCALED) store6(PV::s(I), sv);
 #pragma unroll
         for (int i = 0; i < 6; ++i) part += rv[i] * sv[i];
+        if constexpr (FUSE) {
+            const T dnext = delta - (T)2 * alpha * rq + alpha * alpha * qq;
+            const T beta = delta != (T)0 ? dnext / delta : (T)0;  // a vanished residual restarts with d = r^
+            T dn[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) dn[i] = rv[i] + beta * dv[i];
+            store6(PV::d(I, parity ^ 1), dn);
+            float4* f = reinterpret_cast<float4*>(I.df + kScaledRow * (size_t)node);
+            f[0] = make_float4((float)dn[0], (float)dn[1], (float)dn[2], (float)dn[3]);
+            f[1] = make_float4((float)dn[4], (float)dn[5], 0.f, 0.f);
+        }
     }
     store_block_partial<T>(I, kRegDelta + (parity ^ 1), part);
 }
@@ -2238,10 +2323,17 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
     for (uint32_t it = 0; it < iters; ++it) {
         const int parity = (int)(it & 1u), first = it == 0;
         uint32_t nq;  // CTAs that store the d.q partials
-        // d = s + beta d_prev, then q = A d with its d.q partials
-        if (scaled) MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
-        else if (mixed) MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
-        else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
+        // d = s + beta d_prev, then q = A d with its d.q partials. The scaled
+        // form's update forms each next direction (pcg_update_kernel FUSE),
+        // so its direction kernel runs for the first iteration only.
+        if (scaled) {
+            if (first)
+                MVDR_LAUNCH((pcg_direction_kernel<true, true>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
+        } else if (mixed) {
+            MVDR_LAUNCH((pcg_direction_kernel<true, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
+        } else {
+            MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, parity, first, gnode, gn, it);
+        }
         if (lc.mode == MVDR_MODE_MATRIX_FREE) {
             // J.d per term, then Jt per node (+ damping, q, d.q)
             launch_apply_pair(lc, d, nullptr, nullptr, parity, 1, gterm, gwarp, lc.B, lam, st);
@@ -2251,9 +2343,9 @@ cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam
             if (e != cudaSuccess) return e;
             nq = spmv_grid(lc);
         }
-        if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
-        else if (mixed) MVDR_LAUNCH((pcg_update_kernel<true, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
-        else MVDR_LAUNCH((pcg_update_kernel<false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq);
+        if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq, gn, it);
+        else if (mixed) MVDR_LAUNCH((pcg_update_kernel<true, false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq, gn, it);
+        else MVDR_LAUNCH((pcg_update_kernel<false, false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, parity, gnode, nq, gn, it);
     }
     if (scaled) MVDR_LAUNCH(pcg_unscale_kernel, grid2((lc.max_nodes + 127) / 128, lc.B), 128, 0, st, d);
     return cudaGetLastError();
@@ -2346,9 +2438,10 @@ cudaError_t launch_stage(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& l
             else MVDR_LAUNCH((pcg_direction_kernel<false, false>), grid2(gvec, lc.B), 256, 0, st, d, 0, 0, gnode, ~0u, 1u);
             break;
         case MVDR_STAGE_PCG_UPDATE:
-            if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
-            else if (mixed) MVDR_LAUNCH((pcg_update_kernel<true, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
-            else MVDR_LAUNCH((pcg_update_kernel<false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc));
+            // (the form the solve runs; no residual history)
+            if (scaled) MVDR_LAUNCH((pcg_update_kernel<true, true, true>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc), ~0u, 1u);
+            else if (mixed) MVDR_LAUNCH((pcg_update_kernel<true, false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc), ~0u, 1u);
+            else MVDR_LAUNCH((pcg_update_kernel<false, false, false>), grid2(gnode, lc.B), kPcgNodeThreads, 0, st, d, 0, gnode, spmv_grid(lc), ~0u, 1u);
             break;
         case MVDR_STAGE_SCALE:
             if (!scaled) return cudaErrorInvalidValue;

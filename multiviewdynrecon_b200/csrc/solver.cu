@@ -178,7 +178,7 @@ static size_t layout_instance(Arena& a, InstDesc& I, const LaunchCfg& lc, uint32
     I.jp = lc.mode == MVDR_MODE_MATRIX_FREE ? a.take<float>(6 * (size_t)lc.cap_terms) : nullptr;
     // region 0: energy; 1, 2: PCG delta by iteration parity; 3: d.q; 4: the
     // density term's energy
-    I.partials = a.take<double>(5 * (size_t)partial_slots);
+    I.partials = a.take<double>(7 * (size_t)partial_slots);
     I.part_stride = partial_slots;
     I.energy = a.take<double>(64);
     I.node_err_acc = a.take<unsigned long long>(2 * N);
