@@ -8,8 +8,11 @@ iterations, mixed precision (float Jacobians and PCG vectors; double residual
 chain, JtJ blocks, reductions and block Cholesky).
 Each instance shares the synthetic geometry and has its own random initial
 warp field. Every step re-binds the inputs (which resets each warp field) and
-runs the index build plus all Gauss-Newton iterations of every instance as one
-captured CUDA graph.
+runs the index build plus all Gauss-Newton iterations of every instance. The
+16 instances are solved in two lanes of 8 (`--streams`): each lane is a
+member batch whose whole solve is one captured CUDA graph on a stream of its
+own, so one lane's kernels run in the gaps that the other's latency-bound
+kernels leave.
 
 Outputs one JSON line (rank 0). `value` uses inputs resident in HBM; `e2e`
 uploads every input from pinned host memory and reads every solved warp field
@@ -47,6 +50,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=16, help="instances per GPU")
+    p.add_argument("--streams", type=int, default=2,
+                   help="lanes of the timed batch: member batches of batch/streams instances, each solved as its "
+                        "own graph on its own stream (1: one batch, one graph)")
     p.add_argument("--nodes", type=int, default=4096)
     p.add_argument("--width", type=int, default=640)
     p.add_argument("--height", type=int, default=480)
@@ -278,7 +284,7 @@ def algorithmic_bytes(counts, N, mixed=True, materialized=True):
 def run_ours(args, rank, world, dist):
     import torch
     from multiviewdynrecon_b200 import abi, lib
-    from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, NonRigidSolver
+    from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, NonRigidSolver, StreamedBatch
 
     torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
     dev = torch.cuda.current_device()
@@ -295,10 +301,6 @@ def run_ours(args, rank, world, dist):
         for i, ds in enumerate(dev_scenes):
             batch.set_input(i, ds, stream=stream)
 
-    def step():
-        bind_all()
-        batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
-
     # SpMV tile shape for this workload (one timed sweep of the candidates,
     # or the shape given on the command line)
     with torch.cuda.stream(stream):
@@ -311,11 +313,30 @@ def run_ours(args, rank, world, dist):
         else:
             spmv_shape, spmv_shape_ms = batch.autotune(stream=stream)
 
+    # the timed solver: the batch itself, or its instances in lanes of
+    # concurrent graphs on streams of their own (same tile shape, same
+    # arithmetic per instance)
+    if args.streams > 1:
+        timed = StreamedBatch(cfg, B, lanes=args.streams)
+        timed.set_spmv_shape(abi.SPMV_SHAPES.index(tuple(spmv_shape)))
+        if args.pcg_persistent:
+            timed.set_pcg_persistent(True)
+    else:
+        timed = batch
+
+    def bind_timed():
+        for i, ds in enumerate(dev_scenes):
+            timed.set_input(i, ds, stream=stream)
+
+    def step():
+        bind_timed()
+        timed.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+
     # kernels per solve: one direct (non-graph) solve counted through the ABI
     with torch.cuda.stream(stream):
-        bind_all()
+        bind_timed()
         k0 = lib().mvdr_kernel_launch_count()
-        batch.solve(args.gn, args.pcg, use_graph=False, stream=stream)
+        timed.solve(args.gn, args.pcg, use_graph=False, stream=stream)
         kernels_per_step = lib().mvdr_kernel_launch_count() - k0
         stream.synchronize()
         for _ in range(args.warmup):
@@ -490,7 +511,7 @@ def run_ours(args, rank, world, dist):
         single.close()
         # the same FP32 arithmetic batched and graph-replayed like the headline,
         # to separate the gain of the precision scheme from that of batching
-        pb = BatchSolver(pcfg, B)
+        pb = StreamedBatch(pcfg, B, lanes=args.streams) if args.streams > 1 else BatchSolver(pcfg, B)
         with torch.cuda.stream(stream):
             def pstep():
                 for i, ds in enumerate(dev_scenes):
@@ -504,17 +525,18 @@ def run_ours(args, rank, world, dist):
             pb_ms = time_solves(pstep, max(3, args.steps // 4), max(3, args.warmup), stream)
         plain["batched_graph"] = {"value": round(B * 1e3 / pb_ms, 3), "unit": "solves/s",
                                   "ms_per_step": round(pb_ms, 4),
-                                  "form": f"plain FP32, {B} instances per launch, CUDA graph (as the headline)"}
+                                  "form": f"plain FP32, {B} instances in {max(1, args.streams)} concurrent "
+                                          f"graph lanes (as the headline)"}
         pb.close()
 
     # the PCG residual history of instance 0's last timed solve: delta_k /
     # delta_0 at the start of every PCG iteration, first and last GN iteration
     pcg_history = None
     with torch.cuda.stream(stream):
-        bind_all()
-        batch.solve(args.gn, args.pcg, use_graph=True, stream=stream)
+        bind_timed()
+        timed.solve(args.gn, args.pcg, use_graph=True, stream=stream)
         stream.synchronize()
-    hist = batch.instance(0).get_array(abi.ARRAY_PCG_RESIDUALS)
+    hist = timed.instance(0).get_array(abi.ARRAY_PCG_RESIDUALS)
     if len(hist):
         def ratios(row):
             row = row[np.isfinite(row)]
@@ -527,7 +549,7 @@ def run_ours(args, rank, world, dist):
     accuracy = None
     if not args.no_accuracy:
         with torch.cuda.stream(stream):
-            errs, eerrs = increment_errors_vs_fp64(scenes[0], cfg, args.gn, args.pcg, batch=batch, bind=bind_all,
+            errs, eerrs = increment_errors_vs_fp64(scenes[0], cfg, args.gn, args.pcg, batch=timed, bind=bind_timed,
                                                    stream=stream)
         accuracy = {"dx_rel_err_vs_fp64": [float("%.3g" % e) for e in errs],
                     "dx_rel_err_max": float("%.3g" % max(errs)),
@@ -997,7 +1019,8 @@ def main():
             "value": round(r["value"], 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "instances_per_gpu": args.batch, "views": 3,
+            "config": {"workload": WORKLOAD, "instances_per_gpu": args.batch, "streams": max(1, args.streams),
+                       "instances_per_stream": -(-args.batch // max(1, args.streams)), "views": 3,
                        "image": [args.width, args.height], "nodes": args.nodes, "gn": args.gn, "pcg": args.pcg,
                        "precision": args.precision, "mode": args.mode, "graph": True,
                        "pcg_form": "persistent" if args.pcg_persistent else "launches",

@@ -335,6 +335,89 @@ class BatchSolver:
         return _InstanceView(h, n, self.config)
 
 
+class StreamedBatch:
+    """A batch of independent solves split into `lanes` member batches, each
+    solved (as its own CUDA graph) on a stream of its own. The solve's kernels
+    are latency-bound and one batch leaves the GPU partly idle at every kernel
+    boundary and in its small kernels; a second batch's kernels run in those
+    gaps. Instance i lives in lane k at position i - start[k] (lanes of equal
+    size, the first ones one larger when `count` does not divide).
+
+    The calls take the caller's stream as BatchSolver's do: inputs are bound
+    on it, and solve() starts the lanes after the work already queued there
+    and makes it wait for all of them, so results are read on it as usual.
+    Each instance's arithmetic is the same as in one batch of `count` with
+    the same SpMV tile shape; only the launch grids' instance dimension
+    differs."""
+
+    def __init__(self, config, count, lanes=2):
+        lanes = max(1, min(int(lanes), int(count)))
+        base, extra = divmod(int(count), lanes)
+        self.config = config
+        self.count = count
+        self.sizes = [base + (1 if k < extra else 0) for k in range(lanes)]
+        self.starts = [sum(self.sizes[:k]) for k in range(lanes)]
+        self.lanes = [BatchSolver(config, n) for n in self.sizes]
+        self.streams = [torch.cuda.Stream() for _ in self.lanes]
+
+    def close(self):
+        for b in getattr(self, "lanes", []):
+            b.close()
+
+    def lane_of(self, i):
+        """(lane, position in the lane) of instance i."""
+        if not 0 <= i < self.count:
+            raise IndexError(f"instance {i} of a batch of {self.count}")
+        k = max(k for k in range(len(self.lanes)) if self.starts[k] <= i)
+        return k, i - self.starts[k]
+
+    def set_input(self, i, scene, stream=None):
+        k, j = self.lane_of(i)
+        return self.lanes[k].set_input(j, scene, stream=stream)
+
+    def set_input_host(self, i, host_scene, stream=None):
+        k, j = self.lane_of(i)
+        self.lanes[k].set_input_host(j, host_scene, stream=stream)
+
+    def solve(self, gn, pcg, use_graph=True, stream=None):
+        caller = stream if stream is not None else torch.cuda.current_stream()
+        start = torch.cuda.Event()
+        start.record(caller)
+        done = []
+        for b, s in zip(self.lanes, self.streams):
+            s.wait_event(start)
+            b.solve(gn, pcg, use_graph=use_graph, stream=s)
+            e = torch.cuda.Event()
+            e.record(s)
+            done.append(e)
+        for e in done:
+            caller.wait_event(e)
+
+    def node_se3(self, i, out=None, stream=None):
+        k, j = self.lane_of(i)
+        return self.lanes[k].node_se3(j, out=out, stream=stream)
+
+    def node_se3_async(self, i, out, stream=None):
+        k, j = self.lane_of(i)
+        return self.lanes[k].node_se3_async(j, out, stream=stream)
+
+    def autotune(self, stream=None):
+        """Tune each lane's SpMV tile shape; returns lane 0's result."""
+        return [b.autotune(stream=stream) for b in self.lanes][0]
+
+    def set_spmv_shape(self, index):
+        for b in self.lanes:
+            b.set_spmv_shape(index)
+
+    def set_pcg_persistent(self, on=True):
+        for b in self.lanes:
+            b.set_pcg_persistent(on)
+
+    def instance(self, i):
+        k, j = self.lane_of(i)
+        return self.lanes[k].instance(j)
+
+
 class _InstanceView(NonRigidSolver):
     """A batch member seen through the single-solver interface. Its handle
     belongs to the batch, so closing the view releases nothing."""

@@ -17,7 +17,7 @@ import torch
 
 from conftest import max_relative_error, rel_norm_error, small_scene
 from multiviewdynrecon_b200 import abi
-from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, NonRigidSolver
+from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, NonRigidSolver, StreamedBatch
 
 pytestmark = pytest.mark.gpu
 
@@ -423,6 +423,40 @@ def test_persistent_pcg_solves_the_same_system(precision, tol):
     for i in range(2):
         assert rel_norm_error(out["per"][i], out["ref"][i]) < tol
         assert np.array_equal(out["per"][i], out["per2"][i])
+
+
+def test_streamed_batch_equals_one_batch():
+    """A batch split into lanes of concurrent graphs on their own streams
+    (two lanes of 2 and 1 instances here) gives every instance's warp field
+    bit for bit as one batch of all instances does; results read on the
+    caller's stream after solve() see the lanes' work, also on replays."""
+    scenes = [small_scene("torso"), small_scene("sphere"), small_scene("torso")]  # all 160 x 120
+    caps = dict(max_nodes=max(s.num_nodes for s in scenes), max_views=3, width=160, height=120,
+                use_foreground=True, use_feature=True, use_cross_view=True,
+                max_surfels=max(s.num_surfels for s in scenes),
+                max_feature_terms=max(s.feature.count for s in scenes),
+                max_cross_terms=max(s.cross_view.count for s in scenes))
+    cfg = abi.make_config(None, **caps)
+    dev = [DeviceScene(s) for s in scenes]
+    one, lanes = BatchSolver(cfg, 3), StreamedBatch(cfg, 3, lanes=2)
+    assert lanes.sizes == [2, 1] and lanes.lane_of(2) == (1, 0)
+    caller = torch.cuda.Stream()
+    out = {}
+    for name, b, graph in (("one", one, True), ("direct", lanes, False), ("graph", lanes, True),
+                           ("again", lanes, True)):
+        with torch.cuda.stream(caller):
+            for i, ds in enumerate(dev):
+                b.set_input(i, ds, stream=caller)
+            b.solve(3, 10, use_graph=graph, stream=caller)
+            out[name] = [b.node_se3(i, stream=caller) for i in range(3)]
+        caller.synchronize()
+        out[name] = [t.cpu().numpy() for t in out[name]]
+    for name in ("direct", "graph", "again"):
+        for i in range(3):
+            assert np.array_equal(bits(out[name][i]), bits(out["one"][i])), (name, i)
+    assert all(lanes.instance(i).counts().error_flags == 0 for i in range(3))
+    lanes.close()
+    one.close()
 
 
 def test_autotuned_spmv_shape_solves_the_same_system():
