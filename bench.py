@@ -808,7 +808,7 @@ def run_extra_workload(args):
     documenting configurations beside the headline."""
     import torch
     from multiviewdynrecon_b200 import abi, lib, synth
-    from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene
+    from multiviewdynrecon_b200.solver import BatchSolver, DeviceScene, StreamedBatch
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     t0 = time.perf_counter()
@@ -868,6 +868,22 @@ def run_extra_workload(args):
                              max(3, args.warmup), stream)
             entry = {"solves_per_s": round(B / (ms / 1e3), 3), "ms_per_step": round(ms, 3),
                      "solver_device_mb": solver_mb}
+            if B > 1 and args.streams > 1:
+                # the same instances in concurrent graph lanes (as the headline)
+                lanes = StreamedBatch(cfg, B, lanes=args.streams)
+                if shape is not None:
+                    lanes.set_spmv_shape(abi.SPMV_SHAPES.index(tuple(shape)))
+
+                def lane_step():
+                    for i, ds in enumerate(dev):
+                        lanes.set_input(i, ds, stream=stream)
+                    lanes.solve(gn, pcg, use_graph=True, stream=stream)
+                lms = time_solves(lane_step, args.steps, max(3, args.warmup), stream)
+                entry["one_graph"] = {"solves_per_s": entry["solves_per_s"], "ms_per_step": entry["ms_per_step"]}
+                entry["solves_per_s"] = round(B / (lms / 1e3), 3)
+                entry["ms_per_step"] = round(lms, 3)
+                entry["lanes"] = len(lanes.lanes)
+                lanes.close()
             if mode == abi.MODE_MATERIALIZED:
                 bind()
                 batch.solve(gn, pcg, use_graph=False, stream=stream)
