@@ -335,6 +335,15 @@ class BatchSolver:
         return _InstanceView(h, n, self.config)
 
 
+def lane_sizes(count, lanes):
+    """Sizes of the member batches of a batch of `count` split into `lanes`
+    (at most `count`, at least 1): equal, the first ones one larger when
+    `count` does not divide."""
+    lanes = max(1, min(int(lanes), int(count)))
+    base, extra = divmod(int(count), lanes)
+    return [base + (1 if k < extra else 0) for k in range(lanes)]
+
+
 class StreamedBatch:
     """A batch of independent solves split into `lanes` member batches, each
     solved (as its own CUDA graph) on a stream of its own. The solve's kernels
@@ -351,11 +360,9 @@ class StreamedBatch:
     differs."""
 
     def __init__(self, config, count, lanes=2):
-        lanes = max(1, min(int(lanes), int(count)))
-        base, extra = divmod(int(count), lanes)
         self.config = config
         self.count = count
-        self.sizes = [base + (1 if k < extra else 0) for k in range(lanes)]
+        self.sizes = lane_sizes(count, lanes)
         self.starts = [sum(self.sizes[:k]) for k in range(lanes)]
         self.lanes = [BatchSolver(config, n) for n in self.sizes]
         self.streams = [torch.cuda.Stream() for _ in self.lanes]

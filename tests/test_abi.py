@@ -83,3 +83,18 @@ def test_enum_constants_match_header():
     assert arrays == sorted(k for k in mirror if k.startswith("MVDR_ARRAY_"))
     for k, v in mirror.items():
         assert found.get(k) == v, k
+
+
+def test_lane_sizes_split_a_batch_evenly():
+    """StreamedBatch's member batches: equal sizes, the first ones one larger
+    when the count does not divide; never more lanes than instances."""
+    from multiviewdynrecon_b200.solver import lane_sizes
+    assert lane_sizes(16, 2) == [8, 8]
+    assert lane_sizes(16, 3) == [6, 5, 5]
+    assert lane_sizes(3, 2) == [2, 1]
+    assert lane_sizes(2, 4) == [1, 1]
+    assert lane_sizes(5, 0) == [5]
+    for n in range(1, 40):
+        for k in range(1, 9):
+            s = lane_sizes(n, k)
+            assert sum(s) == n and max(s) - min(s) <= 1 and len(s) == min(n, k)
