@@ -677,7 +677,7 @@ MVDR_API int mvdr_batch_set_spmv_shape(mvdr_batch* batch, uint32_t shape);
 /* on != 0: run each PCG solve of a materialised batch as one persistent
  * cooperative launch (the CTAs split among the instances, each instance's
  * CTAs stepping through its iterations with their own barriers) instead of
- * three launches per iteration; on == 0 restores the launches. Drops the
+ * two or three launches per iteration; on == 0 restores the launches. Drops the
  * captured graphs. MVDR_EINVAL for a matrix-free batch or a batch with more
  * instances than the device holds co-resident CTAs of the kernel. */
 MVDR_API int mvdr_batch_set_pcg_persistent(mvdr_batch* batch, int on);

@@ -314,7 +314,8 @@ class BatchSolver:
 
     def set_pcg_persistent(self, on=True):
         """One persistent cooperative launch per PCG solve (materialised
-        mode) instead of three launches per iteration."""
+        mode) instead of two (mixed precision) or three launches per
+        iteration."""
         check(lib().mvdr_batch_set_pcg_persistent(self.h, 1 if on else 0))
 
     def set_wait_limit(self, limit_ns, extra_arrivals=0):
