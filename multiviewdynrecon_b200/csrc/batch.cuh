@@ -25,6 +25,10 @@ struct Batch {
     std::vector<InstDesc> host;
     InstDesc* d_inst = nullptr;
     uint32_t* d_bars = nullptr;  // persistent PCG barrier counters
+    // the stream beside the solve's stream and the events that fork it from
+    // and join it back (launch_assemble_forked)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void* arena = nullptr;
     size_t arena_bytes = 0;
     size_t per_inst_bytes = 0;

@@ -2255,6 +2255,30 @@ cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty
     return cudaGetLastError();
 }
 
+// diag_rhs_kernel and offdiag_kernel read the same term records and write
+// disjoint outputs (the diagonal blocks, factors and Jt r; the upper blocks),
+// so they run side by side; the scaling reads both.
+cudaError_t launch_assemble_forked(const LaunchCfg& lc, InstDesc* d, const mvdr_penalty& lam, cudaStream_t st,
+                                   cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+    const bool mixed = lc.precision == MVDR_PRECISION_MIXED;
+    cudaError_t e = cudaEventRecord(fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
+    if (e != cudaSuccess) return e;
+    const uint32_t gp = min((lc.cap_pairs + 127) / 128, (uint32_t)lc.sm_count * 8);
+    if (mixed) MVDR_LAUNCH(offdiag_kernel<true>, grid2(gp, lc.B), 128, 0, side, d, lam);
+    else MVDR_LAUNCH(offdiag_kernel<false>, grid2(gp, lc.B), 128, 0, side, d, lam);
+    e = cudaEventRecord(join, side);
+    const uint32_t gn = (lc.max_nodes + kDiagNodes - 1) / kDiagNodes;
+    if (mixed) MVDR_LAUNCH(diag_rhs_kernel<true>, grid2(gn, lc.B), 128, 0, st, d, lam);
+    else MVDR_LAUNCH(diag_rhs_kernel<false>, grid2(gn, lc.B), 128, 0, st, d, lam);
+    // the join is made even after a failed record, so that a capture ends
+    const cudaError_t w = cudaStreamWaitEvent(st, join, 0);
+    if (e == cudaSuccess) e = w;
+    if (e != cudaSuccess) return e;
+    if (mixed) MVDR_LAUNCH(scale_offdiag_kernel, grid2(scale_grid(lc), lc.B), 128, 0, st, d);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d, uint32_t slot, cudaStream_t st) {
     MVDR_LAUNCH(energy_sum_kernel, grid2(1, lc.B), 256, 0, st, d, eval_terms_grid(lc), slot,
                 lc.use_density ? eval_density_grid(lc) : 0u);

@@ -411,6 +411,12 @@ cudaError_t launch_build_index(const LaunchCfg& lc, InstDesc* d_inst, cudaStream
 cudaError_t launch_eval_terms(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, cudaStream_t st);
 cudaError_t launch_assemble(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, bool materialize,
                             cudaStream_t st);
+// The materialised assembly with the off-diagonal blocks on `side` while the
+// diagonal blocks run on `st` (forked after the work queued on `st`, joined
+// back before the scaling, which needs both); inside a stream capture the
+// two become parallel branches of the graph.
+cudaError_t launch_assemble_forked(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, cudaStream_t st,
+                                   cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
 cudaError_t launch_energy(const LaunchCfg& lc, InstDesc* d_inst, uint32_t slot, cudaStream_t st);
 cudaError_t launch_pcg(const LaunchCfg& lc, InstDesc* d_inst, const mvdr_penalty& lam, uint32_t iters, uint32_t gn,
                        cudaStream_t st);

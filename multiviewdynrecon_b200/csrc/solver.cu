@@ -71,6 +71,9 @@ Batch::~Batch() {
         if (o.mem) cudaFree(o.mem);
     if (d_inst) cudaFree(d_inst);
     if (d_bars) cudaFree(d_bars);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (arena) cudaFree(arena);
     for (auto* v : views) delete v;
 }
@@ -290,6 +293,9 @@ static int create_batch(const mvdr_config* cfg, uint32_t B, Batch** out) {
     e = cudaMemset(b->arena, 0, b->arena_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_inst, sizeof(InstDesc) * B);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_bars, sizeof(uint32_t) * 32 * B);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete b;
         return fail(MVDR_ECUDA, std::string("workspace setup failed: ") + cudaGetErrorString(e));
@@ -656,7 +662,10 @@ static int enqueue_iteration(Batch& b, uint32_t iter, uint32_t pcg, cudaStream_t
     }
     {
         NvtxRange r("mvdr/assemble");
-        CU(launch_assemble(b.lc, b.d_inst, lam, b.cfg.mode == MVDR_MODE_MATERIALIZED, st));
+        if (b.cfg.mode == MVDR_MODE_MATERIALIZED)
+            CU(launch_assemble_forked(b.lc, b.d_inst, lam, st, b.side, b.ev_fork, b.ev_join));
+        else
+            CU(launch_assemble(b.lc, b.d_inst, lam, false, st));
     }
     {
         NvtxRange r("mvdr/pcg");
